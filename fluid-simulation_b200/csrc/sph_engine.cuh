@@ -1,0 +1,115 @@
+// Device-side state layout and kernel launchers of the SPH step engine.
+//
+// Layout in HBM (one scene, capacity N, stride Np = N rounded up to 32):
+//   pos   R4 {x,y,z,-}      integrated positions, permuted by the cell sort
+//   vel   R4 {vx,vy,vz,m}   velocity with the particle mass in w
+//   xv    R4 {x,y,z,V}      sorted positions with the current volume in w
+//   acc   R4 {ax,ay,az,-}   total acceleration
+//   ref   u32               reference-order index (the row a download writes)
+//   fid   u32               fluid id
+//   nbr   u32 [K][Np]       fluid neighbor lists, neighbor k of particle i at
+//                           nbr[k*Np+i] (coalesced for thread-per-particle);
+//                           self is implicit and not stored
+//   ncnt  u32 [N]           neighbor counts
+//   bW, bG, bGu             per-particle boundary aggregates (see kernels)
+//   IISPH scratch: vstar R4, s R, aii R, accp R4, p R
+// Cell grid: a Morton key of floor(x / h) modulo 2^(3m) buckets; a counting
+// sort orders particles by bucket and, inside a bucket, by reference index.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sph_math.cuh"
+
+namespace sph {
+
+constexpr int kBlock = 256;
+constexpr int kMaxBodies = 32;
+
+// Per-scene scalars that stay on the device so that a step needs no host
+// round trip (time increment, active count, IISPH convergence state).
+struct Scalars {
+  double dt;                       // time increment used by this step
+  unsigned long long max_speed;    // bits of the max |v| (non-negative double)
+  int n;                           // particles entering this update
+  int n_active;                    // particles after disabling
+  int n_below;                     // particles disabled in this update
+  int max_nbrs;                    // largest fluid neighbor count seen
+  int iterations;                  // IISPH sweeps of the last solve
+  int converged;                   // IISPH loop flag (1 = stop)
+  double err;                      // IISPH average predicted density error (%)
+  double avg_density;              // average mass density after the update
+  unsigned int done_blocks;        // last-block-done counter for reductions
+  int status;                      // 0 ok, 2 not converged within the cap
+  int iterations_eqs1;             // IISPHwOST first solve sweeps
+  int max_bnbrs;                   // largest boundary-sample neighbor count seen
+};
+
+// Parameters that are constant over a step (passed by value).
+template <class R>
+struct StepParams {
+  KernelConst<R> k;
+  double range;          // kernel support radius (search range and cell size)
+  R range2_lo, range2_hi;
+  double spacing;        // rest density grid spacing
+  R V0;                  // rest volume spacing^3
+  R visc_f, visc_b;      // 10 * viscosity (= nu * 2 * (3 + 2))
+  R eps_visc;            // 0.01 * spacing^2
+  R gamma_p;             // boundary pressure weighting
+  int gravity_mode;      // 0 uniform -z, 1 radial
+  R gc[3];               // radial gravity center
+  double disable_below;
+  uint32_t mask;         // Morton coordinate mask (2^m - 1)
+  uint32_t T;            // bucket count; bucket T holds disabled particles
+  int K;                 // neighbor capacity per particle
+  int Np;                // neighbor stride
+  int cfl;               // 1: dt = min(dt_max, cfl * spacing / max|v|)
+  double dt_fixed, dt_max, cfl_number;
+  R stiffness;
+  R omega, min_diag;
+  double tde;            // IISPH target density error (%)
+  int iteration_cap;     // 0 = unbounded (reference)
+};
+
+// Rigid body state, f64 (rigid_body_motion.rs:22-36).
+struct Body {
+  double mass;
+  double inv_inertia_body[9];
+  double com[3];
+  double q[4];  // w, i, j, k
+  double v[3];
+  double L[3];
+  double F[3];
+  double T[3];
+  double inv_inertia_world[9];
+  double omega[3];
+  int dynamic;
+  int pad;
+};
+
+// Dense serendipity node lattice (3n+1 per axis, NaN = absent node).
+struct DevField {
+  double xmin[3], xmax[3], dx;
+  int n[3];
+  long long NX, NY;
+  const double* nodes;
+};
+
+struct VMDesc {
+  DevField sdf, vm;
+  int body;  // index into the body table, -1 for static
+};
+
+// Sample-boundary grid (all sample boundaries of a scene in one sorted set).
+template <class R>
+struct SampleGrid {
+  const R4<R>* xb;   // {x,y,z,V_b} sorted
+  const R4<R>* vb;   // {vx,vy,vz,-}
+  const uint32_t* bid;
+  const uint32_t* orig;
+  const uint32_t* start;  // bucket starts, T+2 entries
+  uint32_t mask;
+};
+
+}  // namespace sph

@@ -1,0 +1,1244 @@
+// CUDA kernels of the SPH step engine (sm_100a). One thread per particle;
+// neighbor lists are stored interleaved (nbr[k*Np+i]) so that a warp's loads
+// of its k-th neighbors are coalesced; gathered neighbor state comes through
+// L1/L2 because the cell sort keeps spatial neighbors close in memory.
+//
+// Reference functions each kernel restates (paths under simulation_lib/src/):
+//   k_integrate_key      integration_schemes/euler_cromer.rs:12-25,
+//                        take_predicted.rs:14-27, sph/mod.rs:674-699 (disable,
+//                        max speed), spatial_hashing.rs:27-46 (cells)
+//   k_sort_*             spatial_hashing.rs:27-37 (populate) as a counting sort
+//   k_neighbors_density  spatial_hashing.rs:75-158, neighbor_search/mod.rs:118-155,
+//                        sph/quantities.rs:14-61 (get_volume)
+//   k_sample_aggregate   boundary_handling/static_sample_boundary.rs:157-168
+//   k_vm_sample          boundary_handling/volume_map_boundary.rs:1259-1424,
+//                        utilities/discretization.rs:437-557
+//   k_accel              sph/non_pressure_accelerations.rs:19-185,
+//                        pressure_solver/mod.rs:90-195, sesph.rs:31-67
+//   k_iisph_*            pressure_solver/iisph.rs:117-560,
+//                        iisph_optimized_source_term.rs:53-217
+//   k_body_*             boundary_handling/rigid_body_motion.rs:135-201
+#pragma once
+
+#include <cfloat>
+#include <cmath>
+
+#include "sph_engine.cuh"
+
+namespace sph {
+
+// ---------------------------------------------------------------------------
+// Reductions: fixed-order block reductions and last-block completion so the
+// result does not depend on scheduling.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0;
+  if (w == 0) {
+    t = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    t = warp_sum(t);
+  }
+  __syncthreads();
+  return t;  // valid in thread 0
+}
+
+// Sum of per-block partials in a fixed order, run by the last block to finish.
+// Returns true in thread 0 of that block with *total set.
+__device__ __forceinline__ bool last_block_total(double block_value, double* partials,
+                                                 unsigned int* counter, double* total,
+                                                 double* sh) {
+  __shared__ bool is_last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = block_value;
+    __threadfence();
+    unsigned t = atomicAdd(counter, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return false;
+  __threadfence();
+  double s = 0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) s += ((volatile double*)partials)[b];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) {
+    *total = s;
+    *counter = 0;
+  }
+  return threadIdx.x == 0;
+}
+
+// ---------------------------------------------------------------------------
+// Rigid-body helpers (f64), nalgebra semantics (rigid_body_motion.rs)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void qrot(const double q[4], const double v[3], double out[3]) {
+  // t = 2 (q.v x v); out = v + w t + q.v x t
+  double tx = 2.0 * (q[2] * v[2] - q[3] * v[1]);
+  double ty = 2.0 * (q[3] * v[0] - q[1] * v[2]);
+  double tz = 2.0 * (q[1] * v[1] - q[2] * v[0]);
+  double cx = q[2] * tz - q[3] * ty, cy = q[3] * tx - q[1] * tz, cz = q[1] * ty - q[2] * tx;
+  out[0] = (tx * q[0] + cx) + v[0];
+  out[1] = (ty * q[0] + cy) + v[1];
+  out[2] = (tz * q[0] + cz) + v[2];
+}
+__device__ __forceinline__ void body_world_to_local(const Body& b, const double p[3], double out[3]) {
+  double d[3] = {p[0] - b.com[0], p[1] - b.com[1], p[2] - b.com[2]};
+  double qi[4] = {b.q[0], -b.q[1], -b.q[2], -b.q[3]};
+  qrot(qi, d, out);
+}
+__device__ __forceinline__ void body_velocity_at(const Body& b, const double p[3], double out[3]) {
+  double r[3] = {p[0] - b.com[0], p[1] - b.com[1], p[2] - b.com[2]};
+  out[0] = b.v[0] + (b.omega[1] * r[2] - b.omega[2] * r[1]);
+  out[1] = b.v[1] + (b.omega[2] * r[0] - b.omega[0] * r[2]);
+  out[2] = b.v[2] + (b.omega[0] * r[1] - b.omega[1] * r[0]);
+}
+
+// ---------------------------------------------------------------------------
+// 1. integrate + cell key + bucket histogram (+ disable test, max speed)
+// ---------------------------------------------------------------------------
+// mode: 0 EulerCromer, 1 TakePredicted, 2 no integration (initial update)
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_integrate_key(
+    Scalars* __restrict__ sc, R4<R>* __restrict__ pos, R4<R>* __restrict__ vel,
+    const R4<R>* __restrict__ acc, const R4<R>* __restrict__ xint, const R4<R>* __restrict__ vint,
+    int mode, uint32_t* __restrict__ key, uint32_t* __restrict__ slot,
+    uint32_t* __restrict__ count, StepParams<R> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = sc->n;
+  double speed = 0.0;
+  if (i < n) {
+    R4<R> x = pos[i], v = vel[i];
+    if (mode == 0) {
+      const R dt = (R)sc->dt;
+      const R4<R> a = acc[i];
+      v.x = v.x + dt * a.x; v.y = v.y + dt * a.y; v.z = v.z + dt * a.z;
+      x.x = x.x + dt * v.x; x.y = x.y + dt * v.y; x.z = x.z + dt * v.z;
+      pos[i] = x;
+      vel[i] = v;
+    } else if (mode == 1) {
+      const R m = v.w;
+      x = xint[i];
+      v = vint[i];
+      v.w = m;
+      pos[i] = x;
+      vel[i] = v;
+    }
+    uint32_t k;
+    if ((double)x.z < P.disable_below) {
+      k = P.T;
+      atomicAdd(&sc->n_below, 1);
+    } else {
+      k = morton_key(cell_coord((double)x.x, P.range), cell_coord((double)x.y, P.range),
+                     cell_coord((double)x.z, P.range), P.mask);
+      const double vx = v.x, vy = v.y, vz = v.z;
+      speed = sqrt((vx * vx + vy * vy) + vz * vz);
+    }
+    key[i] = k;
+    slot[i] = atomicAdd(&count[k], 1u);
+  }
+  // block max of the speed (non-negative doubles order like their bit patterns)
+  unsigned long long bits = (unsigned long long)__double_as_longlong(speed);
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long ob = __shfl_down_sync(0xffffffffu, bits, o);
+    bits = ob > bits ? ob : bits;
+  }
+  __shared__ unsigned long long smax[kBlock / 32];
+  if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = bits;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long m = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = smax[w] > m ? smax[w] : m;
+    if (m) atomicMax(&sc->max_speed, m);
+  }
+}
+
+// Step prologue: active count and the CFL time increment (sph/mod.rs:825-829).
+template <class R>
+__global__ void k_prologue(Scalars* sc, StepParams<R> P) {
+  sc->n_active = sc->n - sc->n_below;
+  if (P.cfl) {
+    const double ms = __longlong_as_double((long long)sc->max_speed);
+    const double c = P.cfl_number * P.spacing / ms;  // +inf at rest
+    sc->dt = fmin(P.dt_max, c);
+  }
+  sc->max_nbrs = 0;
+  sc->max_bnbrs = 0;
+  sc->iterations = 0;
+  sc->iterations_eqs1 = 0;
+  sc->converged = 0;
+  sc->err = INFINITY;
+  sc->status = 0;
+}
+
+// ---------------------------------------------------------------------------
+// 2. exclusive scan of bucket counts (3 phases); clears the counts for reuse
+// ---------------------------------------------------------------------------
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kBlock * kScanItems;
+
+__device__ __forceinline__ uint32_t block_excl_scan_u32(uint32_t v, uint32_t* sh, uint32_t* total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    sh[lane] = s;
+  }
+  __syncthreads();
+  uint32_t base = w > 0 ? sh[w - 1] : 0;
+  if (total) *total = sh[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+__global__ void __launch_bounds__(kBlock) k_scan_tiles(const uint32_t* __restrict__ in, int m,
+                                                      uint32_t* __restrict__ tile_sums) {
+  __shared__ uint32_t sh[32];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) s += base + k < m ? in[base + k] : 0u;
+  uint32_t total;
+  block_excl_scan_u32(s, sh, &total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(1024) k_scan_tile_sums(uint32_t* __restrict__ tile_sums, int ntiles) {
+  __shared__ uint32_t sh[32];
+  // each thread owns a contiguous run of tiles
+  const int per = (ntiles + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per;
+  uint32_t s = 0;
+  for (int k = 0; k < per; ++k) s += b + k < ntiles ? tile_sums[b + k] : 0u;
+  uint32_t run = block_excl_scan_u32(s, sh, nullptr);
+  for (int k = 0; k < per; ++k)
+    if (b + k < ntiles) {
+      uint32_t t = tile_sums[b + k];
+      tile_sums[b + k] = run;
+      run += t;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_scan_apply(uint32_t* __restrict__ in, int m,
+                                                      const uint32_t* __restrict__ tile_sums,
+                                                      uint32_t* __restrict__ out) {
+  __shared__ uint32_t sh[32];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = base + k < m ? in[base + k] : 0u;
+    s += v[k];
+  }
+  uint32_t run = block_excl_scan_u32(s, sh, nullptr) + tile_sums[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k)
+    if (base + k < m) {
+      out[base + k] = run;
+      run += v[k];
+      in[base + k] = 0u;  // counts are rebuilt by the next histogram
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. scatter, in-bucket ordering by reference index, gather
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_scatter(const int* __restrict__ n_ptr,
+                                                   const uint32_t* __restrict__ key,
+                                                   const uint32_t* __restrict__ slot,
+                                                   const uint32_t* __restrict__ start,
+                                                   uint32_t* __restrict__ perm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *n_ptr) return;
+  perm[start[key[i]] + slot[i]] = (uint32_t)i;
+}
+
+// The first slot of every bucket orders the bucket's entries by `order`
+// (the reference index), which makes the sorted order independent of the
+// atomic slot assignment.
+__global__ void __launch_bounds__(kBlock) k_bucket_order(const int* __restrict__ n_ptr,
+                                                        const uint32_t* __restrict__ key,
+                                                        const uint32_t* __restrict__ start,
+                                                        const uint32_t* __restrict__ order,
+                                                        uint32_t* __restrict__ perm) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= *n_ptr) return;
+  const uint32_t k = key[perm[d]];
+  const uint32_t b = start[k];
+  if ((uint32_t)d != b) return;
+  const uint32_t e = start[k + 1];
+  for (uint32_t a = b + 1; a < e; ++a) {
+    const uint32_t pa = perm[a];
+    const uint32_t oa = order[pa];
+    uint32_t c = a;
+    while (c > b) {
+      const uint32_t pc = perm[c - 1];
+      if (order[pc] <= oa) break;
+      perm[c] = pc;
+      --c;
+    }
+    perm[c] = pa;
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_gather_particles(
+    const int* __restrict__ n_ptr, const uint32_t* __restrict__ perm,
+    const R4<R>* __restrict__ pos, const R4<R>* __restrict__ vel, const uint32_t* __restrict__ ref,
+    const uint32_t* __restrict__ fid, R4<R>* __restrict__ pos2, R4<R>* __restrict__ vel2,
+    uint32_t* __restrict__ ref2, uint32_t* __restrict__ fid2) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= *n_ptr) return;
+  const uint32_t j = perm[d];
+  pos2[d] = pos[j];
+  vel2[d] = vel[j];
+  ref2[d] = ref[j];
+  fid2[d] = fid[j];
+}
+
+// boundary samples: key + histogram (no integration)
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_sample_key(const int* __restrict__ n_ptr,
+                                                      const R4<R>* __restrict__ xb,
+                                                      uint32_t* __restrict__ key,
+                                                      uint32_t* __restrict__ slot,
+                                                      uint32_t* __restrict__ count, double range,
+                                                      uint32_t mask) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *n_ptr) return;
+  const R4<R> x = xb[i];
+  const uint32_t k = morton_key(cell_coord((double)x.x, range), cell_coord((double)x.y, range),
+                                cell_coord((double)x.z, range), mask);
+  key[i] = k;
+  slot[i] = atomicAdd(&count[k], 1u);
+}
+
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_gather_samples(
+    const int* __restrict__ n_ptr, const uint32_t* __restrict__ perm,
+    const R4<R>* __restrict__ xb, const R4<R>* __restrict__ vb, const uint32_t* __restrict__ bid,
+    const uint32_t* __restrict__ orig, R4<R>* __restrict__ xb2, R4<R>* __restrict__ vb2,
+    uint32_t* __restrict__ bid2, uint32_t* __restrict__ orig2) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= *n_ptr) return;
+  const uint32_t j = perm[d];
+  xb2[d] = xb[j];
+  vb2[d] = vb[j];
+  bid2[d] = bid[j];
+  orig2[d] = orig[j];
+}
+
+// ---------------------------------------------------------------------------
+// 4. fluid neighbor lists + volume (fused)
+// ---------------------------------------------------------------------------
+template <class R>
+__device__ __forceinline__ void kahan_add(R& s, R& c, R t) {
+  const R y = t - c;
+  const R u = s + y;
+  c = (u - s) - y;
+  s = u;
+}
+
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_neighbors_density(
+    Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, const uint32_t* __restrict__ start,
+    R4<R>* __restrict__ xv, uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncnt,
+    const R* __restrict__ bW, int has_boundary, StepParams<R> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int cnt = 0;
+  if (i < sc->n_active) {
+    const R4<R> xi = pos[i];
+    const int cx = cell_coord((double)xi.x, P.range), cy = cell_coord((double)xi.y, P.range),
+              cz = cell_coord((double)xi.z, P.range);
+    R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
+    R comp = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const uint32_t k = morton_key(cx + dx, cy + dy, cz + dz, P.mask);
+          const uint32_t b = start[k], e = start[k + 1];
+          for (uint32_t j = b; j < e; ++j) {
+            if ((int)j == i) continue;
+            const R4<R> xj = pos[j];
+            if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
+            if (cnt < P.K) nbr[(size_t)cnt * P.Np + i] = j;
+            ++cnt;
+            const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+            kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
+          }
+        }
+    R denom = P.V0 * sum;
+    if (has_boundary) denom += bW[i];
+    const R V = P.V0 / denom;
+    xv[i] = R4<R>{xi.x, xi.y, xi.z, V};
+    ncnt[i] = (uint32_t)cnt;
+  }
+  // block max of the neighbor count
+  for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_down_sync(0xffffffffu, cnt, o));
+  if ((threadIdx.x & 31) == 0 && cnt > 0) atomicMax(&sc->max_nbrs, cnt);
+}
+
+// ---------------------------------------------------------------------------
+// 5. boundary samples: sample boundaries (sorted sample grid) and volume maps
+// ---------------------------------------------------------------------------
+// Aggregates over a particle's boundary neighbors b (all boundaries):
+//   bW  = sum V_b W_ib                                  (volume)
+//   bG  = {sum V_b gradW_ib, sum V_b (v_b . gradW_ib)}  (pressure, source, a_ii)
+//   bGu = {sum gradW_ib, -}                             (SESPHwSplitting)
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_sample_aggregate(
+    Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, SampleGrid<R> G,
+    R* __restrict__ bW, R4<R>* __restrict__ bG, R4<R>* __restrict__ bGu, StepParams<R> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int cnt = 0;
+  if (i < sc->n_active) {
+    const R4<R> xi = pos[i];
+    const int cx = cell_coord((double)xi.x, P.range), cy = cell_coord((double)xi.y, P.range),
+              cz = cell_coord((double)xi.z, P.range);
+    R w = 0, wc = 0;
+    R gx = 0, gy = 0, gz = 0, gv = 0, ux = 0, uy = 0, uz = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const uint32_t k = morton_key(cx + dx, cy + dy, cz + dz, G.mask);
+          const uint32_t b = G.start[k], e = G.start[k + 1];
+          for (uint32_t s = b; s < e; ++s) {
+            const R4<R> xs = G.xb[s];
+            if (!in_range(xi, xs, P.range, P.range2_lo, P.range2_hi)) continue;
+            ++cnt;
+            const R rx = xi.x - xs.x, ry = xi.y - xs.y, rz = xi.z - xs.z;
+            R kw, f;
+            kernel_w_and_grad(rx * rx + ry * ry + rz * rz, P.k, kw, f);
+            kahan_add(w, wc, xs.w * kw);
+            const R vf = xs.w * f;
+            gx += vf * rx; gy += vf * ry; gz += vf * rz;
+            const R4<R> vs = G.vb[s];
+            gv += vf * (vs.x * rx + vs.y * ry + vs.z * rz);
+            ux += f * rx; uy += f * ry; uz += f * rz;
+          }
+        }
+    bW[i] = w;
+    bG[i] = R4<R>{gx, gy, gz, gv};
+    bGu[i] = R4<R>{ux, uy, uz, R(0)};
+  }
+  for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_down_sync(0xffffffffu, cnt, o));
+  if ((threadIdx.x & 31) == 0 && cnt > 0) atomicMax(&sc->max_bnbrs, cnt);
+}
+
+// Serendipity reference nodes (discretization.rs:267-300): lattice offsets and
+// node kind (0 corner, 1/2/3 edge along x/y/z) with reference coordinates.
+__constant__ double c_ser_ref[32][3];
+__constant__ int c_ser_off[32][3];
+__constant__ int c_ser_kind[32];
+
+__device__ bool ser_function(const DevField& F, double px, double py, double pz, double& out) {
+  const double p[3] = {px, py, pz};
+  long long c[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double fi = floor((p[d] - F.xmin[d]) / F.dx);
+    if (p[d] < F.xmin[d] || p[d] > F.xmax[d]) return false;
+    long long idx = (long long)fi;
+    c[d] = idx < (long long)F.n[d] - 1 ? idx : (long long)F.n[d] - 1;
+  }
+  const double o0 = F.xmin[0] + (double)c[0] * F.dx, o1 = F.xmin[1] + (double)c[1] * F.dx,
+               o2 = F.xmin[2] + (double)c[2] * F.dx;
+  const double xi = 2.0 * (p[0] - o0) / F.dx - 1.0;
+  const double eta = 2.0 * (p[1] - o1) / F.dx - 1.0;
+  const double zeta = 2.0 * (p[2] - o2) / F.dx - 1.0;
+  const double r2 = xi * xi + eta * eta + zeta * zeta;
+  const long long bx = 3 * c[0], by = 3 * c[1], bz = 3 * c[2];
+  double s = 0.0;
+  for (int a = 0; a < 32; ++a) {
+    const long long idx =
+        ((bz + c_ser_off[a][2]) * F.NY + (by + c_ser_off[a][1])) * F.NX + (bx + c_ser_off[a][0]);
+    const double v = __ldg(F.nodes + idx);
+    if (v != v) return false;  // pruned cell
+    const double ax = c_ser_ref[a][0], ay = c_ser_ref[a][1], az = c_ser_ref[a][2];
+    double N;
+    switch (c_ser_kind[a]) {
+      case 0:
+        N = (1.0 / 64.0) * (1.0 + xi * ax) * (1.0 + eta * ay) * (1.0 + zeta * az) * (9.0 * r2 - 19.0);
+        break;
+      case 1:
+        N = (9.0 / 64.0) * (1.0 - xi * xi) * (1.0 + 9.0 * xi * ax) * (1.0 + eta * ay) * (1.0 + zeta * az);
+        break;
+      case 2:
+        N = (9.0 / 64.0) * (1.0 - eta * eta) * (1.0 + 9.0 * eta * ay) * (1.0 + xi * ax) * (1.0 + zeta * az);
+        break;
+      default:
+        N = (9.0 / 64.0) * (1.0 - zeta * zeta) * (1.0 + 9.0 * zeta * az) * (1.0 + xi * ax) * (1.0 + eta * ay);
+        break;
+    }
+    s += v * N;
+  }
+  out = s;
+  return true;
+}
+
+__device__ bool ser_gradient(const DevField& F, double px, double py, double pz, double g[3]) {
+  const double h = F.dx / 6.0;
+  double fp, fm;
+  if (!ser_function(F, px + h, py, pz, fp) || !ser_function(F, px - h, py, pz, fm)) return false;
+  g[0] = (fp - fm) / (2.0 * h);
+  if (!ser_function(F, px, py + h, pz, fp) || !ser_function(F, px, py - h, pz, fm)) return false;
+  g[1] = (fp - fm) / (2.0 * h);
+  if (!ser_function(F, px, py, pz + h, fp) || !ser_function(F, px, py, pz - h, fm)) return false;
+  g[2] = (fp - fm) / (2.0 * h);
+  return true;
+}
+
+// One volume-map boundary sample per (particle, boundary): x_b = x - n d with
+// vol = min(VM, 4/3 pi r^3); stored as vmx = {x_b, vol}, vmv = {v_b, kind}
+// where kind 0 = none, 1 = tangent helper x-axis, 2 = helper y-axis.
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_vm_sample(
+    Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, const VMDesc* __restrict__ vms,
+    int nvm, const Body* __restrict__ bodies, R4<R>* __restrict__ vmx, R4<R>* __restrict__ vmv,
+    R* __restrict__ bW, R4<R>* __restrict__ bG, R4<R>* __restrict__ bGu, StepParams<R> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= sc->n_active) return;
+  const R4<R> xr = pos[i];
+  const double p[3] = {(double)xr.x, (double)xr.y, (double)xr.z};
+  const double range = P.range;
+  const double ball = 4.0 / 3.0 * 3.14159265358979323846 * (range * range * range);
+  R w = 0, gx = 0, gy = 0, gz = 0, gv = 0, ux = 0, uy = 0, uz = 0;
+  for (int b = 0; b < nvm; ++b) {
+    const VMDesc& D = vms[b];
+    const Body* body = D.body >= 0 ? &bodies[D.body] : nullptr;
+    double pl[3] = {p[0], p[1], p[2]};
+    if (body) body_world_to_local(*body, p, pl);
+    int kind = 0;
+    double xb[3] = {0, 0, 0}, vb[3] = {0, 0, 0}, vol = 0;
+    double sd;
+    if (ser_function(D.sdf, pl[0], pl[1], pl[2], sd) && sd < range) {
+      double g[3];
+      if (ser_gradient(D.sdf, pl[0], pl[1], pl[2], g)) {
+        if (body) {
+          double gw[3];
+          qrot(body->q, g, gw);
+          g[0] = gw[0]; g[1] = gw[1]; g[2] = gw[2];
+        }
+        const double gn = sqrt((g[0] * g[0] + g[1] * g[1]) + g[2] * g[2]);
+        double vm;
+        if (gn > 0.5 && gn < 2.0 && ser_function(D.vm, pl[0], pl[1], pl[2], vm) && vm > 0.0) {
+          vol = vm < ball ? vm : ball;
+          const double d = fmax(sd + 0.25 * P.spacing, P.spacing);
+          for (int c = 0; c < 3; ++c) xb[c] = p[c] - g[c] / gn * d;
+          if (body) body_velocity_at(*body, xb, vb);
+          const double u[3] = {xb[0] - p[0], xb[1] - p[1], xb[2] - p[2]};
+          const double un = sqrt((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]);
+          kind = fabs(u[0] / un) > 0.9 ? 2 : 1;
+          // aggregates in f64 from the exact sample position
+          const double rx = p[0] - xb[0], ry = p[1] - xb[1], rz = p[2] - xb[2];
+          const double r2 = (rx * rx + ry * ry) + rz * rz;
+          const double rn = sqrt(r2), q = rn / range;
+          const double a1 = q < 1.0 ? 1.0 - q : 0.0, a2 = q < 0.5 ? 0.5 - q : 0.0;
+          const double alpha = 16.0 / 3.14159265358979323846;
+          const double kw = alpha / (range * range * range) * (a1 * a1 * a1 - 4.0 * (a2 * a2 * a2));
+          const double f = rn > 0.0 ? alpha / (range * range * range * range) *
+                                          (-3.0 * a1 * a1 + 12.0 * a2 * a2) / rn
+                                    : 0.0;
+          w += (R)(vol * kw);
+          const double vf = vol * f;
+          gx += (R)(vf * rx); gy += (R)(vf * ry); gz += (R)(vf * rz);
+          gv += (R)(vf * (vb[0] * rx + vb[1] * ry + vb[2] * rz));
+          ux += (R)(f * rx); uy += (R)(f * ry); uz += (R)(f * rz);
+        }
+      }
+    }
+    const size_t o = (size_t)b * P.Np + i;
+    vmx[o] = R4<R>{(R)xb[0], (R)xb[1], (R)xb[2], (R)vol};
+    vmv[o] = R4<R>{(R)vb[0], (R)vb[1], (R)vb[2], (R)kind};
+  }
+  bW[i] = w;
+  bG[i] = R4<R>{gx, gy, gz, gv};
+  bGu[i] = R4<R>{ux, uy, uz, R(0)};
+}
+
+// ---------------------------------------------------------------------------
+// Boundary iteration helpers used by the acceleration passes
+// ---------------------------------------------------------------------------
+template <class R>
+struct BoundaryArgs {
+  int kind;  // 0 none, 1 sample boundaries, 2 volume maps
+  SampleGrid<R> grid;
+  const R4<R>* vmx;
+  const R4<R>* vmv;
+  const VMDesc* vms;
+  int nvm;
+  const Body* bodies;
+  int any_dynamic;
+  const R* bW;
+  const R4<R>* bG;
+  const R4<R>* bGu;
+  double* body_partials;  // [gridDim][kMaxBodies][6] reaction force/torque partials
+  int nbodies;
+};
+
+// Calls fn(xb, vb, Vb, body) for every boundary neighbor of the viscosity
+// request mode: sample-boundary neighbors, or the 4 tangential volume-map
+// samples at x_b +- r/2 t1, x_b +- r/2 t2 (volume_map_boundary.rs:1344-1377).
+template <class R, class Fn>
+__device__ __forceinline__ void for_each_visc_sample(const BoundaryArgs<R>& B, const R4<R>& xi,
+                                                     int i, const StepParams<R>& P, Fn&& fn) {
+  if (B.kind == 1) {
+    const int cx = cell_coord((double)xi.x, P.range), cy = cell_coord((double)xi.y, P.range),
+              cz = cell_coord((double)xi.z, P.range);
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const uint32_t k = morton_key(cx + dx, cy + dy, cz + dz, B.grid.mask);
+          const uint32_t b = B.grid.start[k], e = B.grid.start[k + 1];
+          for (uint32_t s = b; s < e; ++s) {
+            const R4<R> xs = B.grid.xb[s];
+            if (!in_range(xi, xs, P.range, P.range2_lo, P.range2_hi)) continue;
+            const R4<R> vs = B.grid.vb[s];
+            fn(V3<R>{xs.x, xs.y, xs.z}, V3<R>{vs.x, vs.y, vs.z}, xs.w, (int)B.grid.bid[s]);
+          }
+        }
+  } else if (B.kind == 2) {
+    for (int b = 0; b < B.nvm; ++b) {
+      const size_t o = (size_t)b * P.Np + i;
+      const R4<R> vv = B.vmv[o];
+      if (vv.w == R(0)) continue;
+      const R4<R> xx = B.vmx[o];
+      const V3<R> xb{xx.x, xx.y, xx.z};
+      const V3<R> u = xb - V3<R>{xi.x, xi.y, xi.z};
+      const V3<R> tmp = vv.w == R(1) ? V3<R>{1, 0, 0} : V3<R>{0, 1, 0};
+      V3<R> t1 = cross(u, tmp);
+      V3<R> t2 = cross(u, t1);
+      t1 = (R(1) / sqrt(dot(t1, t1))) * t1;
+      t2 = (R(1) / sqrt(dot(t2, t2))) * t2;
+      const R d = R(0.5) * (R)P.range;
+      const V3<R> q[4] = {xb + d * t1, xb - d * t1, xb + d * t2, xb - d * t2};
+      const int body = B.vms[b].body;
+      for (int k = 0; k < 4; ++k) {
+        V3<R> vq{0, 0, 0};
+        if (body >= 0) {
+          const double pq[3] = {(double)q[k].x, (double)q[k].y, (double)q[k].z};
+          double vo[3];
+          body_velocity_at(B.bodies[body], pq, vo);
+          vq = V3<R>{(R)vo[0], (R)vo[1], (R)vo[2]};
+        }
+        fn(q[k], vq, R(0.25) * xx.w, body);
+      }
+    }
+  }
+}
+
+// Calls fn(xb, Vb, body) for every boundary neighbor of the Normal mode.
+template <class R, class Fn>
+__device__ __forceinline__ void for_each_normal_sample(const BoundaryArgs<R>& B, const R4<R>& xi,
+                                                       int i, const StepParams<R>& P, Fn&& fn) {
+  if (B.kind == 1) {
+    const int cx = cell_coord((double)xi.x, P.range), cy = cell_coord((double)xi.y, P.range),
+              cz = cell_coord((double)xi.z, P.range);
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const uint32_t k = morton_key(cx + dx, cy + dy, cz + dz, B.grid.mask);
+          const uint32_t b = B.grid.start[k], e = B.grid.start[k + 1];
+          for (uint32_t s = b; s < e; ++s) {
+            const R4<R> xs = B.grid.xb[s];
+            if (!in_range(xi, xs, P.range, P.range2_lo, P.range2_hi)) continue;
+            fn(V3<R>{xs.x, xs.y, xs.z}, xs.w, (int)B.grid.bid[s]);
+          }
+        }
+  } else if (B.kind == 2) {
+    for (int b = 0; b < B.nvm; ++b) {
+      const size_t o = (size_t)b * P.Np + i;
+      if (B.vmv[o].w == R(0)) continue;
+      const R4<R> xx = B.vmx[o];
+      fn(V3<R>{xx.x, xx.y, xx.z}, xx.w, B.vms[b].body);
+    }
+  }
+}
+
+// Per-block rigid-body force/torque accumulation in f64 (shared memory),
+// flushed to per-block partials that a fixed-order kernel reduces.
+struct BodyAccum {
+  double* sh;  // [kMaxBodies][6]
+  __device__ void add(const Body* bodies, int body, const double F[3], const double x[3]) {
+    const Body& b = bodies[body];
+    const double r[3] = {x[0] - b.com[0], x[1] - b.com[1], x[2] - b.com[2]};
+    atomicAdd(&sh[body * 6 + 0], F[0]);
+    atomicAdd(&sh[body * 6 + 1], F[1]);
+    atomicAdd(&sh[body * 6 + 2], F[2]);
+    atomicAdd(&sh[body * 6 + 3], r[1] * F[2] - r[2] * F[1]);
+    atomicAdd(&sh[body * 6 + 4], r[2] * F[0] - r[0] * F[2]);
+    atomicAdd(&sh[body * 6 + 5], r[0] * F[1] - r[1] * F[0]);
+  }
+};
+
+__device__ __forceinline__ void body_accum_init(double* sh, int nbodies) {
+  for (int t = threadIdx.x; t < nbodies * 6; t += blockDim.x) sh[t] = 0.0;
+  __syncthreads();
+}
+__device__ __forceinline__ void body_accum_flush(double* sh, int nbodies, double* partials) {
+  __syncthreads();
+  for (int t = threadIdx.x; t < nbodies * 6; t += blockDim.x)
+    partials[(size_t)blockIdx.x * kMaxBodies * 6 + t] = sh[t];
+}
+
+// ---------------------------------------------------------------------------
+// 6. accelerations: gravity + viscosity (+ SESPH pressure) (+ v* = v + dt a)
+// ---------------------------------------------------------------------------
+// PRESS: 0 none, 1 SESPH state equation from the volume on the fly
+template <class R, int PRESS>
+__global__ void __launch_bounds__(kBlock) k_accel(
+    const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
+    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B,
+    R4<R>* __restrict__ acc, R4<R>* __restrict__ vstar, R* __restrict__ press, int write_vstar,
+    StepParams<R> P) {
+  __shared__ double sh_body[kMaxBodies * 6];
+  const bool bodies = B.any_dynamic != 0;
+  if (bodies) body_accum_init(sh_body, B.nbodies);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < sc->n_active) {
+    const R4<R> xi = xv[i];
+    const R4<R> vi = vel[i];
+    const R mi = vi.w, Vi = xi.w;
+    R ax, ay, az;
+    if (P.gravity_mode == 0) {
+      ax = 0; ay = 0; az = R(-9.81);
+    } else {
+      const R dx = P.gc[0] - xi.x, dy = P.gc[1] - xi.y, dz = P.gc[2] - xi.z;
+      const R dist = sqrt(dx * dx + dy * dy + dz * dz + R(1e-4));
+      ax = R(9.81) * dx / dist; ay = R(9.81) * dy / dist; az = R(9.81) * dz / dist;
+    }
+    R pi = 0;
+    if (PRESS == 1) pi = P.stiffness * fmax(P.V0 / Vi - R(1), R(0));
+    R sx = 0, sy = 0, sz = 0;   // viscosity
+    R px = 0, py = 0, pz = 0;   // pressure
+    const int cnt = min((int)ncnt[i], P.K);
+    for (int k = 0; k < cnt; ++k) {
+      const uint32_t j = nbr[(size_t)k * P.Np + i];
+      const R4<R> xj = xv[j];
+      const R4<R> vj = vel[j];
+      const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      const R r2 = rx * rx + ry * ry + rz * rz;
+      const R f = kernel_grad_factor(r2, P.k);
+      const R vr = (vi.x - vj.x) * rx + (vi.y - vj.y) * ry + (vi.z - vj.z) * rz;
+      const R s = P.visc_f * xj.w * vr / (r2 + P.eps_visc) * f;
+      sx += s * rx; sy += s * ry; sz += s * rz;
+      if (PRESS == 1) {
+        const R pj = P.stiffness * fmax(P.V0 / xj.w - R(1), R(0));
+        const R t = xj.w * (pi + pj) * f;
+        px += t * rx; py += t * ry; pz += t * rz;
+      }
+    }
+    if (B.kind != 0) {
+      BodyAccum acc_b{sh_body};
+      for_each_visc_sample<R>(B, xi, i, P, [&](V3<R> xb, V3<R> vb, R Vb, int body) {
+        const R rx = xi.x - xb.x, ry = xi.y - xb.y, rz = xi.z - xb.z;
+        const R r2 = rx * rx + ry * ry + rz * rz;
+        const R f = kernel_grad_factor(r2, P.k);
+        const R vr = (vi.x - vb.x) * rx + (vi.y - vb.y) * ry + (vi.z - vb.z) * rz;
+        const R s = P.visc_b * Vb * vr / (r2 + P.eps_visc) * f;
+        sx += s * rx; sy += s * ry; sz += s * rz;
+        if (bodies && body >= 0 && B.bodies[body].dynamic) {
+          const double F[3] = {-(double)mi * (double)(s * rx), -(double)mi * (double)(s * ry),
+                               -(double)mi * (double)(s * rz)};
+          const double xl[3] = {(double)xb.x, (double)xb.y, (double)xb.z};
+          acc_b.add(B.bodies, body, F, xl);
+        }
+      });
+      if (PRESS == 1) {
+        const R4<R> g = B.bG[i];
+        const R c = R(2) * P.gamma_p * pi;  // boundary: 2 gamma V_i V_b p_i gradW / m_i
+        px += c * g.x; py += c * g.y; pz += c * g.z;
+        if (bodies) {
+          for_each_normal_sample<R>(B, xi, i, P, [&](V3<R> xb, R Vb, int body) {
+            if (body < 0 || !B.bodies[body].dynamic) return;
+            const R rx = xi.x - xb.x, ry = xi.y - xb.y, rz = xi.z - xb.z;
+            const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
+            const double c2 = 2.0 * (double)P.gamma_p * (double)Vi * (double)Vb * (double)pi * (double)f;
+            const double F[3] = {c2 * rx, c2 * ry, c2 * rz};
+            const double xl[3] = {(double)xb.x, (double)xb.y, (double)xb.z};
+            acc_b.add(B.bodies, body, F, xl);
+          });
+        }
+      }
+    }
+    const R vm = Vi / mi;
+    ax += sx - vm * px;
+    ay += sy - vm * py;
+    az += sz - vm * pz;
+    acc[i] = R4<R>{ax, ay, az, R(0)};
+    if (write_vstar) {
+      const R dt = (R)sc->dt;
+      vstar[i] = R4<R>{vi.x + dt * ax, vi.y + dt * ay, vi.z + dt * az, R(0)};
+    }
+    if (PRESS == 1) press[i] = pi;
+  }
+  if (bodies) body_accum_flush(sh_body, B.nbodies, B.body_partials);
+}
+
+// ---------------------------------------------------------------------------
+// 7. pressure acceleration from stored pressures (pressure_solver/mod.rs:121-195)
+// ---------------------------------------------------------------------------
+// MODE: 0 -> accp = accel (Jacobi probe, overwrite, no reaction forces)
+//       1 -> acc += accel (reaction forces if mirror)
+//       2 -> acc  = accel (reaction forces if mirror)
+template <class R, int MODE>
+__global__ void __launch_bounds__(kBlock) k_pressure_accel(
+    const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
+    const R* __restrict__ press, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
+    BoundaryArgs<R> B, R4<R>* __restrict__ out, int mirror, int skip_if_converged,
+    StepParams<R> P) {
+  if (skip_if_converged && sc->converged) return;
+  __shared__ double sh_body[kMaxBodies * 6];
+  const bool bodies = mirror && B.any_dynamic != 0;
+  if (bodies) body_accum_init(sh_body, B.nbodies);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < sc->n_active) {
+    const R4<R> xi = xv[i];
+    const R Vi = xi.w, mi = vel[i].w, pi = press[i];
+    R px = 0, py = 0, pz = 0;
+    const int cnt = min((int)ncnt[i], P.K);
+    for (int k = 0; k < cnt; ++k) {
+      const uint32_t j = nbr[(size_t)k * P.Np + i];
+      const R4<R> xj = xv[j];
+      const R pj = press[j];
+      const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
+      const R t = xj.w * (pi + pj) * f;
+      px += t * rx; py += t * ry; pz += t * rz;
+    }
+    if (B.kind != 0) {
+      const R4<R> g = B.bG[i];
+      const R c = R(2) * P.gamma_p * pi;
+      px += c * g.x; py += c * g.y; pz += c * g.z;
+      if (bodies) {
+        BodyAccum acc_b{sh_body};
+        for_each_normal_sample<R>(B, xi, i, P, [&](V3<R> xb, R Vb, int body) {
+          if (body < 0 || !B.bodies[body].dynamic) return;
+          const R rx = xi.x - xb.x, ry = xi.y - xb.y, rz = xi.z - xb.z;
+          const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
+          const double c2 = 2.0 * (double)P.gamma_p * (double)Vi * (double)Vb * (double)pi * (double)f;
+          const double F[3] = {c2 * rx, c2 * ry, c2 * rz};
+          const double xl[3] = {(double)xb.x, (double)xb.y, (double)xb.z};
+          acc_b.add(B.bodies, body, F, xl);
+        });
+      }
+    }
+    const R vm = Vi / mi;
+    const R4<R> a = R4<R>{-vm * px, -vm * py, -vm * pz, R(0)};
+    if (MODE == 1) {
+      R4<R> o = out[i];
+      o.x += a.x; o.y += a.y; o.z += a.z;
+      out[i] = o;
+    } else {
+      out[i] = a;
+    }
+  }
+  if (bodies) body_accum_flush(sh_body, B.nbodies, B.body_partials);
+}
+
+// ---------------------------------------------------------------------------
+// 8. IISPH: source term + diagonal + initial pressure (iisph.rs:117-376)
+// ---------------------------------------------------------------------------
+// VP = 1: volume-preserving source s = 1 - V0/V - dt sum ..., VP = 0: the
+// velocity-divergence source of IISPHwOST's first solve.
+template <class R, int VP>
+__global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
+    const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
+    const R4<R>* __restrict__ vstar, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B, R* __restrict__ s_out,
+    R* __restrict__ aii_out, R* __restrict__ press, StepParams<R> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= sc->n_active) return;
+  const R dt = (R)sc->dt;
+  const R4<R> xi = xv[i];
+  const R4<R> vsi = vstar[i];
+  const R Vi = xi.w, mi = vel[i].w;
+  R div = 0;                       // sum V_j (v*_i - v*_j) . gradW
+  R sfx = 0, sfy = 0, sfz = 0;     // S_f = sum V_j gradW
+  R s2 = 0;                        // sum V_j^2 / m_j |gradW|^2
+  const int cnt = min((int)ncnt[i], P.K);
+  for (int k = 0; k < cnt; ++k) {
+    const uint32_t j = nbr[(size_t)k * P.Np + i];
+    const R4<R> xj = xv[j];
+    const R4<R> vsj = vstar[j];
+    const R mj = vel[j].w;
+    const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+    const R r2 = rx * rx + ry * ry + rz * rz;
+    const R f = kernel_grad_factor(r2, P.k);
+    const R Vf = xj.w * f;
+    div += Vf * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
+    sfx += Vf * rx; sfy += Vf * ry; sfz += Vf * rz;
+    s2 += xj.w * xj.w / mj * (f * f * r2);
+  }
+  R bx = 0, by = 0, bz = 0, bdiv = 0;
+  if (B.kind != 0) {
+    const R4<R> g = B.bG[i];
+    bx = g.x; by = g.y; bz = g.z;
+    bdiv = vsi.x * g.x + vsi.y * g.y + vsi.z * g.z - g.w;  // sum V_b (v*_i - v_b) . gradW
+  }
+  R s = VP ? R(1) - P.V0 / Vi : R(0);
+  s -= dt * (div + bdiv);
+  const R dt2 = dt * dt;
+  const R c = -Vi / mi;
+  const R cx = c * (sfx + R(2) * P.gamma_p * bx), cy = c * (sfy + R(2) * P.gamma_p * by),
+          cz = c * (sfz + R(2) * P.gamma_p * bz);
+  const R aii = dt2 * (cx * (sfx + bx) + cy * (sfy + by) + cz * (sfz + bz)) - dt2 * Vi * s2;
+  s_out[i] = s;
+  aii_out[i] = aii;
+  R p0 = 0;
+  if (aii > P.min_diag || aii < -P.min_diag) p0 = fmax(P.omega * s / aii, R(0));
+  press[i] = p0;
+}
+
+// Jacobi sweep: A_i = dt^2 [sum V_j (a_i - a_j) . gradW + a_i . bG];
+// p_i <- max(p_i + omega (s_i - A_i) / a_ii, 0); residual in f64.
+// AFTER >= 0: stop after AFTER+1 sweeps; AFTER < 0: target density error.
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
+    Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ accp,
+    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B,
+    const R* __restrict__ s_in, const R* __restrict__ aii_in, R* __restrict__ press,
+    double* __restrict__ partials, int after, StepParams<R> P) {
+  if (sc->converged) return;
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = sc->n_active;
+  double e = 0.0;
+  if (i < n) {
+    const R dt = (R)sc->dt;
+    const R4<R> xi = xv[i];
+    const R4<R> ai = accp[i];
+    R sum = 0;
+    const int cnt = min((int)ncnt[i], P.K);
+    for (int k = 0; k < cnt; ++k) {
+      const uint32_t j = nbr[(size_t)k * P.Np + i];
+      const R4<R> xj = xv[j];
+      const R4<R> aj = accp[j];
+      const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+      const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
+      sum += xj.w * f * ((ai.x - aj.x) * rx + (ai.y - aj.y) * ry + (ai.z - aj.z) * rz);
+    }
+    if (B.kind != 0) {
+      const R4<R> g = B.bG[i];
+      sum += ai.x * g.x + ai.y * g.y + ai.z * g.z;
+    }
+    const R A = dt * dt * sum;
+    const R aii = aii_in[i], s = s_in[i];
+    if (aii < -P.min_diag) press[i] = fmax(press[i] + P.omega * (s - A) / aii, R(0));
+    if (s < R(0)) e = fabs((double)A - (double)s);
+  }
+  const double bs = block_sum(e, sh);
+  double total;
+  if (last_block_total(bs, partials, &sc->done_blocks, &total, sh)) {
+    const double err = n > 0 ? total / (double)n * 100.0 : 0.0;
+    const int it = sc->iterations + 1;
+    sc->iterations = it;
+    sc->err = err;
+    bool stop;
+    if (after >= 0) {
+      stop = it > after;
+    } else {
+      stop = it > 2 && err < P.tde;
+      if (!stop && P.iteration_cap > 0 && it >= P.iteration_cap) {
+        stop = true;
+        sc->status = 2;  // not converged within the cap
+      }
+    }
+    if (stop) sc->converged = 1;
+  }
+}
+
+// IISPHwOST between the solves: v* += dt a_p1 (iisph_optimized_source_term.rs:97-110)
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_ost_predict(Scalars* __restrict__ sc,
+                                                       const R4<R>* __restrict__ acc,
+                                                       R4<R>* __restrict__ vstar) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) {
+    sc->iterations_eqs1 = sc->iterations;
+    sc->iterations = 0;
+    sc->converged = 0;
+    sc->err = INFINITY;
+  }
+  if (i >= sc->n_active) return;
+  const R dt = (R)sc->dt;
+  const R4<R> a = acc[i];
+  R4<R> v = vstar[i];
+  v.x += dt * a.x; v.y += dt * a.y; v.z += dt * a.z;
+  vstar[i] = v;
+}
+
+// IISPHwOST commit: x_pred = x + dt v*, x_new = x_pred + dt^2 a, v_new = v* + dt a
+// into the integrator slots (iisph_optimized_source_term.rs:139-216).
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_ost_commit(const Scalars* __restrict__ sc,
+                                                      const R4<R>* __restrict__ xv,
+                                                      const R4<R>* __restrict__ vel,
+                                                      const R4<R>* __restrict__ vstar,
+                                                      const R4<R>* __restrict__ acc,
+                                                      R4<R>* __restrict__ xint,
+                                                      R4<R>* __restrict__ vint) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= sc->n_active) return;
+  const R dt = (R)sc->dt;
+  const R dt2 = dt * dt;
+  const R4<R> x = xv[i], v = vstar[i], a = acc[i];
+  const R xpx = x.x + dt * v.x, xpy = x.y + dt * v.y, xpz = x.z + dt * v.z;
+  xint[i] = R4<R>{xpx + dt2 * a.x, xpy + dt2 * a.y, xpz + dt2 * a.z, R(0)};
+  vint[i] = R4<R>{v.x + dt * a.x, v.y + dt * a.y, v.z + dt * a.z, vel[i].w};
+}
+
+// SESPHwSplitting predicted density (sesph_with_splitting.rs:90-152) and the
+// state equation: rho* = sum_j [m_j W + dt (v*_i - v*_j) . gradW]
+//                      + (m_i/V0) bW + dt v*_i . bGu, p = k max(V0/(m_i/rho*) - 1, 0)
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_split_density(
+    const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
+    const R4<R>* __restrict__ vstar, const uint32_t* __restrict__ nbr,
+    const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B, R* __restrict__ press,
+    R* __restrict__ rho_pred, StepParams<R> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= sc->n_active) return;
+  const R dt = (R)sc->dt;
+  const R4<R> xi = xv[i];
+  const R4<R> vsi = vstar[i];
+  const R mi = vel[i].w;
+  R rho = mi * P.k.cw * R(0.5), comp = 0;  // self term m_i W(0)
+  const int cnt = min((int)ncnt[i], P.K);
+  for (int k = 0; k < cnt; ++k) {
+    const uint32_t j = nbr[(size_t)k * P.Np + i];
+    const R4<R> xj = xv[j];
+    const R4<R> vsj = vstar[j];
+    const R mj = vel[j].w;
+    const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+    R w, f;
+    kernel_w_and_grad(rx * rx + ry * ry + rz * rz, P.k, w, f);
+    const R t = mj * w + dt * f * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
+    kahan_add(rho, comp, t);
+  }
+  if (B.kind != 0) {
+    const R4<R> gu = B.bGu[i];
+    rho += B.bW[i] * mi / P.V0 + dt * (vsi.x * gu.x + vsi.y * gu.y + vsi.z * gu.z);
+  }
+  rho_pred[i] = rho;
+  const R vol = mi / rho;
+  press[i] = P.stiffness * fmax(P.V0 / vol - R(1), R(0));
+}
+
+// ---------------------------------------------------------------------------
+// 9. reductions: average density after the update (sph/mod.rs:444-486) and
+//    measurement sums (density error, kinetic energy) in f64
+// ---------------------------------------------------------------------------
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_avg_density(Scalars* __restrict__ sc,
+                                                       const R4<R>* __restrict__ xv,
+                                                       const R4<R>* __restrict__ vel,
+                                                       double* __restrict__ partials,
+                                                       StepParams<R> P) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = sc->n_active;
+  double d = 0.0;
+  if (i < n) {
+    const double V = (double)xv[i].w, m = (double)vel[i].w, V0 = (double)P.V0;
+    d = V < V0 ? m / V : m / V0;
+  }
+  double total;
+  if (last_block_total(block_sum(d, sh), partials, &sc->done_blocks, &total, sh))
+    sc->avg_density = n > 0 ? total / (double)n : 0.0;
+}
+
+// out[0] = sum (V < V0 ? V0/V : 1), out[1] = sum 1/2 m |v|^2
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_measure(Scalars* __restrict__ sc,
+                                                   const R4<R>* __restrict__ xv,
+                                                   const R4<R>* __restrict__ vel,
+                                                   double* __restrict__ partials,
+                                                   double* __restrict__ out, StepParams<R> P) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = sc->n_active;
+  double de = 0.0, ke = 0.0;
+  if (i < n) {
+    const double V = (double)xv[i].w, V0 = (double)P.V0;
+    de = V < V0 ? V0 / V : 1.0;
+    const R4<R> v = vel[i];
+    const double vx = v.x, vy = v.y, vz = v.z;
+    ke = 0.5 * (double)v.w * ((vx * vx + vy * vy) + vz * vz);
+  }
+  double t0, t1;
+  const double b0 = block_sum(de, sh);
+  if (last_block_total(b0, partials, &sc->done_blocks, &t0, sh)) out[0] = t0;
+  const double b1 = block_sum(ke, sh);
+  if (last_block_total(b1, partials + gridDim.x, &sc->done_blocks, &t1, sh)) out[1] = t1;
+}
+
+// ---------------------------------------------------------------------------
+// 10. rigid bodies (f64)
+// ---------------------------------------------------------------------------
+// Gravity on dynamic bodies: F += m g at the center of mass
+// (non_pressure_accelerations.rs:79-100, static_sample_boundary.rs:328-341).
+__global__ void k_body_gravity(Body* bodies, int nb, int mode, double gx, double gy, double gz) {
+  const int b = threadIdx.x;
+  if (b >= nb || !bodies[b].dynamic) return;
+  Body& B = bodies[b];
+  double a[3];
+  if (mode == 0) {
+    a[0] = 0.0; a[1] = 0.0; a[2] = -9.81;
+  } else {
+    const double d[3] = {gx - B.com[0], gy - B.com[1], gz - B.com[2]};
+    const double dist = sqrt(((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) + 1e-4);
+    for (int c = 0; c < 3; ++c) a[c] = 9.81 * d[c] / dist;
+  }
+  for (int c = 0; c < 3; ++c) B.F[c] += a[c] * B.mass;
+}
+
+// Fixed-order sum of per-block reaction partials into the body accumulators.
+__global__ void k_body_reduce(Body* bodies, int nb, const double* partials, int nblocks) {
+  const int b = blockIdx.x;
+  if (b >= nb || !bodies[b].dynamic) return;
+  __shared__ double sh[32];
+  for (int c = 0; c < 6; ++c) {
+    double s = 0.0;
+    for (int k = threadIdx.x; k < nblocks; k += blockDim.x)
+      s += partials[(size_t)k * kMaxBodies * 6 + b * 6 + c];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) {
+      if (c < 3) bodies[b].F[c] += s;
+      else bodies[b].T[c - 3] += s;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ void mat_rot(const double q[4], double R_[9]) {
+  const double ww = q[0] * q[0], ii = q[1] * q[1], jj = q[2] * q[2], kk = q[3] * q[3];
+  const double ij = q[1] * q[2] * 2.0, wk = q[0] * q[3] * 2.0, wj = q[0] * q[2] * 2.0;
+  const double ik = q[1] * q[3] * 2.0, jk = q[2] * q[3] * 2.0, wi = q[0] * q[1] * 2.0;
+  R_[0] = ww + ii - jj - kk; R_[1] = ij - wk; R_[2] = wj + ik;
+  R_[3] = wk + ij; R_[4] = ww - ii + jj - kk; R_[5] = jk - wi;
+  R_[6] = ik - wj; R_[7] = wi + jk; R_[8] = ww - ii - jj + kk;
+}
+__device__ void body_update_derived(Body& B) {
+  double Rm[9], t[9];
+  mat_rot(B.q, Rm);
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      t[r * 3 + c] = (Rm[r * 3 + 0] * B.inv_inertia_body[0 * 3 + c] +
+                      Rm[r * 3 + 1] * B.inv_inertia_body[1 * 3 + c]) +
+                     Rm[r * 3 + 2] * B.inv_inertia_body[2 * 3 + c];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      B.inv_inertia_world[r * 3 + c] =
+          (t[r * 3 + 0] * Rm[c * 3 + 0] + t[r * 3 + 1] * Rm[c * 3 + 1]) + t[r * 3 + 2] * Rm[c * 3 + 2];
+  for (int r = 0; r < 3; ++r)
+    B.omega[r] = (B.inv_inertia_world[r * 3 + 0] * B.L[0] + B.inv_inertia_world[r * 3 + 1] * B.L[1]) +
+                 B.inv_inertia_world[r * 3 + 2] * B.L[2];
+}
+
+// Euler-Cromer body step with q <- exp(omega dt / 2) q (rigid_body_motion.rs:183-201).
+__global__ void k_body_step(Body* bodies, int nb, const Scalars* sc) {
+  const int b = threadIdx.x;
+  if (b >= nb || !bodies[b].dynamic) return;
+  Body& B = bodies[b];
+  const double dt = sc->dt;
+  for (int c = 0; c < 3; ++c) {
+    const double a = B.F[c] / B.mass;
+    B.v[c] += a * dt;
+  }
+  for (int c = 0; c < 3; ++c) B.com[c] += B.v[c] * dt;
+  for (int c = 0; c < 3; ++c) B.L[c] += B.T[c] * dt;
+  for (int r = 0; r < 3; ++r)
+    B.omega[r] = (B.inv_inertia_world[r * 3 + 0] * B.L[0] + B.inv_inertia_world[r * 3 + 1] * B.L[1]) +
+                 B.inv_inertia_world[r * 3 + 2] * B.L[2];
+  const double h[3] = {B.omega[0] * dt / 2.0, B.omega[1] * dt / 2.0, B.omega[2] * dt / 2.0};
+  const double nn = (h[0] * h[0] + h[1] * h[1]) + h[2] * h[2];
+  double e[4] = {1.0, 0.0, 0.0, 0.0};
+  if (nn > DBL_EPSILON * DBL_EPSILON) {
+    const double nrm = sqrt(nn), s = sin(nrm) / nrm;
+    e[0] = cos(nrm); e[1] = h[0] * s; e[2] = h[1] * s; e[3] = h[2] * s;
+  }
+  const double* q = B.q;
+  const double nq[4] = {e[0] * q[0] - e[1] * q[1] - e[2] * q[2] - e[3] * q[3],
+                        e[0] * q[1] + e[1] * q[0] + e[2] * q[3] - e[3] * q[2],
+                        e[0] * q[2] - e[1] * q[3] + e[2] * q[0] + e[3] * q[1],
+                        e[0] * q[3] + e[1] * q[2] - e[2] * q[1] + e[3] * q[0]};
+  for (int c = 0; c < 4; ++c) B.q[c] = nq[c];
+  for (int c = 0; c < 3; ++c) { B.F[c] = 0.0; B.T[c] = 0.0; }
+  body_update_derived(B);
+}
+
+// World positions/velocities of dynamic sample-boundary samples
+// (static_sample_boundary.rs:392-412): x = R x_body + c, v = v + omega x (x - c).
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_body_samples(const int* __restrict__ n_ptr,
+                                                        const Body* __restrict__ bodies,
+                                                        const R4<R>* __restrict__ x_body,
+                                                        const uint32_t* __restrict__ orig,
+                                                        const uint32_t* __restrict__ bid,
+                                                        R4<R>* __restrict__ xb,
+                                                        R4<R>* __restrict__ vb) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= *n_ptr) return;
+  const Body& B = bodies[bid[d]];
+  if (!B.dynamic) return;
+  const R4<R> xl = x_body[orig[d]];
+  const double pl[3] = {(double)xl.x, (double)xl.y, (double)xl.z};
+  double pw[3];
+  qrot(B.q, pl, pw);
+  for (int c = 0; c < 3; ++c) pw[c] += B.com[c];
+  double vw[3];
+  body_velocity_at(B, pw, vw);
+  const R V = xb[d].w;
+  xb[d] = R4<R>{(R)pw[0], (R)pw[1], (R)pw[2], V};
+  vb[d] = R4<R>{(R)vw[0], (R)vw[1], (R)vw[2], R(0)};
+}
+
+// Boundary pseudo-volumes V_b = gamma_V / sum_{b' same boundary} W_bb'
+// (static_sample_boundary.rs:354-390), on the sorted sample grid.
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_sample_volumes(const int* __restrict__ n_ptr,
+                                                          SampleGrid<R> G, R4<R>* __restrict__ xb,
+                                                          double gamma_v, StepParams<R> P) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= *n_ptr) return;
+  const R4<R> xi = G.xb[d];
+  const uint32_t myb = G.bid[d];
+  const int cx = cell_coord((double)xi.x, P.range), cy = cell_coord((double)xi.y, P.range),
+            cz = cell_coord((double)xi.z, P.range);
+  R sum = 0, comp = 0;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const uint32_t k = morton_key(cx + dx, cy + dy, cz + dz, G.mask);
+        const uint32_t b = G.start[k], e = G.start[k + 1];
+        for (uint32_t s = b; s < e; ++s) {
+          if (G.bid[s] != myb) continue;
+          const R4<R> xs = G.xb[s];
+          if (!in_range(xi, xs, P.range, P.range2_lo, P.range2_hi)) continue;
+          const R rx = xi.x - xs.x, ry = xi.y - xs.y, rz = xi.z - xs.z;
+          kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
+        }
+      }
+  R4<R> o = xi;
+  o.w = (R)(gamma_v / (double)sum);
+  xb[d] = o;
+}
+
+}  // namespace sph

@@ -1,0 +1,1649 @@
+// Host orchestration of the SPH step engine and the C ABI of include/sphgpu.h.
+//
+// A `System<R>` owns one scene's device state and its CUDA stream and runs
+// the reference's step (sph/mod.rs:125-144, update :674-731) as a fixed
+// sequence of kernel launches. The only host synchronisation per step is the
+// final read of the step scalars (and, for IISPH with a target density
+// error, a convergence check after the first batch of sweeps).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sphgpu.h"
+#include "sph_kernels.cuh"
+
+namespace sph {
+
+// ---------------------------------------------------------------------------
+// errors and buffers
+// ---------------------------------------------------------------------------
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+thread_local std::string g_last_error;
+
+static void cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return;
+  const int code = (e == cudaErrorMemoryAllocation) ? SPH_ERR_OOM : SPH_ERR_CUDA;
+  throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count == 0) return;
+    cuda_check(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+    n = count;
+  }
+  void zero(cudaStream_t s) {
+    if (p) cuda_check(cudaMemsetAsync(p, 0, n * sizeof(T), s), "cudaMemsetAsync");
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+static int blocks_for(long long n) { return (int)std::max(1LL, (n + kBlock - 1) / kBlock); }
+static size_t round_up(size_t n, size_t m) { return (n + m - 1) / m * m; }
+
+// ---------------------------------------------------------------------------
+// serendipity reference node tables (discretization.rs:267-300)
+// ---------------------------------------------------------------------------
+static void upload_serendipity_tables() {
+  static bool done_for[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && done_for[dev]) return;
+  double ref[32][3];
+  int off[32][3];
+  int kind[32];
+  int a = 0;
+  const double s[2] = {-1.0, 1.0}, t[2] = {-1.0 / 3.0, 1.0 / 3.0};
+  auto push = [&](double x, double y, double z) {
+    ref[a][0] = x; ref[a][1] = y; ref[a][2] = z;
+    const double r[3] = {x, y, z};
+    for (int d = 0; d < 3; ++d) off[a][d] = (int)std::llround((r[d] + 1.0) * 1.5);
+    auto corner = [](double c) { return std::fabs(std::fabs(c) - 1.0) < 1e-9; };
+    const bool cx = corner(x), cy = corner(y), cz = corner(z);
+    kind[a] = (cx && cy && cz) ? 0 : (!cx ? 1 : (!cy ? 2 : 3));
+    ++a;
+  };
+  for (double z : s) for (double y : s) for (double x : s) push(x, y, z);
+  for (double z : s) for (double y : s) for (double q : t) push(q, y, z);
+  for (double z : s) for (double x : s) for (double q : t) push(x, q, z);
+  for (double y : s) for (double x : s) for (double q : t) push(x, y, q);
+  cuda_check(cudaMemcpyToSymbol(c_ser_ref, ref, sizeof ref), "serendipity tables");
+  cuda_check(cudaMemcpyToSymbol(c_ser_off, off, sizeof off), "serendipity tables");
+  cuda_check(cudaMemcpyToSymbol(c_ser_kind, kind, sizeof kind), "serendipity tables");
+  if (dev >= 0 && dev < 64) done_for[dev] = true;
+}
+
+// ---------------------------------------------------------------------------
+// precision-agnostic interface
+// ---------------------------------------------------------------------------
+class SystemBase {
+ public:
+  virtual ~SystemBase() = default;
+  virtual SystemBase* clone() const = 0;
+  virtual void upload_fluid(size_t n, const double* x, const double* v, const double* m,
+                            const uint32_t* fid) = 0;
+  virtual int add_sample_boundary(size_t nb, const double* x, const sph_rigid_init* rigid) = 0;
+  virtual int add_volume_map(const sph_grid_desc& sd, const double* sn, const sph_grid_desc& vd,
+                             const double* vn, const sph_rigid_init* rigid) = 0;
+  virtual void initialize() = 0;
+  virtual int step(uint32_t n) = 0;
+  virtual double time() const = 0;
+  virtual uint64_t steps() const = 0;
+  virtual void measurement(sph_measurement* m) = 0;
+  virtual size_t num_particles() const = 0;
+  virtual void download(int field, double* out) = 0;
+  virtual void fluid_ids(uint32_t* out) = 0;
+  virtual void fluid_pos(float* out) = 0;
+  virtual void quantity(int q, float* out) = 0;
+  virtual int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
+  virtual int boundary_neighbors(int bi, uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
+  virtual void boundary_volumes(int bi, double* out) = 0;
+  virtual void vm_samples(int bi, uint8_t* has, double* xb, double* vb, double* vol) = 0;
+  virtual void rigid_state(int bi, double* out) = 0;
+  virtual void set_rigid_state(int bi, const double* in) = 0;
+  virtual uint64_t hash_collisions() = 0;
+  virtual void restore(uint64_t steps, double time, size_t n, const double* x, const double* v,
+                       const double* m, const uint32_t* fid, const double* xi, const double* vi) = 0;
+  virtual uint64_t launches() const = 0;
+  virtual void set_profiling(bool on) = 0;
+  virtual bool kernel_time(const std::string& name, double* ms, uint64_t* count) = 0;
+  virtual size_t device_bytes() const = 0;
+  int device = 0;
+};
+
+// ---------------------------------------------------------------------------
+// System<R>
+// ---------------------------------------------------------------------------
+template <class R>
+class System : public SystemBase {
+ public:
+  explicit System(const sph_config& c) : cfg_(c) {
+    device = c.device;
+    cuda_check(cudaSetDevice(c.device), "cudaSetDevice");
+    cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaMallocHost((void**)&h_sc_, sizeof(Scalars)), "cudaMallocHost");
+    cuda_check(cudaMallocHost((void**)&h_meas_, 2 * sizeof(double)), "cudaMallocHost");
+    d_sc_.alloc(1);
+    d_meas_.alloc(2);
+    std::memset(h_sc_, 0, sizeof(Scalars));
+    upload_serendipity_tables();
+  }
+  ~System() override {
+    for (auto& kv : prof_) {
+      for (auto& e : kv.second.pool) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+      }
+    }
+    if (h_sc_) cudaFreeHost(h_sc_);
+    if (h_meas_) cudaFreeHost(h_meas_);
+    if (stream_) cudaStreamDestroy(stream_);
+  }
+
+  SystemBase* clone() const override;
+
+  // ---- setup ---------------------------------------------------------------
+  void upload_fluid(size_t n, const double* x, const double* v, const double* m,
+                    const uint32_t* fid) override {
+    if (n > 0x7fffffffULL) throw Error(SPH_ERR_INVALID, "too many particles");
+    n_ = n;
+    cap_ = std::max<size_t>(n, 1);
+    np_ = round_up(cap_, 32);
+    alloc_particles();
+    std::vector<R4<R>> hp(cap_), hv(cap_);
+    std::vector<uint32_t> hr(cap_), hf(cap_);
+    for (size_t i = 0; i < n; ++i) {
+      hp[i] = R4<R>{(R)x[3 * i], (R)x[3 * i + 1], (R)x[3 * i + 2], R(0)};
+      const double vx = v ? v[3 * i] : 0.0, vy = v ? v[3 * i + 1] : 0.0, vz = v ? v[3 * i + 2] : 0.0;
+      hv[i] = R4<R>{(R)vx, (R)vy, (R)vz, (R)m[i]};
+      hr[i] = (uint32_t)i;
+      hf[i] = fid ? fid[i] : 0u;
+    }
+    copy_h2d(pos_.p, hp.data(), cap_);
+    copy_h2d(vel_.p, hv.data(), cap_);
+    copy_h2d(ref_.p, hr.data(), cap_);
+    copy_h2d(fid_.p, hf.data(), cap_);
+    acc_.zero(stream_);
+    xint_.zero(stream_);
+    vint_.zero(stream_);
+    host_bbox_.clear();
+    for (size_t i = 0; i < n; ++i) bbox_add(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+    fluid_uploaded_ = true;
+  }
+
+  int add_sample_boundary(size_t nb, const double* x, const sph_rigid_init* rigid) override {
+    if (cfg_.boundary_handling != SPH_STATIC_SAMPLE_BOUNDARY)
+      throw Error(SPH_ERR_INVALID, "system uses VolumeMapBoundary; sample boundary rejected");
+    if ((int)bodies_.size() >= kMaxBodies) throw Error(SPH_ERR_INVALID, "too many boundaries");
+    const int bi = (int)bodies_.size();
+    bodies_.push_back(make_body(rigid));
+    sample_offsets_.push_back(h_sample_x_.size() / 3);
+    sample_counts_.push_back(nb);
+    for (size_t s = 0; s < nb; ++s) {
+      h_sample_x_.push_back(x[3 * s]);
+      h_sample_x_.push_back(x[3 * s + 1]);
+      h_sample_x_.push_back(x[3 * s + 2]);
+      h_sample_bid_.push_back((uint32_t)bi);
+    }
+    return bi;
+  }
+
+  int add_volume_map(const sph_grid_desc& sd, const double* sn, const sph_grid_desc& vd,
+                     const double* vn, const sph_rigid_init* rigid) override {
+    if (cfg_.boundary_handling != SPH_VOLUME_MAP_BOUNDARY)
+      throw Error(SPH_ERR_INVALID, "system uses StaticSampleBoundary; volume map rejected");
+    if ((int)bodies_.size() >= kMaxBodies) throw Error(SPH_ERR_INVALID, "too many boundaries");
+    const int bi = (int)bodies_.size();
+    bodies_.push_back(make_body(rigid));
+    auto f = std::make_unique<FieldPair>();
+    f->sdf_desc = sd;
+    f->vm_desc = vd;
+    for (int which = 0; which < 2; ++which) {
+      const sph_grid_desc& g = which ? vd : sd;
+      for (int d = 0; d < 3; ++d)
+        if (g.n[d] < 1 || g.n[d] > 100000) throw Error(SPH_ERR_INVALID, "bad field grid size");
+      const size_t cnt = (size_t)(3 * g.n[0] + 1) * (size_t)(3 * g.n[1] + 1) * (size_t)(3 * g.n[2] + 1);
+      DBuf<double>& buf = which ? f->vm : f->sdf;
+      buf.alloc(cnt);
+      copy_h2d(buf.p, which ? vn : sn, cnt);
+      if (!rigid)
+        bbox_add(g.x_min[0], g.x_min[1], g.x_min[2]), bbox_add(g.x_max[0], g.x_max[1], g.x_max[2]);
+    }
+    fields_.push_back(std::move(f));
+    return bi;
+  }
+
+  void initialize() override {
+    if (!fluid_uploaded_) throw Error(SPH_ERR_STATE, "upload fluid before initialize");
+    const bool has_dyn = std::any_of(bodies_.begin(), bodies_.end(), [](const Body& b) { return b.dynamic; });
+    const bool iisph_ost = cfg_.pressure_solver == SPH_IISPH_W_OST;
+    const bool takes_pred = cfg_.integration_scheme == SPH_TAKE_PREDICTED;
+    if (iisph_ost != takes_pred)  // sph/setup/mod.rs:229-231
+      throw Error(SPH_ERR_INVALID, "IISPHwOST must pair with TakePredicted (and only it)");
+    if (iisph_ost && has_dyn)  // sph/setup/mod.rs:236-238
+      throw Error(SPH_ERR_INVALID, "IISPHwOST does not support dynamic boundaries");
+    choose_grid();
+    setup_params();
+    // bodies
+    nbodies_ = (int)bodies_.size();
+    any_dynamic_ = has_dyn;
+    bodies_d_.alloc(std::max(1, nbodies_));
+    if (nbodies_) copy_h2d(bodies_d_.p, bodies_.data(), (size_t)nbodies_);
+    body_partials_.alloc((size_t)blocks_for((long long)cap_) * kMaxBodies * 6);
+    // boundaries
+    if (cfg_.boundary_handling == SPH_STATIC_SAMPLE_BOUNDARY && !h_sample_bid_.empty())
+      init_sample_boundaries();
+    if (cfg_.boundary_handling == SPH_VOLUME_MAP_BOUNDARY && !fields_.empty()) init_volume_maps();
+    boundary_kind_ = !h_sample_bid_.empty() ? 1 : (!fields_.empty() ? 2 : 0);
+    // scalars
+    Scalars s{};
+    s.n = (int)n_;
+    s.n_active = (int)n_;
+    s.dt = cfg_.cfl_time_step ? 0.0 : cfg_.time_increment;
+    s.err = 0.0;
+    copy_h2d(d_sc_.p, &s, 1);
+    *h_sc_ = s;
+    steps_ = 0;
+    current_time_ = 0.0;
+    update(2);  // System::new_boxed's first update (sph/mod.rs:418-419)
+    initialized_ = true;
+  }
+
+  // ---- stepping ------------------------------------------------------------
+  int step(uint32_t nsteps) override {
+    if (!initialized_) throw Error(SPH_ERR_STATE, "initialize before stepping");
+    int status = SPH_OK;
+    for (uint32_t s = 0; s < nsteps; ++s) {
+      const auto t0 = std::chrono::steady_clock::now();
+      const double dt_used = h_sc_->dt;
+      // integrate happens inside update(mode) fused with the cell keys; the
+      // rigid-body step must come between it and the neighbor search, and
+      // only needs the time increment, so it is issued first on the stream.
+      if (any_dynamic_) launch("body_step", k_body_step, dim3(1), dim3(32), bodies_d_.p, nbodies_, (const Scalars*)d_sc_.p);
+      ++steps_;
+      if (cfg_.cfl_time_step) current_time_ += dt_used;
+      update(cfg_.integration_scheme == SPH_TAKE_PREDICTED ? 1 : 0);
+      if (h_sc_->status == 2) status = SPH_NOT_CONVERGED;
+      wall_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return status;
+  }
+
+  double time() const override {
+    if (cfg_.cfl_time_step) return current_time_;
+    return time_offset_ + (double)(steps_ - time_offset_steps_) * cfg_.time_increment;
+  }
+  uint64_t steps() const override { return steps_; }
+  size_t num_particles() const override { return n_; }
+
+  void measurement(sph_measurement* m) override {
+    const int nb = blocks_for((long long)n_);
+    ensure_partials(2 * (size_t)nb);
+    launch("measure", k_measure<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
+           (const R4<R>*)vel_.p, partials_.p, d_meas_.p, P_);
+    cuda_check(cudaMemcpyAsync(h_meas_, d_meas_.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream_), "memcpy");
+    sync();
+    std::memset(m, 0, sizeof *m);
+    const double nn = (double)n_;
+    const bool sesph_like = cfg_.pressure_solver == SPH_SESPH || cfg_.pressure_solver == SPH_SESPH_W_SPLITTING;
+    m->time = time();
+    m->density = avg_density_;
+    m->density_error = n_ ? 100.0 * (h_meas_[0] / nn - 1.0) : 0.0;
+    m->kinetic_energy = n_ ? h_meas_[1] / nn : 0.0;
+    m->stiffness = sesph_like ? cfg_.stiffness : 0.0;
+    m->fluid_viscosity = cfg_.fluid_viscosity;
+    m->boundary_viscosity = cfg_.boundary_viscosity;
+    m->fluid_depth = 0.0;
+    m->rest_density_grid_spacing = cfg_.rest_density_grid_spacing;
+    m->kernel_support_radius = cfg_.kernel_support_radius;
+    m->time_step_size = h_sc_->dt;
+    m->target_density_error = sesph_like ? 0.0 : cfg_.target_density_error;
+    m->solver_iterations = sesph_like ? 0u : (uint32_t)h_sc_->iterations;
+    m->relaxation_factor = sesph_like ? 0.0 : cfg_.relaxation_factor;
+    m->time_step_wall_clock_time = wall_;
+    m->predicted_density_error = sesph_like ? 0.0 : h_sc_->err;
+  }
+
+  // ---- readback ------------------------------------------------------------
+  void download(int field, double* out) override {
+    std::vector<uint32_t> ref = fetch(ref_.p, n_);
+    auto vec = [&](const R4<R>* src) {
+      std::vector<R4<R>> h = fetch(src, n_);
+      for (size_t d = 0; d < n_; ++d) {
+        const size_t r = ref[d];
+        out[3 * r] = (double)h[d].x; out[3 * r + 1] = (double)h[d].y; out[3 * r + 2] = (double)h[d].z;
+      }
+    };
+    auto scal = [&](const R* src) {
+      std::vector<R> h = fetch(src, n_);
+      for (size_t d = 0; d < n_; ++d) out[ref[d]] = (double)h[d];
+    };
+    switch (field) {
+      case SPH_FIELD_POSITION: vec(xv_.p); return;
+      case SPH_FIELD_VELOCITY: vec(vel_.p); return;
+      case SPH_FIELD_ACCELERATION: vec(acc_.p); return;
+      case SPH_FIELD_MASS: {
+        std::vector<R4<R>> h = fetch(vel_.p, n_);
+        for (size_t d = 0; d < n_; ++d) out[ref[d]] = (double)h[d].w;
+        return;
+      }
+      case SPH_FIELD_VOLUME: {
+        std::vector<R4<R>> h = fetch(xv_.p, n_);
+        for (size_t d = 0; d < n_; ++d) out[ref[d]] = (double)h[d].w;
+        return;
+      }
+      case SPH_FIELD_PRESSURE: scal(press_.p); return;
+      case SPH_FIELD_FLUID_ID: {
+        std::vector<uint32_t> h = fetch(fid_.p, n_);
+        for (size_t d = 0; d < n_; ++d) out[ref[d]] = (double)h[d];
+        return;
+      }
+      case SPH_FIELD_SOURCE_TERM: need_iisph(); scal(s_.p); return;
+      case SPH_FIELD_DIAGONAL: need_iisph(); scal(aii_.p); return;
+      case SPH_FIELD_PREDICTED_VELOCITY:
+        if (cfg_.pressure_solver == SPH_SESPH) throw Error(SPH_ERR_INVALID, "SESPH has no velocity slot");
+        vec(vstar_.p);
+        return;
+      case SPH_FIELD_INTEGRATOR_POSITION:
+        if (cfg_.integration_scheme != SPH_TAKE_PREDICTED) throw Error(SPH_ERR_INVALID, "no integrator slot");
+        vec(xint_.p);
+        return;
+      case SPH_FIELD_INTEGRATOR_VELOCITY:
+        if (cfg_.integration_scheme != SPH_TAKE_PREDICTED) throw Error(SPH_ERR_INVALID, "no integrator slot");
+        vec(vint_.p);
+        return;
+    }
+    throw Error(SPH_ERR_INVALID, "unknown field");
+  }
+
+  void fluid_ids(uint32_t* out) override {
+    std::vector<uint32_t> ref = fetch(ref_.p, n_), h = fetch(fid_.p, n_);
+    for (size_t d = 0; d < n_; ++d) out[ref[d]] = h[d];
+  }
+  void fluid_pos(float* out) override {
+    std::vector<uint32_t> ref = fetch(ref_.p, n_);
+    std::vector<R4<R>> h = fetch(xv_.p, n_);
+    for (size_t d = 0; d < n_; ++d) {
+      const size_t r = ref[d];
+      out[3 * r] = (float)(double)h[d].x; out[3 * r + 1] = (float)(double)h[d].y; out[3 * r + 2] = (float)(double)h[d].z;
+    }
+  }
+  void quantity(int q, float* out) override {  // sph/mod.rs:202-239
+    std::vector<uint32_t> ref = fetch(ref_.p, n_);
+    std::vector<R4<R>> x = fetch(xv_.p, n_), v = fetch(vel_.p, n_);
+    std::vector<R> p;
+    if (q == SPH_Q_PRESSURE) p = fetch(press_.p, n_);
+    const double V0 = cfg_.rest_density_grid_spacing * cfg_.rest_density_grid_spacing * cfg_.rest_density_grid_spacing;
+    for (size_t d = 0; d < n_; ++d) {
+      const double vx = v[d].x, vy = v[d].y, vz = v[d].z, m = v[d].w, V = x[d].w;
+      double val;
+      switch (q) {
+        case SPH_Q_SPEED: val = std::sqrt((vx * vx + vy * vy) + vz * vz); break;
+        case SPH_Q_VOLUME: val = V; break;
+        case SPH_Q_DENSITY: val = m / V; break;
+        case SPH_Q_DENSITY_ERROR: val = V < V0 ? 100. * (V0 / V - 1.) : 0.; break;
+        case SPH_Q_PRESSURE: val = (double)p[d]; break;
+        case SPH_Q_KINETIC_ENERGY: val = 0.5 * m * ((vx * vx + vy * vy) + vz * vz); break;
+        default: throw Error(SPH_ERR_INVALID, "unknown quantity");
+      }
+      out[ref[d]] = (float)val;
+    }
+  }
+
+  int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) override {
+    std::vector<uint32_t> ref = fetch(ref_.p, n_), cnt = fetch(ncnt_.p, n_);
+    std::vector<uint32_t> nb = fetch(nbr_.p, (size_t)K_ * np_);
+    size_t tot = 0;
+    for (size_t d = 0; d < n_; ++d) tot += 1 + std::min<size_t>(cnt[d], (size_t)K_);
+    *total = tot;
+    if (!off || !idx || cap < tot) return SPH_ERR_CAPACITY;
+    std::vector<uint64_t> rowlen(n_);
+    for (size_t d = 0; d < n_; ++d) rowlen[ref[d]] = 1 + std::min<size_t>(cnt[d], (size_t)K_);
+    off[0] = 0;
+    for (size_t r = 0; r < n_; ++r) off[r + 1] = off[r] + rowlen[r];
+    for (size_t d = 0; d < n_; ++d) {
+      const size_t r = ref[d];
+      uint32_t* row = idx + off[r];
+      const size_t c = std::min<size_t>(cnt[d], (size_t)K_);
+      row[0] = ref[d];
+      for (size_t k = 0; k < c; ++k) row[1 + k] = ref[nb[k * np_ + d]];
+      std::sort(row, row + c + 1);
+    }
+    return SPH_OK;
+  }
+
+  int boundary_neighbors(int bi, uint64_t* off, uint32_t* idx, size_t cap, size_t* total) override;
+  void boundary_volumes(int bi, double* out) override {
+    if (boundary_kind_ != 1 || bi < 0 || bi >= (int)sample_counts_.size())
+      throw Error(SPH_ERR_INVALID, "not a sample boundary");
+    std::vector<R4<R>> x = fetch(xb_.p, ns_);
+    std::vector<uint32_t> o = fetch(sorig_.p, ns_);
+    for (size_t s = 0; s < ns_; ++s) {
+      const size_t g = o[s];
+      if (g >= sample_offsets_[bi] && g < sample_offsets_[bi] + sample_counts_[bi])
+        out[g - sample_offsets_[bi]] = (double)x[s].w;
+    }
+  }
+  void vm_samples(int bi, uint8_t* has, double* xbo, double* vbo, double* vol) override {
+    if (boundary_kind_ != 2 || bi < 0 || bi >= (int)fields_.size())
+      throw Error(SPH_ERR_INVALID, "not a volume-map boundary");
+    std::vector<uint32_t> ref = fetch(ref_.p, n_);
+    std::vector<R4<R>> x = fetch(vmx_.p + (size_t)bi * np_, n_), v = fetch(vmv_.p + (size_t)bi * np_, n_);
+    for (size_t d = 0; d < n_; ++d) {
+      const size_t r = ref[d];
+      has[r] = v[d].w != R(0) ? 1 : 0;
+      for (int c = 0; c < 3; ++c) {
+        xbo[3 * r + c] = has[r] ? (double)(&x[d].x)[c] : 0.0;
+        vbo[3 * r + c] = has[r] ? (double)(&v[d].x)[c] : 0.0;
+      }
+      vol[r] = has[r] ? (double)x[d].w : 0.0;
+    }
+  }
+  void rigid_state(int bi, double* out) override {
+    if (bi < 0 || bi >= nbodies_) throw Error(SPH_ERR_INVALID, "bad boundary index");
+    Body b;
+    cuda_check(cudaMemcpyAsync(&b, bodies_d_.p + bi, sizeof(Body), cudaMemcpyDeviceToHost, stream_), "memcpy");
+    sync();
+    if (!b.dynamic) throw Error(SPH_ERR_INVALID, "static boundary has no rigid state");
+    const double v[19] = {b.com[0], b.com[1], b.com[2], b.q[0], b.q[1], b.q[2], b.q[3],
+                          b.v[0], b.v[1], b.v[2], b.L[0], b.L[1], b.L[2],
+                          b.F[0], b.F[1], b.F[2], b.T[0], b.T[1], b.T[2]};
+    std::memcpy(out, v, sizeof v);
+  }
+  void set_rigid_state(int bi, const double* in) override;
+
+  uint64_t hash_collisions() override;
+  void restore(uint64_t steps, double time, size_t n, const double* x, const double* v,
+               const double* m, const uint32_t* fid, const double* xi, const double* vi) override;
+
+  uint64_t launches() const override { return launches_; }
+  void set_profiling(bool on) override { profiling_ = on; }
+  bool kernel_time(const std::string& name, double* ms, uint64_t* count) override {
+    collect_profile();
+    auto it = prof_.find(name);
+    if (it == prof_.end()) return false;
+    *ms = it->second.ms;
+    *count = it->second.count;
+    return true;
+  }
+  size_t device_bytes() const override {
+    size_t b = 0;
+    for (const auto* p : owned_sizes()) b += *p;
+    for (const auto& f : fields_) b += f->sdf.bytes() + f->vm.bytes();
+    return b;
+  }
+
+ private:
+  friend SystemBase* make_system_copy(const SystemBase*);
+  struct FieldPair {
+    sph_grid_desc sdf_desc, vm_desc;
+    DBuf<double> sdf, vm;
+  };
+  struct ProfEntry {
+    double ms = 0;
+    uint64_t count = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+    size_t used = 0;
+  };
+
+  sph_config cfg_;
+  cudaStream_t stream_ = nullptr;
+  Scalars* h_sc_ = nullptr;
+  double* h_meas_ = nullptr;
+  DBuf<Scalars> d_sc_;
+  DBuf<double> d_meas_;
+  StepParams<R> P_{};
+  size_t n_ = 0, cap_ = 0, np_ = 0;
+  int K_ = 64;
+  uint32_t T_ = 64, mask_ = 3;
+  bool fluid_uploaded_ = false, initialized_ = false;
+  uint64_t steps_ = 0;
+  double current_time_ = 0, time_offset_ = 0, wall_ = 0, avg_density_ = 0;
+  uint64_t time_offset_steps_ = 0;
+  int last_iters_ = 3;
+  uint64_t launches_ = 0;
+  bool profiling_ = false;
+  std::map<std::string, ProfEntry> prof_;
+  struct Pending { std::string name; size_t idx; };
+  std::vector<Pending> pending_;
+
+  // particle state
+  DBuf<R4<R>> pos_, pos2_, vel_, vel2_, xv_, acc_, vstar_, accp_, xint_, vint_, bG_, bGu_;
+  DBuf<R> press_, s_, aii_, bW_, rho_pred_;
+  DBuf<uint32_t> ref_, ref2_, fid_, fid2_, key_, slot_, perm_, nbr_, ncnt_;
+  DBuf<uint32_t> count_, start_, tile_sums_;
+  DBuf<double> partials_, body_partials_;
+  // boundaries
+  std::vector<Body> bodies_;
+  DBuf<Body> bodies_d_;
+  int nbodies_ = 0;
+  bool any_dynamic_ = false;
+  int boundary_kind_ = 0;
+  std::vector<double> h_sample_x_;
+  std::vector<uint32_t> h_sample_bid_;
+  std::vector<size_t> sample_offsets_, sample_counts_;
+  size_t ns_ = 0;
+  DBuf<R4<R>> xb_, xb2_, vb_, vb2_, xbody_;
+  DBuf<uint32_t> sbid_, sbid2_, sorig_, sorig2_, skey_, sslot_, sperm_, scount_, sstart_;
+  DBuf<int> ns_d_;
+  std::vector<std::unique_ptr<FieldPair>> fields_;
+  DBuf<VMDesc> vms_;
+  DBuf<R4<R>> vmx_, vmv_;
+  // bounding box of the scene (cells chosen from it)
+  struct BBox {
+    double mn[3], mx[3];
+    bool any = false;
+    void clear() { any = false; }
+  } bbox_;
+  BBox& host_bbox_ = bbox_;
+
+  std::vector<const size_t*> owned_sizes() const { return {}; }
+
+  // ---- helpers ---------------------------------------------------------------
+  void bbox_add(double x, double y, double z) {
+    const double p[3] = {x, y, z};
+    if (!bbox_.any) {
+      for (int d = 0; d < 3; ++d) bbox_.mn[d] = bbox_.mx[d] = p[d];
+      bbox_.any = true;
+      return;
+    }
+    for (int d = 0; d < 3; ++d) {
+      bbox_.mn[d] = std::min(bbox_.mn[d], p[d]);
+      bbox_.mx[d] = std::max(bbox_.mx[d], p[d]);
+    }
+  }
+  template <class T>
+  void copy_h2d(T* dst, const T* src, size_t n) {
+    if (n == 0) return;
+    cuda_check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, stream_), "cudaMemcpy H2D");
+    sync();
+  }
+  template <class T>
+  std::vector<T> fetch(const T* src, size_t n) {
+    std::vector<T> h(n);
+    if (n) {
+      cuda_check(cudaMemcpyAsync(h.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost, stream_), "cudaMemcpy D2H");
+      sync();
+    }
+    return h;
+  }
+  void sync() { cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize"); }
+  void need_iisph() {
+    if (cfg_.pressure_solver != SPH_IISPH && cfg_.pressure_solver != SPH_IISPH_W_OST)
+      throw Error(SPH_ERR_INVALID, "field only exists for IISPH solvers");
+  }
+  void ensure_partials(size_t n) {
+    if (partials_.n < n) partials_.alloc(n);
+  }
+
+  Body make_body(const sph_rigid_init* r) {
+    Body b{};
+    if (!r) {
+      b.dynamic = 0;
+      b.mass = 1;
+      b.q[0] = 1;
+      return b;
+    }
+    if (!(r->mass != 0.0)) throw Error(SPH_ERR_INVALID, "Rigid body mass cannot be zero.");
+    b.dynamic = 1;
+    b.mass = r->mass;
+    std::memcpy(b.inv_inertia_body, r->inertia_inv_body, sizeof b.inv_inertia_body);
+    std::memcpy(b.com, r->center_of_mass, sizeof b.com);
+    std::memcpy(b.q, r->orientation, sizeof b.q);
+    std::memcpy(b.v, r->linear_velocity, sizeof b.v);
+    // L = (R I_body R^T) omega ; derived: I^-1_world, omega (rigid_body_motion.rs:39-77)
+    double Rm[9];
+    host_rot(b.q, Rm);
+    double Iw[9];
+    host_sandwich(Rm, r->inertia_body, Iw);
+    for (int i = 0; i < 3; ++i)
+      b.L[i] = (Iw[i * 3] * r->angular_velocity[0] + Iw[i * 3 + 1] * r->angular_velocity[1]) +
+               Iw[i * 3 + 2] * r->angular_velocity[2];
+    host_sandwich(Rm, b.inv_inertia_body, b.inv_inertia_world);
+    for (int i = 0; i < 3; ++i)
+      b.omega[i] = (b.inv_inertia_world[i * 3] * b.L[0] + b.inv_inertia_world[i * 3 + 1] * b.L[1]) +
+                   b.inv_inertia_world[i * 3 + 2] * b.L[2];
+    return b;
+  }
+  static void host_rot(const double q[4], double R_[9]) {
+    const double ww = q[0] * q[0], ii = q[1] * q[1], jj = q[2] * q[2], kk = q[3] * q[3];
+    const double ij = q[1] * q[2] * 2.0, wk = q[0] * q[3] * 2.0, wj = q[0] * q[2] * 2.0;
+    const double ik = q[1] * q[3] * 2.0, jk = q[2] * q[3] * 2.0, wi = q[0] * q[1] * 2.0;
+    R_[0] = ww + ii - jj - kk; R_[1] = ij - wk; R_[2] = wj + ik;
+    R_[3] = wk + ij; R_[4] = ww - ii + jj - kk; R_[5] = jk - wi;
+    R_[6] = ik - wj; R_[7] = wi + jk; R_[8] = ww - ii - jj + kk;
+  }
+  static void host_sandwich(const double R_[9], const double M[9], double out[9]) {
+    double t[9];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c)
+        t[r * 3 + c] = (R_[r * 3] * M[c] + R_[r * 3 + 1] * M[3 + c]) + R_[r * 3 + 2] * M[6 + c];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c)
+        out[r * 3 + c] = (t[r * 3] * R_[c * 3] + t[r * 3 + 1] * R_[c * 3 + 1]) + t[r * 3 + 2] * R_[c * 3 + 2];
+  }
+
+  void alloc_particles() {
+    const size_t c = cap_;
+    pos_.alloc(c); pos2_.alloc(c); vel_.alloc(c); vel2_.alloc(c); xv_.alloc(c); acc_.alloc(c);
+    ref_.alloc(c); ref2_.alloc(c); fid_.alloc(c); fid2_.alloc(c);
+    key_.alloc(c); slot_.alloc(c); perm_.alloc(c); ncnt_.alloc(c);
+    press_.alloc(c);
+    bW_.alloc(c); bG_.alloc(c); bGu_.alloc(c);
+    const bool needs_vstar = cfg_.pressure_solver != SPH_SESPH;
+    if (needs_vstar) vstar_.alloc(c);
+    if (cfg_.pressure_solver == SPH_IISPH || cfg_.pressure_solver == SPH_IISPH_W_OST) {
+      s_.alloc(c); aii_.alloc(c); accp_.alloc(c);
+    }
+    if (cfg_.pressure_solver == SPH_SESPH_W_SPLITTING) rho_pred_.alloc(c);
+    if (cfg_.integration_scheme == SPH_TAKE_PREDICTED) { xint_.alloc(c); vint_.alloc(c); }
+    K_ = cfg_.neighbor_capacity ? (int)cfg_.neighbor_capacity : 64;
+    nbr_.alloc((size_t)K_ * np_);
+    ensure_partials(2 * (size_t)blocks_for((long long)c));
+    press_.zero(stream_);
+    bW_.zero(stream_); bG_.zero(stream_); bGu_.zero(stream_);
+  }
+
+  void choose_grid() {
+    // Morton buckets: 2^(3m) with 2^m >= the scene extent in cells (so that
+    // cells only share a bucket when they are 2^m cells apart), m in [2, 8].
+    const double h = cfg_.kernel_support_radius;
+    for (size_t s = 0; s < h_sample_x_.size() / 3; ++s)
+      bbox_add(h_sample_x_[3 * s], h_sample_x_[3 * s + 1], h_sample_x_[3 * s + 2]);
+    double ext = 4;
+    if (bbox_.any)
+      for (int d = 0; d < 3; ++d) ext = std::max(ext, (bbox_.mx[d] - bbox_.mn[d]) / h + 3.0);
+    int m = 2;
+    while (m < 8 && (double)(1u << m) < ext) ++m;
+    mask_ = (1u << m) - 1u;
+    T_ = 1u << (3 * m);
+    count_.alloc(T_ + 2);
+    start_.alloc(T_ + 2);
+    count_.zero(stream_);
+    tile_sums_.alloc((size_t)((T_ + 2 + kScanTile - 1) / kScanTile) + 1);
+  }
+
+  void setup_params() {
+    const double h = cfg_.kernel_support_radius, sp = cfg_.rest_density_grid_spacing;
+    P_.k = make_kernel_const<R>(h);
+    P_.range = h;
+    const double band = sizeof(R) == 4 ? 1e-5 : 1e-12;
+    P_.range2_lo = (R)(h * h * (1.0 - band));
+    P_.range2_hi = (R)(h * h * (1.0 + band));
+    P_.spacing = sp;
+    P_.V0 = (R)(sp * sp * sp);
+    P_.visc_f = (R)(cfg_.fluid_viscosity * 2.0 * (3.0 + 2.0));
+    P_.visc_b = (R)(cfg_.boundary_viscosity * 2.0 * (3.0 + 2.0));
+    P_.eps_visc = (R)(0.01 * sp * sp);
+    P_.gamma_p = (R)cfg_.boundary_pressure_acceleration_weighting;
+    P_.gravity_mode = cfg_.gravity_mode;
+    for (int d = 0; d < 3; ++d) P_.gc[d] = (R)cfg_.gravity_center[d];
+    P_.disable_below = cfg_.disable_particles_below;
+    P_.mask = mask_;
+    P_.T = T_;
+    P_.K = K_;
+    P_.Np = (int)np_;
+    P_.cfl = cfg_.cfl_time_step;
+    P_.dt_fixed = cfg_.time_increment;
+    P_.dt_max = cfg_.max_time_increment;
+    P_.cfl_number = cfg_.cfl_number;
+    P_.stiffness = (R)cfg_.stiffness;
+    P_.omega = (R)cfg_.relaxation_factor;
+    P_.min_diag = (R)cfg_.min_diagonal_element;
+    P_.tde = cfg_.target_density_error;
+    P_.iteration_cap = (int)cfg_.max_solver_iterations;
+  }
+
+  // ---- launches ---------------------------------------------------------------
+  template <class Kern, class... Args>
+  void launch(const char* name, Kern kernel, dim3 g, dim3 b, Args... args) {
+    cudaEvent_t e1 = nullptr;
+    if (profiling_) {
+      ProfEntry& pe = prof_[name];
+      if (pe.used == pe.pool.size()) {
+        cudaEvent_t a, c;
+        cuda_check(cudaEventCreate(&a), "event");
+        cuda_check(cudaEventCreate(&c), "event");
+        pe.pool.push_back({a, c});
+      }
+      auto& pr = pe.pool[pe.used];
+      pending_.push_back({name, pe.used});
+      ++pe.used;
+      cuda_check(cudaEventRecord(pr.first, stream_), "event");
+      e1 = pr.second;
+    }
+    kernel<<<g, b, 0, stream_>>>(args...);
+    cuda_check(cudaGetLastError(), name);
+    ++launches_;
+    if (e1) cuda_check(cudaEventRecord(e1, stream_), "event");
+  }
+  void collect_profile() {
+    if (pending_.empty()) return;
+    sync();
+    for (auto& p : pending_) {
+      ProfEntry& pe = prof_[p.name];
+      float ms = 0;
+      cudaEventElapsedTime(&ms, pe.pool[p.idx].first, pe.pool[p.idx].second);
+      pe.ms += ms;
+      pe.count += 1;
+    }
+    pending_.clear();
+    for (auto& kv : prof_) kv.second.used = 0;
+  }
+
+  // exclusive scan of count[0..m) into out, clearing count
+  void scan(uint32_t* count, uint32_t m, uint32_t* out) {
+    const int tiles = (int)((m + kScanTile - 1) / kScanTile);
+    launch("scan", k_scan_tiles, dim3(tiles), dim3(kBlock), (const uint32_t*)count, (int)m, tile_sums_.p);
+    launch("scan", k_scan_tile_sums, dim3(1), dim3(1024), tile_sums_.p, tiles);
+    launch("scan", k_scan_apply, dim3(tiles), dim3(kBlock), count, (int)m, (const uint32_t*)tile_sums_.p, out);
+  }
+
+  void sort_particles() {
+    const int nb = blocks_for((long long)n_);
+    const int* dn = &d_sc_.p->n;
+    scan(count_.p, T_ + 2, start_.p);
+    launch("sort", k_scatter, dim3(nb), dim3(kBlock), dn, (const uint32_t*)key_.p, (const uint32_t*)slot_.p,
+           (const uint32_t*)start_.p, perm_.p);
+    launch("sort", k_bucket_order, dim3(nb), dim3(kBlock), dn, (const uint32_t*)key_.p, (const uint32_t*)start_.p,
+           (const uint32_t*)ref_.p, perm_.p);
+    launch("sort", k_gather_particles<R>, dim3(nb), dim3(kBlock), dn, (const uint32_t*)perm_.p,
+           (const R4<R>*)pos_.p, (const R4<R>*)vel_.p, (const uint32_t*)ref_.p, (const uint32_t*)fid_.p,
+           pos2_.p, vel2_.p, ref2_.p, fid2_.p);
+    std::swap(pos_.p, pos2_.p);
+    std::swap(vel_.p, vel2_.p);
+    std::swap(ref_.p, ref2_.p);
+    std::swap(fid_.p, fid2_.p);
+  }
+
+  void sort_samples() {
+    const int nb = blocks_for((long long)ns_);
+    const int* dn = ns_d_.p;
+    launch("sample_sort", k_sample_key<R>, dim3(nb), dim3(kBlock), dn, (const R4<R>*)xb_.p, skey_.p, sslot_.p,
+           scount_.p, P_.range, mask_);
+    scan(scount_.p, T_ + 2, sstart_.p);
+    launch("sample_sort", k_scatter, dim3(nb), dim3(kBlock), dn, (const uint32_t*)skey_.p, (const uint32_t*)sslot_.p,
+           (const uint32_t*)sstart_.p, sperm_.p);
+    launch("sample_sort", k_bucket_order, dim3(nb), dim3(kBlock), dn, (const uint32_t*)skey_.p,
+           (const uint32_t*)sstart_.p, (const uint32_t*)sorig_.p, sperm_.p);
+    launch("sample_sort", k_gather_samples<R>, dim3(nb), dim3(kBlock), dn, (const uint32_t*)sperm_.p,
+           (const R4<R>*)xb_.p, (const R4<R>*)vb_.p, (const uint32_t*)sbid_.p, (const uint32_t*)sorig_.p,
+           xb2_.p, vb2_.p, sbid2_.p, sorig2_.p);
+    std::swap(xb_.p, xb2_.p);
+    std::swap(vb_.p, vb2_.p);
+    std::swap(sbid_.p, sbid2_.p);
+    std::swap(sorig_.p, sorig2_.p);
+  }
+
+  SampleGrid<R> sample_grid() const {
+    SampleGrid<R> G;
+    G.xb = xb_.p; G.vb = vb_.p; G.bid = sbid_.p; G.orig = sorig_.p; G.start = sstart_.p; G.mask = mask_;
+    return G;
+  }
+
+  void init_sample_boundaries() {
+    ns_ = h_sample_bid_.size();
+    xb_.alloc(ns_); xb2_.alloc(ns_); vb_.alloc(ns_); vb2_.alloc(ns_); xbody_.alloc(ns_);
+    sbid_.alloc(ns_); sbid2_.alloc(ns_); sorig_.alloc(ns_); sorig2_.alloc(ns_);
+    skey_.alloc(ns_); sslot_.alloc(ns_); sperm_.alloc(ns_);
+    scount_.alloc(T_ + 2); sstart_.alloc(T_ + 2);
+    scount_.zero(stream_);
+    ns_d_.alloc(1);
+    const int nsi = (int)ns_;
+    copy_h2d(ns_d_.p, &nsi, 1);
+    std::vector<R4<R>> hx(ns_), hb(ns_);
+    std::vector<uint32_t> ho(ns_);
+    for (size_t s = 0; s < ns_; ++s) {
+      hx[s] = R4<R>{(R)h_sample_x_[3 * s], (R)h_sample_x_[3 * s + 1], (R)h_sample_x_[3 * s + 2], R(0)};
+      hb[s] = hx[s];
+      ho[s] = (uint32_t)s;
+    }
+    copy_h2d(xb_.p, hx.data(), ns_);
+    copy_h2d(xbody_.p, hb.data(), ns_);
+    copy_h2d(sbid_.p, h_sample_bid_.data(), ns_);
+    copy_h2d(sorig_.p, ho.data(), ns_);
+    vb_.zero(stream_);
+    const int nb = blocks_for((long long)ns_);
+    // dynamic boundaries: world positions from the initial pose
+    // (StaticSampleBoundary::initialize -> update_positions_and_velocities)
+    if (any_dynamic_)
+      launch("body_samples", k_body_samples<R>, dim3(nb), dim3(kBlock), (const int*)ns_d_.p,
+             (const Body*)bodies_d_.p, (const R4<R>*)xbody_.p, (const uint32_t*)sorig_.p,
+             (const uint32_t*)sbid_.p, xb_.p, vb_.p);
+    sort_samples();
+    launch("sample_volumes", k_sample_volumes<R>, dim3(nb), dim3(kBlock), (const int*)ns_d_.p, sample_grid(),
+           xb2_.p, cfg_.boundary_rest_volume_weighting, P_);
+    // the volumes were written into the spare buffer; carry the other lanes over
+    std::vector<R4<R>> vols = fetch(xb2_.p, ns_);
+    std::vector<R4<R>> cur = fetch(xb_.p, ns_);
+    for (size_t s = 0; s < ns_; ++s) cur[s].w = vols[s].w;
+    copy_h2d(xb_.p, cur.data(), ns_);
+  }
+
+  void init_volume_maps() {
+    const int nvm = (int)fields_.size();
+    std::vector<VMDesc> h(nvm);
+    for (int b = 0; b < nvm; ++b) {
+      auto fill = [](DevField& F, const sph_grid_desc& g, const double* nodes) {
+        for (int d = 0; d < 3; ++d) {
+          F.xmin[d] = g.x_min[d];
+          F.xmax[d] = g.x_max[d];
+          F.n[d] = (int)g.n[d];
+        }
+        F.dx = g.dx;
+        F.NX = 3 * g.n[0] + 1;
+        F.NY = 3 * g.n[1] + 1;
+        F.nodes = nodes;
+      };
+      fill(h[b].sdf, fields_[b]->sdf_desc, fields_[b]->sdf.p);
+      fill(h[b].vm, fields_[b]->vm_desc, fields_[b]->vm.p);
+      h[b].body = bodies_[b].dynamic ? b : -1;
+    }
+    vms_.alloc(nvm);
+    copy_h2d(vms_.p, h.data(), (size_t)nvm);
+    vmx_.alloc((size_t)nvm * np_);
+    vmv_.alloc((size_t)nvm * np_);
+    vmv_.zero(stream_);
+  }
+
+  BoundaryArgs<R> bargs() {
+    BoundaryArgs<R> B{};
+    B.kind = boundary_kind_;
+    if (boundary_kind_ == 1) B.grid = sample_grid();
+    B.vmx = vmx_.p;
+    B.vmv = vmv_.p;
+    B.vms = vms_.p;
+    B.nvm = (int)fields_.size();
+    B.bodies = bodies_d_.p;
+    B.any_dynamic = any_dynamic_ ? 1 : 0;
+    B.bW = bW_.p;
+    B.bG = bG_.p;
+    B.bGu = bGu_.p;
+    B.body_partials = body_partials_.p;
+    B.nbodies = nbodies_;
+    return B;
+  }
+
+  void body_reduce(int producer_blocks) {
+    if (!any_dynamic_) return;
+    launch("body_reduce", k_body_reduce, dim3(nbodies_), dim3(kBlock), bodies_d_.p, nbodies_,
+           (const double*)body_partials_.p, producer_blocks);
+  }
+
+  // One Jacobi iteration: pressure accelerations of the current pressures, then
+  // the pressure update with the residual reduction.
+  void iisph_iteration(int after) {
+    const int nb = blocks_for((long long)n_);
+    launch("iisph_pressure_accel", k_pressure_accel<R, 0>, dim3(nb), dim3(kBlock), (const Scalars*)d_sc_.p,
+           (const R4<R>*)xv_.p, (const R4<R>*)vel_.p, (const R*)press_.p, (const uint32_t*)nbr_.p,
+           (const uint32_t*)ncnt_.p, bargs(), accp_.p, 0, 1, P_);
+    launch("iisph_jacobi", k_iisph_jacobi<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
+           (const R4<R>*)accp_.p, (const uint32_t*)nbr_.p, (const uint32_t*)ncnt_.p, bargs(),
+           (const R*)s_.p, (const R*)aii_.p, press_.p, partials_.p, after, P_);
+  }
+
+  // resolve_pressure_globally's loop (iisph.rs:419-550). Sweeps run on the
+  // device and stop themselves once converged; the host only checks the flag
+  // after a batch sized by the previous solve.
+  void solve_loop(int after) {
+    int batch = after >= 0 ? after + 1 : std::max(3, last_iters_);
+    if (after < 0 && cfg_.max_solver_iterations) batch = std::min(batch, (int)cfg_.max_solver_iterations);
+    for (int k = 0; k < batch; ++k) iisph_iteration(after);
+    if (after >= 0) return;
+    int launched = batch;
+    for (;;) {
+      cuda_check(cudaMemcpyAsync(&h_sc_->converged, &d_sc_.p->converged, sizeof(int), cudaMemcpyDeviceToHost, stream_), "memcpy");
+      sync();
+      if (h_sc_->converged) break;
+      const int more = launched < 16 ? 2 : 4;
+      for (int k = 0; k < more; ++k) iisph_iteration(after);
+      launched += more;
+    }
+  }
+
+  void calc_acceleration() {
+    const int nb = blocks_for((long long)n_);
+    if (any_dynamic_)
+      launch("body_gravity", k_body_gravity, dim3(1), dim3(32), bodies_d_.p, nbodies_, cfg_.gravity_mode,
+             cfg_.gravity_center[0], cfg_.gravity_center[1], cfg_.gravity_center[2]);
+    const Scalars* csc = d_sc_.p;
+    const auto xv = (const R4<R>*)xv_.p;
+    const auto vel = (const R4<R>*)vel_.p;
+    const auto nbr = (const uint32_t*)nbr_.p;
+    const auto ncnt = (const uint32_t*)ncnt_.p;
+    switch (cfg_.pressure_solver) {
+      case SPH_SESPH:
+        launch("accel_sesph", k_accel<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(), acc_.p,
+               vstar_.p, press_.p, 0, P_);
+        body_reduce(nb);
+        break;
+      case SPH_SESPH_W_SPLITTING:
+        launch("accel_nonpressure", k_accel<R, 0>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
+               acc_.p, vstar_.p, press_.p, 1, P_);
+        body_reduce(nb);
+        launch("split_density", k_split_density<R>, dim3(nb), dim3(kBlock), csc, xv, vel,
+               (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), press_.p, rho_pred_.p, P_);
+        launch("pressure_accel", k_pressure_accel<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel,
+               (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
+        body_reduce(nb);
+        break;
+      case SPH_IISPH:
+        launch("accel_nonpressure", k_accel<R, 0>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
+               acc_.p, vstar_.p, press_.p, 1, P_);
+        body_reduce(nb);
+        launch("iisph_source_diag", k_iisph_source_diag<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel,
+               (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), s_.p, aii_.p, press_.p, P_);
+        solve_loop(-1);
+        launch("pressure_accel", k_pressure_accel<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel,
+               (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
+        body_reduce(nb);
+        break;
+      case SPH_IISPH_W_OST:
+        launch("accel_nonpressure", k_accel<R, 0>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
+               acc_.p, vstar_.p, press_.p, 1, P_);
+        launch("iisph_source_diag", k_iisph_source_diag<R, 0>, dim3(nb), dim3(kBlock), csc, xv, vel,
+               (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), s_.p, aii_.p, press_.p, P_);
+        solve_loop(3);
+        launch("pressure_accel", k_pressure_accel<R, 2>, dim3(nb), dim3(kBlock), csc, xv, vel,
+               (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
+        launch("ost_predict", k_ost_predict<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)acc_.p, vstar_.p);
+        launch("iisph_source_diag", k_iisph_source_diag<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel,
+               (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), s_.p, aii_.p, press_.p, P_);
+        solve_loop(-1);
+        launch("pressure_accel", k_pressure_accel<R, 2>, dim3(nb), dim3(kBlock), csc, xv, vel,
+               (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
+        launch("ost_commit", k_ost_commit<R>, dim3(nb), dim3(kBlock), csc, xv, vel, (const R4<R>*)vstar_.p,
+               (const R4<R>*)acc_.p, xint_.p, vint_.p);
+        break;
+    }
+  }
+
+ public:
+  // System::update (sph/mod.rs:674-731); mode 0/1 integrate first (EulerCromer
+  // / TakePredicted, euler_cromer.rs:12-25 / take_predicted.rs:14-27), 2 not.
+  void update(int mode) {
+    const int nb = blocks_for((long long)n_);
+    const bool sample_dyn = boundary_kind_ == 1 && any_dynamic_;
+    launch("integrate_key", k_integrate_key<R>, dim3(nb), dim3(kBlock), d_sc_.p, pos_.p, vel_.p,
+           (const R4<R>*)acc_.p, (const R4<R>*)xint_.p, (const R4<R>*)vint_.p, mode, key_.p, slot_.p,
+           count_.p, P_);
+    launch("prologue", k_prologue<R>, dim3(1), dim3(1), d_sc_.p, P_);
+    sort_particles();
+    if (sample_dyn) {
+      const int sb = blocks_for((long long)ns_);
+      launch("body_samples", k_body_samples<R>, dim3(sb), dim3(kBlock), (const int*)ns_d_.p,
+             (const Body*)bodies_d_.p, (const R4<R>*)xbody_.p, (const uint32_t*)sorig_.p,
+             (const uint32_t*)sbid_.p, xb_.p, vb_.p);
+      sort_samples();
+    }
+    if (boundary_kind_ == 1)
+      launch("boundary_samples", k_sample_aggregate<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
+             sample_grid(), bW_.p, bG_.p, bGu_.p, P_);
+    else if (boundary_kind_ == 2)
+      launch("boundary_samples", k_vm_sample<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
+             (const VMDesc*)vms_.p, (int)fields_.size(), (const Body*)bodies_d_.p, vmx_.p, vmv_.p, bW_.p,
+             bG_.p, bGu_.p, P_);
+    launch("neighbors_density", k_neighbors_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
+           (const uint32_t*)start_.p, xv_.p, nbr_.p, ncnt_.p, (const R*)bW_.p, boundary_kind_ ? 1 : 0, P_);
+    calc_acceleration();
+    launch("avg_density", k_avg_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
+           (const R4<R>*)vel_.p, partials_.p, P_);
+    cuda_check(cudaMemcpyAsync(h_sc_, d_sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, stream_), "memcpy");
+    sync();
+    collect_profile();
+    avg_density_ = h_sc_->avg_density;
+    if (h_sc_->iterations > 0) last_iters_ = h_sc_->iterations;
+    if (h_sc_->max_nbrs > K_) {
+      // Neighbor capacity exceeded: grow it and redo the update on the same
+      // (already integrated) state. Reaction forces gathered so far are
+      // discarded first; they are rebuilt by the redo.
+      K_ = (int)round_up((size_t)h_sc_->max_nbrs + 8, 8);
+      P_.K = K_;
+      nbr_.alloc((size_t)K_ * np_);
+      zero_body_forces();
+      finish_disable();
+      update(2);
+      return;
+    }
+    finish_disable();
+  }
+
+ private:
+  void zero_body_forces() {
+    if (!any_dynamic_) return;
+    std::vector<Body> hb = fetch(bodies_d_.p, (size_t)nbodies_);
+    for (auto& b : hb) for (int c = 0; c < 3; ++c) { b.F[c] = 0; b.T[c] = 0; }
+    copy_h2d(bodies_d_.p, hb.data(), hb.size());
+  }
+
+  // Reference-order bookkeeping after disabling particles below the threshold:
+  // Fluid::disable swaps each removed particle with the last active one
+  // (fluid.rs:159-210), which renumbers the survivors. The device already
+  // moved the removed particles behind the active range; replay the swaps on
+  // the reference indices here.
+  void finish_disable() {
+    const int below = h_sc_->n_below;
+    const size_t n_old = (size_t)h_sc_->n;
+    const size_t n_new = (size_t)h_sc_->n_active;
+    // set up the scalars for the next update
+    Scalars next = *h_sc_;
+    next.n = (int)n_new;
+    next.n_below = 0;
+    next.max_speed = 0;
+    if (below > 0) {
+      std::vector<uint32_t> ref_all = fetch(ref_.p, n_old);
+      std::vector<char> is_below(n_old, 0);
+      for (size_t d = n_new; d < n_old; ++d) is_below[ref_all[d]] = 1;
+      std::vector<uint32_t> cur(n_old);
+      for (size_t k = 0; k < n_old; ++k) cur[k] = (uint32_t)k;
+      size_t id = 0, nact = n_old;
+      while (id < nact) {
+        if (is_below[cur[id]]) {
+          --nact;
+          std::swap(cur[id], cur[nact]);
+        } else {
+          ++id;
+        }
+      }
+      std::vector<uint32_t> newref(n_old, 0);
+      for (size_t k = 0; k < n_new; ++k) newref[cur[k]] = (uint32_t)k;
+      for (size_t d = 0; d < n_new; ++d) ref_all[d] = newref[ref_all[d]];
+      copy_h2d(ref_.p, ref_all.data(), n_new);
+      n_ = n_new;
+    }
+    copy_h2d(d_sc_.p, &next, 1);
+    *h_sc_ = next;
+  }
+};
+
+// ---- pieces defined out of line ------------------------------------------------
+template <class R>
+SystemBase* System<R>::clone() const {
+  throw Error(SPH_ERR_INVALID, "clone is provided by sph_clone through checkpoint replay");
+}
+
+template <class R>
+void System<R>::set_rigid_state(int bi, const double* in) {
+  if (bi < 0 || bi >= nbodies_) throw Error(SPH_ERR_INVALID, "bad boundary index");
+  Body b = fetch(bodies_d_.p + bi, 1)[0];
+  if (!b.dynamic) throw Error(SPH_ERR_INVALID, "static boundary has no rigid state");
+  std::memcpy(b.com, in, 3 * sizeof(double));
+  std::memcpy(b.q, in + 3, 4 * sizeof(double));
+  std::memcpy(b.v, in + 7, 3 * sizeof(double));
+  std::memcpy(b.L, in + 10, 3 * sizeof(double));
+  std::memcpy(b.F, in + 13, 3 * sizeof(double));
+  std::memcpy(b.T, in + 16, 3 * sizeof(double));
+  double Rm[9];
+  host_rot(b.q, Rm);
+  host_sandwich(Rm, b.inv_inertia_body, b.inv_inertia_world);
+  for (int i = 0; i < 3; ++i)
+    b.omega[i] = (b.inv_inertia_world[i * 3] * b.L[0] + b.inv_inertia_world[i * 3 + 1] * b.L[1]) +
+                 b.inv_inertia_world[i * 3 + 2] * b.L[2];
+  copy_h2d(bodies_d_.p + bi, &b, 1);
+  bodies_[bi] = b;
+}
+
+// Enumerates sample-boundary neighbors of every particle (count, then fill).
+template <class R>
+__global__ void k_export_sample_neighbors(const Scalars* __restrict__ sc, const R4<R>* __restrict__ pos,
+                                          SampleGrid<R> G, uint32_t* __restrict__ counts,
+                                          const uint64_t* __restrict__ offs, uint32_t* __restrict__ out,
+                                          StepParams<R> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= sc->n_active) return;
+  const R4<R> xi = pos[i];
+  const int cx = cell_coord((double)xi.x, P.range), cy = cell_coord((double)xi.y, P.range),
+            cz = cell_coord((double)xi.z, P.range);
+  uint32_t c = 0;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const uint32_t k = morton_key(cx + dx, cy + dy, cz + dz, G.mask);
+        for (uint32_t s = G.start[k]; s < G.start[k + 1]; ++s) {
+          if (!in_range(xi, G.xb[s], P.range, P.range2_lo, P.range2_hi)) continue;
+          if (out) out[offs[i] + c] = G.orig[s];
+          ++c;
+        }
+      }
+  if (!out) counts[i] = c;
+}
+
+template <class R>
+int System<R>::boundary_neighbors(int bi, uint64_t* off, uint32_t* idx, size_t cap, size_t* total) {
+  if (boundary_kind_ != 1 || bi < 0 || bi >= (int)sample_counts_.size())
+    throw Error(SPH_ERR_INVALID, "not a sample boundary");
+  const int nb = blocks_for((long long)n_);
+  DBuf<uint32_t> counts;
+  counts.alloc(std::max<size_t>(n_, 1));
+  launch("export", k_export_sample_neighbors<R>, dim3(nb), dim3(kBlock), (const Scalars*)d_sc_.p,
+         (const R4<R>*)xv_.p, sample_grid(), counts.p, (const uint64_t*)nullptr, (uint32_t*)nullptr, P_);
+  std::vector<uint32_t> hc = fetch(counts.p, n_);
+  std::vector<uint64_t> hoff(n_ + 1, 0);
+  for (size_t d = 0; d < n_; ++d) hoff[d + 1] = hoff[d] + hc[d];
+  DBuf<uint64_t> doff;
+  doff.alloc(n_ + 1);
+  copy_h2d(doff.p, hoff.data(), n_ + 1);
+  DBuf<uint32_t> dout;
+  dout.alloc(std::max<uint64_t>(hoff[n_], 1));
+  launch("export", k_export_sample_neighbors<R>, dim3(nb), dim3(kBlock), (const Scalars*)d_sc_.p,
+         (const R4<R>*)xv_.p, sample_grid(), counts.p, (const uint64_t*)doff.p, dout.p, P_);
+  std::vector<uint32_t> all = fetch(dout.p, hoff[n_]);
+  std::vector<uint32_t> ref = fetch(ref_.p, n_);
+  const size_t lo = sample_offsets_[bi], hi = lo + sample_counts_[bi];
+  std::vector<std::vector<uint32_t>> rows(n_);
+  for (size_t d = 0; d < n_; ++d)
+    for (uint64_t k = hoff[d]; k < hoff[d + 1]; ++k)
+      if (all[k] >= lo && all[k] < hi) rows[ref[d]].push_back((uint32_t)(all[k] - lo));
+  size_t tot = 0;
+  for (auto& r : rows) tot += r.size();
+  *total = tot;
+  if (!off || !idx || cap < tot) return SPH_ERR_CAPACITY;
+  off[0] = 0;
+  for (size_t r = 0; r < n_; ++r) {
+    std::sort(rows[r].begin(), rows[r].end());
+    std::copy(rows[r].begin(), rows[r].end(), idx + off[r]);
+    off[r + 1] = off[r] + rows[r].size();
+  }
+  return SPH_OK;
+}
+
+// XOR-prime hash (spatial_hashing.rs:49-71) of the 27 stencil cells of every
+// particle; counts particles whose stencil has two cells in one hash bucket,
+// the only case where the reference's neighbor lists hold duplicates.
+__device__ __forceinline__ unsigned long long ref_hash(int k, int l, int m) {
+  auto u = [](int v) -> unsigned long long {
+    return v >= 0 ? (unsigned long long)v * 2ull : (unsigned long long)(-(long long)v) * 2ull + 1ull;
+  };
+  return (u(k) * 73856093ull) ^ (u(l) * 19349663ull) ^ (u(m) * 83492791ull);
+}
+template <class R>
+__global__ void k_hash_collisions(const Scalars* __restrict__ sc, const R4<R>* __restrict__ pos,
+                                  unsigned long long* __restrict__ out, double range) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= sc->n_active) return;
+  const R4<R> x = pos[i];
+  const int cx = cell_coord((double)x.x, range), cy = cell_coord((double)x.y, range),
+            cz = cell_coord((double)x.z, range);
+  unsigned long long h[27];
+  int a = 0;
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dz = -1; dz <= 1; ++dz) h[a++] = ref_hash(cx + dx, cy + dy, cz + dz);
+  for (int p = 0; p < 27; ++p)
+    for (int q = p + 1; q < 27; ++q)
+      if (h[p] == h[q]) {
+        atomicAdd(out, 1ull);
+        return;
+      }
+}
+
+template <class R>
+uint64_t System<R>::hash_collisions() {
+  DBuf<unsigned long long> d;
+  d.alloc(1);
+  d.zero(stream_);
+  launch("diagnostics", k_hash_collisions<R>, dim3(blocks_for((long long)n_)), dim3(kBlock),
+         (const Scalars*)d_sc_.p, (const R4<R>*)xv_.p, d.p, P_.range);
+  return fetch(d.p, 1)[0];
+}
+
+template <class R>
+void System<R>::restore(uint64_t steps, double time, size_t n, const double* x, const double* v,
+                        const double* m, const uint32_t* fid, const double* xi, const double* vi) {
+  if (!initialized_) throw Error(SPH_ERR_STATE, "initialize before restoring a checkpoint");
+  if (n > cap_) throw Error(SPH_ERR_INVALID, "checkpoint holds more particles than the system");
+  n_ = n;
+  std::vector<R4<R>> hp(n), hv(n), hxi(n), hvi(n);
+  std::vector<uint32_t> hr(n), hf(n);
+  for (size_t i = 0; i < n; ++i) {
+    hp[i] = R4<R>{(R)x[3 * i], (R)x[3 * i + 1], (R)x[3 * i + 2], R(0)};
+    hv[i] = R4<R>{(R)v[3 * i], (R)v[3 * i + 1], (R)v[3 * i + 2], (R)m[i]};
+    hr[i] = (uint32_t)i;
+    hf[i] = fid ? fid[i] : 0u;
+    if (xi) hxi[i] = R4<R>{(R)xi[3 * i], (R)xi[3 * i + 1], (R)xi[3 * i + 2], R(0)};
+    if (vi) hvi[i] = R4<R>{(R)vi[3 * i], (R)vi[3 * i + 1], (R)vi[3 * i + 2], (R)m[i]};
+  }
+  copy_h2d(pos_.p, hp.data(), n);
+  copy_h2d(vel_.p, hv.data(), n);
+  copy_h2d(ref_.p, hr.data(), n);
+  copy_h2d(fid_.p, hf.data(), n);
+  if (cfg_.integration_scheme == SPH_TAKE_PREDICTED) {
+    if (xi) copy_h2d(xint_.p, hxi.data(), n); else xint_.zero(stream_);
+    if (vi) copy_h2d(vint_.p, hvi.data(), n); else vint_.zero(stream_);
+  }
+  acc_.zero(stream_);
+  steps_ = steps;
+  if (cfg_.cfl_time_step) {
+    current_time_ = time;
+  }
+  Scalars s = *h_sc_;
+  s.n = (int)n;
+  s.n_active = (int)n;
+  s.n_below = 0;
+  s.max_speed = 0;
+  copy_h2d(d_sc_.p, &s, 1);
+  *h_sc_ = s;
+  update(2);  // continue_from_checkpoint (sph/mod.rs:362-378)
+}
+
+static SystemBase* create_system(const sph_config& c) {
+  if (c.precision == SPH_F64) return new System<double>(c);
+  return new System<float>(c);
+}
+
+}  // namespace sph
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+using sph::Error;
+using sph::SystemBase;
+
+struct sph_system {
+  std::unique_ptr<SystemBase> impl;
+  sph_config cfg;
+  // Replay log for sph_clone: the inputs that built the system.
+  struct Fluid { std::vector<double> x, v, m; std::vector<uint32_t> fid; } fluid;
+  struct SampleB { std::vector<double> x; bool dyn; sph_rigid_init rigid; };
+  struct VMB { sph_grid_desc sd, vd; std::vector<double> sn, vn; bool dyn; sph_rigid_init rigid; };
+  std::vector<int> order;  // 0 sample, 1 vm
+  std::vector<SampleB> samples;
+  std::vector<VMB> vms;
+  bool initialized = false;
+};
+
+template <class F>
+static int guarded(F&& f) {
+  try {
+    f();
+    return SPH_OK;
+  } catch (const Error& e) {
+    sph::g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    sph::g_last_error = "host allocation failed";
+    return SPH_ERR_OOM;
+  } catch (const std::exception& e) {
+    sph::g_last_error = e.what();
+    return SPH_ERR_CUDA;
+  }
+}
+
+static void set_device(const sph_system_t* h) { cudaSetDevice(h->cfg.device); }
+
+extern "C" {
+
+void sph_config_default(sph_config* c) {
+  std::memset(c, 0, sizeof *c);
+  c->kernel_fn = SPH_CUBIC_BSPLINE_3D;
+  c->integration_scheme = SPH_EULER_CROMER;
+  c->pressure_solver = SPH_IISPH;
+  c->neighbor_search = SPH_SPATIAL_HASHING;
+  c->boundary_handling = SPH_VOLUME_MAP_BOUNDARY;
+  c->precision = SPH_F32;
+  c->cfl_time_step = 0;
+  c->gravity_mode = SPH_GRAVITY_UNIFORM;
+  c->rest_density_grid_spacing = 0.8;
+  c->kernel_support_radius = 1.6;
+  c->disable_particles_below = -50.0;
+  c->fluid_viscosity = 0.2;
+  c->boundary_viscosity = 0.2;
+  c->boundary_pressure_acceleration_weighting = 0.7;
+  c->boundary_rest_volume_weighting = 1.0;
+  c->stiffness = 15000000.0;
+  c->target_density_error = 0.05;
+  c->relaxation_factor = 0.5;
+  c->min_diagonal_element = 1e-10;
+  c->time_increment = 0.006;
+  c->max_time_increment = 0.01;
+  c->cfl_number = 0.4;
+  c->max_solver_iterations = 0;
+  c->neighbor_capacity = 64;
+  c->device = 0;
+}
+
+int sph_create(const sph_config* cfg, sph_system_t** out) {
+  return guarded([&] {
+    if (!cfg || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (cfg->kernel_fn != SPH_CUBIC_BSPLINE_3D) throw Error(SPH_ERR_INVALID, "unknown kernel function");
+    if (cfg->neighbor_search != SPH_SPATIAL_HASHING) throw Error(SPH_ERR_INVALID, "unknown neighbor search");
+    if (cfg->integration_scheme < 0 || cfg->integration_scheme > 1)
+      throw Error(SPH_ERR_INVALID, "integration scheme not supported by the GPU engine");
+    if (cfg->pressure_solver < 0 || cfg->pressure_solver > 3) throw Error(SPH_ERR_INVALID, "unknown pressure solver");
+    if (cfg->boundary_handling < 0 || cfg->boundary_handling > 1)
+      throw Error(SPH_ERR_INVALID, "unknown boundary handling");
+    if (!(cfg->kernel_support_radius > 0) || !(cfg->rest_density_grid_spacing > 0))
+      throw Error(SPH_ERR_INVALID, "support radius and spacing must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+      throw Error(SPH_ERR_CUDA, "no CUDA device available");
+    if (cfg->device < 0 || cfg->device >= ndev) throw Error(SPH_ERR_INVALID, "device ordinal out of range");
+    auto h = std::make_unique<sph_system>();
+    h->cfg = *cfg;
+    h->impl.reset(sph::create_system(*cfg));
+    *out = h.release();
+  });
+}
+
+void sph_destroy(sph_system_t* h) {
+  if (!h) return;
+  set_device(h);
+  delete h;
+}
+
+int sph_upload_fluid(sph_system_t* h, size_t n, const double* x, const double* v, const double* m,
+                     const uint32_t* fid) {
+  return guarded([&] {
+    if (!h || (n && (!x || !m))) throw Error(SPH_ERR_INVALID, "null argument");
+    if (h->initialized) throw Error(SPH_ERR_STATE, "fluid is uploaded before initialize");
+    set_device(h);
+    h->impl->upload_fluid(n, x, v, m, fid);
+    h->fluid.x.assign(x, x + 3 * n);
+    h->fluid.v = v ? std::vector<double>(v, v + 3 * n) : std::vector<double>(3 * n, 0.0);
+    h->fluid.m.assign(m, m + n);
+    h->fluid.fid = fid ? std::vector<uint32_t>(fid, fid + n) : std::vector<uint32_t>(n, 0u);
+  });
+}
+
+int sph_add_sample_boundary(sph_system_t* h, size_t nb, const double* x, const sph_rigid_init* rigid,
+                            int* bi) {
+  return guarded([&] {
+    if (!h || (nb && !x)) throw Error(SPH_ERR_INVALID, "null argument");
+    if (h->initialized) throw Error(SPH_ERR_STATE, "boundaries are added before initialize");
+    set_device(h);
+    const int idx = h->impl->add_sample_boundary(nb, x, rigid);
+    if (bi) *bi = idx;
+    sph_system::SampleB s;
+    s.x.assign(x, x + 3 * nb);
+    s.dyn = rigid != nullptr;
+    if (rigid) s.rigid = *rigid;
+    h->samples.push_back(std::move(s));
+    h->order.push_back(0);
+  });
+}
+
+int sph_add_volume_map_boundary(sph_system_t* h, const sph_grid_desc* sdf, const double* sn,
+                                const sph_grid_desc* vm, const double* vn, const sph_rigid_init* rigid,
+                                int* bi) {
+  return guarded([&] {
+    if (!h || !sdf || !sn || !vm || !vn) throw Error(SPH_ERR_INVALID, "null argument");
+    if (h->initialized) throw Error(SPH_ERR_STATE, "boundaries are added before initialize");
+    set_device(h);
+    const int idx = h->impl->add_volume_map(*sdf, sn, *vm, vn, rigid);
+    if (bi) *bi = idx;
+    sph_system::VMB b;
+    b.sd = *sdf;
+    b.vd = *vm;
+    auto cnt = [](const sph_grid_desc& g) {
+      return (size_t)(3 * g.n[0] + 1) * (size_t)(3 * g.n[1] + 1) * (size_t)(3 * g.n[2] + 1);
+    };
+    b.sn.assign(sn, sn + cnt(*sdf));
+    b.vn.assign(vn, vn + cnt(*vm));
+    b.dyn = rigid != nullptr;
+    if (rigid) b.rigid = *rigid;
+    h->vms.push_back(std::move(b));
+    h->order.push_back(1);
+  });
+}
+
+int sph_initialize(sph_system_t* h) {
+  return guarded([&] {
+    if (!h) throw Error(SPH_ERR_INVALID, "null argument");
+    if (h->initialized) throw Error(SPH_ERR_STATE, "already initialized");
+    set_device(h);
+    h->impl->initialize();
+    h->initialized = true;
+  });
+}
+
+int sph_step(sph_system_t* h, uint32_t n) {
+  int st = SPH_OK;
+  int rc = guarded([&] {
+    if (!h) throw Error(SPH_ERR_INVALID, "null argument");
+    set_device(h);
+    st = h->impl->step(n);
+  });
+  return rc != SPH_OK ? rc : st;
+}
+
+int sph_time(const sph_system_t* h, double* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    *out = h->impl->time();
+  });
+}
+int sph_time_steps_propagated(const sph_system_t* h, uint64_t* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    *out = h->impl->steps();
+  });
+}
+int sph_take_measurement(sph_system_t* h, sph_measurement* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->measurement(out);
+  });
+}
+int sph_num_particles(const sph_system_t* h, size_t* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    *out = h->impl->num_particles();
+  });
+}
+int sph_get_fluid_ids(sph_system_t* h, uint32_t* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    set_device(h);
+    h->impl->fluid_ids(out);
+  });
+}
+int sph_get_fluid_pos(sph_system_t* h, float* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    set_device(h);
+    h->impl->fluid_pos(out);
+  });
+}
+int sph_get_quantity_of_fluid_samples(sph_system_t* h, int q, float* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->quantity(q, out);
+  });
+}
+int sph_download(sph_system_t* h, int field, double* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->download(field, out);
+  });
+}
+int sph_get_fluid_neighbors(sph_system_t* h, uint64_t* off, uint32_t* idx, size_t cap, size_t* total) {
+  int st = SPH_OK;
+  int rc = guarded([&] {
+    if (!h || !total) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    st = h->impl->fluid_neighbors(off, idx, cap, total);
+  });
+  return rc != SPH_OK ? rc : st;
+}
+int sph_get_boundary_neighbors(sph_system_t* h, int bi, uint64_t* off, uint32_t* idx, size_t cap,
+                               size_t* total) {
+  int st = SPH_OK;
+  int rc = guarded([&] {
+    if (!h || !total) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    st = h->impl->boundary_neighbors(bi, off, idx, cap, total);
+  });
+  return rc != SPH_OK ? rc : st;
+}
+int sph_get_boundary_volumes(sph_system_t* h, int bi, double* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->boundary_volumes(bi, out);
+  });
+}
+int sph_get_volume_map_samples(sph_system_t* h, int bi, uint8_t* has, double* xb, double* vb, double* vol) {
+  return guarded([&] {
+    if (!h || !has || !xb || !vb || !vol) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->vm_samples(bi, has, xb, vb, vol);
+  });
+}
+int sph_get_rigid_state(sph_system_t* h, int bi, double* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->rigid_state(bi, out);
+  });
+}
+int sph_set_rigid_state(sph_system_t* h, int bi, const double* in) {
+  return guarded([&] {
+    if (!h || !in) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->set_rigid_state(bi, in);
+  });
+}
+int sph_hash_collisions(sph_system_t* h, uint64_t* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    *out = h->impl->hash_collisions();
+  });
+}
+int sph_continue_from_checkpoint(sph_system_t* h, uint64_t steps, double t, size_t n, const double* x,
+                                 const double* v, const double* m, const uint32_t* fid, const double* xi,
+                                 const double* vi) {
+  return guarded([&] {
+    if (!h || (n && (!x || !v || !m))) throw Error(SPH_ERR_INVALID, "null argument");
+    set_device(h);
+    h->impl->restore(steps, t, n, x, v, m, fid, xi, vi);
+  });
+}
+
+// Deep copy: rebuild from the recorded inputs, then restore the source's
+// current dynamic state (fluid, rigid bodies, step counter and time).
+int sph_clone(const sph_system_t* src, sph_system_t** out) {
+  return guarded([&] {
+    if (!src || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!src->initialized) throw Error(SPH_ERR_STATE, "clone an initialized system");
+    set_device(src);
+    sph_system_t* h = nullptr;
+    int rc = sph_create(&src->cfg, &h);
+    if (rc) throw Error(rc, sph_last_error());
+    std::unique_ptr<sph_system_t, void (*)(sph_system_t*)> guard(h, sph_destroy);
+    const size_t n0 = src->fluid.m.size();
+    rc = sph_upload_fluid(h, n0, src->fluid.x.data(), src->fluid.v.data(), src->fluid.m.data(),
+                          src->fluid.fid.data());
+    if (rc) throw Error(rc, sph_last_error());
+    size_t si = 0, vi = 0;
+    for (int kind : src->order) {
+      if (kind == 0) {
+        const auto& s = src->samples[si++];
+        rc = sph_add_sample_boundary(h, s.x.size() / 3, s.x.data(), s.dyn ? &s.rigid : nullptr, nullptr);
+      } else {
+        const auto& b = src->vms[vi++];
+        rc = sph_add_volume_map_boundary(h, &b.sd, b.sn.data(), &b.vd, b.vn.data(), b.dyn ? &b.rigid : nullptr,
+                                         nullptr);
+      }
+      if (rc) throw Error(rc, sph_last_error());
+    }
+    rc = sph_initialize(h);
+    if (rc) throw Error(rc, sph_last_error());
+    SystemBase* s = const_cast<SystemBase*>(src->impl.get());
+    const size_t n = s->num_particles();
+    std::vector<double> x(3 * n), v(3 * n), m(n), fidd(n), xi, vvi;
+    s->download(SPH_FIELD_POSITION, x.data());
+    s->download(SPH_FIELD_VELOCITY, v.data());
+    s->download(SPH_FIELD_MASS, m.data());
+    s->download(SPH_FIELD_FLUID_ID, fidd.data());
+    std::vector<uint32_t> fid(n);
+    for (size_t i = 0; i < n; ++i) fid[i] = (uint32_t)fidd[i];
+    if (src->cfg.integration_scheme == SPH_TAKE_PREDICTED) {
+      xi.resize(3 * n);
+      vvi.resize(3 * n);
+      s->download(SPH_FIELD_INTEGRATOR_POSITION, xi.data());
+      s->download(SPH_FIELD_INTEGRATOR_VELOCITY, vvi.data());
+    }
+    for (int b = 0; b < (int)src->order.size(); ++b) {
+      double st[19];
+      bool dyn = false;
+      try {
+        s->rigid_state(b, st);
+        dyn = true;
+      } catch (const Error&) {
+      }
+      if (dyn) h->impl->set_rigid_state(b, st);
+    }
+    h->impl->restore(s->steps(), s->time(), n, x.data(), v.data(), m.data(), fid.data(),
+                     xi.empty() ? nullptr : xi.data(), vvi.empty() ? nullptr : vvi.data());
+    *out = guard.release();
+  });
+}
+
+int sph_launch_count(const sph_system_t* h, uint64_t* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    *out = h->impl->launches();
+  });
+}
+int sph_set_profiling(sph_system_t* h, int enabled) {
+  return guarded([&] {
+    if (!h) throw Error(SPH_ERR_INVALID, "null argument");
+    h->impl->set_profiling(enabled != 0);
+  });
+}
+int sph_kernel_time(sph_system_t* h, const char* kernel, double* ms, uint64_t* launches) {
+  return guarded([&] {
+    if (!h || !kernel || !ms || !launches) throw Error(SPH_ERR_INVALID, "null argument");
+    set_device(h);
+    if (!h->impl->kernel_time(kernel, ms, launches)) throw Error(SPH_ERR_INVALID, "no timing for that kernel");
+  });
+}
+int sph_device_bytes(const sph_system_t* h, size_t* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    *out = h->impl->device_bytes();
+  });
+}
+
+const char* sph_last_error(void) { return sph::g_last_error.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+"""ctypes declarations of the engine's C ABI (include/sphgpu.h).
+
+The shared library is built in-tree (`libsphgpu.so` next to this file). There
+is no fallback: if the library or a CUDA device is missing, the calls fail
+with an explicit error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsphgpu.so")
+
+# status codes
+SPH_OK, SPH_ERR_INVALID, SPH_ERR_OOM, SPH_ERR_CUDA = 0, 1, 2, 3
+SPH_NOT_CONVERGED, SPH_ERR_STATE, SPH_ERR_CAPACITY = 4, 5, 6
+
+# procedure variants
+CUBIC_BSPLINE_3D = 0
+EULER_CROMER, TAKE_PREDICTED = 0, 1
+SESPH, SESPH_W_SPLITTING, IISPH, IISPH_W_OST = 0, 1, 2, 3
+SPATIAL_HASHING = 0
+STATIC_SAMPLE_BOUNDARY, VOLUME_MAP_BOUNDARY = 0, 1
+F32, F64 = 0, 1
+GRAVITY_UNIFORM, GRAVITY_RADIAL = 0, 1
+
+# download fields
+FIELD_POSITION, FIELD_VELOCITY, FIELD_ACCELERATION = 0, 1, 2
+FIELD_MASS, FIELD_VOLUME, FIELD_PRESSURE, FIELD_FLUID_ID = 3, 4, 5, 6
+FIELD_SOURCE_TERM, FIELD_DIAGONAL, FIELD_PREDICTED_VELOCITY = 8, 9, 10
+FIELD_INTEGRATOR_POSITION, FIELD_INTEGRATOR_VELOCITY = 11, 12
+VECTOR_FIELDS = {FIELD_POSITION, FIELD_VELOCITY, FIELD_ACCELERATION, FIELD_PREDICTED_VELOCITY,
+                 FIELD_INTEGRATOR_POSITION, FIELD_INTEGRATOR_VELOCITY}
+
+# scalar quantities (render_info ScalarQuantity)
+Q_SPEED, Q_VOLUME, Q_DENSITY, Q_DENSITY_ERROR, Q_PRESSURE, Q_KINETIC_ENERGY = range(6)
+
+
+class SphConfig(C.Structure):
+    _fields_ = [
+        ("kernel_fn", C.c_int), ("integration_scheme", C.c_int), ("pressure_solver", C.c_int),
+        ("neighbor_search", C.c_int), ("boundary_handling", C.c_int), ("precision", C.c_int),
+        ("cfl_time_step", C.c_int), ("gravity_mode", C.c_int),
+        ("rest_density_grid_spacing", C.c_double), ("kernel_support_radius", C.c_double),
+        ("disable_particles_below", C.c_double), ("fluid_viscosity", C.c_double),
+        ("boundary_viscosity", C.c_double),
+        ("boundary_pressure_acceleration_weighting", C.c_double),
+        ("boundary_rest_volume_weighting", C.c_double), ("stiffness", C.c_double),
+        ("target_density_error", C.c_double), ("relaxation_factor", C.c_double),
+        ("min_diagonal_element", C.c_double), ("time_increment", C.c_double),
+        ("max_time_increment", C.c_double), ("cfl_number", C.c_double),
+        ("gravity_center", C.c_double * 3), ("max_solver_iterations", C.c_uint32),
+        ("neighbor_capacity", C.c_uint32), ("device", C.c_int),
+    ]
+
+
+class SphRigidInit(C.Structure):
+    _fields_ = [
+        ("mass", C.c_double), ("inertia_body", C.c_double * 9),
+        ("inertia_inv_body", C.c_double * 9), ("center_of_mass", C.c_double * 3),
+        ("orientation", C.c_double * 4), ("linear_velocity", C.c_double * 3),
+        ("angular_velocity", C.c_double * 3),
+    ]
+
+
+class SphGridDesc(C.Structure):
+    _fields_ = [("x_min", C.c_double * 3), ("x_max", C.c_double * 3), ("dx", C.c_double),
+                ("n", C.c_int64 * 3)]
+
+
+class SphMeasurement(C.Structure):
+    _fields_ = [
+        ("time", C.c_double), ("density", C.c_double), ("density_error", C.c_double),
+        ("kinetic_energy", C.c_double), ("stiffness", C.c_double),
+        ("fluid_viscosity", C.c_double), ("boundary_viscosity", C.c_double),
+        ("fluid_depth", C.c_double), ("rest_density_grid_spacing", C.c_double),
+        ("kernel_support_radius", C.c_double), ("time_step_size", C.c_double),
+        ("target_density_error", C.c_double), ("solver_iterations", C.c_uint32),
+        ("relaxation_factor", C.c_double), ("time_step_wall_clock_time", C.c_double),
+        ("predicted_density_error", C.c_double),
+    ]
+
+
+class SPHError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"sphgpu error {code}: {msg}")
+        self.code = code
+
+
+# every exported symbol: name -> (restype, argtypes)
+_vp = C.c_void_p
+_dp = np.ctypeslib.ndpointer(np.float64, flags="C")
+_fp = np.ctypeslib.ndpointer(np.float32, flags="C")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C")
+_sz = C.c_size_t
+SIGNATURES = {
+    "sph_config_default": (None, [C.POINTER(SphConfig)]),
+    "sph_create": (C.c_int, [C.POINTER(SphConfig), C.POINTER(_vp)]),
+    "sph_destroy": (None, [_vp]),
+    "sph_clone": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "sph_upload_fluid": (C.c_int, [_vp, _sz, _dp, _dp, _dp, _u32p]),
+    "sph_add_sample_boundary": (C.c_int, [_vp, _sz, _dp, C.POINTER(SphRigidInit), C.POINTER(C.c_int)]),
+    "sph_add_volume_map_boundary": (C.c_int, [_vp, C.POINTER(SphGridDesc), _dp, C.POINTER(SphGridDesc),
+                                              _dp, C.POINTER(SphRigidInit), C.POINTER(C.c_int)]),
+    "sph_initialize": (C.c_int, [_vp]),
+    "sph_step": (C.c_int, [_vp, C.c_uint32]),
+    "sph_time": (C.c_int, [_vp, C.POINTER(C.c_double)]),
+    "sph_time_steps_propagated": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "sph_take_measurement": (C.c_int, [_vp, C.POINTER(SphMeasurement)]),
+    "sph_num_particles": (C.c_int, [_vp, C.POINTER(_sz)]),
+    "sph_get_fluid_ids": (C.c_int, [_vp, _u32p]),
+    "sph_get_fluid_pos": (C.c_int, [_vp, _fp]),
+    "sph_get_quantity_of_fluid_samples": (C.c_int, [_vp, C.c_int, _fp]),
+    "sph_download": (C.c_int, [_vp, C.c_int, _dp]),
+    "sph_get_fluid_neighbors": (C.c_int, [_vp, _vp, _vp, _sz, C.POINTER(_sz)]),
+    "sph_get_boundary_neighbors": (C.c_int, [_vp, C.c_int, _vp, _vp, _sz, C.POINTER(_sz)]),
+    "sph_get_boundary_volumes": (C.c_int, [_vp, C.c_int, _dp]),
+    "sph_get_volume_map_samples": (C.c_int, [_vp, C.c_int, _u8p, _dp, _dp, _dp]),
+    "sph_get_rigid_state": (C.c_int, [_vp, C.c_int, _dp]),
+    "sph_set_rigid_state": (C.c_int, [_vp, C.c_int, _dp]),
+    "sph_hash_collisions": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "sph_continue_from_checkpoint": (C.c_int, [_vp, C.c_uint64, C.c_double, _sz, _dp, _dp, _dp, _u32p,
+                                               _vp, _vp]),
+    "sph_spatial_hashing_find_samples": (C.c_int, [C.c_double, _sz, _dp, _sz, _dp, _vp, _vp, _sz,
+                                                   C.POINTER(_sz), C.c_int]),
+    "sph_kernel_function": (C.c_int, [_sz, _dp, C.c_double, _dp, C.c_int, C.c_int]),
+    "sph_kernel_gradient": (C.c_int, [_sz, _dp, C.c_double, _dp, C.c_int, C.c_int]),
+    "sph_last_error": (C.c_char_p, []),
+    "sph_launch_count": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "sph_set_profiling": (C.c_int, [_vp, C.c_int]),
+    "sph_kernel_time": (C.c_int, [_vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    "sph_device_bytes": (C.c_int, [_vp, C.POINTER(_sz)]),
+}
+
+_lib = None
+
+
+def load():
+    """Load libsphgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `make -C fluid-simulation_b200/csrc` "
+            "(or __graft_entry__.build()); the engine has no CPU fallback")
+    L = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc, allow=()):
+    if rc == SPH_OK or rc in allow:
+        return rc
+    msg = load().sph_last_error()
+    raise SPHError(rc, msg.decode() if msg else "")

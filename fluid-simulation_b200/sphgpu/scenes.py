@@ -1,0 +1,184 @@
+"""Seeded synthetic scenes for the SPH engine.
+
+Fluid blocks are cubic lattices with uniform jitter, stored as f32-representable
+values so that an f64 checker sees exactly the positions the f32 engine holds
+(the reference injects such a state through its `--state` checkpoint path,
+sim_lib sph/setup/mod.rs:142-153). Containers are the reference's cube mesh
+(cube_face_normals_inwards.obj: 8 vertices, 12 inward-facing triangles) under
+the reference's mesh transform (utilities/triangle_mesh.rs:314-334: scale,
+then rotate, then translate).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# Unit cube [-1, 1]^3 with inward-facing triangles, vertex order of the
+# reference's OBJ file.
+CUBE_VERTICES = np.array([
+    [1, 1, 1], [1, 1, -1], [1, -1, 1], [1, -1, -1],
+    [-1, 1, 1], [-1, 1, -1], [-1, -1, 1], [-1, -1, -1]], dtype=np.float64)
+CUBE_FACES_INWARD = np.array([
+    [3, 5, 1], [8, 3, 4], [6, 7, 8], [8, 2, 6], [4, 1, 2], [2, 5, 6],
+    [3, 7, 5], [8, 7, 3], [6, 5, 7], [8, 4, 2], [4, 3, 1], [2, 1, 5]], dtype=np.uint32) - 1
+CUBE_FACES_OUTWARD = CUBE_FACES_INWARD[:, ::-1].copy()
+
+
+def euler_to_matrix(rx, ry, rz):
+    """nalgebra Rotation3::from_euler_angles(roll, pitch, yaw) = Rz * Ry * Rx."""
+    cx, sx, cy, sy, cz, sz = np.cos(rx), np.sin(rx), np.cos(ry), np.sin(ry), np.cos(rz), np.sin(rz)
+    Rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    Ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    Rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    return Rz @ Ry @ Rx
+
+
+def transform_mesh(verts, translation=(0, 0, 0), rotation_euler_deg=(0, 0, 0), scale=(1, 1, 1)):
+    v = np.asarray(verts, np.float64) * np.broadcast_to(np.asarray(scale, np.float64), (3,))
+    R = euler_to_matrix(*np.radians(rotation_euler_deg))
+    return v @ R.T + np.asarray(translation, np.float64)
+
+
+def sample_triangle_surface(v0, v1, v2, spacing):
+    """Isotropic raster of one triangle (utilities/sampling.rs:59-106)."""
+    e1, e2 = v1 - v0, v2 - v0
+    l1 = np.sqrt((e1[0] * e1[0] + e1[1] * e1[1]) + e1[2] * e1[2])
+    if l1 < 1e-12:
+        return np.zeros((0, 3))
+    eu = e1 / l1
+    proj = (e2[0] * eu[0] + e2[1] * eu[1]) + e2[2] * eu[2]
+    perp = e2 - eu * proj
+    pl = np.sqrt((perp[0] * perp[0] + perp[1] * perp[1]) + perp[2] * perp[2])
+    if pl < 1e-12:
+        return np.zeros((0, 3))
+    ev = perp / pl
+    p = np.array([[0.0, 0.0], [l1, 0.0], [proj, pl]])
+    min_x, max_x = p[:, 0].min(), p[:, 0].max()
+    min_y, max_y = p[:, 1].min(), p[:, 1].max()
+    nx = int(np.ceil((max_x - min_x) / spacing))
+    ny = int(np.ceil((max_y - min_y) / spacing))
+    out = []
+    a, b, c = p
+    for j in range(ny + 1):
+        y = min_y + j * spacing
+        for i in range(nx + 1):
+            x = min_x + i * spacing
+            q = np.array([x, y])
+            d1 = _cross2(b - a, q - a)
+            d2 = _cross2(c - b, q - b)
+            d3 = _cross2(a - c, q - c)
+            has_neg = d1 < 0.0 or d2 < 0.0 or d3 < 0.0
+            has_pos = d1 > 0.0 or d2 > 0.0 or d3 > 0.0
+            if not (has_neg and has_pos):
+                out.append(v0 + eu * x + ev * y)
+    return np.array(out).reshape(-1, 3)
+
+
+def _cross2(a, b):
+    return a[0] * b[1] - a[1] * b[0]
+
+
+def sample_triangle_mesh_surface(verts, faces, spacing):
+    """All triangles in order (utilities/sampling.rs:169-178)."""
+    parts = [sample_triangle_surface(verts[f[0]], verts[f[1]], verts[f[2]], spacing) for f in faces]
+    return np.concatenate(parts, axis=0) if parts else np.zeros((0, 3))
+
+
+def lattice_block(counts, spacing, origin, jitter=0.01, seed=0):
+    """Cubic lattice of counts[0]*counts[1]*counts[2] particles starting half a
+    spacing inside `origin`, with uniform jitter of +-jitter*spacing per axis;
+    returned as f32-representable f64 values (x fastest)."""
+    nx, ny, nz = counts
+    rng = np.random.default_rng(seed)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    base = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64)
+    pos = np.asarray(origin, np.float64) + (base + 0.5) * spacing
+    pos += rng.uniform(-jitter * spacing, jitter * spacing, size=pos.shape)
+    return pos.astype(np.float32).astype(np.float64)
+
+
+@dataclass
+class Scene:
+    """Inputs of one system: configuration, fluid state and boundaries."""
+    procedures: dict
+    parameters: dict
+    cfl_time_step: bool
+    position: np.ndarray
+    mass: np.ndarray
+    velocity: np.ndarray | None = None
+    fluid_id: np.ndarray | None = None
+    sample_boundaries: list = field(default_factory=list)   # [(positions, RigidInit|None)]
+    volume_maps: list = field(default_factory=list)         # [(sdf, vm, RigidInit|None)]
+    mesh: tuple | None = None                               # (verts, faces) of the container
+    description: str = ""
+
+
+def dam_break_sesph_8k(jitter_seed=0, n_side=20):
+    """SESPH dam break: a 20^3 lattice (spacing 0.02, +-1 % jitter) in the
+    corner of a 0.6 m cube container of StaticSampleBoundary samples taken at
+    0.7 * spacing from the reference's inward cube mesh scaled 0.3; support 2h,
+    rest density 1000, stiffness 1000, viscosity 0.01, dt 1e-3, EulerCromer."""
+    h = 0.02
+    verts = transform_mesh(CUBE_VERTICES, scale=(0.3, 0.3, 0.3))
+    samples = sample_triangle_mesh_surface(verts, CUBE_FACES_INWARD, 0.7 * h)
+    pos = lattice_block((n_side, n_side, n_side), h, origin=(-0.3, -0.3, -0.3), jitter=0.01,
+                        seed=jitter_seed)
+    return Scene(
+        procedures={"kernel_function": "CubicBSpline3D", "integration_scheme": "EulerCromer",
+                    "pressure_solver": "SESPH", "neighbor_search": "SpatialHashing",
+                    "boundary_handling": "StaticSampleBoundary"},
+        parameters={"rest_density_grid_spacing": h, "kernel_support_radius": 2 * h,
+                    "disable_particles_below": -50.0, "fluid_viscosity": 0.01,
+                    "boundary_viscosity": 0.01, "boundary_pressure_acceleration_weighting": 0.7,
+                    "boundary_rest_volume_weighting": 1.0, "stiffness": 1000.0,
+                    "time_increment": 1e-3},
+        cfl_time_step=False, position=pos, mass=np.full(pos.shape[0], 1000.0 * h ** 3),
+        sample_boundaries=[(samples, None)], mesh=(verts, CUBE_FACES_INWARD),
+        description=f"SESPH dam break {pos.shape[0]} particles, sample boundary {samples.shape[0]}")
+
+
+def dam_break_iisph_box(n_side=100, spacing=0.01, jitter_seed=0, box=(2.0, 1.0, 1.0)):
+    """IISPH dam break: an n_side^3 lattice (+-1 % jitter) against the -x end of a
+    box container (the reference's inward cube mesh scaled to `box`) handled as a
+    VolumeMapBoundary with the reference's field spacing dx = 4 * spacing;
+    omega 0.5, target density error 0.1 %, CFL 0.4 with dt <= 2e-3."""
+    h = spacing
+    verts = transform_mesh(CUBE_VERTICES, scale=(box[0] / 2, box[1] / 2, box[2] / 2))
+    lo = -0.5 * np.asarray(box)
+    pos = lattice_block((n_side, n_side, n_side), h, origin=lo, jitter=0.01, seed=jitter_seed)
+    return Scene(
+        procedures={"kernel_function": "CubicBSpline3D", "integration_scheme": "EulerCromer",
+                    "pressure_solver": "IISPH", "neighbor_search": "SpatialHashing",
+                    "boundary_handling": "VolumeMapBoundary"},
+        parameters={"rest_density_grid_spacing": h, "kernel_support_radius": 2 * h,
+                    "disable_particles_below": -50.0, "fluid_viscosity": 0.01,
+                    "boundary_viscosity": 0.01, "boundary_pressure_acceleration_weighting": 0.7,
+                    "boundary_rest_volume_weighting": 1.0, "target_density_error": 0.1,
+                    "relaxation_factor": 0.5, "min_diagonal_element": 1e-10,
+                    "max_time_increment": 2e-3, "cfl_number": 0.4},
+        cfl_time_step=True, position=pos, mass=np.full(pos.shape[0], 1000.0 * h ** 3),
+        mesh=(verts, CUBE_FACES_INWARD),
+        description=f"IISPH dam break {pos.shape[0]} particles in a {box} box volume map")
+
+
+def build_system(scene: Scene, precision="f32", device=0, fields=None, extra_parameters=None):
+    """Create, fill and initialize a GpuSystem for `scene`. `fields` supplies the
+    (sdf, vm) volume-map fields of the container when the scene uses one."""
+    from .system import GpuSystem, make_config
+    params = dict(scene.parameters)
+    params["device"] = device
+    if extra_parameters:
+        params.update(extra_parameters)
+    cfg = make_config(scene.procedures, params, precision=precision,
+                      cfl_time_step=scene.cfl_time_step)
+    s = GpuSystem(cfg)
+    s.upload_fluid(scene.position, scene.velocity, scene.mass, scene.fluid_id)
+    for pts, rigid in scene.sample_boundaries:
+        s.add_sample_boundary(pts, rigid)
+    for sdf, vm, rigid in scene.volume_maps:
+        s.add_volume_map_boundary(sdf, vm, rigid)
+    if fields is not None:
+        s.add_volume_map_boundary(fields[0], fields[1])
+    s.initialize()
+    return s

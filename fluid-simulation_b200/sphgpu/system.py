@@ -1,0 +1,359 @@
+"""GPU-backed `SPHSystem` (reference: simulation_lib/src/sph/mod.rs:40-69).
+
+`GpuSystem` mirrors the reference's object-safe system trait — `time`,
+`time_steps_propagated`, `step_forward_in_time`, `take_measurement`,
+`get_fluid_ids`, `get_fluid_pos`, `get_fluid_checkpoint`,
+`get_quantity_of_fluid_samples`, `continue_from_checkpoint`, clone — over the
+C ABI. Composition follows the reference's `Procedures` (sph/setup/input.rs:
+101-134) and `Parameters` names; all state stays on the device between calls.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _capi as A
+
+PROCEDURES = {
+    "kernel_function": {"CubicBSpline3D": A.CUBIC_BSPLINE_3D},
+    "integration_scheme": {"EulerCromer": A.EULER_CROMER, "TakePredicted": A.TAKE_PREDICTED},
+    "pressure_solver": {"SESPH": A.SESPH, "SESPHwSplitting": A.SESPH_W_SPLITTING, "IISPH": A.IISPH,
+                        "IISPHwOST": A.IISPH_W_OST},
+    "neighbor_search": {"SpatialHashing": A.SPATIAL_HASHING},
+    "boundary_handling": {"StaticSampleBoundary": A.STATIC_SAMPLE_BOUNDARY,
+                          "VolumeMapBoundary": A.VOLUME_MAP_BOUNDARY},
+}
+
+PARAMETER_KEYS = (
+    "rest_density_grid_spacing", "kernel_support_radius", "disable_particles_below",
+    "fluid_viscosity", "boundary_viscosity", "boundary_pressure_acceleration_weighting",
+    "boundary_rest_volume_weighting", "stiffness", "target_density_error", "relaxation_factor",
+    "min_diagonal_element", "time_increment", "max_time_increment", "cfl_number",
+    "max_solver_iterations", "neighbor_capacity", "device",
+)
+
+
+def make_config(procedures: dict | None = None, parameters: dict | None = None,
+                precision: str = "f32", cfl_time_step: bool = False,
+                gravity: dict | None = None) -> A.SphConfig:
+    """Build an `sph_config` from reference-style procedure names and parameters."""
+    L = A.load()
+    c = A.SphConfig()
+    L.sph_config_default(C.byref(c))
+    procedures = procedures or {}
+    field_of = {"kernel_function": "kernel_fn", "integration_scheme": "integration_scheme",
+                "pressure_solver": "pressure_solver", "neighbor_search": "neighbor_search",
+                "boundary_handling": "boundary_handling"}
+    for key, value in procedures.items():
+        if key not in PROCEDURES:
+            raise ValueError(f"unknown procedure {key!r}")
+        if value not in PROCEDURES[key]:
+            raise ValueError(f"unknown {key} variant {value!r}")
+        setattr(c, field_of[key], PROCEDURES[key][value])
+    for key, value in (parameters or {}).items():
+        if key not in PARAMETER_KEYS:
+            raise ValueError(f"unknown parameter {key!r}")
+        setattr(c, key, value)
+    c.precision = {"f32": A.F32, "f64": A.F64}[precision]
+    c.cfl_time_step = 1 if cfl_time_step else 0
+    if gravity:
+        if gravity.get("type", "Uniform") == "Radial":
+            c.gravity_mode = A.GRAVITY_RADIAL
+            c.gravity_center[:] = gravity["center"]
+        else:
+            c.gravity_mode = A.GRAVITY_UNIFORM
+    return c
+
+
+@dataclass
+class RigidInit:
+    """Initial state of a dynamic boundary (RigidBodyMotion::new)."""
+    mass: float
+    inertia_body: np.ndarray
+    center_of_mass: tuple
+    orientation: tuple = (1.0, 0.0, 0.0, 0.0)  # w, i, j, k
+    linear_velocity: tuple = (0.0, 0.0, 0.0)
+    angular_velocity: tuple = (0.0, 0.0, 0.0)
+
+    def to_c(self) -> A.SphRigidInit:
+        r = A.SphRigidInit()
+        I = np.asarray(self.inertia_body, np.float64).reshape(3, 3)
+        r.mass = float(self.mass)
+        r.inertia_body[:] = I.ravel().tolist()
+        r.inertia_inv_body[:] = np.linalg.inv(I).ravel().tolist()
+        r.center_of_mass[:] = list(self.center_of_mass)
+        r.orientation[:] = list(self.orientation)
+        r.linear_velocity[:] = list(self.linear_velocity)
+        r.angular_velocity[:] = list(self.angular_velocity)
+        return r
+
+    def to_array32(self) -> np.ndarray:
+        """The 32-double layout the oracle's rigid-body entry points take."""
+        I = np.asarray(self.inertia_body, np.float64).reshape(3, 3)
+        return np.concatenate([[self.mass], I.ravel(), np.linalg.inv(I).ravel(),
+                               self.center_of_mass, self.orientation, self.linear_velocity,
+                               self.angular_velocity]).astype(np.float64)
+
+
+def grid_desc(x_min, x_max, dx, n) -> A.SphGridDesc:
+    g = A.SphGridDesc()
+    g.x_min[:] = [float(v) for v in x_min]
+    g.x_max[:] = [float(v) for v in x_max]
+    g.dx = float(dx)
+    g.n[:] = [int(v) for v in n]
+    return g
+
+
+class GpuSystem:
+    """A `System<K,I,P,N,B>` whose state lives on one GPU."""
+
+    def __init__(self, config: A.SphConfig):
+        self._L = A.load()
+        self._cfg = config
+        h = C.c_void_p()
+        A.check(self._L.sph_create(C.byref(config), C.byref(h)))
+        self._h = h
+        self._boundaries = []
+
+    # ---- lifetime --------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.sph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def clone(self) -> "GpuSystem":
+        o = GpuSystem.__new__(GpuSystem)
+        o._L, o._cfg, o._boundaries = self._L, self._cfg, list(self._boundaries)
+        h = C.c_void_p()
+        A.check(self._L.sph_clone(self._h, C.byref(h)))
+        o._h = h
+        return o
+
+    # ---- setup -----------------------------------------------------------------
+    def upload_fluid(self, position, velocity=None, mass=None, fluid_id=None):
+        pos = np.ascontiguousarray(position, np.float64).reshape(-1, 3)
+        n = pos.shape[0]
+        vel = np.ascontiguousarray(np.zeros((n, 3)) if velocity is None else velocity,
+                                   np.float64).reshape(-1, 3)
+        m = np.ascontiguousarray(np.broadcast_to(mass, (n,)), np.float64)
+        fid = np.ascontiguousarray(np.zeros(n) if fluid_id is None else fluid_id, np.uint32)
+        A.check(self._L.sph_upload_fluid(self._h, n, pos.ravel(), vel.ravel(), m, fid))
+
+    def add_sample_boundary(self, positions, rigid: RigidInit | None = None) -> int:
+        p = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+        bi = C.c_int()
+        r = C.byref(rigid.to_c()) if rigid is not None else None
+        A.check(self._L.sph_add_sample_boundary(self._h, p.shape[0], p.ravel(), r, C.byref(bi)))
+        self._boundaries.append(("samples", p.shape[0]))
+        return bi.value
+
+    def add_volume_map_boundary(self, sdf, vm, rigid: RigidInit | None = None) -> int:
+        """sdf / vm: objects with x_min, x_max, dx, n, nodes (dense lattice, NaN absent)."""
+        bi = C.c_int()
+        r = C.byref(rigid.to_c()) if rigid is not None else None
+        sd = grid_desc(sdf.x_min, sdf.x_max, sdf.dx, sdf.n)
+        vd = grid_desc(vm.x_min, vm.x_max, vm.dx, vm.n)
+        A.check(self._L.sph_add_volume_map_boundary(
+            self._h, C.byref(sd), np.ascontiguousarray(sdf.nodes, np.float64).ravel(), C.byref(vd),
+            np.ascontiguousarray(vm.nodes, np.float64).ravel(), r, C.byref(bi)))
+        self._boundaries.append(("volume_map", 0))
+        return bi.value
+
+    def initialize(self):
+        A.check(self._L.sph_initialize(self._h))
+
+    # ---- SPHSystem -------------------------------------------------------------
+    def time(self) -> float:
+        t = C.c_double()
+        A.check(self._L.sph_time(self._h, C.byref(t)))
+        return t.value
+
+    def time_steps_propagated(self) -> int:
+        s = C.c_uint64()
+        A.check(self._L.sph_time_steps_propagated(self._h, C.byref(s)))
+        return s.value
+
+    def step_forward_in_time(self, n_steps: int = 1) -> int:
+        """Advance n_steps; returns SPH_OK or SPH_NOT_CONVERGED (capped IISPH)."""
+        return A.check(self._L.sph_step(self._h, int(n_steps)), allow=(A.SPH_NOT_CONVERGED,))
+
+    def take_measurement(self) -> dict:
+        m = A.SphMeasurement()
+        A.check(self._L.sph_take_measurement(self._h, C.byref(m)))
+        return {name: getattr(m, name) for name, _ in A.SphMeasurement._fields_}
+
+    @property
+    def n(self) -> int:
+        s = C.c_size_t()
+        A.check(self._L.sph_num_particles(self._h, C.byref(s)))
+        return s.value
+
+    def get_fluid_ids(self) -> np.ndarray:
+        out = np.zeros(self.n, np.uint32)
+        A.check(self._L.sph_get_fluid_ids(self._h, out))
+        return out
+
+    def get_fluid_pos(self) -> np.ndarray:
+        out = np.zeros(3 * self.n, np.float32)
+        A.check(self._L.sph_get_fluid_pos(self._h, out))
+        return out.reshape(-1, 3)
+
+    def get_quantity_of_fluid_samples(self, quantity: int) -> np.ndarray:
+        out = np.zeros(self.n, np.float32)
+        A.check(self._L.sph_get_quantity_of_fluid_samples(self._h, int(quantity), out))
+        return out
+
+    def download(self, field: int) -> np.ndarray:
+        n = self.n
+        shape = (n, 3) if field in A.VECTOR_FIELDS else (n,)
+        out = np.zeros(int(np.prod(shape)), np.float64)
+        A.check(self._L.sph_download(self._h, int(field), out))
+        return out.reshape(shape)
+
+    def get_fluid_checkpoint(self) -> dict:
+        """FluidCheckpoint (fluid.rs:352-447): ids, positions, velocities, masses."""
+        ck = {"fluid_id": self.get_fluid_ids(), "position": self.download(A.FIELD_POSITION),
+              "velocity": self.download(A.FIELD_VELOCITY), "mass": self.download(A.FIELD_MASS),
+              "time_steps_propagated": self.time_steps_propagated(), "current_time": self.time()}
+        if self._cfg.integration_scheme == A.TAKE_PREDICTED:
+            ck["integrator_position"] = self.download(A.FIELD_INTEGRATOR_POSITION)
+            ck["integrator_velocity"] = self.download(A.FIELD_INTEGRATOR_VELOCITY)
+        return ck
+
+    def continue_from_checkpoint(self, ck: dict):
+        pos = np.ascontiguousarray(ck["position"], np.float64).reshape(-1, 3)
+        n = pos.shape[0]
+        vel = np.ascontiguousarray(ck["velocity"], np.float64).reshape(-1, 3)
+        m = np.ascontiguousarray(ck["mass"], np.float64)
+        fid = np.ascontiguousarray(ck["fluid_id"], np.uint32)
+        xi = ck.get("integrator_position")
+        vi = ck.get("integrator_velocity")
+        xi = None if xi is None else np.ascontiguousarray(xi, np.float64).ravel()
+        vi = None if vi is None else np.ascontiguousarray(vi, np.float64).ravel()
+        A.check(self._L.sph_continue_from_checkpoint(
+            self._h, int(ck["time_steps_propagated"]), float(ck["current_time"]), n, pos.ravel(),
+            vel.ravel(), m, fid, None if xi is None else xi.ctypes.data_as(C.c_void_p),
+            None if vi is None else vi.ctypes.data_as(C.c_void_p)))
+
+    # ---- parity helpers ----------------------------------------------------------
+    def fluid_neighbors(self):
+        """(offsets[n+1], indices) in reference index space, rows sorted, self included."""
+        total = C.c_size_t()
+        rc = self._L.sph_get_fluid_neighbors(self._h, None, None, 0, C.byref(total))
+        A.check(rc, allow=(A.SPH_ERR_CAPACITY,))
+        off = np.zeros(self.n + 1, np.uint64)
+        idx = np.zeros(max(total.value, 1), np.uint32)
+        A.check(self._L.sph_get_fluid_neighbors(self._h, off.ctypes.data_as(C.c_void_p),
+                                                idx.ctypes.data_as(C.c_void_p), idx.size,
+                                                C.byref(total)))
+        return off, idx[:total.value]
+
+    def boundary_neighbors(self, bi: int):
+        total = C.c_size_t()
+        rc = self._L.sph_get_boundary_neighbors(self._h, bi, None, None, 0, C.byref(total))
+        A.check(rc, allow=(A.SPH_ERR_CAPACITY,))
+        off = np.zeros(self.n + 1, np.uint64)
+        idx = np.zeros(max(total.value, 1), np.uint32)
+        A.check(self._L.sph_get_boundary_neighbors(self._h, bi, off.ctypes.data_as(C.c_void_p),
+                                                   idx.ctypes.data_as(C.c_void_p), idx.size,
+                                                   C.byref(total)))
+        return off, idx[:total.value]
+
+    def boundary_volumes(self, bi: int, nb: int) -> np.ndarray:
+        out = np.zeros(nb)
+        A.check(self._L.sph_get_boundary_volumes(self._h, bi, out))
+        return out
+
+    def volume_map_samples(self, bi: int):
+        n = self.n
+        has = np.zeros(n, np.uint8)
+        xb, vb, vol = np.zeros(3 * n), np.zeros(3 * n), np.zeros(n)
+        A.check(self._L.sph_get_volume_map_samples(self._h, bi, has, xb, vb, vol))
+        return has.astype(bool), xb.reshape(n, 3), vb.reshape(n, 3), vol
+
+    def rigid_state(self, bi: int) -> np.ndarray:
+        out = np.zeros(19)
+        A.check(self._L.sph_get_rigid_state(self._h, bi, out))
+        return out
+
+    def set_rigid_state(self, bi: int, state19):
+        A.check(self._L.sph_set_rigid_state(self._h, bi, np.ascontiguousarray(state19, np.float64)))
+
+    def hash_collisions(self) -> int:
+        out = C.c_uint64()
+        A.check(self._L.sph_hash_collisions(self._h, C.byref(out)))
+        return out.value
+
+    # ---- instrumentation -----------------------------------------------------------
+    def launch_count(self) -> int:
+        out = C.c_uint64()
+        A.check(self._L.sph_launch_count(self._h, C.byref(out)))
+        return out.value
+
+    def set_profiling(self, enabled: bool):
+        A.check(self._L.sph_set_profiling(self._h, 1 if enabled else 0))
+
+    def kernel_time(self, name: str):
+        ms, cnt = C.c_double(), C.c_uint64()
+        rc = self._L.sph_kernel_time(self._h, name.encode(), C.byref(ms), C.byref(cnt))
+        if rc:
+            return None
+        return ms.value, cnt.value
+
+    def device_bytes(self) -> int:
+        out = C.c_size_t()
+        A.check(self._L.sph_device_bytes(self._h, C.byref(out)))
+        return out.value
+
+
+# ---- per-trait shims ------------------------------------------------------------------
+def find_samples(search_range, positions, samples, device=0):
+    """NeighborSearch::find_samples (SpatialHashing) on the GPU -> (offsets, indices)."""
+    L = A.load()
+    pos = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+    smp = np.ascontiguousarray(samples, np.float64).reshape(-1, 3)
+    total = C.c_size_t()
+    rc = L.sph_spatial_hashing_find_samples(float(search_range), pos.shape[0], pos.ravel(),
+                                            smp.shape[0], smp.ravel(), None, None, 0,
+                                            C.byref(total), device)
+    A.check(rc, allow=(A.SPH_ERR_CAPACITY,))
+    off = np.zeros(pos.shape[0] + 1, np.uint64)
+    idx = np.zeros(max(total.value, 1), np.uint32)
+    A.check(L.sph_spatial_hashing_find_samples(float(search_range), pos.shape[0], pos.ravel(),
+                                               smp.shape[0], smp.ravel(),
+                                               off.ctypes.data_as(C.c_void_p),
+                                               idx.ctypes.data_as(C.c_void_p), idx.size,
+                                               C.byref(total), device))
+    return off, idx[:total.value]
+
+
+def kernel_function(r, h, precision="f32", device=0):
+    L = A.load()
+    rr = np.ascontiguousarray(r, np.float64).reshape(-1, 3)
+    out = np.zeros(rr.shape[0])
+    A.check(L.sph_kernel_function(rr.shape[0], rr.ravel(), float(h), out,
+                                  A.F64 if precision == "f64" else A.F32, device))
+    return out
+
+
+def kernel_gradient(r, h, precision="f32", device=0):
+    L = A.load()
+    rr = np.ascontiguousarray(r, np.float64).reshape(-1, 3)
+    out = np.zeros(3 * rr.shape[0])
+    A.check(L.sph_kernel_gradient(rr.shape[0], rr.ravel(), float(h), out,
+                                  A.F64 if precision == "f64" else A.F32, device))
+    return out.reshape(-1, 3)

@@ -1,0 +1,270 @@
+/*
+ * sphgpu.h — C ABI of the B200 SPH step engine.
+ *
+ * This is the boundary a host written in any language binds (the reference's
+ * Rust workspace through an `extern "C"` FFI crate; Python through ctypes).
+ * Plain pointers and sizes only. Every entry point returns an `int` status
+ * (`SPH_OK` or an `SPH_ERR_*` / `SPH_NOT_CONVERGED` code) and never unwinds
+ * across the boundary; `sph_last_error()` returns the calling thread's
+ * message for the last failure.
+ *
+ * Reference interfaces (SammyMcFly/fluid-simulation, paths under
+ * simulation_lib/src/) that each entry point replaces are cited beside it.
+ * The production seam is the object-safe `SPHSystem` trait
+ * (sph/mod.rs:40-69): a handle owns all particle state on the GPU and copies
+ * it back only when asked (recording / render frames / checkpoints).
+ *
+ * Threading: a handle is driven by one host thread at a time; each handle
+ * owns its CUDA stream.
+ */
+#ifndef SPHGPU_H
+#define SPHGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum sph_status {
+  SPH_OK = 0,
+  SPH_ERR_INVALID = 1,      /* bad argument or unsupported combination */
+  SPH_ERR_OOM = 2,          /* device allocation failed */
+  SPH_ERR_CUDA = 3,         /* CUDA runtime error (no device, launch failure) */
+  SPH_NOT_CONVERGED = 4,    /* IISPH hit `max_solver_iterations` (step still completed) */
+  SPH_ERR_STATE = 5,        /* call out of order (e.g. step before initialize) */
+  SPH_ERR_CAPACITY = 6,     /* a caller buffer is too small; required size returned */
+};
+
+/* ---- procedure variants (sph/setup/input.rs:101-134 `Procedures`) ------ */
+enum sph_kernel_fn { SPH_CUBIC_BSPLINE_3D = 0 };                 /* kernel/mod.rs:9-12 */
+enum sph_integration_scheme {                                      /* integration_schemes/mod.rs:15-21 */
+  SPH_EULER_CROMER = 0,
+  SPH_TAKE_PREDICTED = 1,
+};
+enum sph_pressure_solver {                                         /* pressure_solver/mod.rs:29-35 */
+  SPH_SESPH = 0,
+  SPH_SESPH_W_SPLITTING = 1,
+  SPH_IISPH = 2,
+  SPH_IISPH_W_OST = 3,
+};
+enum sph_neighbor_search { SPH_SPATIAL_HASHING = 0 };             /* neighbor_search/mod.rs:13-16 */
+enum sph_boundary_handling {                                       /* boundary_handling/mod.rs:33-37 */
+  SPH_STATIC_SAMPLE_BOUNDARY = 0,
+  SPH_VOLUME_MAP_BOUNDARY = 1,
+};
+enum sph_precision { SPH_F32 = 0, SPH_F64 = 1 };
+enum sph_gravity_mode { SPH_GRAVITY_UNIFORM = 0, SPH_GRAVITY_RADIAL = 1 };
+
+/* ---- configuration: `Parameters` (sph/setup/input.rs:56-260) + procedures */
+typedef struct sph_config {
+  int kernel_fn;                /* enum sph_kernel_fn */
+  int integration_scheme;       /* enum sph_integration_scheme */
+  int pressure_solver;          /* enum sph_pressure_solver */
+  int neighbor_search;          /* enum sph_neighbor_search */
+  int boundary_handling;        /* enum sph_boundary_handling */
+  int precision;                /* enum sph_precision: state and bulk arithmetic */
+  int cfl_time_step;            /* 0: fixed time_increment; 1: CFL (feature `cfl_time_step`) */
+  int gravity_mode;             /* enum sph_gravity_mode */
+  double rest_density_grid_spacing;
+  double kernel_support_radius;
+  double disable_particles_below;
+  double fluid_viscosity;
+  double boundary_viscosity;
+  double boundary_pressure_acceleration_weighting;  /* gamma_p */
+  double boundary_rest_volume_weighting;            /* gamma_V */
+  double stiffness;                                 /* SESPH k */
+  double target_density_error;                      /* IISPH, in percent */
+  double relaxation_factor;                         /* IISPH omega */
+  double min_diagonal_element;                      /* IISPH epsilon */
+  double time_increment;                            /* fixed dt */
+  double max_time_increment;                        /* CFL dt cap */
+  double cfl_number;
+  double gravity_center[3];                         /* radial gravity */
+  uint32_t max_solver_iterations; /* 0 = unbounded like the reference; else a cap
+                                     that ends the solve with SPH_NOT_CONVERGED */
+  uint32_t neighbor_capacity;     /* fluid neighbors stored per particle; 0 = 64 */
+  int device;                     /* CUDA device ordinal */
+} sph_config;
+
+/* Fills `cfg` with the reference's defaults for the numeric fields
+ * (params.toml semantics) and CubicBSpline3D / EulerCromer / IISPH /
+ * SpatialHashing / VolumeMapBoundary, f32. */
+void sph_config_default(sph_config* cfg);
+
+/* Rigid-body initial state for a dynamic boundary
+ * (rigid_body_motion.rs:39-65 `RigidBodyMotion::new`). */
+typedef struct sph_rigid_init {
+  double mass;
+  double inertia_body[9];       /* row-major, body frame */
+  double inertia_inv_body[9];   /* row-major, body frame */
+  double center_of_mass[3];     /* world */
+  double orientation[4];        /* quaternion w, i, j, k */
+  double linear_velocity[3];
+  double angular_velocity[3];
+} sph_rigid_init;
+
+/* Dense cubic-serendipity node lattice of a volume-map field
+ * (utilities/discretization.rs:81-94): n cells per axis, 3n+1 nodes per
+ * axis, node (kx,ky,kz) at nodes[(kz*(3n_y+1)+ky)*(3n_x+1)+kx] and position
+ * x_min + k*dx/3. NaN marks an absent (pruned) node. */
+typedef struct sph_grid_desc {
+  double x_min[3];
+  double x_max[3];
+  double dx;
+  int64_t n[3];
+} sph_grid_desc;
+
+/* Measurement row (measurement.rs:59-78). */
+typedef struct sph_measurement {
+  double time;
+  double density;
+  double density_error;
+  double kinetic_energy;
+  double stiffness;
+  double fluid_viscosity;
+  double boundary_viscosity;
+  double fluid_depth;
+  double rest_density_grid_spacing;
+  double kernel_support_radius;
+  double time_step_size;
+  double target_density_error;
+  uint32_t solver_iterations;
+  double relaxation_factor;
+  double time_step_wall_clock_time;
+  double predicted_density_error;
+} sph_measurement;
+
+/* Per-particle fields for sph_download (reference index order). */
+enum sph_field {
+  SPH_FIELD_POSITION = 0,        /* 3 doubles per particle */
+  SPH_FIELD_VELOCITY = 1,        /* 3 */
+  SPH_FIELD_ACCELERATION = 2,    /* 3 */
+  SPH_FIELD_MASS = 3,            /* 1 */
+  SPH_FIELD_VOLUME = 4,          /* 1 */
+  SPH_FIELD_PRESSURE = 5,        /* 1 */
+  SPH_FIELD_FLUID_ID = 6,        /* 1 (as double) */
+  SPH_FIELD_SOURCE_TERM = 8,     /* 1, IISPH s_f (iisph.rs:31) */
+  SPH_FIELD_DIAGONAL = 9,        /* 1, IISPH a_ff (iisph.rs:32) */
+  SPH_FIELD_PREDICTED_VELOCITY = 10, /* 3, solver velocity slot 0 */
+  SPH_FIELD_INTEGRATOR_POSITION = 11,/* 3, integrator position slot 0 */
+  SPH_FIELD_INTEGRATOR_VELOCITY = 12,/* 3, integrator velocity slot 0 */
+};
+
+/* Scalar quantities of render_info.rs `ScalarQuantity` (sph/mod.rs:202-239). */
+enum sph_quantity {
+  SPH_Q_SPEED = 0, SPH_Q_VOLUME = 1, SPH_Q_DENSITY = 2, SPH_Q_DENSITY_ERROR = 3,
+  SPH_Q_PRESSURE = 4, SPH_Q_KINETIC_ENERGY = 5,
+};
+
+typedef struct sph_system sph_system_t;
+
+/* ---- lifetime (SPHSystem, sph/mod.rs:40-71; System::new_boxed :389-421) -- */
+/* Creates an empty system on cfg->device. Rejects the pairings the reference
+ * rejects in SystemConstructor::new (sph/setup/mod.rs:229-244). */
+int sph_create(const sph_config* cfg, sph_system_t** out);
+void sph_destroy(sph_system_t* h);
+/* Deep copy of all device state (SPHSystem: DynClone, BE/lib.rs:111). */
+int sph_clone(const sph_system_t* h, sph_system_t** out);
+
+/* Fluid samples (Fluid::add_samples fluid.rs:79-104 / the `--state` restore
+ * path sph/setup/mod.rs:142-153): positions/velocities 3*n doubles, masses n
+ * doubles, fluid ids n (may be NULL = 0). */
+int sph_upload_fluid(sph_system_t* h, size_t n, const double* position, const double* velocity,
+                     const double* mass, const uint32_t* fluid_id);
+
+/* StaticSampleBoundary::add_static_boundary / add_dynamic_boundary
+ * (static_sample_boundary.rs:48-140): surface samples (3*nb doubles), world
+ * frame for static boundaries (rigid == NULL), body frame (centered on the
+ * center of mass) for dynamic ones. Writes the boundary index. */
+int sph_add_sample_boundary(sph_system_t* h, size_t nb, const double* positions,
+                            const sph_rigid_init* rigid, int* boundary_index);
+
+/* VolumeMapBoundary::add_static_boundary / add_dynamic_boundary
+ * (volume_map_boundary.rs:1113-1249) with prebuilt fields. */
+int sph_add_volume_map_boundary(sph_system_t* h, const sph_grid_desc* sdf, const double* sdf_nodes,
+                                const sph_grid_desc* vm, const double* vm_nodes,
+                                const sph_rigid_init* rigid, int* boundary_index);
+
+/* BoundaryHandling::initialize (boundary_handling/mod.rs:62-67) followed by
+ * the first update() of System::new_boxed (sph/mod.rs:418-419). */
+int sph_initialize(sph_system_t* h);
+
+/* ---- stepping (sph/mod.rs:125-144, 674-731) ----------------------------- */
+/* Advances n_steps time steps. Returns SPH_NOT_CONVERGED (after finishing
+ * all steps) if an IISPH solve hit the configured iteration cap. */
+int sph_step(sph_system_t* h, uint32_t n_steps);
+int sph_time(const sph_system_t* h, double* out);                         /* :107-116 */
+int sph_time_steps_propagated(const sph_system_t* h, uint64_t* out);     /* :118-120 */
+int sph_take_measurement(sph_system_t* h, sph_measurement* out);          /* :147-184 */
+int sph_num_particles(const sph_system_t* h, size_t* out);
+
+/* ---- readback ----------------------------------------------------------- */
+int sph_get_fluid_ids(sph_system_t* h, uint32_t* out);                    /* :186-188 */
+int sph_get_fluid_pos(sph_system_t* h, float* out);                       /* :190-196 */
+int sph_get_quantity_of_fluid_samples(sph_system_t* h, int quantity, float* out); /* :202-239 */
+int sph_download(sph_system_t* h, int field, double* out);
+/* Fluid neighbor lists in reference index space, self included, each row
+ * sorted ascending (NeighborList, neighbor_search/mod.rs:49-161).
+ * offsets: n+1 entries. If `capacity` < total, returns SPH_ERR_CAPACITY and
+ * writes the required total. */
+int sph_get_fluid_neighbors(sph_system_t* h, uint64_t* offsets, uint32_t* indices,
+                            size_t capacity, size_t* total);
+/* Sample-boundary neighbors of boundary `bi` (indices into its samples). */
+int sph_get_boundary_neighbors(sph_system_t* h, int bi, uint64_t* offsets, uint32_t* indices,
+                               size_t capacity, size_t* total);
+/* Pseudo volumes of the samples of sample boundary `bi` (upload order). */
+int sph_get_boundary_volumes(sph_system_t* h, int bi, double* out);
+/* Volume-map samples of boundary `bi` per particle: has[n] (0/1),
+ * x_b[3n], v_b[3n], vol[n] (volume_map_boundary.rs:1287-1342). */
+int sph_get_volume_map_samples(sph_system_t* h, int bi, uint8_t* has, double* xb, double* vb,
+                               double* vol);
+/* Rigid-body state of boundary `bi`: com[3], q[4] (w,i,j,k), v[3], L[3],
+ * F[3], T[3] (RigidBodyMotionCheckpoint, rigid_body_motion.rs:230-245). */
+int sph_get_rigid_state(sph_system_t* h, int bi, double* out19);
+int sph_set_rigid_state(sph_system_t* h, int bi, const double* in19);
+/* Number of XOR-prime hash collisions between cells of one 3x3x3 stencil
+ * among occupied cells at the last update (spatial_hashing.rs:49-71). */
+int sph_hash_collisions(sph_system_t* h, uint64_t* out);
+
+/* ---- checkpoints (sph/mod.rs:833-915, continue_from_checkpoint :362-378) - */
+/* Restores fluid state (reference order) and the step counter / time, zeroes
+ * solver slots, then runs update(). */
+int sph_continue_from_checkpoint(sph_system_t* h, uint64_t time_steps_propagated,
+                                 double current_time, size_t n, const double* position,
+                                 const double* velocity, const double* mass,
+                                 const uint32_t* fluid_id, const double* integrator_position,
+                                 const double* integrator_velocity);
+
+/* ---- per-trait shims (upload -> kernel -> download), for per-trait parity - */
+/* NeighborSearch::find_samples with SpatialHashing (neighbor_search/mod.rs:18-28,
+ * spatial_hashing.rs:130-158): neighbors of each of the n positions among the
+ * ns samples (cell size = search range), rows in stencil order x->y->z then
+ * ascending sample index. */
+int sph_spatial_hashing_find_samples(double search_range, size_t n, const double* positions,
+                                     size_t ns, const double* samples, uint64_t* offsets,
+                                     uint32_t* indices, size_t capacity, size_t* total, int device);
+/* KernelFn (kernel/mod.rs:17-46) for CubicBSpline3D on n vectors (3n doubles). */
+int sph_kernel_function(size_t n, const double* r, double h, double* out_w, int precision,
+                        int device);
+int sph_kernel_gradient(size_t n, const double* r, double h, double* out_grad, int precision,
+                        int device);
+
+/* ---- diagnostics -------------------------------------------------------- */
+const char* sph_last_error(void);
+/* Kernel launches issued by this handle since creation (all of its CUDA
+ * kernels, every step). */
+int sph_launch_count(const sph_system_t* h, uint64_t* out);
+/* Event-timed duration (ms) of the named kernel class over the last
+ * sph_step call when profiling is enabled with sph_set_profiling. */
+int sph_set_profiling(sph_system_t* h, int enabled);
+int sph_kernel_time(sph_system_t* h, const char* kernel, double* ms, uint64_t* launches);
+/* Device-resident bytes held by the handle. */
+int sph_device_bytes(const sph_system_t* h, size_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPHGPU_H */

@@ -1,0 +1,392 @@
+"""ctypes binding of the SPH oracle (test infrastructure only).
+
+The oracle is a CPU f64 restatement of the reference's SPH step path
+(SammyMcFly/fluid-simulation, ``simulation_lib``). Only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline legs import this
+module; the engine never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+F_POSITION, F_VELOCITY, F_ACCELERATION, F_MASS, F_VOLUME, F_PRESSURE = 0, 1, 2, 3, 4, 5
+F_FLUID_ID, F_ORIGIN, F_SOURCE, F_DIAGONAL, F_SOLVER_VEL = 6, 7, 8, 9, 10
+F_INTEGRATOR_POS, F_INTEGRATOR_VEL = 11, 12
+_VEC_FIELDS = {F_POSITION, F_VELOCITY, F_ACCELERATION, F_SOLVER_VEL, F_INTEGRATOR_POS,
+               F_INTEGRATOR_VEL}
+
+MEASUREMENT_FIELDS = (
+    "time", "density", "density_error", "kinetic_energy", "stiffness", "fluid_viscosity",
+    "boundary_viscosity", "fluid_depth", "rest_density_grid_spacing", "kernel_support_radius",
+    "time_step_size", "target_density_error", "solver_iterations", "relaxation_factor",
+    "time_step_wall_clock_time", "predicted_density_error")
+
+
+class OracleConfig(C.Structure):
+    _fields_ = [
+        ("integration_scheme", C.c_int), ("pressure_solver", C.c_int),
+        ("boundary_handling", C.c_int), ("cfl_time_step", C.c_int),
+        ("rest_density_grid_spacing", C.c_double), ("kernel_support_radius", C.c_double),
+        ("disable_particles_below", C.c_double), ("fluid_viscosity", C.c_double),
+        ("boundary_viscosity", C.c_double),
+        ("boundary_pressure_acceleration_weighting", C.c_double),
+        ("boundary_rest_volume_weighting", C.c_double), ("stiffness", C.c_double),
+        ("target_density_error", C.c_double), ("relaxation_factor", C.c_double),
+        ("min_diagonal_element", C.c_double), ("time_increment", C.c_double),
+        ("max_time_increment", C.c_double), ("cfl_number", C.c_double),
+        ("gravity_mode", C.c_int), ("gravity_center", C.c_double * 3),
+        ("max_solver_iterations", C.c_uint),
+    ]
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        build()
+    L = C.CDLL(_LIB_PATH)
+    vp, d, sz, i = C.c_void_p, C.c_double, C.c_size_t, C.c_int
+    dp = np.ctypeslib.ndpointer(np.float64, flags="C")
+    u64p = np.ctypeslib.ndpointer(np.uint64, flags="C")
+    u32p = np.ctypeslib.ndpointer(np.uint32, flags="C")
+    i64p = np.ctypeslib.ndpointer(np.int64, flags="C")
+    u8p = np.ctypeslib.ndpointer(np.uint8, flags="C")
+    sig = {
+        "oracle_system_create": (vp, [C.POINTER(OracleConfig)]),
+        "oracle_destroy": (None, [vp]),
+        "oracle_clone": (vp, [vp]),
+        "oracle_upload_fluid": (i, [vp, sz, dp, dp, dp, u32p]),
+        "oracle_add_sample_boundary": (i, [vp, sz, dp, vp]),
+        "oracle_add_volume_map_boundary": (i, [vp, dp, i64p, dp, dp, i64p, dp, vp]),
+        "oracle_initialize": (i, [vp]),
+        "oracle_step": (i, [vp, i]),
+        "oracle_num_particles": (sz, [vp]),
+        "oracle_measure": (None, [vp, dp]),
+        "oracle_time": (d, [vp]),
+        "oracle_steps": (C.c_ulonglong, [vp]),
+        "oracle_hash_duplicates": (sz, [vp]),
+        "oracle_download": (i, [vp, i, dp]),
+        "oracle_fluid_neighbor_total": (sz, [vp]),
+        "oracle_fluid_neighbors": (None, [vp, u64p, u64p]),
+        "oracle_boundary_neighbor_total": (sz, [vp, sz]),
+        "oracle_boundary_neighbors": (None, [vp, sz, u64p, u64p]),
+        "oracle_boundary_volumes": (i, [vp, sz, dp]),
+        "oracle_vm_samples": (i, [vp, sz, u8p, dp, dp, dp]),
+        "oracle_rigid_state": (i, [vp, sz, dp]),
+        "oracle_kernel_w": (d, [d]),
+        "oracle_kernel_dqw": (d, [d]),
+        "oracle_kernel_function": (d, [dp, d]),
+        "oracle_kernel_gradient": (None, [dp, d, dp]),
+        "oracle_map_int_to_uint": (C.c_ulonglong, [i]),
+        "oracle_hash": (C.c_ulonglong, [i, i, i]),
+        "oracle_get_cell": (None, [dp, d, np.ctypeslib.ndpointer(np.int32, flags="C")]),
+        "oracle_find_samples": (vp, [d, d, sz, dp, sz, dp]),
+        "oracle_nl_total": (sz, [vp]),
+        "oracle_nl_duplicates": (sz, [vp]),
+        "oracle_nl_copy": (None, [vp, u64p, u64p]),
+        "oracle_nl_free": (None, [vp]),
+        "oracle_gauss_legendre": (i, [i, dp, dp]),
+        "oracle_mesh_signed_distance": (d, [dp, sz, u32p, sz, dp]),
+        "oracle_build_fields": (vp, [dp, sz, u32p, sz, d, d, i]),
+        "oracle_build_sdf_only": (vp, [dp, sz, u32p, sz, d, d]),
+        "oracle_fields_free": (None, [vp]),
+        "oracle_field_desc": (None, [vp, i, dp, i64p]),
+        "oracle_field_nodes": (None, [vp, i, dp]),
+        "oracle_serendipity_function": (i, [dp, i64p, dp, dp, dp]),
+        "oracle_serendipity_gradient": (i, [dp, i64p, dp, dp, dp]),
+        "oracle_volume_at": (i, [dp, i64p, dp, dp, d, i, dp]),
+        "oracle_rigid_body_step": (i, [dp, dp, dp, i, d, i, dp]),
+        "oracle_iisph_probe": (i, [dp, dp, d, d, d, d, d, d, d, d, vp, d, i, dp]),
+        "oracle_num_threads": (i, []),
+        "oracle_set_num_threads": (None, [i]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# ---- free functions -------------------------------------------------------------
+def kernel_w(q):
+    return lib().oracle_kernel_w(float(q))
+
+
+def kernel_dqw(q):
+    return lib().oracle_kernel_dqw(float(q))
+
+
+def kernel_function(r, h):
+    return lib().oracle_kernel_function(_f64(r), float(h))
+
+
+def kernel_gradient(r, h):
+    out = np.zeros(3)
+    lib().oracle_kernel_gradient(_f64(r), float(h), out)
+    return out
+
+
+def map_int_to_uint(k):
+    return lib().oracle_map_int_to_uint(int(k))
+
+
+def cell_hash(k, l, m):
+    return lib().oracle_hash(int(k), int(l), int(m))
+
+
+def get_cell(p, cell_size):
+    out = np.zeros(3, np.int32)
+    lib().oracle_get_cell(_f64(p), float(cell_size), out)
+    return out
+
+
+def find_samples(search_range, positions, samples, cell_size=None):
+    """SpatialHashing::find_samples; returns (offsets, indices, duplicates)."""
+    L = lib()
+    pos = _f64(positions).reshape(-1, 3)
+    smp = _f64(samples).reshape(-1, 3)
+    h = L.oracle_find_samples(float(search_range), float(cell_size or search_range),
+                              pos.shape[0], pos.ravel(), smp.shape[0], smp.ravel())
+    try:
+        tot = L.oracle_nl_total(h)
+        off = np.zeros(pos.shape[0] + 1, np.uint64)
+        idx = np.zeros(max(tot, 1), np.uint64)
+        L.oracle_nl_copy(h, off, idx)
+        return off, idx[:tot], L.oracle_nl_duplicates(h)
+    finally:
+        L.oracle_nl_free(h)
+
+
+def gauss_legendre(deg):
+    x, w = np.zeros(deg), np.zeros(deg)
+    lib().oracle_gauss_legendre(deg, x, w)
+    return x, w
+
+
+def mesh_signed_distance(verts, faces, p):
+    v = _f64(verts).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+    return lib().oracle_mesh_signed_distance(v.ravel(), v.shape[0], f.ravel(), f.shape[0], _f64(p))
+
+
+class Field:
+    """A serendipity field in dense-lattice form (NaN = absent node)."""
+
+    def __init__(self, x_min, x_max, dx, n, nodes):
+        self.x_min = np.asarray(x_min, np.float64)
+        self.x_max = np.asarray(x_max, np.float64)
+        self.dx = float(dx)
+        self.n = np.asarray(n, np.int64)
+        self.nodes = np.ascontiguousarray(nodes, np.float64).ravel()
+
+    @property
+    def desc(self):
+        return np.concatenate([self.x_min, self.x_max, [self.dx]]).astype(np.float64)
+
+    def function(self, p):
+        out = np.zeros(1)
+        rc = lib().oracle_serendipity_function(self.desc, self.n, self.nodes, _f64(p), out)
+        return None if rc else float(out[0])
+
+    def gradient(self, p):
+        out = np.zeros(3)
+        rc = lib().oracle_serendipity_gradient(self.desc, self.n, self.nodes, _f64(p), out)
+        return None if rc else out
+
+
+def build_fields(verts, faces, dx, r, degree=30, sdf_only=False):
+    """DiscretizedBoundaryFields::new on the CPU -> (sdf Field, vm Field or None)."""
+    L = lib()
+    v = _f64(verts).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, np.uint32).reshape(-1, 3)
+    if sdf_only:
+        h = L.oracle_build_sdf_only(v.ravel(), v.shape[0], f.ravel(), f.shape[0], float(dx), float(r))
+    else:
+        h = L.oracle_build_fields(v.ravel(), v.shape[0], f.ravel(), f.shape[0], float(dx), float(r),
+                                  int(degree))
+    try:
+        out = []
+        for which in (0, 1):
+            if sdf_only and which == 1:
+                out.append(None)
+                continue
+            desc, n = np.zeros(7), np.zeros(3, np.int64)
+            L.oracle_field_desc(h, which, desc, n)
+            nodes = np.zeros(int(np.prod(3 * n + 1)))
+            L.oracle_field_nodes(h, which, nodes)
+            out.append(Field(desc[:3], desc[3:6], desc[6], n, nodes))
+        return out[0], out[1]
+    finally:
+        L.oracle_fields_free(h)
+
+
+def volume_at(sdf: Field, p, r, degree=30):
+    out = np.zeros(1)
+    rc = lib().oracle_volume_at(sdf.desc, sdf.n, sdf.nodes, _f64(p), float(r), int(degree), out)
+    return None if rc else float(out[0])
+
+
+def rigid_body_step(init32, forces, locations, dt, n_steps=1):
+    out = np.zeros(19)
+    fr = _f64(forces).reshape(-1, 3)
+    lc = _f64(locations).reshape(-1, 3)
+    lib().oracle_rigid_body_step(_f64(init32), fr.ravel(), lc.ravel(), fr.shape[0], float(dt),
+                                 int(n_steps), out)
+    return out
+
+
+def iisph_probe(pos, vel, mass, volume, dt, h, spacing, gamma_p, omega, eps, bpos, bvol, after):
+    """Single particle + one boundary sample IISPH solve; returns
+    (pressure, a_ff, s_f, sweeps)."""
+    out = np.zeros(4)
+    keep = None if bpos is None else _f64(bpos)
+    lib().oracle_iisph_probe(_f64(pos), _f64(vel), float(mass), float(volume), float(dt), float(h),
+                             float(spacing), float(gamma_p), float(omega), float(eps),
+                             None if keep is None else keep.ctypes.data_as(C.c_void_p),
+                             float(bvol), int(after), out)
+    return out[0], out[1], out[2], int(out[3])
+
+
+def set_num_threads(n):
+    lib().oracle_set_num_threads(int(n))
+
+
+def num_threads():
+    return lib().oracle_num_threads()
+
+
+# ---- system ---------------------------------------------------------------------
+def make_config(cfg: dict) -> OracleConfig:
+    c = OracleConfig()
+    for name, _ in OracleConfig._fields_:
+        if name == "gravity_center":
+            c.gravity_center[:] = cfg.get("gravity_center", (0.0, 0.0, 0.0))
+        elif name in cfg:
+            setattr(c, name, cfg[name])
+    return c
+
+
+class OracleSystem:
+    """An f64 CPU `System<K,I,P,N,B>` restatement driven through its C API."""
+
+    def __init__(self, cfg: dict):
+        self._cfg = make_config(cfg)
+        self.h = lib().oracle_system_create(C.byref(self._cfg))
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h and _lib is not None:
+            _lib.oracle_destroy(h)
+            self.h = None
+
+    def clone(self):
+        o = OracleSystem.__new__(OracleSystem)
+        o._cfg = self._cfg
+        o.h = lib().oracle_clone(self.h)
+        return o
+
+    def upload_fluid(self, pos, vel, mass, fluid_id=None):
+        pos = _f64(pos).reshape(-1, 3)
+        n = pos.shape[0]
+        vel = _f64(vel if vel is not None else np.zeros((n, 3))).reshape(-1, 3)
+        mass = _f64(np.broadcast_to(mass, (n,)))
+        fid = np.ascontiguousarray(fluid_id if fluid_id is not None else np.zeros(n), np.uint32)
+        assert lib().oracle_upload_fluid(self.h, n, pos.ravel(), vel.ravel(), mass, fid) == 0
+
+    def add_sample_boundary(self, positions, rigid=None):
+        p = _f64(positions).reshape(-1, 3)
+        r = None if rigid is None else _f64(rigid).ctypes.data_as(C.c_void_p)
+        keep = None if rigid is None else _f64(rigid)
+        if keep is not None:
+            r = keep.ctypes.data_as(C.c_void_p)
+        assert lib().oracle_add_sample_boundary(self.h, p.shape[0], p.ravel(), r) == 0
+
+    def add_volume_map_boundary(self, sdf: Field, vm: Field, rigid=None):
+        keep = None if rigid is None else _f64(rigid)
+        r = None if keep is None else keep.ctypes.data_as(C.c_void_p)
+        assert lib().oracle_add_volume_map_boundary(self.h, sdf.desc, sdf.n, sdf.nodes, vm.desc,
+                                                    vm.n, vm.nodes, r) == 0
+
+    def initialize(self):
+        assert lib().oracle_initialize(self.h) == 0
+
+    def step(self, n=1):
+        assert lib().oracle_step(self.h, int(n)) == 0
+
+    @property
+    def n(self):
+        return lib().oracle_num_particles(self.h)
+
+    def time(self):
+        return lib().oracle_time(self.h)
+
+    def time_steps_propagated(self):
+        return lib().oracle_steps(self.h)
+
+    def hash_duplicates(self):
+        return lib().oracle_hash_duplicates(self.h)
+
+    def measurement(self) -> dict:
+        out = np.zeros(16)
+        lib().oracle_measure(self.h, out)
+        return dict(zip(MEASUREMENT_FIELDS, out.tolist()))
+
+    def download(self, field):
+        n = self.n
+        shape = (n, 3) if field in _VEC_FIELDS else (n,)
+        out = np.zeros(int(np.prod(shape)))
+        rc = lib().oracle_download(self.h, int(field), out)
+        if rc:
+            raise RuntimeError(f"oracle field {field} unavailable")
+        return out.reshape(shape)
+
+    def fluid_neighbors(self):
+        tot = lib().oracle_fluid_neighbor_total(self.h)
+        off = np.zeros(self.n + 1, np.uint64)
+        idx = np.zeros(max(tot, 1), np.uint64)
+        lib().oracle_fluid_neighbors(self.h, off, idx)
+        return off, idx[:tot]
+
+    def boundary_neighbors(self, bi):
+        tot = lib().oracle_boundary_neighbor_total(self.h, bi)
+        off = np.zeros(self.n + 1, np.uint64)
+        idx = np.zeros(max(tot, 1), np.uint64)
+        lib().oracle_boundary_neighbors(self.h, bi, off, idx)
+        return off, idx[:tot]
+
+    def boundary_volumes(self, bi, nb):
+        out = np.zeros(nb)
+        assert lib().oracle_boundary_volumes(self.h, bi, out) == 0
+        return out
+
+    def vm_samples(self, bi):
+        n = self.n
+        has = np.zeros(n, np.uint8)
+        xb, vb, vol = np.zeros(3 * n), np.zeros(3 * n), np.zeros(n)
+        assert lib().oracle_vm_samples(self.h, bi, has, xb, vb, vol) == 0
+        return has.astype(bool), xb.reshape(n, 3), vb.reshape(n, 3), vol
+
+    def rigid_state(self, bi):
+        out = np.zeros(19)
+        if lib().oracle_rigid_state(self.h, bi, out):
+            return None
+        return out

@@ -1,0 +1,479 @@
+// C entry points of the SPH oracle for the test harness (ctypes).
+// TEST INFRASTRUCTURE ONLY: loaded by tests/, smoke() and bench.py's CPU
+// baseline leg; never by the engine.
+#include <cstring>
+#include <stdexcept>
+
+#include "sph_oracle.hpp"
+
+using namespace oracle;
+
+extern "C" {
+
+// Same field meaning as `sph_config` of the engine's C ABI; kept separate so
+// the oracle has no dependency on the product.
+typedef struct oracle_config {
+  int integration_scheme;  // 0 EulerCromer, 1 TakePredicted
+  int pressure_solver;     // 0 SESPH, 1 SESPHwSplitting, 2 IISPH, 3 IISPHwOST
+  int boundary_handling;   // 0 StaticSampleBoundary, 1 VolumeMapBoundary
+  int cfl_time_step;
+  double rest_density_grid_spacing, kernel_support_radius, disable_particles_below;
+  double fluid_viscosity, boundary_viscosity;
+  double boundary_pressure_acceleration_weighting, boundary_rest_volume_weighting;
+  double stiffness, target_density_error, relaxation_factor, min_diagonal_element;
+  double time_increment, max_time_increment, cfl_number;
+  int gravity_mode;
+  double gravity_center[3];
+  unsigned max_solver_iterations;  // 0 = unbounded (reference semantics)
+} oracle_config;
+
+struct OracleHandle {
+  System sys;
+  double rest_volume_weighting = 1.0;
+};
+
+static void read_rigid(const double* r, RigidBodyMotion& out) {
+  // layout: mass, inertia_body[9] (row-major), inertia_inv_body[9], com[3],
+  //         quat (w,i,j,k)[4], lin_vel[3], ang_vel[3]  -> 32 doubles
+  M3 ib, iib;
+  for (int i = 0; i < 9; ++i) { ib.m[i / 3][i % 3] = r[1 + i]; iib.m[i / 3][i % 3] = r[10 + i]; }
+  V3 com{r[19], r[20], r[21]};
+  Quat q{r[22], r[23], r[24], r[25]};
+  V3 lv{r[26], r[27], r[28]}, av{r[29], r[30], r[31]};
+  out = RigidBodyMotion(r[0], ib, iib, com, q, lv, av);
+}
+
+void* oracle_system_create(const oracle_config* c) {
+  auto* h = new OracleHandle();
+  System& s = h->sys;
+  s.integrator = (Integrator)c->integration_scheme;
+  s.solver = (Solver)c->pressure_solver;
+  if (c->boundary_handling == 0) s.boundary = std::make_unique<StaticSampleBoundary>();
+  else s.boundary = std::make_unique<VolumeMapBoundary>();
+  SystemParameters& p = s.params;
+  p.cfl = c->cfl_time_step != 0;
+  p.time_increment = p.cfl ? 0.0 : c->time_increment;
+  p.max_time_increment = c->max_time_increment;
+  p.cfl_number = c->cfl_number;
+  p.kernel_support_radius = c->kernel_support_radius;
+  p.disable_particles_below = c->disable_particles_below;
+  p.rest_density_grid_spacing = c->rest_density_grid_spacing;
+  p.rest_volume = c->rest_density_grid_spacing * c->rest_density_grid_spacing *
+                  c->rest_density_grid_spacing;
+  p.fluid_viscosity = c->fluid_viscosity;
+  p.boundary_viscosity = c->boundary_viscosity;
+  p.boundary_pressure_acceleration_weighting = c->boundary_pressure_acceleration_weighting;
+  p.gravity = c->gravity_mode == 1 ? Gravity::Radial : Gravity::Uniform;
+  p.gravity_center = {c->gravity_center[0], c->gravity_center[1], c->gravity_center[2]};
+  s.sp.stiffness = c->stiffness;
+  s.sp.target_density_error = c->target_density_error;
+  s.sp.relaxation_factor = c->relaxation_factor;
+  s.sp.min_diagonal_element = c->min_diagonal_element;
+  s.sp.iteration_cap = c->max_solver_iterations ? c->max_solver_iterations : 0xffffffffu;
+  h->rest_volume_weighting = c->boundary_rest_volume_weighting;
+  return h;
+}
+
+void oracle_destroy(void* h) { delete (OracleHandle*)h; }
+void* oracle_clone(void* h) { return new OracleHandle(*(OracleHandle*)h); }
+
+int oracle_upload_fluid(void* hh, size_t n, const double* pos, const double* vel,
+                        const double* mass, const unsigned* fid) {
+  Fluid& f = ((OracleHandle*)hh)->sys.fluid;
+  f = Fluid();
+  f.num_active = n;
+  f.position.resize(n); f.velocity.resize(n); f.acceleration.assign(n, V3{});
+  f.mass.resize(n); f.volume.assign(n, 0.); f.pressure.assign(n, 0.);
+  f.fluid_id.resize(n); f.origin.resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    f.position[i] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    f.velocity[i] = vel ? V3{vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]} : V3{};
+    f.mass[i] = mass[i];
+    f.fluid_id[i] = fid ? fid[i] : 0u;
+    f.origin[i] = (uint32_t)i;
+  }
+  return 0;
+}
+
+int oracle_add_sample_boundary(void* hh, size_t nb, const double* pos, const double* rigid) {
+  auto* sb = dynamic_cast<StaticSampleBoundary*>(((OracleHandle*)hh)->sys.boundary.get());
+  if (!sb) return 1;
+  SampleBoundary b;
+  b.dynamic = rigid != nullptr;
+  std::vector<V3> p(nb);
+  for (size_t i = 0; i < nb; ++i) p[i] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  if (b.dynamic) {
+    b.xb_body = p;
+    b.xb.assign(nb, V3{});
+    read_rigid(rigid, b.state);
+  } else {
+    b.xb = p;
+  }
+  b.vb.assign(nb, V3{});
+  b.vol.assign(nb, 0.);
+  sb->boundaries.push_back(std::move(b));
+  return 0;
+}
+
+static void read_field(const double* desc, const long long* n, const double* nodes,
+                       Serendipity& s) {
+  s.x_min = {desc[0], desc[1], desc[2]};
+  s.x_max = {desc[3], desc[4], desc[5]};
+  s.dx = desc[6];
+  for (int d = 0; d < 3; ++d) s.n[d] = n[d];
+  size_t cnt = (size_t)(s.NX() * s.NY() * s.NZ());
+  s.nodes.assign(nodes, nodes + cnt);
+}
+
+int oracle_add_volume_map_boundary(void* hh, const double* sdf_desc, const long long* sdf_n,
+                                   const double* sdf_nodes, const double* vm_desc,
+                                   const long long* vm_n, const double* vm_nodes,
+                                   const double* rigid) {
+  auto* vb = dynamic_cast<VolumeMapBoundary*>(((OracleHandle*)hh)->sys.boundary.get());
+  if (!vb) return 1;
+  VMBoundary b;
+  read_field(sdf_desc, sdf_n, sdf_nodes, b.sdf);
+  read_field(vm_desc, vm_n, vm_nodes, b.vm);
+  b.dynamic = rigid != nullptr;
+  if (b.dynamic) read_rigid(rigid, b.state);
+  vb->boundaries.push_back(std::move(b));
+  return 0;
+}
+
+int oracle_initialize(void* hh) {
+  auto* h = (OracleHandle*)hh;
+  try {
+    h->sys.boundary->initialize(h->sys.params.kernel_support_radius, h->rest_volume_weighting);
+    h->sys.new_boxed();
+  } catch (...) {
+    return 1;
+  }
+  return 0;
+}
+
+int oracle_step(void* hh, int n) {
+  auto* h = (OracleHandle*)hh;
+  for (int i = 0; i < n; ++i) h->sys.step_forward_in_time();
+  return 0;
+}
+
+size_t oracle_num_particles(void* hh) { return ((OracleHandle*)hh)->sys.fluid.len(); }
+
+// 16 doubles in Measurement order (solver_iterations as double)
+void oracle_measure(void* hh, double* out) {
+  Measurement m = ((OracleHandle*)hh)->sys.take_measurement();
+  double v[16] = {m.time, m.density, m.density_error, m.kinetic_energy, m.stiffness,
+                  m.fluid_viscosity, m.boundary_viscosity, m.fluid_depth,
+                  m.rest_density_grid_spacing, m.kernel_support_radius, m.time_step_size,
+                  m.target_density_error, (double)m.solver_iterations, m.relaxation_factor,
+                  m.time_step_wall_clock_time, m.predicted_density_error};
+  std::memcpy(out, v, sizeof v);
+}
+
+double oracle_time(void* hh) { return ((OracleHandle*)hh)->sys.time(); }
+unsigned long long oracle_steps(void* hh) { return ((OracleHandle*)hh)->sys.time_steps_propagated; }
+size_t oracle_hash_duplicates(void* hh) { return ((OracleHandle*)hh)->sys.hash_duplicates; }
+
+// field ids: 0 position, 1 velocity, 2 acceleration, 3 mass, 4 volume,
+// 5 pressure, 6 fluid_id, 7 origin, 8 s_f, 9 a_ff, 10 solver velocity slot 0,
+// 11 integrator position slot 0, 12 integrator velocity slot 0
+int oracle_download(void* hh, int field, double* dst) {
+  System& s = ((OracleHandle*)hh)->sys;
+  Fluid& f = s.fluid;
+  size_t n = f.len();
+  auto vec3 = [&](const std::vector<V3>& v) {
+    if (v.size() < n) return 1;
+    for (size_t i = 0; i < n; ++i) { dst[3 * i] = v[i].x; dst[3 * i + 1] = v[i].y; dst[3 * i + 2] = v[i].z; }
+    return 0;
+  };
+  auto sc = [&](const std::vector<double>& v) {
+    if (v.size() < n) return 1;
+    for (size_t i = 0; i < n; ++i) dst[i] = v[i];
+    return 0;
+  };
+  switch (field) {
+    case 0: return vec3(f.position);
+    case 1: return vec3(f.velocity);
+    case 2: return vec3(f.acceleration);
+    case 3: return sc(f.mass);
+    case 4: return sc(f.volume);
+    case 5: return sc(f.pressure);
+    case 6: for (size_t i = 0; i < n; ++i) dst[i] = f.fluid_id[i]; return 0;
+    case 7: for (size_t i = 0; i < n; ++i) dst[i] = f.origin[i]; return 0;
+    case 8: return sc(s.iisph.s_f);
+    case 9: return sc(s.iisph.a_ff);
+    case 10: return f.solver_velocity_slots.empty() ? 1 : vec3(f.solver_velocity_slots[0]);
+    case 11: return f.integrator_position_slots.empty() ? 1 : vec3(f.integrator_position_slots[0]);
+    case 12: return f.integrator_velocity_slots.empty() ? 1 : vec3(f.integrator_velocity_slots[0]);
+  }
+  return 1;
+}
+
+// Fluid neighbor list (in the oracle's current index space).
+size_t oracle_fluid_neighbor_total(void* hh) { return ((OracleHandle*)hh)->sys.fluid_nl.indices.size(); }
+void oracle_fluid_neighbors(void* hh, unsigned long long* offsets, unsigned long long* indices) {
+  const NeighborList& nl = ((OracleHandle*)hh)->sys.fluid_nl;
+  for (size_t i = 0; i < nl.offsets.size(); ++i) offsets[i] = nl.offsets[i];
+  for (size_t i = 0; i < nl.indices.size(); ++i) indices[i] = nl.indices[i];
+}
+// Sample-boundary neighbor list of boundary `bi`.
+size_t oracle_boundary_neighbor_total(void* hh, size_t bi) {
+  auto* sb = dynamic_cast<StaticSampleBoundary*>(((OracleHandle*)hh)->sys.boundary.get());
+  return sb && bi < sb->boundaries.size() ? sb->boundaries[bi].nl.indices.size() : 0;
+}
+void oracle_boundary_neighbors(void* hh, size_t bi, unsigned long long* offsets,
+                               unsigned long long* indices) {
+  auto* sb = dynamic_cast<StaticSampleBoundary*>(((OracleHandle*)hh)->sys.boundary.get());
+  const NeighborList& nl = sb->boundaries[bi].nl;
+  for (size_t i = 0; i < nl.offsets.size(); ++i) offsets[i] = nl.offsets[i];
+  for (size_t i = 0; i < nl.indices.size(); ++i) indices[i] = nl.indices[i];
+}
+// Pseudo volumes of sample boundary `bi`.
+int oracle_boundary_volumes(void* hh, size_t bi, double* dst) {
+  auto* sb = dynamic_cast<StaticSampleBoundary*>(((OracleHandle*)hh)->sys.boundary.get());
+  if (!sb || bi >= sb->boundaries.size()) return 1;
+  std::memcpy(dst, sb->boundaries[bi].vol.data(), sb->boundaries[bi].vol.size() * sizeof(double));
+  return 0;
+}
+// Volume-map boundary samples of boundary `bi` for every particle:
+// has[n], xb[3n], vb[3n], vol[n] (zeros where absent).
+int oracle_vm_samples(void* hh, size_t bi, unsigned char* has, double* xb, double* vb, double* vol) {
+  auto* vb_ = dynamic_cast<VolumeMapBoundary*>(((OracleHandle*)hh)->sys.boundary.get());
+  if (!vb_ || bi >= vb_->boundaries.size()) return 1;
+  const VMBoundary& b = vb_->boundaries[bi];
+  size_t n = b.nl_normal.num_samples();
+  for (size_t i = 0; i < n; ++i) {
+    size_t c = b.nl_normal.count(i);
+    has[i] = c ? 1 : 0;
+    if (c) {
+      size_t k = *b.nl_normal.begin(i);
+      xb[3 * i] = b.spos[k].x; xb[3 * i + 1] = b.spos[k].y; xb[3 * i + 2] = b.spos[k].z;
+      vb[3 * i] = b.svel[k].x; vb[3 * i + 1] = b.svel[k].y; vb[3 * i + 2] = b.svel[k].z;
+      vol[i] = b.svol[k];
+    } else {
+      for (int d = 0; d < 3; ++d) { xb[3 * i + d] = 0; vb[3 * i + d] = 0; }
+      vol[i] = 0;
+    }
+  }
+  return 0;
+}
+// Rigid body state of boundary `bi`: com[3], quat[4] (w,i,j,k), lin_vel[3],
+// ang_mom[3], force[3], torque[3] -> 19 doubles. Returns 1 for static ones.
+int oracle_rigid_state(void* hh, size_t bi, double* out) {
+  BoundaryHandling* b = ((OracleHandle*)hh)->sys.boundary.get();
+  if (bi >= b->count()) return 1;
+  RigidBodyMotion* m = b->at(bi).motion();
+  if (!m) return 1;
+  double v[19] = {m->center_of_mass.x, m->center_of_mass.y, m->center_of_mass.z,
+                  m->orientation.w, m->orientation.x, m->orientation.y, m->orientation.z,
+                  m->linear_velocity.x, m->linear_velocity.y, m->linear_velocity.z,
+                  m->angular_momentum.x, m->angular_momentum.y, m->angular_momentum.z,
+                  m->force.x, m->force.y, m->force.z, m->torque.x, m->torque.y, m->torque.z};
+  std::memcpy(out, v, sizeof v);
+  return 0;
+}
+
+// ---- free functions ---------------------------------------------------------
+double oracle_kernel_w(double q) { return kernel_w(q); }
+double oracle_kernel_dqw(double q) { return kernel_dqw(q); }
+double oracle_kernel_function(const double* r, double h) { return kernel_function({r[0], r[1], r[2]}, h); }
+void oracle_kernel_gradient(const double* r, double h, double* out) {
+  V3 g = kernel_gradient({r[0], r[1], r[2]}, h);
+  out[0] = g.x; out[1] = g.y; out[2] = g.z;
+}
+unsigned long long oracle_map_int_to_uint(int k) { return SpatialHashing::map_int_to_uint(k); }
+unsigned long long oracle_hash(int k, int l, int m) { return SpatialHashing::hash(k, l, m); }
+void oracle_get_cell(const double* p, double cs, int* out) {
+  int32_t c[3];
+  SpatialHashing::get_cell({p[0], p[1], p[2]}, cs, c);
+  out[0] = c[0]; out[1] = c[1]; out[2] = c[2];
+}
+
+struct NLHandle { NeighborList nl; size_t dups; };
+void* oracle_find_samples(double range, double cell_size, size_t n, const double* pos, size_t ns,
+                          const double* samples) {
+  std::vector<V3> p(n), s(ns);
+  for (size_t i = 0; i < n; ++i) p[i] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  for (size_t i = 0; i < ns; ++i) s[i] = {samples[3 * i], samples[3 * i + 1], samples[3 * i + 2]};
+  auto* h = new NLHandle();
+  SpatialHashing sh(cell_size);
+  sh.find_samples(range, p, s, h->nl);
+  h->dups = sh.last_duplicates;
+  return h;
+}
+size_t oracle_nl_total(void* h) { return ((NLHandle*)h)->nl.indices.size(); }
+size_t oracle_nl_duplicates(void* h) { return ((NLHandle*)h)->dups; }
+void oracle_nl_copy(void* hh, unsigned long long* offsets, unsigned long long* indices) {
+  const NeighborList& nl = ((NLHandle*)hh)->nl;
+  for (size_t i = 0; i < nl.offsets.size(); ++i) offsets[i] = nl.offsets[i];
+  for (size_t i = 0; i < nl.indices.size(); ++i) indices[i] = nl.indices[i];
+}
+void oracle_nl_free(void* h) { delete (NLHandle*)h; }
+
+int oracle_gauss_legendre(int deg, double* x, double* w) {
+  std::vector<double> xs, ws;
+  gauss_legendre(deg, xs, ws);
+  std::memcpy(x, xs.data(), deg * sizeof(double));
+  std::memcpy(w, ws.data(), deg * sizeof(double));
+  return 0;
+}
+
+static TriMeshD make_mesh(const double* verts, size_t nv, const unsigned* faces, size_t nf) {
+  TriMeshD m;
+  m.v.resize(nv);
+  for (size_t i = 0; i < nv; ++i) m.v[i] = {verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]};
+  m.f.assign(faces, faces + 3 * nf);
+  return m;
+}
+double oracle_mesh_signed_distance(const double* verts, size_t nv, const unsigned* faces,
+                                   size_t nf, const double* p) {
+  return mesh_signed_distance(make_mesh(verts, nv, faces, nf), {p[0], p[1], p[2]});
+}
+
+struct FieldHandle { Serendipity sdf, vm; };
+void* oracle_build_fields(const double* verts, size_t nv, const unsigned* faces, size_t nf,
+                          double dx, double r, int degree) {
+  TriMeshD m = make_mesh(verts, nv, faces, nf);
+  auto* h = new FieldHandle();
+  build_sdf_field(m, dx, r, h->sdf);
+  build_volume_map_field(m, h->sdf, dx, r, degree, h->vm);
+  return h;
+}
+// Builds only the SDF; the volume map is built from `sdf_nodes` supplied later.
+void* oracle_build_sdf_only(const double* verts, size_t nv, const unsigned* faces, size_t nf,
+                            double dx, double r) {
+  TriMeshD m = make_mesh(verts, nv, faces, nf);
+  auto* h = new FieldHandle();
+  build_sdf_field(m, dx, r, h->sdf);
+  return h;
+}
+void oracle_fields_free(void* h) { delete (FieldHandle*)h; }
+// which: 0 sdf, 1 vm. desc[7] = x_min, x_max, dx; n[3]
+void oracle_field_desc(void* hh, int which, double* desc, long long* n) {
+  const Serendipity& s = which ? ((FieldHandle*)hh)->vm : ((FieldHandle*)hh)->sdf;
+  desc[0] = s.x_min.x; desc[1] = s.x_min.y; desc[2] = s.x_min.z;
+  desc[3] = s.x_max.x; desc[4] = s.x_max.y; desc[5] = s.x_max.z; desc[6] = s.dx;
+  for (int d = 0; d < 3; ++d) n[d] = s.n[d];
+}
+void oracle_field_nodes(void* hh, int which, double* dst) {
+  const Serendipity& s = which ? ((FieldHandle*)hh)->vm : ((FieldHandle*)hh)->sdf;
+  std::memcpy(dst, s.nodes.data(), s.nodes.size() * sizeof(double));
+}
+// Evaluate a field given as raw arrays: returns 0 ok, 1 error.
+int oracle_serendipity_function(const double* desc, const long long* n, const double* nodes,
+                                const double* p, double* out) {
+  Serendipity s;
+  s.x_min = {desc[0], desc[1], desc[2]}; s.x_max = {desc[3], desc[4], desc[5]}; s.dx = desc[6];
+  for (int d = 0; d < 3; ++d) s.n[d] = n[d];
+  s.nodes.assign(nodes, nodes + (size_t)(s.NX() * s.NY() * s.NZ()));
+  return s.function({p[0], p[1], p[2]}, *out) ? 0 : 1;
+}
+int oracle_serendipity_gradient(const double* desc, const long long* n, const double* nodes,
+                                const double* p, double* out) {
+  Serendipity s;
+  s.x_min = {desc[0], desc[1], desc[2]}; s.x_max = {desc[3], desc[4], desc[5]}; s.dx = desc[6];
+  for (int d = 0; d < 3; ++d) s.n[d] = n[d];
+  s.nodes.assign(nodes, nodes + (size_t)(s.NX() * s.NY() * s.NZ()));
+  V3 g;
+  if (!s.gradient({p[0], p[1], p[2]}, g)) return 1;
+  out[0] = g.x; out[1] = g.y; out[2] = g.z;
+  return 0;
+}
+// One ball-volume evaluation (SDFnWrapper::volume) on a raw SDF field.
+int oracle_volume_at(const double* desc, const long long* n, const double* nodes, const double* p,
+                     double r, int degree, double* out) {
+  Serendipity s;
+  s.x_min = {desc[0], desc[1], desc[2]}; s.x_max = {desc[3], desc[4], desc[5]}; s.dx = desc[6];
+  for (int d = 0; d < 3; ++d) s.n[d] = n[d];
+  s.nodes.assign(nodes, nodes + (size_t)(s.NX() * s.NY() * s.NZ()));
+  bool ok;
+  *out = volume_at(s, {p[0], p[1], p[2]}, r, degree, ok);
+  return ok ? 0 : 1;
+}
+
+// Rigid body: one step from a 32-double init (see read_rigid) with an applied
+// force/torque; writes the 19-double state of oracle_rigid_state.
+int oracle_rigid_body_step(const double* init, const double* force, const double* location,
+                           int n_forces, double dt, int n_steps, double* out) {
+  RigidBodyMotion m;
+  read_rigid(init, m);
+  for (int s = 0; s < n_steps; ++s) {
+    for (int k = 0; k < n_forces; ++k)
+      m.add_force({force[3 * k], force[3 * k + 1], force[3 * k + 2]},
+                  {location[3 * k], location[3 * k + 1], location[3 * k + 2]});
+    m.step_forward_in_time(dt);
+  }
+  double v[19] = {m.center_of_mass.x, m.center_of_mass.y, m.center_of_mass.z,
+                  m.orientation.w, m.orientation.x, m.orientation.y, m.orientation.z,
+                  m.linear_velocity.x, m.linear_velocity.y, m.linear_velocity.z,
+                  m.angular_momentum.x, m.angular_momentum.y, m.angular_momentum.z,
+                  m.force.x, m.force.y, m.force.z, m.torque.x, m.torque.y, m.torque.z};
+  std::memcpy(out, v, sizeof v);
+  return 0;
+}
+
+int oracle_num_threads() { return num_threads(); }
+void oracle_set_num_threads(int n) { set_num_threads(n); }
+
+}  // extern "C"
+
+extern "C" {
+// Single fluid particle with one static boundary sample of given volume
+// (the reference's IISPH MockBoundary tests, simulation_lib/tests/sph/
+// pressure_solver/iisph.rs:158-490): runs set_pred_vel, the volume-preserving
+// source term and resolve_pressure_globally with AfterIteration(after) (after
+// < 0: only the initial guess). out: pressure, a_ff, s_f, sweeps.
+int oracle_iisph_probe(const double* pos, const double* vel, double mass, double volume, double dt,
+                       double h, double spacing, double gamma_p, double omega, double eps,
+                       const double* bpos, double bvol, int after, double* out) {
+  System s;
+  s.params.time_increment = dt;
+  s.params.kernel_support_radius = h;
+  s.params.rest_density_grid_spacing = spacing;
+  s.params.rest_volume = spacing * spacing * spacing;
+  s.params.boundary_pressure_acceleration_weighting = gamma_p;
+  s.sp.relaxation_factor = omega;
+  s.sp.min_diagonal_element = eps;
+  auto sb = std::make_unique<StaticSampleBoundary>();
+  if (bpos) {
+    SampleBoundary b;
+    b.xb = {V3{bpos[0], bpos[1], bpos[2]}};
+    b.vb = {V3{}};
+    b.vol = {bvol};
+    b.nl.indices = {0};
+    b.nl.offsets = {0, 1};
+    sb->boundaries.push_back(std::move(b));
+  }
+  s.boundary = std::move(sb);
+  Fluid& f = s.fluid;
+  f.num_active = 1;
+  f.position = {V3{pos[0], pos[1], pos[2]}};
+  f.velocity = {V3{vel[0], vel[1], vel[2]}};
+  f.acceleration = {V3{}};
+  f.mass = {mass};
+  f.volume = {volume};
+  f.pressure = {0.0};
+  f.fluid_id = {0};
+  f.origin = {0};
+  f.resize_slots(0, 0, 1, 1);
+  s.fluid_nl.indices.clear();
+  s.fluid_nl.offsets = {0, 0};
+  s.iisph.s_f.assign(1, 0.0);
+  s.iisph.a_ff.assign(1, 0.0);
+  s.iisph.pressure_acc_f.assign(1, V3{});
+  s.set_pred_vel_by_applying_acc(false);
+  s.set_source_term_vp();
+  if (after < 0) {
+    s.set_diagonal_element();
+    s.iisph_initialize(true);
+    s.iisph.last_solver_iterations = 0;
+  } else {
+    s.resolve_pressure_globally(true, (uint32_t)after, 0.0, true);
+  }
+  out[0] = f.pressure[0];
+  out[1] = s.iisph.a_ff[0];
+  out[2] = s.iisph.s_f[0];
+  out[3] = s.iisph.last_solver_iterations;
+  return 0;
+}
+}

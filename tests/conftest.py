@@ -1,0 +1,64 @@
+"""Shared test setup: import paths, the `gpu` marker, and helpers."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "fluid-simulation_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and libsphgpu.so")
+
+
+def has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    import oracle as O
+    O.lib()
+    return O
+
+
+def oracle_config(scene):
+    """Oracle config dict for a sphgpu Scene (same field meaning as sph_config)."""
+    from sphgpu.system import PROCEDURES
+    cfg = dict(scene.parameters)
+    cfg.pop("device", None)
+    cfg.pop("neighbor_capacity", None)
+    cfg["integration_scheme"] = PROCEDURES["integration_scheme"][scene.procedures["integration_scheme"]]
+    cfg["pressure_solver"] = PROCEDURES["pressure_solver"][scene.procedures["pressure_solver"]]
+    cfg["boundary_handling"] = PROCEDURES["boundary_handling"][scene.procedures["boundary_handling"]]
+    cfg["cfl_time_step"] = 1 if scene.cfl_time_step else 0
+    if "time_increment" not in cfg:
+        cfg["time_increment"] = 0.0
+    return cfg
+
+
+def build_oracle(scene, fields=None):
+    import oracle as O
+    s = O.OracleSystem(oracle_config(scene))
+    s.upload_fluid(scene.position, scene.velocity, scene.mass, scene.fluid_id)
+    for pts, rigid in scene.sample_boundaries:
+        s.add_sample_boundary(pts, None if rigid is None else rigid.to_array32())
+    for sdf, vm, rigid in scene.volume_maps:
+        s.add_volume_map_boundary(sdf, vm, None if rigid is None else rigid.to_array32())
+    if fields is not None:
+        s.add_volume_map_boundary(fields[0], fields[1])
+    s.initialize()
+    return s
+
+
+def rel_err(a, b, floor):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)) if a.size else 0.0

@@ -1,0 +1,218 @@
+"""Parity of the CUDA engine (through the C ABI) with the f64 oracle.
+
+Bars (the engine's state is f32 with compensated density sums; an f64 twin of
+every kernel exists for the precision study):
+  * neighbor sets and cell-derived data: bit-exact (multisets compared after a
+    per-particle sort) on identical input states, both precisions;
+  * per-particle fields from the same input state: f64 engine within 1e-9
+    relative of the oracle; f32 engine within the tolerances stated per test
+    (volume/density 1e-5 relative, the north-star bar being 1e-4);
+  * IISPH sweep counts: equal for f64, within +-1 for f32.
+"""
+import numpy as np
+import pytest
+
+from conftest import build_oracle, rel_err
+
+pytestmark = pytest.mark.gpu
+
+F32_DENSITY_RTOL = 1e-5     # volume / density, f32 engine vs f64 oracle
+F64_RTOL = 1e-9             # any field, f64 engine vs f64 oracle
+
+
+@pytest.fixture(scope="module")
+def A():
+    from sphgpu import _capi
+    _capi.load()
+    return _capi
+
+
+def rows(off, idx):
+    return [sorted(idx[int(off[i]):int(off[i + 1])].tolist()) for i in range(len(off) - 1)]
+
+
+# ---------------------------------------------------------------------------------------
+# per-trait shims
+# ---------------------------------------------------------------------------------------
+def test_kernel_function_and_gradient_match_oracle(oracle):
+    from sphgpu import kernel_function, kernel_gradient
+    rng = np.random.default_rng(1)
+    h = 0.04
+    r = rng.uniform(-h, h, size=(2000, 3))
+    r[0] = 0.0
+    r[1] = [h, 0, 0]
+    w64 = kernel_function(r, h, precision="f64")
+    g64 = kernel_gradient(r, h, precision="f64")
+    w_ref = np.array([oracle.kernel_function(x, h) for x in r])
+    g_ref = np.array([oracle.kernel_gradient(x, h) for x in r])
+    scale_w = oracle.kernel_function([0, 0, 0], h)
+    scale_g = np.abs(g_ref).max()
+    assert np.max(np.abs(w64 - w_ref)) <= 1e-13 * scale_w
+    assert np.max(np.abs(g64 - g_ref)) <= 1e-13 * scale_g
+    w32 = kernel_function(r, h, precision="f32")
+    g32 = kernel_gradient(r, h, precision="f32")
+    assert np.max(np.abs(w32 - w_ref)) <= 1e-6 * scale_w
+    assert np.max(np.abs(g32 - g_ref)) <= 1e-6 * scale_g
+    assert np.all(g64[0] == 0.0) and w64[1] == 0.0 and np.all(g64[1] == 0.0)
+
+
+def test_find_samples_is_bit_exact_including_order(oracle):
+    from sphgpu import find_samples
+    rng = np.random.default_rng(7)
+    pts = rng.uniform(-0.5, 0.5, size=(3000, 3)).astype(np.float32).astype(np.float64)
+    samples = rng.uniform(-0.6, 0.6, size=(2500, 3))
+    # pairs placed exactly at the search range (strict < must exclude them)
+    samples[:10] = pts[:10] + np.array([0.1, 0, 0])
+    for rng_, s in ((0.1, samples), (0.1, pts)):
+        off_g, idx_g = find_samples(rng_, pts, s)
+        off_o, idx_o, dups = oracle.find_samples(rng_, pts, s)
+        assert dups == 0
+        assert np.array_equal(off_g, off_o)
+        assert np.array_equal(idx_g.astype(np.uint64), idx_o)  # same stencil/bucket order
+
+
+def test_find_samples_empty_inputs():
+    from sphgpu import find_samples
+    off, idx = find_samples(0.1, np.zeros((0, 3)), np.zeros((5, 3)))
+    assert off.tolist() == [0] and idx.size == 0
+    off, idx = find_samples(0.1, np.zeros((3, 3)), np.zeros((0, 3)))
+    assert off.tolist() == [0, 0, 0, 0] and idx.size == 0
+
+
+# ---------------------------------------------------------------------------------------
+# SESPH dam break with a StaticSampleBoundary container (8,000 particles)
+# ---------------------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def sesph_scene():
+    from sphgpu import scenes
+    return scenes.dam_break_sesph_8k()
+
+
+@pytest.fixture(scope="module")
+def sesph_oracle(sesph_scene):
+    return build_oracle(sesph_scene)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_sesph_first_update_matches_oracle(A, oracle, sesph_scene, sesph_oracle, precision):
+    from sphgpu import scenes
+    g = scenes.build_system(sesph_scene, precision=precision)
+    o = sesph_oracle
+    # neighbor sets: bit-exact multisets
+    off_g, idx_g = g.fluid_neighbors()
+    off_o, idx_o = o.fluid_neighbors()
+    assert rows(off_g, idx_g) == rows(off_o, idx_o)
+    off_gb, idx_gb = g.boundary_neighbors(0)
+    off_ob, idx_ob = o.boundary_neighbors(0)
+    assert rows(off_gb, idx_gb) == rows(off_ob, idx_ob)
+    assert o.hash_duplicates() == 0 and g.hash_collisions() == 0
+    nb = sesph_scene.sample_boundaries[0][0].shape[0]
+    tol = F64_RTOL if precision == "f64" else 1e-5
+    assert rel_err(g.boundary_volumes(0, nb), o.boundary_volumes(0, nb), 1e-30) < tol
+    V_g, V_o = g.download(A.FIELD_VOLUME), o.download(oracle.F_VOLUME)
+    assert rel_err(V_g, V_o, 1e-30) < (F64_RTOL if precision == "f64" else F32_DENSITY_RTOL)
+    p_g, p_o = g.download(A.FIELD_PRESSURE), o.download(oracle.F_PRESSURE)
+    pscale = np.abs(p_o).max()
+    assert np.max(np.abs(p_g - p_o)) <= (1e-8 if precision == "f64" else 2e-3) * pscale
+    a_g, a_o = g.download(A.FIELD_ACCELERATION), o.download(oracle.F_ACCELERATION)
+    ascale = np.abs(a_o).max()
+    assert np.max(np.abs(a_g - a_o)) <= (1e-8 if precision == "f64" else 2e-3) * ascale
+    mg, mo = g.take_measurement(), o.measurement()
+    assert abs(mg["density"] - mo["density"]) <= (1e-9 if precision == "f64" else 1e-5) * mo["density"]
+    assert abs(mg["density_error"] - mo["density_error"]) <= (1e-8 if precision == "f64" else 1e-3)
+
+
+def test_sesph_multistep_tracks_oracle(A, oracle, sesph_scene):
+    from sphgpu import scenes
+    g = scenes.build_system(sesph_scene, precision="f32")
+    o = build_oracle(sesph_scene)
+    for _ in range(4):
+        g.step_forward_in_time(25)
+        o.step(25)
+        mg, mo = g.take_measurement(), o.measurement()
+        assert abs(mg["time"] - mo["time"]) < 1e-12
+        assert abs(mg["density"] - mo["density"]) < 1e-3 * mo["density"]
+        assert abs(mg["kinetic_energy"] - mo["kinetic_energy"]) <= 2e-2 * mo["kinetic_energy"] + 1e-9
+    x_g, x_o = g.download(A.FIELD_POSITION), o.download(oracle.F_POSITION)
+    # trajectories after 100 steps: RMS deviation far below the particle spacing
+    assert np.sqrt(np.mean(np.sum((x_g - x_o) ** 2, axis=1))) < 1e-3 * 0.02
+
+
+# ---------------------------------------------------------------------------------------
+# IISPH with a VolumeMapBoundary box (small, fields built by the oracle)
+# ---------------------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def vm_case(oracle):
+    from sphgpu import scenes
+    sc = scenes.dam_break_iisph_box(n_side=16, spacing=0.02, box=(0.64, 0.32, 0.32))
+    verts, faces = sc.mesh
+    sdf, vm = oracle.build_fields(verts, faces, 4 * 0.02, 2 * 0.02, 30)
+    o = build_oracle(sc, fields=(sdf, vm))
+    return sc, (sdf, vm), o
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_iisph_volume_map_first_update_matches_oracle(A, oracle, vm_case, precision):
+    from sphgpu import scenes
+    sc, fields, o = vm_case
+    g = scenes.build_system(sc, precision=precision, fields=fields)
+    assert rows(*g.fluid_neighbors()) == rows(*o.fluid_neighbors())
+    has_g, xb_g, vb_g, vol_g = g.volume_map_samples(0)
+    has_o, xb_o, vb_o, vol_o = o.vm_samples(0)
+    assert np.array_equal(has_g, has_o) and has_o.sum() > 0
+    tol = 1e-9 if precision == "f64" else 2e-6
+    assert np.max(np.abs(xb_g - xb_o)) < tol * 1.0
+    assert rel_err(vol_g[has_o], vol_o[has_o], 1e-30) < (1e-9 if precision == "f64" else 1e-6)
+    assert rel_err(g.download(A.FIELD_VOLUME), o.download(oracle.F_VOLUME), 1e-30) < (
+        F64_RTOL if precision == "f64" else F32_DENSITY_RTOL)
+    s_g, s_o = g.download(A.FIELD_SOURCE_TERM), o.download(oracle.F_SOURCE)
+    a_g, a_o = g.download(A.FIELD_DIAGONAL), o.download(oracle.F_DIAGONAL)
+    assert np.max(np.abs(s_g - s_o)) <= (1e-10 if precision == "f64" else 2e-5)
+    assert rel_err(a_g, a_o, np.abs(a_o).max() * 1e-6) < (1e-8 if precision == "f64" else 1e-4)
+    mg, mo = g.take_measurement(), o.measurement()
+    if precision == "f64":
+        assert mg["solver_iterations"] == mo["solver_iterations"]
+        assert abs(mg["predicted_density_error"] - mo["predicted_density_error"]) < 1e-8
+    else:
+        assert abs(mg["solver_iterations"] - mo["solver_iterations"]) <= 1
+    p_g, p_o = g.download(A.FIELD_PRESSURE), o.download(oracle.F_PRESSURE)
+    pscale = np.abs(p_o).max()
+    assert np.max(np.abs(p_g - p_o)) <= (1e-7 if precision == "f64" else 5e-2) * pscale
+    acc_g, acc_o = g.download(A.FIELD_ACCELERATION), o.download(oracle.F_ACCELERATION)
+    ascale = np.abs(acc_o).max()
+    assert np.max(np.abs(acc_g - acc_o)) <= (1e-7 if precision == "f64" else 5e-2) * ascale
+
+
+def test_iisph_volume_map_steps_track_oracle(A, oracle, vm_case):
+    from sphgpu import scenes
+    sc, fields, _ = vm_case
+    g = scenes.build_system(sc, precision="f32", fields=fields)
+    o = build_oracle(sc, fields=fields)
+    for _ in range(5):
+        g.step_forward_in_time(4)
+        o.step(4)
+        mg, mo = g.take_measurement(), o.measurement()
+        assert abs(mg["time"] - mo["time"]) < 1e-6 * max(mo["time"], 1e-9)
+        assert abs(mg["time_step_size"] - mo["time_step_size"]) < 1e-5 * mo["time_step_size"]
+        assert abs(mg["density"] - mo["density"]) < 1e-4 * mo["density"]
+        assert abs(mg["solver_iterations"] - mo["solver_iterations"]) <= 1
+        assert abs(mg["predicted_density_error"] - mo["predicted_density_error"]) < 2e-3
+
+
+# ---------------------------------------------------------------------------------------
+# disabling particles below the threshold keeps the reference's swap-remove order
+# ---------------------------------------------------------------------------------------
+def test_disable_below_threshold_matches_swap_remove_order(A, oracle, sesph_scene):
+    from sphgpu import scenes
+    sc = scenes.dam_break_sesph_8k()
+    sc.parameters = dict(sc.parameters, disable_particles_below=-0.28)
+    g = scenes.build_system(sc, precision="f64")
+    o = build_oracle(sc)
+    assert g.n == o.n < 8000
+    ids_o = o.download(oracle.F_ORIGIN)
+    x0 = sc.position[ids_o.astype(int)]
+    assert np.array_equal(g.download(A.FIELD_POSITION), x0)
+    g.step_forward_in_time(3)
+    o.step(3)
+    assert g.n == o.n
+    assert np.max(np.abs(g.download(A.FIELD_POSITION) - o.download(oracle.F_POSITION))) < 1e-9

@@ -1,0 +1,333 @@
+"""Pins the oracle to the reference's own known-answer tests.
+
+The reference (Rust) cannot be built here, so the oracle's fidelity rests on
+the formula-level assertions of the reference's test suite, restated below
+against the oracle (sim_lib = simulation_lib):
+  kernel      tests/sph/kernel/cubic_spline.rs:17-232
+  hashing     src/neighbor_search/spatial_hashing.rs:173-390
+  volume      src/sph/quantities.rs:437-633
+  IISPH       tests/sph/pressure_solver/iisph.rs:429-490
+  IISPHwOST   src/sph/pressure_solver/iisph_optimized_source_term.rs:530-582
+  EulerCromer tests/sph/integration_schemes/euler_cromer.rs:91-300
+  rigid body  tests/sph/boundary_handling/rigid_body_motion.rs:44-642
+  serendipity tests/utilities/discretization.rs:21-212
+  mesh SDF    src/sph/boundary_handling/volume_map_boundary.rs:2809-2835
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import build_oracle
+
+ALPHA = 16.0 / math.pi
+
+
+# ---- kernel -------------------------------------------------------------------------
+def test_kernel_known_values(oracle):
+    assert abs(oracle.kernel_w(0.0) - 0.5) < 1e-12
+    assert abs(oracle.kernel_w(0.5) - 0.125) < 1e-12
+    for q in (1.0, 1.5, 10.0):
+        assert oracle.kernel_w(q) == 0.0
+    assert oracle.kernel_dqw(1.0) == 0.0 and oracle.kernel_dqw(2.0) == 0.0
+    h = 1.0
+    assert oracle.kernel_function([1.0, 0, 0], h) == 0.0
+    assert abs(oracle.kernel_function([0, 0, 0], 2.0) - ALPHA / 8.0 * 0.5) < 1e-12
+
+
+def test_kernel_derivative_matches_finite_difference(oracle):
+    eps = 1e-6
+    for q in (0.05, 0.2, 0.35, 0.55, 0.7, 0.9):
+        num = (oracle.kernel_w(q + eps) - oracle.kernel_w(q - eps)) / (2 * eps)
+        assert abs(oracle.kernel_dqw(q) - num) < 1e-4
+
+
+def test_kernel_gradient_zero_at_origin_and_antisymmetric(oracle):
+    assert np.all(oracle.kernel_gradient([0, 0, 0], 1.0) == 0.0)
+    r = np.array([0.1, -0.2, 0.3])
+    g1, g2 = oracle.kernel_gradient(r, 1.0), oracle.kernel_gradient(-r, 1.0)
+    assert np.allclose(g1, -g2, atol=1e-15)
+    # gradient points from the neighbor towards the evaluated point: W decreases
+    assert np.dot(g1, r) < 0
+
+
+def test_kernel_integrates_to_one(oracle):
+    # radial Gauss-Legendre quadrature of 4 pi r^2 W(r) on the two polynomial
+    # pieces [0, h/2] and [h/2, h] (exact for these degrees)
+    x, w = oracle.gauss_legendre(8)
+    h = 0.7
+    tot = 0.0
+    for a, b in ((0.0, 0.5 * h), (0.5 * h, h)):
+        for xi, wi in zip(x, w):
+            r = 0.5 * (b - a) * xi + 0.5 * (a + b)
+            tot += 0.5 * (b - a) * wi * 4 * math.pi * r * r * oracle.kernel_function([r, 0, 0], h)
+    assert abs(tot - 1.0) < 1e-12
+
+
+# ---- spatial hashing ------------------------------------------------------------------
+def test_map_int_to_uint_and_hash(oracle):
+    assert [oracle.map_int_to_uint(k) for k in (0, 1, 5)] == [0, 2, 10]
+    assert [oracle.map_int_to_uint(k) for k in (-1, -5)] == [3, 11]
+    vals = [oracle.map_int_to_uint(k) for k in range(-100, 101)]
+    assert len(set(vals)) == len(vals)
+    assert oracle.cell_hash(0, 0, 0) != oracle.cell_hash(1, 0, 0)
+    assert oracle.cell_hash(1, 2, 3) == oracle.cell_hash(1, 2, 3)
+    # (2k)*73856093 ^ ... by hand
+    assert oracle.cell_hash(1, -1, 2) == (2 * 73856093) ^ (3 * 19349663) ^ (4 * 83492791)
+
+
+def test_hash_has_no_collisions_over_41_cubed(oracle):
+    seen = set()
+    for k in range(-20, 21):
+        for l in range(-20, 21):
+            for m in range(-20, 21):
+                seen.add(oracle.cell_hash(k, l, m))
+    assert len(seen) == 41 ** 3
+
+
+@pytest.mark.parametrize("p,cs,cell", [
+    ((0.5, 0.5, 0.5), 1.0, (0, 0, 0)), ((2.3, 4.7, 1.1), 1.0, (2, 4, 1)),
+    ((-0.5, -1.5, -3.9), 1.0, (-1, -2, -4)), ((1.5, 3.0, 0.9), 2.0, (0, 1, 0)),
+    ((1.0, 2.0, 3.0), 1.0, (1, 2, 3))])
+def test_get_cell(oracle, p, cs, cell):
+    assert tuple(oracle.get_cell(p, cs)) == cell
+
+
+def _row(off, idx, i):
+    return list(idx[int(off[i]):int(off[i + 1])])
+
+
+def test_find_samples_semantics(oracle):
+    # close neighbor + self
+    off, idx, _ = oracle.find_samples(1.0, [[0, 0, 0], [0.5, 0, 0]], [[0, 0, 0], [0.5, 0, 0]])
+    assert set(_row(off, idx, 0)) == {0, 1}
+    # far neighbor excluded
+    off, idx, _ = oracle.find_samples(2.0, [[0, 0, 0]], [[0, 0, 0], [10, 0, 0]], cell_size=1.0)
+    assert _row(off, idx, 0) == [0]
+    # exactly at the range: strict <
+    off, idx, _ = oracle.find_samples(2.0, [[0, 0, 0]], [[0, 0, 0], [2, 0, 0]], cell_size=2.0)
+    assert 1 not in _row(off, idx, 0)
+    # negative positions and across zero
+    off, idx, _ = oracle.find_samples(1.0, [[-1, -1, -1]], [[-1, -1, -1], [-1.5, -1, -1]])
+    assert 1 in _row(off, idx, 0)
+    off, idx, _ = oracle.find_samples(0.2, [[-0.05, 0, 0]], [[-0.05, 0, 0], [0.05, 0, 0]], cell_size=1.0)
+    assert 1 in _row(off, idx, 0)
+
+
+def test_find_samples_matches_brute_force(oracle):
+    rng = np.random.default_rng(3)
+    pts = rng.uniform(-1, 1, size=(600, 3))
+    off, idx, dups = oracle.find_samples(0.25, pts, pts)
+    assert dups == 0
+    d = np.sqrt(((pts[:, None, :] - pts[None, :, :]) ** 2).sum(-1))
+    for i in range(0, 600, 37):
+        assert sorted(_row(off, idx, i)) == sorted(np.nonzero(d[i] < 0.25)[0].tolist())
+
+
+# ---- volume / density -------------------------------------------------------------------
+def _lattice(n, dx):
+    g = np.arange(n) * dx
+    return np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+
+
+def _isolated_system(oracle, pos, vel=None, solver=0, integrator=0, dt=0.01, h=0.04, spacing=0.02,
+                     mass=None):
+    from sphgpu import scenes
+    sc = scenes.Scene(
+        procedures={"integration_scheme": "TakePredicted" if integrator else "EulerCromer",
+                    "pressure_solver": ["SESPH", "SESPHwSplitting", "IISPH", "IISPHwOST"][solver],
+                    "boundary_handling": "VolumeMapBoundary"},
+        parameters={"rest_density_grid_spacing": spacing, "kernel_support_radius": h,
+                    "disable_particles_below": -50.0, "fluid_viscosity": 0.0,
+                    "boundary_viscosity": 0.0, "boundary_pressure_acceleration_weighting": 0.7,
+                    "boundary_rest_volume_weighting": 1.0, "stiffness": 1000.0,
+                    "target_density_error": 0.01, "relaxation_factor": 0.5,
+                    "min_diagonal_element": 1e-9, "time_increment": dt},
+        cfl_time_step=False, position=np.asarray(pos, np.float64),
+        mass=np.full(len(pos), 1000.0 * spacing ** 3 if mass is None else mass),
+        velocity=None if vel is None else np.asarray(vel, np.float64))
+    return build_oracle(sc)
+
+
+def test_volume_is_rest_volume_over_kernel_sum(oracle):
+    h, dx = 0.04, 0.02
+    pos = _lattice(7, dx)
+    s = _isolated_system(oracle, pos, h=h, spacing=dx)
+    V = s.download(oracle.F_VOLUME)
+    V0 = dx ** 3
+    i = 3 * 49 + 3 * 7 + 3  # lattice center
+    acc = sum(V0 * oracle.kernel_function(pos[i] - pos[j], h) for j in range(len(pos))
+              if np.linalg.norm(pos[i] - pos[j]) < h)
+    assert abs(V[i] - V0 / acc) < 1e-12 * V0
+    # the lattice interior recovers the rest density within 15 %
+    rho = 1000.0 * dx ** 3 / V[i]
+    assert abs(rho - 1000.0) / 1000.0 < 0.15
+
+
+def test_isolated_particle_volume_is_inverse_self_weight(oracle):
+    s = _isolated_system(oracle, [[0.1, 0.2, 0.3]])
+    V = s.download(oracle.F_VOLUME)[0]
+    assert abs(V - 1.0 / oracle.kernel_function([0, 0, 0], 0.04)) < 1e-15
+
+
+# ---- integration --------------------------------------------------------------------------
+def test_euler_cromer_recurrence_isolated_particle(oracle):
+    # isolated SESPH particle: V > V0 so no pressure; acceleration = gravity
+    x0, v0, dt = np.array([1.0, 2.0, 3.0]), np.array([0.5, -0.25, 0.125]), 0.01
+    s = _isolated_system(oracle, [x0], [v0], dt=dt)
+    g = np.array([0, 0, -9.81])
+    assert np.allclose(s.download(oracle.F_ACCELERATION)[0], g, atol=1e-14)
+    s.step(1)
+    v1 = v0 + dt * g
+    x1 = x0 + dt * v1  # position update uses the new velocity
+    assert np.allclose(s.download(oracle.F_VELOCITY)[0], v1, atol=1e-12)
+    assert np.allclose(s.download(oracle.F_POSITION)[0], x1, atol=1e-12)
+    s.step(1)
+    v2 = v1 + dt * g
+    assert np.allclose(s.download(oracle.F_POSITION)[0], x1 + dt * v2, atol=1e-12)
+    assert abs(s.time() - 2 * dt) < 1e-15
+
+
+def test_iisph_w_ost_isolated_particle_trace(oracle):
+    # iisph_optimized_source_term.rs:530-582: gravity only enters v*, the
+    # acceleration is overwritten by the (zero) pressure acceleration.
+    x0, v0, dt = np.array([1.0, 2.0, 3.0]), np.array([0.5, 0.0, 0.0]), 0.05
+    s = _isolated_system(oracle, [x0], [v0], solver=3, integrator=1, dt=dt, h=1.0, spacing=0.3)
+    g = np.array([0, 0, -9.81])
+    assert s.download(oracle.F_PRESSURE)[0] == 0.0
+    assert np.all(s.download(oracle.F_ACCELERATION)[0] == 0.0)
+    v_pred = v0 + dt * g
+    assert np.allclose(s.download(oracle.F_INTEGRATOR_VEL)[0], v_pred, atol=1e-9)
+    assert np.allclose(s.download(oracle.F_INTEGRATOR_POS)[0], x0 + dt * v_pred, atol=1e-9)
+
+
+# ---- IISPH ----------------------------------------------------------------------------------
+def _probe_inputs():
+    h, dt, spacing, gamma = 1.0, 0.05, 0.3, 0.5
+    V = spacing ** 3 * 0.5   # compressed -> s_f < 0
+    return dict(pos=[0, 0, 0], vel=[0, 0, 0], mass=0.5, volume=V, dt=dt, h=h, spacing=spacing,
+                gamma_p=gamma, omega=0.5, eps=1e-9, bpos=[0.2, 0, 0], bvol=0.01)
+
+
+def test_iisph_diagonal_and_initial_pressure_match_formula(oracle):
+    a = _probe_inputs()
+    p, aff, sf, it = oracle.iisph_probe(**a, after=-1)
+    gb = a["bvol"] * oracle.kernel_gradient(-np.array(a["bpos"]), a["h"])
+    c_f = -a["volume"] / a["mass"] * (2.0 * a["gamma_p"] * gb)
+    aff_expected = a["dt"] ** 2 * np.dot(c_f, gb)
+    s_expected = 1.0 - a["spacing"] ** 3 / a["volume"]
+    assert abs(aff - aff_expected) < 1e-12 and aff < 0
+    assert abs(sf - s_expected) < 1e-12
+    # initialize(): p0 = max(omega s / a_ff, 0) (the value the reference test
+    # asserts for its `AfterIteration(0)` call)
+    p_expected = max(0.5 * s_expected / aff_expected, 0.0)
+    assert abs(p - p_expected) < 1e-12 * p_expected and p > 0
+
+
+def test_iisph_after_iteration_counts_follow_the_code(oracle):
+    # converged(AfterIteration(n)) stops when iter > n: n+1 sweeps. One sweep
+    # on an isolated particle with one boundary sample gives
+    # p1 = (1 - omega) p0 + omega s / a_ff = 0.75 s / a_ff.
+    a = _probe_inputs()
+    p, aff, sf, it = oracle.iisph_probe(**a, after=0)
+    assert it == 1
+    assert abs(p - 0.75 * sf / aff) < 1e-12 * abs(0.75 * sf / aff)
+    _, _, _, it3 = oracle.iisph_probe(**a, after=3)
+    assert it3 == 4
+
+
+def test_iisph_expansion_never_gives_negative_pressure(oracle):
+    a = _probe_inputs()
+    a["volume"] = a["spacing"] ** 3 * 2.0  # expanded -> s_f > 0
+    p, aff, sf, _ = oracle.iisph_probe(**a, after=0)
+    assert sf > 0 and p == 0.0
+
+
+# ---- rigid body -----------------------------------------------------------------------------
+def _rigid_init(mass=2.0, I=(1.0, 2.0, 3.0), com=(0, 0, 0), q=(1, 0, 0, 0), v=(0, 0, 0), w=(0, 0, 0)):
+    Ib = np.diag(I)
+    return np.concatenate([[mass], Ib.ravel(), np.linalg.inv(Ib).ravel(), com, q, v, w]).astype(np.float64)
+
+
+def test_rigid_body_semi_implicit_linear_step(oracle):
+    init = _rigid_init(mass=2.0)
+    dt = 0.1
+    st = oracle.rigid_body_step(init, [[0, 0, 4.0]], [[0, 0, 0]], dt, 1)
+    v = 4.0 / 2.0 * dt
+    assert np.allclose(st[7:10], [0, 0, v])
+    assert np.allclose(st[0:3], [0, 0, v * dt])  # com uses the new velocity
+    assert np.allclose(st[13:19], 0.0)           # forces reset after the step
+
+
+def test_rigid_body_rotation_angle_is_preserved(oracle):
+    # constant angular velocity about z for n steps -> rotation angle w n dt
+    w, dt, n = 0.7, 0.01, 50
+    init = _rigid_init(I=(1.0, 1.0, 1.0), w=(0, 0, w))
+    st = oracle.rigid_body_step(init, [[0, 0, 0]], [[0, 0, 0]], dt, n)
+    q = st[3:7]
+    angle = 2 * math.atan2(np.linalg.norm(q[1:]), q[0])
+    assert abs(angle - w * n * dt) < 1e-12
+    assert abs(np.linalg.norm(q) - 1.0) < 1e-12
+
+
+def test_rigid_body_torque_from_off_center_force(oracle):
+    init = _rigid_init()
+    st = oracle.rigid_body_step(init, [[0, 1.0, 0]], [[1.0, 0, 0]], 0.1, 1)
+    # torque = r x F = (1,0,0) x (0,1,0) = (0,0,1); L = T dt
+    assert np.allclose(st[10:13], [0, 0, 0.1])
+
+
+# ---- serendipity / volume map --------------------------------------------------------------
+def _field(oracle, fn, n=(2, 2, 2), dx=0.5, x_min=(0, 0, 0)):
+    n = np.array(n)
+    NX, NY, NZ = 3 * n + 1
+    nodes = np.full(NX * NY * NZ, np.nan)
+    for kz in range(NZ):
+        for ky in range(NY):
+            for kx in range(NX):
+                # only nodes with at most one off-corner coordinate belong to a cell
+                if sum(k % 3 != 0 for k in (kx, ky, kz)) <= 1:
+                    p = np.array(x_min) + np.array([kx, ky, kz]) / 3.0 * dx
+                    nodes[(kz * NY + ky) * NX + kx] = fn(p)
+    x_min = np.array(x_min, np.float64)
+    return oracle.Field(x_min, x_min + n * dx, dx, n, nodes)
+
+
+def test_serendipity_reproduces_constant_and_linear_fields(oracle):
+    F = _field(oracle, lambda p: 2.5)
+    for p in ([0.1, 0.2, 0.3], [0.9, 0.7, 0.4], [0.5, 0.5, 0.5]):
+        assert abs(F.function(p) - 2.5) < 1e-12
+        assert np.allclose(F.gradient(p), 0.0, atol=1e-9)
+    L = _field(oracle, lambda p: 1.0 + 2 * p[0] - p[1] + 0.5 * p[2])
+    for p in ([0.1, 0.2, 0.3], [0.6, 0.35, 0.8]):
+        assert abs(L.function(p) - (1.0 + 2 * p[0] - p[1] + 0.5 * p[2])) < 1e-9
+        assert np.allclose(L.gradient(p), [2, -1, 0.5], atol=1e-6)
+    assert F.function([2.0, 0.1, 0.1]) is None   # out of bounds
+
+
+def test_gauss_legendre_ball_volume(oracle):
+    # SDF uniformly far inside the boundary -> integrand 1 -> ball volume, and
+    # the band case integrates the cubic extension function
+    sdf = _field(oracle, lambda p: -0.01, n=(4, 4, 4), dx=0.5)
+    r = 0.2
+    assert abs(oracle.volume_at(sdf, [1.0, 1.0, 1.0], r) - 4 / 3 * math.pi * r ** 3) < 1e-12
+    sdf0 = _field(oracle, lambda p: 0.0, n=(4, 4, 4), dx=0.5)
+    v = oracle.volume_at(sdf0, [1.0, 1.0, 1.0], r)
+    assert abs(v - 4 / 3 * math.pi * r ** 3) < 1e-9  # sd = 0 -> extension 1
+    far = _field(oracle, lambda p: 5.0, n=(4, 4, 4), dx=0.5)
+    assert oracle.volume_at(far, [1.0, 1.0, 1.0], r) == 0.0
+
+
+def test_mesh_signed_distance_cube(oracle):
+    from sphgpu import scenes
+    out = scenes.CUBE_FACES_OUTWARD
+    inw = scenes.CUBE_FACES_INWARD
+    v = scenes.CUBE_VERTICES
+    # outward cube: outside positive (face distance), inside negative
+    assert abs(oracle.mesh_signed_distance(v, out, [2.5, 0.1, -0.2]) - 1.5) < 1e-12
+    assert abs(oracle.mesh_signed_distance(v, out, [0.5, 0.1, -0.2]) + 0.5) < 1e-12
+    # inward cube (a container): inside positive
+    assert abs(oracle.mesh_signed_distance(v, inw, [0.5, 0.1, -0.2]) - 0.5) < 1e-12
+    # outside near an edge: euclidean distance to the edge, negative for the container
+    d = oracle.mesh_signed_distance(v, inw, [1.3, 1.4, 0.0])
+    assert abs(d + math.hypot(0.3, 0.4)) < 1e-12
