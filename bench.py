@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""Throughput benchmark: IISPH dam break at 1M particles, particle-updates/s.
+
+Workload (one "step" = one SPH time step, sim_lib sph/mod.rs:125-144, of the
+whole scene): a 100^3 lattice (spacing 0.01 m, +-1 % seeded jitter, rest
+density 1000) against the -x end of a 2 x 1 x 1 m box handled as a
+VolumeMapBoundary (fields at the reference's dx = 4 * spacing, built on the
+GPU before timing), IISPH with omega 0.5, target density error 0.1 %, at most
+100 sweeps per solve, CFL time step (0.4, dt <= 2e-3), viscosity 0.01, f32
+state. Inputs are synthetic and seeded.
+
+Arms:
+  default          the CUDA engine through the C ABI; `value` is device time
+                   (CUDA events on the engine's stream), `e2e` runs the same
+                   steps through sph_step_host with host buffers in and out.
+  --impl reference the reference's CPU algorithm (the f64 C++ restatement in
+                   oracle/, all host threads) on a bounded sample of the same
+                   configuration (a 50^3 block), same metric.
+Multi-GPU: scenes are independent, so N GPUs run N replicas (weak scaling,
+no collective on the data path); rank 0 prints the JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "fluid-simulation_b200"))
+
+METRIC = "particle-updates/s at 1M IISPH (VolumeMapBoundary dam break)"
+UNIT = "particle-updates/s"
+# Algorithmic bytes per particle for each kernel class (f32 words; neighbor
+# gathers cache-served and counted 0), after the per-pass stream model of the
+# IISPH step: reads/writes of the per-particle SoA state each pass touches.
+BYTES_PER_PARTICLE = {
+    "iisph_jacobi": 60,          # R x,V, acc_p, s, a_ii, p, boundary agg.  W p
+    "iisph_pressure_accel": 52,  # R x,V, m, p, boundary agg.               W acc_p
+    "iisph_source_diag": 72,     # R x,v,a,V,m, boundary agg.              W s,a_ii,p
+    "accel_nonpressure": 60,     # R x,v,V,m, boundary samples             W a, v*
+    "pressure_accel": 64,        # R x,V,m,p,a, boundary agg.              W a
+    "neighbors_density": 32,     # R x, boundary agg.                      W V
+    "boundary_samples": 28,      # R x                                     W samples
+    "integrate_key": 60,         # R x,v,a                                 W x,v
+    "sort": 84,                  # R x,key,idx; permute x,v,ids
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    p.add_argument("--n-side", type=int, default=100)
+    p.add_argument("--max-iters", type=int, default=100)
+    p.add_argument("--cpu-sample-side", type=int, default=50)
+    p.add_argument("--cpu-steps", type=int, default=2)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--profile", action="store_true", help="per-kernel CUDA-event timing (default on)")
+    return p.parse_args()
+
+
+def scene(n_side, max_iters):
+    from sphgpu import scenes
+    sc = scenes.dam_break_iisph_box(n_side=n_side)
+    sc.parameters = dict(sc.parameters, max_solver_iterations=max_iters)
+    return sc
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def run_cpu(n_side, steps, warmup, max_iters, fields):
+    """The reference's CPU algorithm (oracle restatement, all host threads) on
+    a bounded n_side^3 sample of the workload. Returns (updates/s, seconds, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from sphgpu.system import PROCEDURES
+    sc = scene(n_side, max_iters)
+    cfg = dict(sc.parameters)
+    cfg.update(integration_scheme=PROCEDURES["integration_scheme"][sc.procedures["integration_scheme"]],
+               pressure_solver=PROCEDURES["pressure_solver"][sc.procedures["pressure_solver"]],
+               boundary_handling=1, cfl_time_step=1, time_increment=0.0)
+    cfg.pop("device", None)
+    s = O.OracleSystem(cfg)
+    s.upload_fluid(sc.position, None, sc.mass)
+    s.add_volume_map_boundary(O.Field(fields[0].x_min, fields[0].x_max, fields[0].dx, fields[0].n,
+                                      fields[0].nodes),
+                              O.Field(fields[1].x_min, fields[1].x_max, fields[1].dx, fields[1].n,
+                                      fields[1].nodes))
+    s.initialize()
+    if warmup:
+        s.step(warmup)
+    t0 = time.perf_counter()
+    updates = 0
+    for _ in range(steps):
+        s.step(1)
+        updates += s.n
+    dt = time.perf_counter() - t0
+    return updates / dt, dt, O.num_threads(), sc.position.shape[0]
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return reference_arm(args, ws, rank)
+    import torch
+    import torch.distributed as dist
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    from sphgpu import capi, scenes
+    from sphgpu.fields import build_volume_map_fields
+
+    sc = scene(args.n_side, args.max_iters)
+    verts, faces = sc.mesh
+    sp = sc.parameters["rest_density_grid_spacing"]
+    fields = build_volume_map_fields(verts, faces, 4 * sp, sc.parameters["kernel_support_radius"],
+                                     30, device=local)
+    sysm = scenes.build_system(sc, precision="f32", device=local, fields=fields)
+    stream = torch.cuda.ExternalStream(sysm.stream(), device=local)
+    for _ in range(args.warmup):
+        sysm.step_forward_in_time(1)
+    launches0 = sysm.launch_count()
+    sysm.set_profiling(True)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    updates, iters = 0, []
+    for _ in range(args.steps):
+        sysm.step_forward_in_time(1)
+        st = sysm.step_stats()
+        updates += st["particles"]
+        iters.append(st["solver_iterations"])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches = sysm.launch_count() - launches0
+    kernel_times = {}
+    for name in BYTES_PER_PARTICLE:
+        kt = sysm.kernel_time(name)
+        if kt:
+            kernel_times[name] = kt
+    sysm.set_profiling(False)
+    # whole-job aggregate: sum of updates over ranks / max time over ranks
+    if ws > 1:
+        t = torch.tensor([ms, float(updates)], device="cuda", dtype=torch.float64)
+        tmax = t.clone()
+        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+        ms_max, total_updates = float(tmax[0]), float(t[1])
+    else:
+        ms_max, total_updates = ms, float(updates)
+    value = total_updates / (ms_max / 1000.0)
+
+    # e2e: the plugin call with host buffers (reference order), copies inside
+    e2e = None
+    if not args.no_e2e:
+        n = sysm.n
+        xin = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+        vin = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+        xout = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+        vout = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+        xin.numpy()[:] = sysm.download(capi.FIELD_POSITION)
+        vin.numpy()[:] = sysm.download(capi.FIELD_VELOCITY)
+        torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e_updates = 0
+        for _ in range(args.steps):
+            sysm.step_host(1, xin, vin, xout, vout)
+            e_updates += sysm.n
+            xin, xout = xout, xin
+            vin, vout = vout, vin
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if ws > 1:
+            t = torch.tensor([ems, float(e_updates)], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
+            dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
+            ems, e_updates = float(t[0]), float(t[1])
+        e2e = {"value": e_updates / (ems / 1000.0), "unit": UNIT,
+               "h2d_bytes_per_step": 2 * 3 * 8 * n, "d2h_bytes_per_step": 2 * 3 * 8 * n}
+
+    peak, peak_kind = peaks()
+    roofline = None
+    if kernel_times:
+        dom = max(kernel_times, key=lambda k: kernel_times[k][0])
+        tot_ms, cnt = kernel_times[dom]
+        avg_s = tot_ms / cnt / 1000.0
+        n_particles = updates / max(args.steps, 1)
+        bytes_per_launch = BYTES_PER_PARTICLE[dom] * n_particles
+        achieved = bytes_per_launch / avg_s / 1e9
+        roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
+                    "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                    "traffic": None, "bytes_per_launch": bytes_per_launch,
+                    "avg_launch_us": round(avg_s * 1e6, 2), "launches": cnt,
+                    "kernel_share": {k: round(v[0] / sum(x[0] for x in kernel_times.values()), 4)
+                                     for k, v in sorted(kernel_times.items(), key=lambda kv: -kv[1][0])}}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        v, secs, cores, n_cpu = run_cpu(args.cpu_sample_side, args.cpu_steps, 0, args.max_iters, fields)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{args.cpu_steps} steps of a {n_cpu}-particle ({args.cpu_sample_side}^3) block of "
+                         f"the same configuration, f64 C++ restatement of the reference CPU path, "
+                         f"{secs:.1f} s"}
+
+    if ws > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice + jitter)",
+            "config": {"workload": f"IISPH dam break, {args.n_side}^3 particles, 2x1x1 m VolumeMapBoundary box",
+                       "particles_per_gpu": args.n_side ** 3, "solver": "IISPH", "omega": 0.5,
+                       "target_density_error_pct": 0.1, "max_solver_iterations": args.max_iters,
+                       "cfl": 0.4, "max_dt": 2e-3, "precision": "f32 state, f64 reductions",
+                       "parallelism": f"replicas x{ws}",
+                       "l2": "working set > L2 (neighbor lists alone exceed 126 MB); no flush needed",
+                       "mean_solver_iterations": statistics.mean(iters) if iters else None},
+            "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    # the CPU arm needs the same boundary fields; build them with the oracle's
+    # CPU restatement of the reference's field construction when no GPU build
+    # is available (bounded: coarse box fields, once)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sc = scene(args.cpu_sample_side, args.max_iters)
+    verts, faces = sc.mesh
+    sp = sc.parameters["rest_density_grid_spacing"]
+    sdf, vm = O.build_fields(verts, faces, 4 * sp, sc.parameters["kernel_support_radius"], 30)
+    v, secs, cores, n_cpu = run_cpu(args.cpu_sample_side, args.steps, args.warmup, args.max_iters, (sdf, vm))
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs * 1000.0 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice + jitter)",
+        "impl": "reference",
+        "config": {"workload": f"IISPH dam break, {args.n_side}^3 particles, 2x1x1 m VolumeMapBoundary box",
+                   "sample_particles": n_cpu, "max_solver_iterations": args.max_iters},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} timed steps of a {n_cpu}-particle ({args.cpu_sample_side}^3) "
+                                   f"block of the same configuration (f64 C++ restatement of the reference CPU "
+                                   f"path; the Rust reference cannot be built here)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

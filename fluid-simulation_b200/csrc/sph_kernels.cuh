@@ -1082,11 +1082,31 @@ __global__ void __launch_bounds__(kBlock) k_measure(Scalars* __restrict__ sc,
     const double vx = v.x, vy = v.y, vz = v.z;
     ke = 0.5 * (double)v.w * ((vx * vx + vy * vy) + vz * vz);
   }
-  double t0, t1;
   const double b0 = block_sum(de, sh);
-  if (last_block_total(b0, partials, &sc->done_blocks, &t0, sh)) out[0] = t0;
   const double b1 = block_sum(ke, sh);
-  if (last_block_total(b1, partials + gridDim.x, &sc->done_blocks, &t1, sh)) out[1] = t1;
+  // one completion counter for both sums
+  __shared__ bool is_last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = b0;
+    partials[gridDim.x + blockIdx.x] = b1;
+    __threadfence();
+    is_last = atomicAdd(&sc->done_blocks, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  double s0 = 0, s1 = 0;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    s0 += ((volatile double*)partials)[b];
+    s1 += ((volatile double*)partials)[gridDim.x + b];
+  }
+  s0 = block_sum(s0, sh);
+  s1 = block_sum(s1, sh);
+  if (threadIdx.x == 0) {
+    out[0] = s0;
+    out[1] = s1;
+    sc->done_blocks = 0;
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/sphgpu.h"
+#include "sph_fields.cuh"
 #include "sph_kernels.cuh"
 
 namespace sph {
@@ -129,12 +130,49 @@ class SystemBase {
   virtual uint64_t hash_collisions() = 0;
   virtual void restore(uint64_t steps, double time, size_t n, const double* x, const double* v,
                        const double* m, const uint32_t* fid, const double* xi, const double* vi) = 0;
+  virtual int step_host(uint32_t n, const double* xi, const double* vi, double* xo, double* vo) = 0;
+  virtual void* stream() const = 0;
+  virtual void step_stats(sph_step_stats* out) const = 0;
   virtual uint64_t launches() const = 0;
   virtual void set_profiling(bool on) = 0;
   virtual bool kernel_time(const std::string& name, double* ms, uint64_t* count) = 0;
   virtual size_t device_bytes() const = 0;
   int device = 0;
 };
+
+// Host-buffer state exchange in reference index order (sph_step_host).
+template <class R>
+__global__ void k_state_in(int n, const uint32_t* __restrict__ ref, const double* __restrict__ x,
+                           const double* __restrict__ v, R4<R>* __restrict__ pos, R4<R>* __restrict__ vel) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= n) return;
+  const size_t r = ref[d];
+  if (x) {
+    R4<R> p = pos[d];
+    p.x = (R)x[3 * r]; p.y = (R)x[3 * r + 1]; p.z = (R)x[3 * r + 2];
+    pos[d] = p;
+  }
+  if (v) {
+    R4<R> q = vel[d];
+    q.x = (R)v[3 * r]; q.y = (R)v[3 * r + 1]; q.z = (R)v[3 * r + 2];
+    vel[d] = q;
+  }
+}
+template <class R>
+__global__ void k_state_out(int n, const uint32_t* __restrict__ ref, const R4<R>* __restrict__ xv,
+                            const R4<R>* __restrict__ vel, double* __restrict__ x, double* __restrict__ v) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= n) return;
+  const size_t r = ref[d];
+  if (x) {
+    const R4<R> p = xv[d];
+    x[3 * r] = (double)p.x; x[3 * r + 1] = (double)p.y; x[3 * r + 2] = (double)p.z;
+  }
+  if (v) {
+    const R4<R> q = vel[d];
+    v[3 * r] = (double)q.x; v[3 * r + 1] = (double)q.y; v[3 * r + 2] = (double)q.z;
+  }
+}
 
 // ---------------------------------------------------------------------------
 // System<R>
@@ -481,6 +519,46 @@ class System : public SystemBase {
   void restore(uint64_t steps, double time, size_t n, const double* x, const double* v,
                const double* m, const uint32_t* fid, const double* xi, const double* vi) override;
 
+  int step_host(uint32_t nsteps, const double* xi, const double* vi, double* xo, double* vo) override {
+    if (!initialized_) throw Error(SPH_ERR_STATE, "initialize before stepping");
+    const size_t n3 = 3 * n_;
+    const int nb = blocks_for((long long)n_);
+    if (xi || vi) {
+      stage_x_.alloc(std::max<size_t>(n3, 3));
+      stage_v_.alloc(std::max<size_t>(n3, 3));
+      if (xi) cuda_check(cudaMemcpyAsync(stage_x_.p, xi, n3 * sizeof(double), cudaMemcpyHostToDevice, stream_), "H2D");
+      if (vi) cuda_check(cudaMemcpyAsync(stage_v_.p, vi, n3 * sizeof(double), cudaMemcpyHostToDevice, stream_), "H2D");
+      launch("state_io", k_state_in<R>, dim3(nb), dim3(kBlock), (int)n_, (const uint32_t*)ref_.p,
+             (const double*)(xi ? stage_x_.p : nullptr), (const double*)(vi ? stage_v_.p : nullptr), pos_.p, vel_.p);
+      // the positions the step integrates from live in xv too
+      if (xi) cuda_check(cudaMemcpyAsync(xv_.p, pos_.p, n_ * sizeof(R4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
+    }
+    const int st = step(nsteps);
+    if (xo || vo) {
+      stage_x_.alloc(std::max<size_t>(n3, 3));
+      stage_v_.alloc(std::max<size_t>(n3, 3));
+      launch("state_io", k_state_out<R>, dim3(blocks_for((long long)n_)), dim3(kBlock), (int)n_,
+             (const uint32_t*)ref_.p, (const R4<R>*)xv_.p, (const R4<R>*)vel_.p, xo ? stage_x_.p : nullptr,
+             vo ? stage_v_.p : nullptr);
+      if (xo) cuda_check(cudaMemcpyAsync(xo, stage_x_.p, 3 * n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H");
+      if (vo) cuda_check(cudaMemcpyAsync(vo, stage_v_.p, 3 * n_ * sizeof(double), cudaMemcpyDeviceToHost, stream_), "D2H");
+      sync();
+    }
+    return st;
+  }
+  void* stream() const override { return (void*)stream_; }
+  void step_stats(sph_step_stats* o) const override {
+    std::memset(o, 0, sizeof *o);
+    o->particles = n_;
+    o->solver_iterations = (uint32_t)h_sc_->iterations;
+    o->solver_iterations_first = (uint32_t)h_sc_->iterations_eqs1;
+    o->max_neighbors = (uint32_t)h_sc_->max_nbrs;
+    o->max_boundary_neighbors = (uint32_t)h_sc_->max_bnbrs;
+    o->predicted_density_error = h_sc_->err;
+    o->time_increment = h_sc_->dt;
+    o->average_density = h_sc_->avg_density;
+    o->not_converged = h_sc_->status == 2;
+  }
   uint64_t launches() const override { return launches_; }
   void set_profiling(bool on) override { profiling_ = on; }
   bool kernel_time(const std::string& name, double* ms, uint64_t* count) override {
@@ -537,7 +615,7 @@ class System : public SystemBase {
   DBuf<R> press_, s_, aii_, bW_, rho_pred_;
   DBuf<uint32_t> ref_, ref2_, fid_, fid2_, key_, slot_, perm_, nbr_, ncnt_;
   DBuf<uint32_t> count_, start_, tile_sums_;
-  DBuf<double> partials_, body_partials_;
+  DBuf<double> partials_, body_partials_, stage_x_, stage_v_;
   // boundaries
   std::vector<Body> bodies_;
   DBuf<Body> bodies_d_;
@@ -1431,6 +1509,27 @@ int sph_step(sph_system_t* h, uint32_t n) {
   return rc != SPH_OK ? rc : st;
 }
 
+int sph_step_host(sph_system_t* h, uint32_t n, const double* xi, const double* vi, double* xo, double* vo) {
+  int st = SPH_OK;
+  int rc = guarded([&] {
+    if (!h) throw Error(SPH_ERR_INVALID, "null argument");
+    set_device(h);
+    st = h->impl->step_host(n, xi, vi, xo, vo);
+  });
+  return rc != SPH_OK ? rc : st;
+}
+int sph_get_step_stats(const sph_system_t* h, sph_step_stats* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    h->impl->step_stats(out);
+  });
+}
+int sph_get_stream(const sph_system_t* h, void** stream) {
+  return guarded([&] {
+    if (!h || !stream) throw Error(SPH_ERR_INVALID, "null argument");
+    *stream = h->impl->stream();
+  });
+}
 int sph_time(const sph_system_t* h, double* out) {
   return guarded([&] {
     if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
@@ -1645,5 +1744,183 @@ int sph_device_bytes(const sph_system_t* h, size_t* out) {
 }
 
 const char* sph_last_error(void) { return sph::g_last_error.c_str(); }
+
+}  // extern "C"
+
+// ---- volume-map field construction ----------------------------------------------
+static void mesh_aabb(const double* v, size_t nv, double mn[3], double mx[3]) {
+  for (int d = 0; d < 3; ++d) { mn[d] = INFINITY; mx[d] = -INFINITY; }
+  for (size_t i = 0; i < nv; ++i)
+    for (int d = 0; d < 3; ++d) {
+      mn[d] = std::min(mn[d], v[3 * i + d]);
+      mx[d] = std::max(mx[d], v[3 * i + d]);
+    }
+}
+
+extern "C" int sph_volume_map_grids(const double* verts, size_t nv, double dx, double r, sph_grid_desc* sg,
+                         sph_grid_desc* vg) {
+  return guarded([&] {
+    if (!verts || nv == 0 || !sg || !vg || !(dx > 0) || !(r > 0)) throw Error(SPH_ERR_INVALID, "invalid argument");
+    double mn[3], mx[3];
+    mesh_aabb(verts, nv, mn, mx);
+    const double pads[2] = {3.1 * r, 2.0 * r + dx / 6.0};
+    sph_grid_desc* gs[2] = {sg, vg};
+    for (int w = 0; w < 2; ++w) {
+      for (int d = 0; d < 3; ++d) {
+        gs[w]->x_min[d] = mn[d] - pads[w];
+        gs[w]->x_max[d] = mx[d] + pads[w];
+        gs[w]->n[d] = (int64_t)std::llround((gs[w]->x_max[d] - gs[w]->x_min[d]) / dx);
+        if (gs[w]->n[d] < 1) throw Error(SPH_ERR_INVALID, "grid has no cells");
+      }
+      gs[w]->dx = dx;
+    }
+  });
+}
+
+static sph::LatticeDesc lattice_of(const sph_grid_desc& g) {
+  sph::LatticeDesc L;
+  for (int d = 0; d < 3; ++d) {
+    L.xmin[d] = g.x_min[d];
+    L.n[d] = g.n[d];
+  }
+  L.dx = g.dx;
+  L.NX = 3 * g.n[0] + 1;
+  L.NY = 3 * g.n[1] + 1;
+  L.NZ = 3 * g.n[2] + 1;
+  return L;
+}
+
+template <class T>
+static T* dev_upload(const T* h, size_t n) {
+  T* d = nullptr;
+  sph::cuda_check(cudaMalloc((void**)&d, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  if (n) sph::cuda_check(cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy");
+  return d;
+}
+
+static void prune_and_download(const sph::LatticeDesc& L, double* raw, int has_lo, double lo, int has_hi,
+                               double hi, double* out) {
+  const long long total = L.NX * L.NY * L.NZ;
+  const long long ncell = L.n[0] * L.n[1] * L.n[2];
+  unsigned char* keep = nullptr;
+  double* fin = nullptr;
+  sph::cuda_check(cudaMalloc((void**)&keep, total), "cudaMalloc");
+  sph::cuda_check(cudaMalloc((void**)&fin, total * sizeof(double)), "cudaMalloc");
+  cudaMemset(keep, 0, total);
+  sph::k_prune_cells<<<(unsigned)((ncell + 255) / 256), 256>>>(L, raw, has_lo, lo, has_hi, hi, keep);
+  sph::k_apply_keep<<<(unsigned)((total + 255) / 256), 256>>>(total, raw, keep, fin);
+  sph::cuda_check(cudaGetLastError(), "prune");
+  sph::cuda_check(cudaMemcpy(out, fin, total * sizeof(double), cudaMemcpyDeviceToHost), "cudaMemcpy");
+  cudaFree(keep);
+  cudaFree(fin);
+}
+
+extern "C" {
+
+int sph_build_sdf_field(const double* verts, size_t nv, const uint32_t* faces, size_t nf, const sph_grid_desc* g,
+                        double r, double* out, int device) {
+  return guarded([&] {
+    if (!verts || !faces || !g || !out || nf == 0) throw Error(SPH_ERR_INVALID, "invalid argument");
+    sph::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    sph::upload_serendipity_tables();
+    // per-triangle geometry and pseudo-normals
+    auto V = [&](uint32_t i, int d) { return verts[3 * (size_t)i + d]; };
+    std::vector<double> tri(9 * nf), fn(3 * nf), en(9 * nf, 0.0), vn(9 * nf, 0.0);
+    for (size_t t = 0; t < nf; ++t) {
+      for (int k = 0; k < 3; ++k)
+        for (int d = 0; d < 3; ++d) {
+          if (faces[3 * t + k] >= nv) throw Error(SPH_ERR_INVALID, "face index out of range");
+          tri[9 * t + 3 * k + d] = V(faces[3 * t + k], d);
+        }
+      const double* a = &tri[9 * t];
+      const double e1[3] = {a[3] - a[0], a[4] - a[1], a[5] - a[2]}, e2[3] = {a[6] - a[0], a[7] - a[1], a[8] - a[2]};
+      const double n[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+      const double nn = std::sqrt((n[0] * n[0] + n[1] * n[1]) + n[2] * n[2]);
+      for (int d = 0; d < 3; ++d) fn[3 * t + d] = n[d] / nn;
+    }
+    auto angle_at = [&](size_t t, uint32_t vid) {
+      const uint32_t i0 = faces[3 * t], i1 = faces[3 * t + 1], i2 = faces[3 * t + 2];
+      uint32_t o1, o2;
+      if (vid == i0) { o1 = i1; o2 = i2; } else if (vid == i1) { o1 = i2; o2 = i0; } else { o1 = i0; o2 = i1; }
+      double e1[3], e2[3];
+      for (int d = 0; d < 3; ++d) { e1[d] = V(o1, d) - V(vid, d); e2[d] = V(o2, d) - V(vid, d); }
+      double cs = ((e1[0] * e2[0] + e1[1] * e2[1]) + e1[2] * e2[2]) /
+                  (std::sqrt((e1[0] * e1[0] + e1[1] * e1[1]) + e1[2] * e1[2]) *
+                   std::sqrt((e2[0] * e2[0] + e2[1] * e2[1]) + e2[2] * e2[2]));
+      cs = std::max(-1.0, std::min(1.0, cs));
+      return std::acos(cs);
+    };
+    std::vector<std::vector<size_t>> incident(nv);
+    for (size_t t = 0; t < nf; ++t)
+      for (int k = 0; k < 3; ++k) incident[faces[3 * t + k]].push_back(t);
+    for (size_t t = 0; t < nf; ++t) {
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t vid = faces[3 * t + k];
+        for (size_t u : incident[vid]) {
+          const double ang = angle_at(u, vid);
+          for (int d = 0; d < 3; ++d) vn[9 * t + 3 * k + d] += fn[3 * u + d] * ang;
+        }
+        const uint32_t ea = faces[3 * t + k], eb = faces[3 * t + (k + 1) % 3];
+        for (size_t u : incident[ea]) {
+          bool hb = false;
+          for (int m = 0; m < 3; ++m) hb |= faces[3 * u + m] == eb;
+          if (hb)
+            for (int d = 0; d < 3; ++d) en[9 * t + 3 * k + d] += fn[3 * u + d];
+        }
+      }
+    }
+    sph::MeshDev M;
+    double* dtri = dev_upload(tri.data(), tri.size());
+    double* dfn = dev_upload(fn.data(), fn.size());
+    double* den = dev_upload(en.data(), en.size());
+    double* dvn = dev_upload(vn.data(), vn.size());
+    M.tri = dtri; M.fn = dfn; M.en = den; M.vn = dvn; M.nt = (int)nf;
+    const sph::LatticeDesc L = lattice_of(*g);
+    const long long total = L.NX * L.NY * L.NZ;
+    double* raw = nullptr;
+    sph::cuda_check(cudaMalloc((void**)&raw, total * sizeof(double)), "cudaMalloc");
+    sph::k_sdf_nodes<<<(unsigned)((total + 255) / 256), 256>>>(M, L, raw);
+    sph::cuda_check(cudaGetLastError(), "k_sdf_nodes");
+    const double pad = 3.1 * r;
+    prune_and_download(L, raw, 1, -pad, 1, pad, out);
+    cudaFree(raw); cudaFree(dtri); cudaFree(dfn); cudaFree(den); cudaFree(dvn);
+  });
+}
+
+int sph_build_volume_map_field(const sph_grid_desc* sg, const double* sdf_nodes, const sph_grid_desc* vg, double r,
+                               int degree, double* out, int device) {
+  return guarded([&] {
+    if (!sg || !sdf_nodes || !vg || !out || degree < 1 || degree > sph::kMaxGL)
+      throw Error(SPH_ERR_INVALID, "invalid argument");
+    sph::cuda_check(cudaSetDevice(device), "cudaSetDevice");
+    sph::upload_serendipity_tables();
+    std::vector<double> gx, gw;
+    sph::gauss_legendre_nodes(degree, gx, gw);
+    sph::cuda_check(cudaMemcpyToSymbol(sph::c_gl_x, gx.data(), degree * sizeof(double)), "gl nodes");
+    sph::cuda_check(cudaMemcpyToSymbol(sph::c_gl_w, gw.data(), degree * sizeof(double)), "gl weights");
+    const sph::LatticeDesc LS = lattice_of(*sg);
+    const size_t ns = (size_t)(LS.NX * LS.NY * LS.NZ);
+    double* dsdf = dev_upload(sdf_nodes, ns);
+    sph::DevField F;
+    for (int d = 0; d < 3; ++d) {
+      F.xmin[d] = sg->x_min[d];
+      F.xmax[d] = sg->x_max[d];
+      F.n[d] = (int)sg->n[d];
+    }
+    F.dx = sg->dx;
+    F.NX = LS.NX;
+    F.NY = LS.NY;
+    F.nodes = dsdf;
+    const sph::LatticeDesc L = lattice_of(*vg);
+    const long long total = L.NX * L.NY * L.NZ;
+    double* raw = nullptr;
+    sph::cuda_check(cudaMalloc((void**)&raw, total * sizeof(double)), "cudaMalloc");
+    sph::k_volume_map_nodes<<<(unsigned)total, 256>>>(F, L, r, degree, raw);
+    sph::cuda_check(cudaGetLastError(), "k_volume_map_nodes");
+    prune_and_download(L, raw, 1, 0.0, 0, 0.0, out);
+    cudaFree(raw);
+    cudaFree(dsdf);
+  });
+}
 
 }  // extern "C"

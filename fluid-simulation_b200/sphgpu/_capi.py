@@ -84,6 +84,14 @@ class SphMeasurement(C.Structure):
     ]
 
 
+class SphStepStats(C.Structure):
+    _fields_ = [("particles", C.c_uint64), ("solver_iterations", C.c_uint32),
+                ("solver_iterations_first", C.c_uint32), ("max_neighbors", C.c_uint32),
+                ("max_boundary_neighbors", C.c_uint32), ("predicted_density_error", C.c_double),
+                ("time_increment", C.c_double), ("average_density", C.c_double),
+                ("not_converged", C.c_int)]
+
+
 class SPHError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"sphgpu error {code}: {msg}")
@@ -109,6 +117,9 @@ SIGNATURES = {
                                               _dp, C.POINTER(SphRigidInit), C.POINTER(C.c_int)]),
     "sph_initialize": (C.c_int, [_vp]),
     "sph_step": (C.c_int, [_vp, C.c_uint32]),
+    "sph_step_host": (C.c_int, [_vp, C.c_uint32, _vp, _vp, _vp, _vp]),
+    "sph_get_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "sph_get_step_stats": (C.c_int, [_vp, C.POINTER(SphStepStats)]),
     "sph_time": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "sph_time_steps_propagated": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "sph_take_measurement": (C.c_int, [_vp, C.POINTER(SphMeasurement)]),
@@ -130,6 +141,12 @@ SIGNATURES = {
                                                    C.POINTER(_sz), C.c_int]),
     "sph_kernel_function": (C.c_int, [_sz, _dp, C.c_double, _dp, C.c_int, C.c_int]),
     "sph_kernel_gradient": (C.c_int, [_sz, _dp, C.c_double, _dp, C.c_int, C.c_int]),
+    "sph_volume_map_grids": (C.c_int, [_dp, _sz, C.c_double, C.c_double, C.POINTER(SphGridDesc),
+                                       C.POINTER(SphGridDesc)]),
+    "sph_build_sdf_field": (C.c_int, [_dp, _sz, _u32p, _sz, C.POINTER(SphGridDesc), C.c_double, _dp,
+                                      C.c_int]),
+    "sph_build_volume_map_field": (C.c_int, [C.POINTER(SphGridDesc), _dp, C.POINTER(SphGridDesc),
+                                             C.c_double, C.c_int, _dp, C.c_int]),
     "sph_last_error": (C.c_char_p, []),
     "sph_launch_count": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
     "sph_set_profiling": (C.c_int, [_vp, C.c_int]),

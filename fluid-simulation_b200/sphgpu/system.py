@@ -191,6 +191,32 @@ class GpuSystem:
         """Advance n_steps; returns SPH_OK or SPH_NOT_CONVERGED (capped IISPH)."""
         return A.check(self._L.sph_step(self._h, int(n_steps)), allow=(A.SPH_NOT_CONVERGED,))
 
+    def step_host(self, n_steps, position_in=None, velocity_in=None, position_out=None,
+                  velocity_out=None) -> int:
+        """sph_step_host: host arrays (reference order, float64 [n,3]) in and out;
+        pinned arrays (e.g. torch pin_memory) make the copies fastest."""
+        def ptr(a):
+            if a is None:
+                return None
+            if hasattr(a, "data_ptr"):
+                return C.c_void_p(a.data_ptr())
+            return a.ctypes.data_as(C.c_void_p)
+        return A.check(self._L.sph_step_host(self._h, int(n_steps), ptr(position_in), ptr(velocity_in),
+                                             ptr(position_out), ptr(velocity_out)),
+                       allow=(A.SPH_NOT_CONVERGED,))
+
+    def step_stats(self) -> dict:
+        """Scalars of the last update (no device work)."""
+        st = A.SphStepStats()
+        A.check(self._L.sph_get_step_stats(self._h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in A.SphStepStats._fields_}
+
+    def stream(self) -> int:
+        """cudaStream_t of the handle as an integer (torch.cuda.ExternalStream)."""
+        s = C.c_void_p()
+        A.check(self._L.sph_get_stream(self._h, C.byref(s)))
+        return s.value or 0
+
     def take_measurement(self) -> dict:
         m = A.SphMeasurement()
         A.check(self._L.sph_take_measurement(self._h, C.byref(m)))

@@ -166,7 +166,7 @@ typedef struct sph_system sph_system_t;
  * rejects in SystemConstructor::new (sph/setup/mod.rs:229-244). */
 int sph_create(const sph_config* cfg, sph_system_t** out);
 void sph_destroy(sph_system_t* h);
-/* Deep copy of all device state (SPHSystem: DynClone, BE/lib.rs:111). */
+/* Deep copy of all device state (SPHSystem: DynClone, sci-phi-backend/src/lib.rs:111). */
 int sph_clone(const sph_system_t* h, sph_system_t** out);
 
 /* Fluid samples (Fluid::add_samples fluid.rs:79-104 / the `--state` restore
@@ -196,6 +196,17 @@ int sph_initialize(sph_system_t* h);
 /* Advances n_steps time steps. Returns SPH_NOT_CONVERGED (after finishing
  * all steps) if an IISPH solve hit the configured iteration cap. */
 int sph_step(sph_system_t* h, uint32_t n_steps);
+/* The plugin-style step on host buffers: overwrites the fluid's positions and
+ * velocities from host arrays (reference index order, 3n doubles each; either
+ * may be NULL to keep the device state), advances n_steps, and copies the new
+ * positions and velocities back (either output may be NULL). Host-to-device
+ * and device-to-host copies are part of the call; pinned buffers make them
+ * fastest. */
+int sph_step_host(sph_system_t* h, uint32_t n_steps, const double* position_in,
+                  const double* velocity_in, double* position_out, double* velocity_out);
+/* The CUDA stream (cudaStream_t) every kernel of this handle runs on, for
+ * callers that time or order work against it. */
+int sph_get_stream(const sph_system_t* h, void** stream);
 int sph_time(const sph_system_t* h, double* out);                         /* :107-116 */
 int sph_time_steps_propagated(const sph_system_t* h, uint64_t* out);     /* :118-120 */
 int sph_take_measurement(sph_system_t* h, sph_measurement* out);          /* :147-184 */
@@ -252,7 +263,41 @@ int sph_kernel_function(size_t n, const double* r, double h, double* out_w, int 
 int sph_kernel_gradient(size_t n, const double* r, double h, double* out_grad, int precision,
                         int device);
 
+/* ---- volume-map field construction (volume_map_boundary.rs:1547-1741) --- */
+/* Grids of a closed triangle mesh's fields: the signed-distance field over the
+ * mesh AABB padded by 3.1 r, the volume map padded by 2 r + dx/6, with n =
+ * round(extent / dx) cells per axis (discretization.rs:99-113). */
+int sph_volume_map_grids(const double* verts, size_t nv, double dx, double kernel_support_radius,
+                         sph_grid_desc* sdf_grid, sph_grid_desc* vm_grid);
+/* Signed-distance node values of the mesh (3*nv vertex coordinates, 3*nf
+ * vertex indices; the side the face winding points to is positive), pruned to
+ * the band |sd| <= 3.1 r (NaN elsewhere). nodes_out: (3n_x+1)(3n_y+1)(3n_z+1). */
+int sph_build_sdf_field(const double* verts, size_t nv, const uint32_t* faces, size_t nf,
+                        const sph_grid_desc* grid, double kernel_support_radius, double* nodes_out,
+                        int device);
+/* Volume-map node values: the Gauss-Legendre ball integral (degree
+ * `quadrature_degree`, the reference uses 30) of the cubic extension function
+ * of the discretized signed distance, clamped to [0, 4/3 pi r^3]. */
+int sph_build_volume_map_field(const sph_grid_desc* sdf_grid, const double* sdf_nodes,
+                               const sph_grid_desc* vm_grid, double kernel_support_radius,
+                               int quadrature_degree, double* nodes_out, int device);
+
 /* ---- diagnostics -------------------------------------------------------- */
+/* Scalars of the last completed update, read from the host copy the step
+ * already made (no device work). */
+typedef struct sph_step_stats {
+  uint64_t particles;           /* active particles after the update */
+  uint32_t solver_iterations;   /* IISPH sweeps of the (last) pressure solve */
+  uint32_t solver_iterations_first; /* IISPHwOST: sweeps of the first solve */
+  uint32_t max_neighbors;       /* largest fluid neighbor count (self excluded) */
+  uint32_t max_boundary_neighbors;
+  double predicted_density_error;
+  double time_increment;        /* dt the next step integrates with */
+  double average_density;
+  int not_converged;            /* 1 if the solve stopped at max_solver_iterations */
+} sph_step_stats;
+int sph_get_step_stats(const sph_system_t* h, sph_step_stats* out);
+
 const char* sph_last_error(void);
 /* Kernel launches issued by this handle since creation (all of its CUDA
  * kernels, every step). */

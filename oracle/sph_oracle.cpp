@@ -1166,7 +1166,7 @@ void System::resolve_pressure_globally(bool after_iteration, uint32_t n_after, d
   double err = std::numeric_limits<double>::infinity();
   auto converged = [&]() {  // :378-393
     if (after_iteration) return it_count > n_after;
-    return (it_count > 2 && err < tde) || it_count > sp.iteration_cap;
+    return (it_count > 2 && err < tde) || it_count >= sp.iteration_cap;
   };
   std::vector<double> e(n);
   while (!converged()) {

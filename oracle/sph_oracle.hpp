@@ -325,7 +325,7 @@ struct SolverParams {
   double target_density_error = 0.1;
   double relaxation_factor = 0.5;
   double min_diagonal_element = 1e-10;
-  uint32_t iteration_cap = 0xffffffffu;  // reference: u32::MAX
+  uint32_t iteration_cap = 0xffffffffu;  // sweeps; the reference has none (u32::MAX)
 };
 
 struct IISPHState {

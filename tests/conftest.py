@@ -35,6 +35,7 @@ def oracle_config(scene):
     cfg = dict(scene.parameters)
     cfg.pop("device", None)
     cfg.pop("neighbor_capacity", None)
+    cfg.setdefault("max_solver_iterations", 0)
     cfg["integration_scheme"] = PROCEDURES["integration_scheme"][scene.procedures["integration_scheme"]]
     cfg["pressure_solver"] = PROCEDURES["pressure_solver"][scene.procedures["pressure_solver"]]
     cfg["boundary_handling"] = PROCEDURES["boundary_handling"][scene.procedures["boundary_handling"]]

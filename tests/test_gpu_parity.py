@@ -141,10 +141,17 @@ def test_sesph_multistep_tracks_oracle(A, oracle, sesph_scene):
 # ---------------------------------------------------------------------------------------
 # IISPH with a VolumeMapBoundary box (small, fields built by the oracle)
 # ---------------------------------------------------------------------------------------
+# The reference's volume-map boundary contributes strongly near walls, so an
+# uncapped IISPH solve of this small scene needs hundreds of sweeps; both the
+# engine and the oracle cap it here (the north-star configuration caps at 100).
+VM_CAP = 40
+
+
 @pytest.fixture(scope="module")
 def vm_case(oracle):
     from sphgpu import scenes
     sc = scenes.dam_break_iisph_box(n_side=16, spacing=0.02, box=(0.64, 0.32, 0.32))
+    sc.parameters = dict(sc.parameters, max_solver_iterations=VM_CAP)
     verts, faces = sc.mesh
     sdf, vm = oracle.build_fields(verts, faces, 4 * 0.02, 2 * 0.02, 30)
     o = build_oracle(sc, fields=(sdf, vm))
@@ -183,20 +190,25 @@ def test_iisph_volume_map_first_update_matches_oracle(A, oracle, vm_case, precis
     assert np.max(np.abs(acc_g - acc_o)) <= (1e-7 if precision == "f64" else 5e-2) * ascale
 
 
-def test_iisph_volume_map_steps_track_oracle(A, oracle, vm_case):
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_iisph_volume_map_steps_track_oracle(A, oracle, vm_case, precision):
+    # three steps with CFL time increments (the wall-adjacent layer is pushed
+    # away hard in this configuration, so only a short horizon is compared)
     from sphgpu import scenes
     sc, fields, _ = vm_case
-    g = scenes.build_system(sc, precision="f32", fields=fields)
+    g = scenes.build_system(sc, precision=precision, fields=fields)
     o = build_oracle(sc, fields=fields)
-    for _ in range(5):
-        g.step_forward_in_time(4)
-        o.step(4)
+    for _ in range(3):
+        g.step_forward_in_time(1)
+        o.step(1)
         mg, mo = g.take_measurement(), o.measurement()
-        assert abs(mg["time"] - mo["time"]) < 1e-6 * max(mo["time"], 1e-9)
-        assert abs(mg["time_step_size"] - mo["time_step_size"]) < 1e-5 * mo["time_step_size"]
-        assert abs(mg["density"] - mo["density"]) < 1e-4 * mo["density"]
-        assert abs(mg["solver_iterations"] - mo["solver_iterations"]) <= 1
-        assert abs(mg["predicted_density_error"] - mo["predicted_density_error"]) < 2e-3
+        tol = 1e-8 if precision == "f64" else 1e-4
+        assert abs(mg["time"] - mo["time"]) < tol * mo["time"]
+        assert abs(mg["time_step_size"] - mo["time_step_size"]) < tol * mo["time_step_size"]
+        assert abs(mg["density"] - mo["density"]) < tol * mo["density"]
+        assert mg["solver_iterations"] == mo["solver_iterations"] == VM_CAP
+    x_g, x_o = g.download(A.FIELD_POSITION), o.download(oracle.F_POSITION)
+    assert np.max(np.abs(x_g - x_o)) < (1e-9 if precision == "f64" else 1e-5)
 
 
 # ---------------------------------------------------------------------------------------
