@@ -7,9 +7,9 @@
 //   acc   R4 {ax,ay,az,-}   total acceleration
 //   ref   u32               reference-order index (the row a download writes)
 //   fid   u32               fluid id
-//   nbr   u32 [K][Np]       fluid neighbor lists, neighbor k of particle i at
-//                           nbr[k*Np+i] (coalesced for thread-per-particle);
-//                           self is implicit and not stored
+//   nbr   u32 [Np/32][K/4][32][4]  fluid neighbor lists, warp-tiled: lane
+//                           `i%32` of tile `i/32` keeps neighbors 4g..4g+3 in
+//                           one 16-byte group; self is implicit, not stored
 //   ncnt  u32 [N]           neighbor counts
 //   bW, bG, bGu             per-particle boundary aggregates (see kernels)
 //   IISPH scratch: vstar R4, s R, aii R, accp R4, p R
@@ -70,6 +70,7 @@ struct StepParams {
   R omega, min_diag;
   double tde;            // IISPH target density error (%)
   int iteration_cap;     // 0 = unbounded (reference)
+  int sorted_lists;      // 1: neighbor lists in ascending index order
 };
 
 // Rigid body state, f64 (rigid_body_motion.rs:22-36).

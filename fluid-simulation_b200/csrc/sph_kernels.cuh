@@ -1,7 +1,9 @@
 // CUDA kernels of the SPH step engine (sm_100a). One thread per particle;
-// neighbor lists are stored interleaved (nbr[k*Np+i]) so that a warp's loads
-// of its k-th neighbors are coalesced; gathered neighbor state comes through
-// L1/L2 because the cell sort keeps spatial neighbors close in memory.
+// neighbor lists are stored warp-tiled (see nbr_slot): the 32 particles of a
+// warp own one contiguous block, and each lane reads four consecutive
+// neighbors with one 128-bit load, so a warp streams its lists as 512-byte
+// coalesced, page-local reads. Gathered neighbor state comes through L1/L2
+// because the cell sort keeps spatial neighbors close in memory.
 //
 // Reference functions each kernel restates (paths under simulation_lib/src/):
 //   k_integrate_key      integration_schemes/euler_cromer.rs:12-25,
@@ -346,6 +348,14 @@ __global__ void __launch_bounds__(kBlock) k_gather_samples(
 
 // ---------------------------------------------------------------------------
 // 4. fluid neighbor lists + volume (fused)
+//
+// Neighbor-list layout: particle i = 32*t + lane keeps its k-th neighbor at
+//   ((t * K/4 + k/4) * 32 + lane) * 4 + k % 4      (K a multiple of 4)
+// i.e. tile-major, then groups of four neighbors, then lane.
+__device__ __forceinline__ size_t nbr_slot(int i, int k, int K) {
+  const size_t t = (size_t)(i >> 5), lane = (size_t)(i & 31);
+  return ((t * (size_t)(K >> 2) + (size_t)(k >> 2)) * 32 + lane) * 4 + (size_t)(k & 3);
+}
 // ---------------------------------------------------------------------------
 template <class R>
 __device__ __forceinline__ void kahan_add(R& s, R& c, R t) {
@@ -368,21 +378,36 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
               cz = cell_coord((double)xi.z, P.range);
     R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
     R comp = 0;
-    for (int dz = -1; dz <= 1; ++dz)
-      for (int dy = -1; dy <= 1; ++dy)
-        for (int dx = -1; dx <= 1; ++dx) {
-          const uint32_t k = morton_key(cx + dx, cy + dy, cz + dz, P.mask);
+    // Visit the 27 stencil buckets in ascending key (= memory) order so every
+    // list comes out sorted by neighbor index: lanes of a warp then gather
+    // their k-th neighbors from nearby addresses in the passes that follow.
+    uint32_t keys[27];
+#pragma unroll
+    for (int s = 0; s < 27; ++s)
+      keys[s] = morton_key(cx + (s % 3) - 1, cy + (s / 3) % 3 - 1, cz + s / 9 - 1, P.mask);
+#pragma unroll
+    for (int pass = 0; pass < (P.sorted_lists ? 27 : 0); ++pass) {
+#pragma unroll
+      for (int s = pass & 1; s + 1 < 27; s += 2) {
+        const uint32_t a = keys[s], b = keys[s + 1];
+        keys[s] = min(a, b);
+        keys[s + 1] = max(a, b);
+      }
+    }
+#pragma unroll 1
+    for (int s = 0; s < 27; ++s) {
+          const uint32_t k = keys[s];
           const uint32_t b = start[k], e = start[k + 1];
           for (uint32_t j = b; j < e; ++j) {
             if ((int)j == i) continue;
             const R4<R> xj = pos[j];
             if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
-            if (cnt < P.K) nbr[(size_t)cnt * P.Np + i] = j;
+            if (cnt < P.K) nbr[nbr_slot(i, cnt, P.K)] = j;
             ++cnt;
             const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
             kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
           }
-        }
+    }
     R denom = P.V0 * sum;
     if (has_boundary) denom += bW[i];
     const R V = P.V0 / denom;
@@ -698,10 +723,58 @@ __device__ __forceinline__ void body_accum_flush(double* sh, int nbodies, double
 }
 
 // ---------------------------------------------------------------------------
+// Neighbor gather loop. The stored neighbor indices of NB iterations are
+// fetched first with streaming (evict-first) loads, then the NB gathers are
+// issued, then consumed: NB independent DRAM/L2 round trips in flight per
+// thread instead of one dependent chain per neighbor.
+// ---------------------------------------------------------------------------
+template <int NB, class Load, class Use>
+__device__ __forceinline__ void for_each_neighbor(const uint32_t* __restrict__ nbr, int K, int i,
+                                                  int cnt, Load&& load, Use&& use) {
+  static_assert(NB % 4 == 0, "neighbors are read in groups of four");
+  const uint4* base = reinterpret_cast<const uint4*>(nbr) + nbr_slot(i, 0, K) / 4;
+  for (int k0 = 0; k0 < cnt; k0 += NB) {
+    uint32_t j[NB];
+#pragma unroll
+    for (int g = 0; g < NB / 4; ++g) {
+      // group k0/4+g of this lane sits 32 uint4 after the previous group
+      const uint4 q = k0 + 4 * g < cnt ? __ldcs(base + (size_t)(k0 / 4 + g) * 32) : make_uint4(i, i, i, i);
+      j[4 * g + 0] = k0 + 4 * g + 0 < cnt ? q.x : (uint32_t)i;
+      j[4 * g + 1] = k0 + 4 * g + 1 < cnt ? q.y : (uint32_t)i;
+      j[4 * g + 2] = k0 + 4 * g + 2 < cnt ? q.z : (uint32_t)i;
+      j[4 * g + 3] = k0 + 4 * g + 3 < cnt ? q.w : (uint32_t)i;
+    }
+    decltype(load(0u)) d[NB];
+#pragma unroll
+    for (int u = 0; u < NB; ++u) d[u] = load(j[u]);
+#pragma unroll
+    for (int u = 0; u < NB; ++u)
+      if (k0 + u < cnt) use(d[u]);
+  }
+}
+
+template <class R>
+struct XP {  // position+volume and one scalar
+  R4<R> x;
+  R s;
+};
+template <class R>
+struct XV {  // position+volume and one vector
+  R4<R> x;
+  R4<R> v;
+};
+template <class R>
+struct XVM {  // position+volume, one vector and one scalar
+  R4<R> x;
+  R4<R> v;
+  R m;
+};
+
+// ---------------------------------------------------------------------------
 // 6. accelerations: gravity + viscosity (+ SESPH pressure) (+ v* = v + dt a)
 // ---------------------------------------------------------------------------
 // PRESS: 0 none, 1 SESPH state equation from the volume on the fly
-template <class R, int PRESS>
+template <class R, int PRESS, int NB>
 __global__ void __launch_bounds__(kBlock) k_accel(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B,
@@ -728,22 +801,23 @@ __global__ void __launch_bounds__(kBlock) k_accel(
     R sx = 0, sy = 0, sz = 0;   // viscosity
     R px = 0, py = 0, pz = 0;   // pressure
     const int cnt = min((int)ncnt[i], P.K);
-    for (int k = 0; k < cnt; ++k) {
-      const uint32_t j = nbr[(size_t)k * P.Np + i];
-      const R4<R> xj = xv[j];
-      const R4<R> vj = vel[j];
-      const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-      const R r2 = rx * rx + ry * ry + rz * rz;
-      const R f = kernel_grad_factor(r2, P.k);
-      const R vr = (vi.x - vj.x) * rx + (vi.y - vj.y) * ry + (vi.z - vj.z) * rz;
-      const R s = P.visc_f * xj.w * vr / (r2 + P.eps_visc) * f;
-      sx += s * rx; sy += s * ry; sz += s * rz;
-      if (PRESS == 1) {
-        const R pj = P.stiffness * fmax(P.V0 / xj.w - R(1), R(0));
-        const R t = xj.w * (pi + pj) * f;
-        px += t * rx; py += t * ry; pz += t * rz;
-      }
-    }
+    for_each_neighbor<NB>(
+        nbr, P.K, i, cnt, [&](uint32_t j) { return XV<R>{xv[j], vel[j]}; },
+        [&](const XV<R>& d) {
+          const R4<R>& xj = d.x;
+          const R4<R>& vj = d.v;
+          const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+          const R r2 = rx * rx + ry * ry + rz * rz;
+          const R f = kernel_grad_factor(r2, P.k);
+          const R vr = (vi.x - vj.x) * rx + (vi.y - vj.y) * ry + (vi.z - vj.z) * rz;
+          const R s = P.visc_f * xj.w * vr / (r2 + P.eps_visc) * f;
+          sx += s * rx; sy += s * ry; sz += s * rz;
+          if (PRESS == 1) {
+            const R pj = P.stiffness * fmax(P.V0 / xj.w - R(1), R(0));
+            const R t = xj.w * (pi + pj) * f;
+            px += t * rx; py += t * ry; pz += t * rz;
+          }
+        });
     if (B.kind != 0) {
       BodyAccum acc_b{sh_body};
       for_each_visc_sample<R>(B, xi, i, P, [&](V3<R> xb, V3<R> vb, R Vb, int body) {
@@ -797,7 +871,7 @@ __global__ void __launch_bounds__(kBlock) k_accel(
 // MODE: 0 -> accp = accel (Jacobi probe, overwrite, no reaction forces)
 //       1 -> acc += accel (reaction forces if mirror)
 //       2 -> acc  = accel (reaction forces if mirror)
-template <class R, int MODE>
+template <class R, int MODE, int NB>
 __global__ void __launch_bounds__(kBlock) k_pressure_accel(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     const R* __restrict__ press, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
@@ -813,15 +887,14 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
     const R Vi = xi.w, mi = vel[i].w, pi = press[i];
     R px = 0, py = 0, pz = 0;
     const int cnt = min((int)ncnt[i], P.K);
-    for (int k = 0; k < cnt; ++k) {
-      const uint32_t j = nbr[(size_t)k * P.Np + i];
-      const R4<R> xj = xv[j];
-      const R pj = press[j];
-      const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-      const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
-      const R t = xj.w * (pi + pj) * f;
-      px += t * rx; py += t * ry; pz += t * rz;
-    }
+    for_each_neighbor<NB>(
+        nbr, P.K, i, cnt, [&](uint32_t j) { return XP<R>{xv[j], press[j]}; },
+        [&](const XP<R>& d) {
+          const R rx = xi.x - d.x.x, ry = xi.y - d.x.y, rz = xi.z - d.x.z;
+          const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
+          const R t = d.x.w * (pi + d.s) * f;
+          px += t * rx; py += t * ry; pz += t * rz;
+        });
     if (B.kind != 0) {
       const R4<R> g = B.bG[i];
       const R c = R(2) * P.gamma_p * pi;
@@ -857,7 +930,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
 // ---------------------------------------------------------------------------
 // VP = 1: volume-preserving source s = 1 - V0/V - dt sum ..., VP = 0: the
 // velocity-divergence source of IISPHwOST's first solve.
-template <class R, int VP>
+template <class R, int VP, int NB>
 __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     const R4<R>* __restrict__ vstar, const uint32_t* __restrict__ nbr,
@@ -873,19 +946,19 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
   R sfx = 0, sfy = 0, sfz = 0;     // S_f = sum V_j gradW
   R s2 = 0;                        // sum V_j^2 / m_j |gradW|^2
   const int cnt = min((int)ncnt[i], P.K);
-  for (int k = 0; k < cnt; ++k) {
-    const uint32_t j = nbr[(size_t)k * P.Np + i];
-    const R4<R> xj = xv[j];
-    const R4<R> vsj = vstar[j];
-    const R mj = vel[j].w;
-    const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-    const R r2 = rx * rx + ry * ry + rz * rz;
-    const R f = kernel_grad_factor(r2, P.k);
-    const R Vf = xj.w * f;
-    div += Vf * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
-    sfx += Vf * rx; sfy += Vf * ry; sfz += Vf * rz;
-    s2 += xj.w * xj.w / mj * (f * f * r2);
-  }
+  for_each_neighbor<NB>(
+      nbr, P.K, i, cnt, [&](uint32_t j) { return XVM<R>{xv[j], vstar[j], vel[j].w}; },
+      [&](const XVM<R>& d) {
+        const R4<R>& xj = d.x;
+        const R4<R>& vsj = d.v;
+        const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+        const R r2 = rx * rx + ry * ry + rz * rz;
+        const R f = kernel_grad_factor(r2, P.k);
+        const R Vf = xj.w * f;
+        div += Vf * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
+        sfx += Vf * rx; sfy += Vf * ry; sfz += Vf * rz;
+        s2 += xj.w * xj.w / d.m * (f * f * r2);
+      });
   R bx = 0, by = 0, bz = 0, bdiv = 0;
   if (B.kind != 0) {
     const R4<R> g = B.bG[i];
@@ -909,7 +982,7 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
 // Jacobi sweep: A_i = dt^2 [sum V_j (a_i - a_j) . gradW + a_i . bG];
 // p_i <- max(p_i + omega (s_i - A_i) / a_ii, 0); residual in f64.
 // AFTER >= 0: stop after AFTER+1 sweeps; AFTER < 0: target density error.
-template <class R>
+template <class R, int NB>
 __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
     Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ accp,
     const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B,
@@ -926,14 +999,13 @@ __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
     const R4<R> ai = accp[i];
     R sum = 0;
     const int cnt = min((int)ncnt[i], P.K);
-    for (int k = 0; k < cnt; ++k) {
-      const uint32_t j = nbr[(size_t)k * P.Np + i];
-      const R4<R> xj = xv[j];
-      const R4<R> aj = accp[j];
-      const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-      const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
-      sum += xj.w * f * ((ai.x - aj.x) * rx + (ai.y - aj.y) * ry + (ai.z - aj.z) * rz);
-    }
+    for_each_neighbor<NB>(
+        nbr, P.K, i, cnt, [&](uint32_t j) { return XV<R>{xv[j], accp[j]}; },
+        [&](const XV<R>& d) {
+          const R rx = xi.x - d.x.x, ry = xi.y - d.x.y, rz = xi.z - d.x.z;
+          const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
+          sum += d.x.w * f * ((ai.x - d.v.x) * rx + (ai.y - d.v.y) * ry + (ai.z - d.v.z) * rz);
+        });
     if (B.kind != 0) {
       const R4<R> g = B.bG[i];
       sum += ai.x * g.x + ai.y * g.y + ai.z * g.z;
@@ -1007,7 +1079,7 @@ __global__ void __launch_bounds__(kBlock) k_ost_commit(const Scalars* __restrict
 // SESPHwSplitting predicted density (sesph_with_splitting.rs:90-152) and the
 // state equation: rho* = sum_j [m_j W + dt (v*_i - v*_j) . gradW]
 //                      + (m_i/V0) bW + dt v*_i . bGu, p = k max(V0/(m_i/rho*) - 1, 0)
-template <class R>
+template <class R, int NB>
 __global__ void __launch_bounds__(kBlock) k_split_density(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     const R4<R>* __restrict__ vstar, const uint32_t* __restrict__ nbr,
@@ -1021,17 +1093,17 @@ __global__ void __launch_bounds__(kBlock) k_split_density(
   const R mi = vel[i].w;
   R rho = mi * P.k.cw * R(0.5), comp = 0;  // self term m_i W(0)
   const int cnt = min((int)ncnt[i], P.K);
-  for (int k = 0; k < cnt; ++k) {
-    const uint32_t j = nbr[(size_t)k * P.Np + i];
-    const R4<R> xj = xv[j];
-    const R4<R> vsj = vstar[j];
-    const R mj = vel[j].w;
-    const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-    R w, f;
-    kernel_w_and_grad(rx * rx + ry * ry + rz * rz, P.k, w, f);
-    const R t = mj * w + dt * f * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
-    kahan_add(rho, comp, t);
-  }
+  for_each_neighbor<NB>(
+      nbr, P.K, i, cnt, [&](uint32_t j) { return XVM<R>{xv[j], vstar[j], vel[j].w}; },
+      [&](const XVM<R>& d) {
+        const R4<R>& xj = d.x;
+        const R4<R>& vsj = d.v;
+        const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+        R w, f;
+        kernel_w_and_grad(rx * rx + ry * ry + rz * rz, P.k, w, f);
+        const R t = d.m * w + dt * f * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
+        kahan_add(rho, comp, t);
+      });
   if (B.kind != 0) {
     const R4<R> gu = B.bGu[i];
     rho += B.bW[i] * mi / P.V0 + dt * (vsi.x * gu.x + vsi.y * gu.y + vsi.z * gu.z);

@@ -9,11 +9,13 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/sphgpu.h"
@@ -182,6 +184,11 @@ class System : public SystemBase {
  public:
   explicit System(const sph_config& c) : cfg_(c) {
     device = c.device;
+    if (const char* e = std::getenv("SPHGPU_SORTED_LISTS")) sorted_lists_ = std::atoi(e) != 0;
+    if (const char* e = std::getenv("SPHGPU_GATHER_BATCH")) {
+      const int v = std::atoi(e);
+      nb_ = (v == 4 || v == 8) ? v : 4;
+    }
     cuda_check(cudaSetDevice(c.device), "cudaSetDevice");
     cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaMallocHost((void**)&h_sc_, sizeof(Scalars)), "cudaMallocHost");
@@ -456,6 +463,9 @@ class System : public SystemBase {
   int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) override {
     std::vector<uint32_t> ref = fetch(ref_.p, n_), cnt = fetch(ncnt_.p, n_);
     std::vector<uint32_t> nb = fetch(nbr_.p, (size_t)K_ * np_);
+    auto slot = [&](size_t i, size_t k) {
+      return (((i >> 5) * (size_t)(K_ >> 2) + (k >> 2)) * 32 + (i & 31)) * 4 + (k & 3);
+    };
     size_t tot = 0;
     for (size_t d = 0; d < n_; ++d) tot += 1 + std::min<size_t>(cnt[d], (size_t)K_);
     *total = tot;
@@ -469,7 +479,7 @@ class System : public SystemBase {
       uint32_t* row = idx + off[r];
       const size_t c = std::min<size_t>(cnt[d], (size_t)K_);
       row[0] = ref[d];
-      for (size_t k = 0; k < c; ++k) row[1 + k] = ref[nb[k * np_ + d]];
+      for (size_t k = 0; k < c; ++k) row[1 + k] = ref[nb[slot(d, k)]];
       std::sort(row, row + c + 1);
     }
     return SPH_OK;
@@ -604,6 +614,8 @@ class System : public SystemBase {
   double current_time_ = 0, time_offset_ = 0, wall_ = 0, avg_density_ = 0;
   uint64_t time_offset_steps_ = 0;
   int last_iters_ = 3;
+  int nb_ = 4;  // neighbor gather batch (prefetch width) of the neighbor passes
+  bool sorted_lists_ = true;   // neighbor lists in ascending index order
   uint64_t launches_ = 0;
   bool profiling_ = false;
   std::map<std::string, ProfEntry> prof_;
@@ -740,7 +752,7 @@ class System : public SystemBase {
     }
     if (cfg_.pressure_solver == SPH_SESPH_W_SPLITTING) rho_pred_.alloc(c);
     if (cfg_.integration_scheme == SPH_TAKE_PREDICTED) { xint_.alloc(c); vint_.alloc(c); }
-    K_ = cfg_.neighbor_capacity ? (int)cfg_.neighbor_capacity : 64;
+    K_ = (int)round_up(cfg_.neighbor_capacity ? cfg_.neighbor_capacity : 64, 4);
     nbr_.alloc((size_t)K_ * np_);
     ensure_partials(2 * (size_t)blocks_for((long long)c));
     press_.zero(stream_);
@@ -795,9 +807,17 @@ class System : public SystemBase {
     P_.min_diag = (R)cfg_.min_diagonal_element;
     P_.tde = cfg_.target_density_error;
     P_.iteration_cap = (int)cfg_.max_solver_iterations;
+    P_.sorted_lists = sorted_lists_ ? 1 : 0;
   }
 
   // ---- launches ---------------------------------------------------------------
+  template <class F>
+  void with_nb(F&& f) {
+    switch (nb_) {
+      case 4: f(std::integral_constant<int, 4>{}); break;
+      default: f(std::integral_constant<int, 8>{}); break;
+    }
+  }
   template <class Kern, class... Args>
   void launch(const char* name, Kern kernel, dim3 g, dim3 b, Args... args) {
     cudaEvent_t e1 = nullptr;
@@ -977,12 +997,15 @@ class System : public SystemBase {
   // the pressure update with the residual reduction.
   void iisph_iteration(int after) {
     const int nb = blocks_for((long long)n_);
-    launch("iisph_pressure_accel", k_pressure_accel<R, 0>, dim3(nb), dim3(kBlock), (const Scalars*)d_sc_.p,
-           (const R4<R>*)xv_.p, (const R4<R>*)vel_.p, (const R*)press_.p, (const uint32_t*)nbr_.p,
-           (const uint32_t*)ncnt_.p, bargs(), accp_.p, 0, 1, P_);
-    launch("iisph_jacobi", k_iisph_jacobi<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
-           (const R4<R>*)accp_.p, (const uint32_t*)nbr_.p, (const uint32_t*)ncnt_.p, bargs(),
-           (const R*)s_.p, (const R*)aii_.p, press_.p, partials_.p, after, P_);
+    with_nb([&](auto NBc) {
+      constexpr int NB = decltype(NBc)::value;
+      launch("iisph_pressure_accel", k_pressure_accel<R, 0, NB>, dim3(nb), dim3(kBlock), (const Scalars*)d_sc_.p,
+             (const R4<R>*)xv_.p, (const R4<R>*)vel_.p, (const R*)press_.p, (const uint32_t*)nbr_.p,
+             (const uint32_t*)ncnt_.p, bargs(), accp_.p, 0, 1, P_);
+      launch("iisph_jacobi", k_iisph_jacobi<R, NB>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
+             (const R4<R>*)accp_.p, (const uint32_t*)nbr_.p, (const uint32_t*)ncnt_.p, bargs(),
+             (const R*)s_.p, (const R*)aii_.p, press_.p, partials_.p, after, P_);
+    });
   }
 
   // resolve_pressure_globally's loop (iisph.rs:419-550). Sweeps run on the
@@ -1014,51 +1037,54 @@ class System : public SystemBase {
     const auto vel = (const R4<R>*)vel_.p;
     const auto nbr = (const uint32_t*)nbr_.p;
     const auto ncnt = (const uint32_t*)ncnt_.p;
+    with_nb([&](auto NBc) {
+    constexpr int NB = decltype(NBc)::value;
     switch (cfg_.pressure_solver) {
       case SPH_SESPH:
-        launch("accel_sesph", k_accel<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(), acc_.p,
+        launch("accel_sesph", k_accel<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(), acc_.p,
                vstar_.p, press_.p, 0, P_);
         body_reduce(nb);
         break;
       case SPH_SESPH_W_SPLITTING:
-        launch("accel_nonpressure", k_accel<R, 0>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
+        launch("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
         body_reduce(nb);
-        launch("split_density", k_split_density<R>, dim3(nb), dim3(kBlock), csc, xv, vel,
+        launch("split_density", k_split_density<R, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), press_.p, rho_pred_.p, P_);
-        launch("pressure_accel", k_pressure_accel<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel,
+        launch("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
                (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
         body_reduce(nb);
         break;
       case SPH_IISPH:
-        launch("accel_nonpressure", k_accel<R, 0>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
+        launch("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
         body_reduce(nb);
-        launch("iisph_source_diag", k_iisph_source_diag<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel,
+        launch("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), s_.p, aii_.p, press_.p, P_);
         solve_loop(-1);
-        launch("pressure_accel", k_pressure_accel<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel,
+        launch("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
                (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
         body_reduce(nb);
         break;
       case SPH_IISPH_W_OST:
-        launch("accel_nonpressure", k_accel<R, 0>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
+        launch("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
-        launch("iisph_source_diag", k_iisph_source_diag<R, 0>, dim3(nb), dim3(kBlock), csc, xv, vel,
+        launch("iisph_source_diag", k_iisph_source_diag<R, 0, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), s_.p, aii_.p, press_.p, P_);
         solve_loop(3);
-        launch("pressure_accel", k_pressure_accel<R, 2>, dim3(nb), dim3(kBlock), csc, xv, vel,
+        launch("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
                (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
         launch("ost_predict", k_ost_predict<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)acc_.p, vstar_.p);
-        launch("iisph_source_diag", k_iisph_source_diag<R, 1>, dim3(nb), dim3(kBlock), csc, xv, vel,
+        launch("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), s_.p, aii_.p, press_.p, P_);
         solve_loop(-1);
-        launch("pressure_accel", k_pressure_accel<R, 2>, dim3(nb), dim3(kBlock), csc, xv, vel,
+        launch("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
                (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
         launch("ost_commit", k_ost_commit<R>, dim3(nb), dim3(kBlock), csc, xv, vel, (const R4<R>*)vstar_.p,
                (const R4<R>*)acc_.p, xint_.p, vint_.p);
         break;
     }
+    });
   }
 
  public:
@@ -1100,7 +1126,7 @@ class System : public SystemBase {
       // Neighbor capacity exceeded: grow it and redo the update on the same
       // (already integrated) state. Reaction forces gathered so far are
       // discarded first; they are rebuilt by the redo.
-      K_ = (int)round_up((size_t)h_sc_->max_nbrs + 8, 8);
+      K_ = (int)round_up((size_t)h_sc_->max_nbrs + 8, 8);  // multiple of 4 (128-bit groups)
       P_.K = K_;
       nbr_.alloc((size_t)K_ * np_);
       zero_body_forces();
