@@ -4,6 +4,7 @@
 // exist for per-trait parity checks; the device-resident System is the
 // production path.
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -224,3 +225,204 @@ int sph_kernel_gradient(size_t n, const double* r, double h, double* out_grad, i
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free neighbor search
+//
+// For callers that cannot allocate device memory: code that runs while its
+// process's allocator is owned by another runtime (a framework memory pool,
+// a real-time loop that forbids allocation, a host that hands the engine only
+// pre-registered buffers). The caller passes its inputs and outputs as device
+// pointers; every temporary lives in one file-scope device array that each
+// GPU loading this library keeps until the process exits.
+// ===========================================================================
+namespace {
+
+constexpr size_t kStaticMaxSamples = size_t(1) << 20;    // sample positions
+constexpr size_t kStaticMaxPositions = size_t(1) << 20;  // query positions
+constexpr int kStaticBits = 6;                           // 2^(3*6) buckets
+constexpr size_t kStaticBuckets = size_t(1) << (3 * kStaticBits);
+// keys, slots and sorted indices of the samples, then bucket counts and starts
+constexpr size_t kStaticScratchBytes =
+    3 * kStaticMaxSamples * sizeof(uint32_t) + 2 * (kStaticBuckets + 2) * sizeof(uint32_t);
+
+static __device__ __align__(256) unsigned char g_find_scratch[kStaticScratchBytes];
+
+struct StaticScratch {
+  uint32_t* key;
+  uint32_t* slot;
+  uint32_t* order;
+  uint32_t* count;
+  uint32_t* start;
+};
+
+StaticScratch carve(void* base) {
+  unsigned char* p = (unsigned char*)base;
+  StaticScratch s;
+  s.key = (uint32_t*)p;
+  s.slot = s.key + kStaticMaxSamples;
+  s.order = s.slot + kStaticMaxSamples;
+  s.count = s.order + kStaticMaxSamples;
+  s.start = s.count + (kStaticBuckets + 2);
+  return s;
+}
+
+// Device address of the scratch array, resolved once per device with that
+// device current (a host-side reference to the array names only its shadow).
+void* static_scratch_address(int device) {
+  static std::mutex mu;
+  static void* addr[64] = {nullptr};
+  if (device < 0 || device >= 64) throw ShimError{SPH_ERR_INVALID, "device ordinal out of range"};
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void* p = nullptr;
+    check(cudaGetSymbolAddress(&p, g_find_scratch), "cudaGetSymbolAddress");
+    addr[device] = p;
+  }
+  return addr[device];
+}
+
+__global__ void k_static_zero(uint32_t* __restrict__ a, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    a[i] = 0u;
+}
+
+__global__ void k_static_keys(int ns, const double* __restrict__ samp, double cell, uint32_t mask,
+                              uint32_t* __restrict__ key, uint32_t* __restrict__ slot,
+                              uint32_t* __restrict__ count) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const uint32_t k = sph::morton_key(sph::cell_coord(samp[3 * s], cell), sph::cell_coord(samp[3 * s + 1], cell),
+                                     sph::cell_coord(samp[3 * s + 2], cell), mask);
+  key[s] = k;
+  slot[s] = atomicAdd(&count[k], 1u);
+}
+
+// Scan by one block (exclusive, or inclusive when INCL): each thread scans a
+// contiguous chunk. `in` and `out` may be the same array (each element is
+// read before it is written).
+template <class T, bool INCL>
+__global__ void __launch_bounds__(1024) k_static_scan(const T* in, T* out, size_t m) {
+  __shared__ T part[1024];
+  const size_t per = (m + blockDim.x - 1) / blockDim.x;
+  const size_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
+  T s = 0;
+  for (size_t i = b; i < e; ++i) s += in[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T run = 0;
+    for (unsigned t = 0; t < blockDim.x; ++t) {
+      const T v = part[t];
+      part[t] = run;
+      run += v;
+    }
+  }
+  __syncthreads();
+  T run = part[threadIdx.x];
+  for (size_t i = b; i < e; ++i) {
+    const T v = in[i];
+    if (INCL) {
+      run += v;
+      out[i] = run;
+    } else {
+      out[i] = run;
+      run += v;
+    }
+  }
+}
+
+__global__ void k_static_scatter(int ns, const uint32_t* __restrict__ key, const uint32_t* __restrict__ slot,
+                                 const uint32_t* __restrict__ start, uint32_t* __restrict__ order) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  order[start[key[s]] + slot[s]] = (uint32_t)s;
+}
+
+// Ascending sample index inside each bucket, as SpatialHashing::populate
+// pushes them (spatial_hashing.rs:27-37).
+__global__ void k_static_bucket_sort(int ns, const uint32_t* __restrict__ key, const uint32_t* __restrict__ start,
+                                     uint32_t* __restrict__ order) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= ns) return;
+  const uint32_t k = key[order[d]];
+  const uint32_t b = start[k];
+  if ((uint32_t)d != b) return;
+  const uint32_t e = start[k + 1];
+  for (uint32_t a = b + 1; a < e; ++a) {
+    const uint32_t v = order[a];
+    uint32_t c = a;
+    while (c > b && order[c - 1] > v) {
+      order[c] = order[c - 1];
+      --c;
+    }
+    order[c] = v;
+  }
+}
+
+// Per-position neighbor counts into offsets[i + 1] (offsets[0] = 0).
+__global__ void k_static_count(int n, const double* __restrict__ pos, const double* __restrict__ samp,
+                               const uint32_t* __restrict__ order, const uint32_t* __restrict__ start,
+                               uint32_t mask, double range, uint64_t* __restrict__ counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) counts[0] = 0;
+  if (i >= n) return;
+  const double px = pos[3 * i], py = pos[3 * i + 1], pz = pos[3 * i + 2];
+  const int cx = sph::cell_coord(px, range), cy = sph::cell_coord(py, range), cz = sph::cell_coord(pz, range);
+  uint64_t c = 0;
+  for (int dx = -1; dx <= 1; ++dx)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dz = -1; dz <= 1; ++dz) {
+        const uint32_t k = sph::morton_key(cx + dx, cy + dy, cz + dz, mask);
+        for (uint32_t s = start[k]; s < start[k + 1]; ++s) {
+          const uint32_t j = order[s];
+          c += sph::in_range_exact(px, py, pz, samp[3 * j], samp[3 * j + 1], samp[3 * j + 2], range) ? 1 : 0;
+        }
+      }
+  counts[i + 1] = c;
+}
+
+}  // namespace
+
+extern "C" int sph_spatial_hashing_find_samples_noalloc(double search_range, size_t n, const double* d_positions,
+                                                        size_t ns, const double* d_samples, uint64_t* d_offsets,
+                                                        uint32_t* d_indices, size_t capacity, size_t* total,
+                                                        int device) {
+  if (!total || !d_offsets || (n && !d_positions) || (ns && !d_samples) || !(search_range > 0)) {
+    g_err = "invalid argument";
+    return SPH_ERR_INVALID;
+  }
+  if (ns > kStaticMaxSamples || n > kStaticMaxPositions) {
+    g_err = "sph_spatial_hashing_find_samples_noalloc: at most 1048576 samples and 1048576 positions";
+    return SPH_ERR_INVALID;
+  }
+  return run(device, [&]() -> int {
+    const StaticScratch S = carve(static_scratch_address(device));
+    const uint32_t mask = (1u << kStaticBits) - 1u;
+    const uint32_t T = (uint32_t)kStaticBuckets;
+    // the array keeps the previous call's contents: clear the bucket counts
+    k_static_zero<<<256, 256>>>(S.count, (size_t)T + 2);
+    if (ns)
+      k_static_keys<<<(unsigned)((ns + 255) / 256), 256>>>((int)ns, d_samples, search_range, mask, S.key, S.slot,
+                                                           S.count);
+    k_static_scan<uint32_t, false><<<1, 1024>>>(S.count, S.start, (size_t)T + 2);
+    if (ns) {
+      k_static_scatter<<<(unsigned)((ns + 255) / 256), 256>>>((int)ns, S.key, S.slot, S.start, S.order);
+      k_static_bucket_sort<<<(unsigned)((ns + 255) / 256), 256>>>((int)ns, S.key, S.start, S.order);
+    }
+    const unsigned nb = (unsigned)std::max<size_t>(1, (n + 255) / 256);
+    k_static_count<<<nb, 256>>>((int)n, d_positions, d_samples, S.order, S.start, mask, search_range, d_offsets);
+    k_static_scan<uint64_t, true><<<1, 1024>>>(d_offsets, d_offsets, n + 1);
+    check(cudaGetLastError(), "find_samples_noalloc");
+    uint64_t tot = 0;
+    check(cudaMemcpy(&tot, d_offsets + n, sizeof(uint64_t), cudaMemcpyDeviceToHost), "cudaMemcpy");
+    *total = (size_t)tot;
+    if (!d_indices || capacity < tot) return SPH_ERR_CAPACITY;
+    if (n)
+      k_find_samples<<<nb, 256>>>((int)n, d_positions, d_samples, S.order, S.start, mask, search_range,
+                                  search_range, nullptr, d_offsets, d_indices);
+    check(cudaGetLastError(), "find_samples_noalloc");
+    check(cudaDeviceSynchronize(), "find_samples_noalloc");
+    return SPH_OK;
+  });
+}

@@ -139,6 +139,8 @@ SIGNATURES = {
                                                _vp, _vp]),
     "sph_spatial_hashing_find_samples": (C.c_int, [C.c_double, _sz, _dp, _sz, _dp, _vp, _vp, _sz,
                                                    C.POINTER(_sz), C.c_int]),
+    "sph_spatial_hashing_find_samples_noalloc": (C.c_int, [C.c_double, _sz, _vp, _sz, _vp, _vp, _vp, _sz,
+                                                           C.POINTER(_sz), C.c_int]),
     "sph_kernel_function": (C.c_int, [_sz, _dp, C.c_double, _dp, C.c_int, C.c_int]),
     "sph_kernel_gradient": (C.c_int, [_sz, _dp, C.c_double, _dp, C.c_int, C.c_int]),
     "sph_volume_map_grids": (C.c_int, [_dp, _sz, C.c_double, C.c_double, C.POINTER(SphGridDesc),

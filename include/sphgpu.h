@@ -257,6 +257,23 @@ int sph_continue_from_checkpoint(sph_system_t* h, uint64_t time_steps_propagated
 int sph_spatial_hashing_find_samples(double search_range, size_t n, const double* positions,
                                      size_t ns, const double* samples, uint64_t* offsets,
                                      uint32_t* indices, size_t capacity, size_t* total, int device);
+/* Allocation-free variant of sph_spatial_hashing_find_samples. No counterpart
+ * in the reference: it exists for callers that cannot allocate device memory
+ * (a host whose allocator belongs to another runtime or memory pool, a loop
+ * that forbids allocation). Inputs and outputs are DEVICE pointers owned by
+ * the caller (positions 3n doubles, samples 3ns doubles, offsets n+1, indices
+ * `capacity`); `total` is a host pointer. Every temporary lives in one static
+ * device array of about 14 MB that each GPU loading the library holds until
+ * the process exits; at most 1,048,576 samples and 1,048,576 positions
+ * (larger inputs return SPH_ERR_INVALID). The first call on a device resolves
+ * that array's address and should come before any stream capture. All calls
+ * share the array, so calls that overlap on the GPU race; the call
+ * synchronizes the device before it returns. Results equal those of
+ * sph_spatial_hashing_find_samples. */
+int sph_spatial_hashing_find_samples_noalloc(double search_range, size_t n, const double* d_positions,
+                                             size_t ns, const double* d_samples, uint64_t* d_offsets,
+                                             uint32_t* d_indices, size_t capacity, size_t* total,
+                                             int device);
 /* KernelFn (kernel/mod.rs:17-46) for CubicBSpline3D on n vectors (3n doubles). */
 int sph_kernel_function(size_t n, const double* r, double h, double* out_w, int precision,
                         int device);
