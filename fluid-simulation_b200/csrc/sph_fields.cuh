@@ -29,7 +29,7 @@ struct MeshDev {
 };
 
 __device__ __forceinline__ double dot3(const double* a, const double* b) {
-  return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2];
+  return add_(add_(mul_(a[0], b[0]), mul_(a[1], b[1])), mul_(a[2], b[2]));
 }
 
 // Closest point on triangle abc to p (Ericson, Real-Time Collision Detection
@@ -37,42 +37,42 @@ __device__ __forceinline__ double dot3(const double* a, const double* b) {
 __device__ void closest_on_tri(const double* p, const double* a, const double* b, const double* c,
                                double* q, int& feat) {
   double ab[3], ac[3], ap[3];
-  for (int d = 0; d < 3; ++d) { ab[d] = b[d] - a[d]; ac[d] = c[d] - a[d]; ap[d] = p[d] - a[d]; }
+  for (int d = 0; d < 3; ++d) { ab[d] = sub_(b[d], a[d]); ac[d] = sub_(c[d], a[d]); ap[d] = sub_(p[d], a[d]); }
   const double d1 = dot3(ab, ap), d2 = dot3(ac, ap);
   if (d1 <= 0 && d2 <= 0) { feat = 1; for (int d = 0; d < 3; ++d) q[d] = a[d]; return; }
   double bp[3];
-  for (int d = 0; d < 3; ++d) bp[d] = p[d] - b[d];
+  for (int d = 0; d < 3; ++d) bp[d] = sub_(p[d], b[d]);
   const double d3 = dot3(ab, bp), d4 = dot3(ac, bp);
   if (d3 >= 0 && d4 <= d3) { feat = 2; for (int d = 0; d < 3; ++d) q[d] = b[d]; return; }
-  const double vc = d1 * d4 - d3 * d2;
+  const double vc = sub_(mul_(d1, d4), mul_(d3, d2));
   if (vc <= 0 && d1 >= 0 && d3 <= 0) {
     feat = 4;
-    const double v = d1 / (d1 - d3);
-    for (int d = 0; d < 3; ++d) q[d] = a[d] + ab[d] * v;
+    const double v = div_(d1, sub_(d1, d3));
+    for (int d = 0; d < 3; ++d) q[d] = add_(a[d], mul_(ab[d], v));
     return;
   }
   double cp[3];
-  for (int d = 0; d < 3; ++d) cp[d] = p[d] - c[d];
+  for (int d = 0; d < 3; ++d) cp[d] = sub_(p[d], c[d]);
   const double d5 = dot3(ab, cp), d6 = dot3(ac, cp);
   if (d6 >= 0 && d5 <= d6) { feat = 3; for (int d = 0; d < 3; ++d) q[d] = c[d]; return; }
-  const double vb = d5 * d2 - d1 * d6;
+  const double vb = sub_(mul_(d5, d2), mul_(d1, d6));
   if (vb <= 0 && d2 >= 0 && d6 <= 0) {
     feat = 6;
-    const double w = d2 / (d2 - d6);
-    for (int d = 0; d < 3; ++d) q[d] = a[d] + ac[d] * w;
+    const double w = div_(d2, sub_(d2, d6));
+    for (int d = 0; d < 3; ++d) q[d] = add_(a[d], mul_(ac[d], w));
     return;
   }
-  const double va = d3 * d6 - d5 * d4;
-  if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+  const double va = sub_(mul_(d3, d6), mul_(d5, d4));
+  if (va <= 0 && sub_(d4, d3) >= 0 && sub_(d5, d6) >= 0) {
     feat = 5;
-    const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
-    for (int d = 0; d < 3; ++d) q[d] = b[d] + (c[d] - b[d]) * w;
+    const double w = div_(sub_(d4, d3), add_(sub_(d4, d3), sub_(d5, d6)));
+    for (int d = 0; d < 3; ++d) q[d] = add_(b[d], mul_(sub_(c[d], b[d]), w));
     return;
   }
   feat = 0;
-  const double denom = 1.0 / (va + vb + vc);
-  const double v = vb * denom, w = vc * denom;
-  for (int d = 0; d < 3; ++d) q[d] = a[d] + ab[d] * v + ac[d] * w;
+  const double denom = div_(1.0, add_(add_(va, vb), vc));
+  const double v = mul_(vb, denom), w = mul_(vc, denom);
+  for (int d = 0; d < 3; ++d) q[d] = add_(add_(a[d], mul_(ab[d], v)), mul_(ac[d], w));
 }
 
 // Signed distance: negative where p - proj points against the closest
@@ -85,16 +85,16 @@ __device__ double mesh_sd(const MeshDev& M, const double* p) {
     double q[3];
     int f;
     closest_on_tri(p, T, T + 3, T + 6, q, f);
-    const double dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
-    const double d2 = (dx * dx + dy * dy) + dz * dz;
+    const double dx = sub_(p[0], q[0]), dy = sub_(p[1], q[1]), dz = sub_(p[2], q[2]);
+    const double d2 = add_(add_(mul_(dx, dx), mul_(dy, dy)), mul_(dz, dz));
     if (d2 < best) { best = d2; bt = t; bf = f; bq[0] = q[0]; bq[1] = q[1]; bq[2] = q[2]; }
   }
   const double* n;
   if (bf == 0) n = M.fn + 3 * bt;
   else if (bf <= 3) n = M.vn + 9 * bt + 3 * (bf - 1);
   else n = M.en + 9 * bt + 3 * (bf - 4);
-  const double diff[3] = {p[0] - bq[0], p[1] - bq[1], p[2] - bq[2]};
-  const double dist = sqrt(dot3(diff, diff));
+  const double diff[3] = {sub_(p[0], bq[0]), sub_(p[1], bq[1]), sub_(p[2], bq[2])};
+  const double dist = __dsqrt_rn(dot3(diff, diff));
   return dot3(diff, n) < 0.0 ? -dist : dist;
 }
 
@@ -117,8 +117,9 @@ __global__ void k_sdf_nodes(MeshDev M, LatticeDesc L, double* __restrict__ raw) 
   const long long kx = k % L.NX, ky = (k / L.NX) % L.NY, kz = k / (L.NX * L.NY);
   if (!is_cell_node(kx, ky, kz)) { raw[k] = NAN; return; }
   // discretization.rs:160-166: x_min + key / 3 * dx
-  const double p[3] = {L.xmin[0] + (double)kx / 3.0 * L.dx, L.xmin[1] + (double)ky / 3.0 * L.dx,
-                       L.xmin[2] + (double)kz / 3.0 * L.dx};
+  const double p[3] = {add_(L.xmin[0], mul_(div_((double)kx, 3.0), L.dx)),
+                       add_(L.xmin[1], mul_(div_((double)ky, 3.0), L.dx)),
+                       add_(L.xmin[2], mul_(div_((double)kz, 3.0), L.dx))};
   raw[k] = mesh_sd(M, p);
 }
 
@@ -159,9 +160,9 @@ __constant__ double c_gl_w[kMaxGL];
 __device__ __forceinline__ double cubic_extension(double sd, double r) {
   if (sd >= r) return 0.0;
   if (sd <= 0.0) return 1.0;
-  const double q = sd / r;
-  const double a = 1.0 - q, b = q < 0.5 ? 0.5 - q : 0.0;
-  return (a * a * a - 4.0 * (b * b * b)) / 0.5;
+  const double q = div_(sd, r);
+  const double a = sub_(1.0, q), b = q < 0.5 ? sub_(0.5, q) : 0.0;
+  return div_(sub_(mul_(mul_(a, a), a), mul_(4.0, mul_(mul_(b, b), b))), 0.5);
 }
 
 // One block per volume-map node: SDFnWrapper::volume (volume_map_boundary.rs:
@@ -177,8 +178,9 @@ __global__ void __launch_bounds__(256) k_volume_map_nodes(DevField sdf, LatticeD
   __shared__ int state;  // 0 integrate, 1 value set, 2 error
   __shared__ double value;
   __shared__ int err;
-  const double c[3] = {L.xmin[0] + (double)kx / 3.0 * L.dx, L.xmin[1] + (double)ky / 3.0 * L.dx,
-                       L.xmin[2] + (double)kz / 3.0 * L.dx};
+  const double c[3] = {add_(L.xmin[0], mul_(div_((double)kx, 3.0), L.dx)),
+                       add_(L.xmin[1], mul_(div_((double)ky, 3.0), L.dx)),
+                       add_(L.xmin[2], mul_(div_((double)kz, 3.0), L.dx))};
   const double PI = 3.14159265358979323846;
   const double ball = 4.0 / 3.0 * PI * (r * r * r);
   if (threadIdx.x == 0) {
@@ -201,30 +203,31 @@ __global__ void __launch_bounds__(256) k_volume_map_nodes(DevField sdf, LatticeD
   // innermost integrals over phi for every (r_i, theta_j) pair
   for (int pj = threadIdx.x; pj < deg * deg; pj += blockDim.x) {
     const int i = pj / deg, j = pj % deg;
-    const double rr = 0.5 * (r * c_gl_x[i] + r);
-    const double th = 0.5 * (PI * c_gl_x[j] + PI);
+    const double rr = mul_(0.5, add_(mul_(r, c_gl_x[i]), r));
+    const double th = mul_(0.5, add_(mul_(PI, c_gl_x[j]), PI));
     const double st = sin(th), ct = cos(th);
     double s = 0.0;
     for (int q = 0; q < deg; ++q) {
-      const double ph = 0.5 * ((2.0 * PI) * c_gl_x[q] + 2.0 * PI);
-      const double p0 = c[0] + rr * st * cos(ph);
-      const double p1 = c[1] + rr * st * sin(ph);
-      const double p2 = c[2] + rr * ct;
+      const double ph = mul_(0.5, add_(mul_(2.0 * PI, c_gl_x[q]), 2.0 * PI));
+      const double rs = mul_(rr, st);
+      const double p0 = add_(c[0], mul_(rs, cos(ph)));
+      const double p1 = add_(c[1], mul_(rs, sin(ph)));
+      const double p2 = add_(c[2], mul_(rr, ct));
       double sd;
       if (!ser_function(sdf, p0, p1, p2, sd)) { err = 1; break; }
-      s += cubic_extension(sd, r) * c_gl_w[q];
+      s = add_(s, mul_(cubic_extension(sd, r), c_gl_w[q]));
     }
-    inner[pj] = 0.5 * (2.0 * PI) * s;
+    inner[pj] = mul_(mul_(0.5, 2.0 * PI), s);
   }
   __syncthreads();
   if (threadIdx.x < deg) {
     const int i = threadIdx.x;
     double s = 0.0;
     for (int j = 0; j < deg; ++j) {
-      const double th = 0.5 * (PI * c_gl_x[j] + PI);
-      s += sin(th) * inner[i * deg + j] * c_gl_w[j];
+      const double th = mul_(0.5, add_(mul_(PI, c_gl_x[j]), PI));
+      s = add_(s, mul_(mul_(sin(th), inner[i * deg + j]), c_gl_w[j]));
     }
-    mid[i] = 0.5 * PI * s;
+    mid[i] = mul_(mul_(0.5, PI), s);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -234,10 +237,10 @@ __global__ void __launch_bounds__(256) k_volume_map_nodes(DevField sdf, LatticeD
     }
     double s = 0.0;
     for (int i = 0; i < deg; ++i) {
-      const double rr = 0.5 * (r * c_gl_x[i] + r);
-      s += (rr * rr) * mid[i] * c_gl_w[i];
+      const double rr = mul_(0.5, add_(mul_(r, c_gl_x[i]), r));
+      s = add_(s, mul_(mul_(mul_(rr, rr), mid[i]), c_gl_w[i]));
     }
-    raw[k] = fmin(fmax(0.5 * r * s, 0.0), ball);
+    raw[k] = fmin(fmax(mul_(mul_(0.5, r), s), 0.0), ball);
   }
 }
 

@@ -472,22 +472,33 @@ __constant__ double c_ser_ref[32][3];
 __constant__ int c_ser_off[32][3];
 __constant__ int c_ser_kind[32];
 
+// f64 arithmetic that the compiler may not contract into FMAs, so that the
+// field evaluation rounds exactly like the reference's (discretization.rs:
+// 437-557 is plain f64 without fused operations): threshold decisions such
+// as sd < r, sd <= -r or 0.5 < |grad| < 2 then fall on the same side.
+__device__ __forceinline__ double mul_(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add_(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double div_(double a, double b) { return __ddiv_rn(a, b); }
+
 __device__ bool ser_function(const DevField& F, double px, double py, double pz, double& out) {
   const double p[3] = {px, py, pz};
   long long c[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const double fi = floor((p[d] - F.xmin[d]) / F.dx);
+    const double fi = floor(div_(sub_(p[d], F.xmin[d]), F.dx));
     if (p[d] < F.xmin[d] || p[d] > F.xmax[d]) return false;
     long long idx = (long long)fi;
     c[d] = idx < (long long)F.n[d] - 1 ? idx : (long long)F.n[d] - 1;
   }
-  const double o0 = F.xmin[0] + (double)c[0] * F.dx, o1 = F.xmin[1] + (double)c[1] * F.dx,
-               o2 = F.xmin[2] + (double)c[2] * F.dx;
-  const double xi = 2.0 * (p[0] - o0) / F.dx - 1.0;
-  const double eta = 2.0 * (p[1] - o1) / F.dx - 1.0;
-  const double zeta = 2.0 * (p[2] - o2) / F.dx - 1.0;
-  const double r2 = xi * xi + eta * eta + zeta * zeta;
+  const double o0 = add_(F.xmin[0], mul_((double)c[0], F.dx));
+  const double o1 = add_(F.xmin[1], mul_((double)c[1], F.dx));
+  const double o2 = add_(F.xmin[2], mul_((double)c[2], F.dx));
+  const double xi = sub_(div_(mul_(2.0, sub_(p[0], o0)), F.dx), 1.0);
+  const double eta = sub_(div_(mul_(2.0, sub_(p[1], o1)), F.dx), 1.0);
+  const double zeta = sub_(div_(mul_(2.0, sub_(p[2], o2)), F.dx), 1.0);
+  const double r2 = add_(add_(mul_(xi, xi), mul_(eta, eta)), mul_(zeta, zeta));
+  const double e19 = sub_(mul_(9.0, r2), 19.0);
   const long long bx = 3 * c[0], by = 3 * c[1], bz = 3 * c[2];
   double s = 0.0;
   for (int a = 0; a < 32; ++a) {
@@ -496,36 +507,38 @@ __device__ bool ser_function(const DevField& F, double px, double py, double pz,
     const double v = __ldg(F.nodes + idx);
     if (v != v) return false;  // pruned cell
     const double ax = c_ser_ref[a][0], ay = c_ser_ref[a][1], az = c_ser_ref[a][2];
+    const double lx = add_(1.0, mul_(xi, ax)), ly = add_(1.0, mul_(eta, ay)), lz = add_(1.0, mul_(zeta, az));
     double N;
     switch (c_ser_kind[a]) {
-      case 0:
-        N = (1.0 / 64.0) * (1.0 + xi * ax) * (1.0 + eta * ay) * (1.0 + zeta * az) * (9.0 * r2 - 19.0);
+      case 0:  // (1/64)(1+xi a)(1+eta b)(1+zeta c)(9 r^2 - 19)
+        N = mul_(mul_(mul_(mul_(1.0 / 64.0, lx), ly), lz), e19);
         break;
-      case 1:
-        N = (9.0 / 64.0) * (1.0 - xi * xi) * (1.0 + 9.0 * xi * ax) * (1.0 + eta * ay) * (1.0 + zeta * az);
+      case 1:  // (9/64)(1-xi^2)(1+9 xi a)(1+eta b)(1+zeta c)
+        N = mul_(mul_(mul_(mul_(9.0 / 64.0, sub_(1.0, mul_(xi, xi))), add_(1.0, mul_(mul_(9.0, xi), ax))), ly), lz);
         break;
-      case 2:
-        N = (9.0 / 64.0) * (1.0 - eta * eta) * (1.0 + 9.0 * eta * ay) * (1.0 + xi * ax) * (1.0 + zeta * az);
+      case 2:  // (9/64)(1-eta^2)(1+9 eta b)(1+xi a)(1+zeta c)
+        N = mul_(mul_(mul_(mul_(9.0 / 64.0, sub_(1.0, mul_(eta, eta))), add_(1.0, mul_(mul_(9.0, eta), ay))), lx), lz);
         break;
-      default:
-        N = (9.0 / 64.0) * (1.0 - zeta * zeta) * (1.0 + 9.0 * zeta * az) * (1.0 + xi * ax) * (1.0 + eta * ay);
+      default:  // (9/64)(1-zeta^2)(1+9 zeta c)(1+xi a)(1+eta b)
+        N = mul_(mul_(mul_(mul_(9.0 / 64.0, sub_(1.0, mul_(zeta, zeta))), add_(1.0, mul_(mul_(9.0, zeta), az))), lx), ly);
         break;
     }
-    s += v * N;
+    s = add_(s, mul_(v, N));
   }
   out = s;
   return true;
 }
 
 __device__ bool ser_gradient(const DevField& F, double px, double py, double pz, double g[3]) {
-  const double h = F.dx / 6.0;
+  const double h = div_(F.dx, 6.0);
+  const double h2 = mul_(2.0, h);
   double fp, fm;
-  if (!ser_function(F, px + h, py, pz, fp) || !ser_function(F, px - h, py, pz, fm)) return false;
-  g[0] = (fp - fm) / (2.0 * h);
-  if (!ser_function(F, px, py + h, pz, fp) || !ser_function(F, px, py - h, pz, fm)) return false;
-  g[1] = (fp - fm) / (2.0 * h);
-  if (!ser_function(F, px, py, pz + h, fp) || !ser_function(F, px, py, pz - h, fm)) return false;
-  g[2] = (fp - fm) / (2.0 * h);
+  if (!ser_function(F, add_(px, h), py, pz, fp) || !ser_function(F, sub_(px, h), py, pz, fm)) return false;
+  g[0] = div_(sub_(fp, fm), h2);
+  if (!ser_function(F, px, add_(py, h), pz, fp) || !ser_function(F, px, sub_(py, h), pz, fm)) return false;
+  g[1] = div_(sub_(fp, fm), h2);
+  if (!ser_function(F, px, py, add_(pz, h), fp) || !ser_function(F, px, py, sub_(pz, h), fm)) return false;
+  g[2] = div_(sub_(fp, fm), h2);
   return true;
 }
 
@@ -560,12 +573,12 @@ __global__ void __launch_bounds__(kBlock) k_vm_sample(
           qrot(body->q, g, gw);
           g[0] = gw[0]; g[1] = gw[1]; g[2] = gw[2];
         }
-        const double gn = sqrt((g[0] * g[0] + g[1] * g[1]) + g[2] * g[2]);
+        const double gn = __dsqrt_rn(add_(add_(mul_(g[0], g[0]), mul_(g[1], g[1])), mul_(g[2], g[2])));
         double vm;
         if (gn > 0.5 && gn < 2.0 && ser_function(D.vm, pl[0], pl[1], pl[2], vm) && vm > 0.0) {
           vol = vm < ball ? vm : ball;
-          const double d = fmax(sd + 0.25 * P.spacing, P.spacing);
-          for (int c = 0; c < 3; ++c) xb[c] = p[c] - g[c] / gn * d;
+          const double d = fmax(add_(sd, mul_(0.25, P.spacing)), P.spacing);
+          for (int c = 0; c < 3; ++c) xb[c] = sub_(p[c], mul_(div_(g[c], gn), d));
           if (body) body_velocity_at(*body, xb, vb);
           const double u[3] = {xb[0] - p[0], xb[1] - p[1], xb[2] - p[2]};
           const double un = sqrt((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]);

@@ -182,3 +182,59 @@ def build_system(scene: Scene, precision="f32", device=0, fields=None, extra_par
         s.add_volume_map_boundary(fields[0], fields[1])
     s.initialize()
     return s
+
+
+def icosphere(subdivisions=4, radius=1.0, inward=False):
+    """Subdivided icosahedron (10*4^s+2 vertices, 20*4^s triangles); outward
+    winding unless `inward` (a container)."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(p, np.float64) / np.linalg.norm(p) for p in v]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    V = np.array(verts) * radius
+    F = np.array(faces, np.uint32)
+    if inward:
+        F = F[:, ::-1].copy()
+    return V, F
+
+
+def box_inertia(mass, side):
+    """Inertia tensor of a solid cube of the given side about its center."""
+    i = mass * side * side / 6.0
+    return np.diag([i, i, i])
+
+
+def floating_cube_scene(n_side=12, spacing=0.02, body_side=0.12, body_density=500.0, seed=0):
+    """SESPH pool in the 0.6 m sample-boundary cube with a dynamic sample-boundary
+    cube body (two-way coupled RigidBodyMotion) just above the water."""
+    sc = dam_break_sesph_8k(jitter_seed=seed, n_side=n_side)
+    verts = transform_mesh(CUBE_VERTICES, scale=(body_side / 2,) * 3)
+    samples = sample_triangle_mesh_surface(verts, CUBE_FACES_OUTWARD, 0.7 * spacing)
+    top = sc.position[:, 2].max()
+    mass = body_density * body_side ** 3
+    from .system import RigidInit
+    rigid = RigidInit(mass=mass, inertia_body=box_inertia(mass, body_side),
+                      center_of_mass=(-0.15, -0.15, top + 0.5 * body_side + 0.25 * spacing),
+                      orientation=(np.cos(0.1), np.sin(0.1), 0.0, 0.0),
+                      angular_velocity=(0.0, 0.5, 0.0))
+    sc.sample_boundaries.append((samples, rigid))
+    sc.description += f", dynamic cube body with {samples.shape[0]} samples"
+    return sc
