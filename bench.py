@@ -62,7 +62,8 @@ def parse():
     p.add_argument("--n-side", type=int, default=100)
     p.add_argument("--max-iters", type=int, default=100)
     p.add_argument("--cpu-sample-side", type=int, default=50)
-    p.add_argument("--cpu-steps", type=int, default=2)
+    p.add_argument("--cpu-steps", type=int, default=3)
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--profile", action="store_true", help="per-kernel CUDA-event timing (default on)")
@@ -145,9 +146,26 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def run_cpu(n_side, steps, warmup, max_iters, fields):
+# ncu summaries of the dominant kernels (committed under profiles/): DRAM
+# read + write bytes of one launch of the bench workload.
+TRAFFIC_PROFILES = {"iisph_jacobi": "profiles/iisph_jacobi_1M_volume_map.md"}
+
+
+def profiled_traffic(kernel):
+    path = os.path.join(ROOT, TRAFFIC_PROFILES.get(kernel, ""))
+    if not os.path.isfile(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return int(line.split(":")[1])
+    return None
+
+
+def run_cpu(n_side, steps, warmup, max_iters, fields, min_seconds=0.0):
     """The reference's CPU algorithm (oracle restatement, all host threads) on
-    a bounded n_side^3 sample of the workload. Returns (updates/s, seconds, cores)."""
+    a bounded n_side^3 sample of the workload: `steps` timed steps, more while
+    less than `min_seconds` of CPU work has been timed (at most 4x `steps`).
+    Returns (updates/s, seconds, cores, particles, steps, mean sweeps)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from sphgpu.system import PROCEDURES
@@ -167,12 +185,14 @@ def run_cpu(n_side, steps, warmup, max_iters, fields):
     if warmup:
         s.step(warmup)
     t0 = time.perf_counter()
-    updates = 0
-    for _ in range(steps):
+    updates, done, sweeps = 0, 0, []
+    while done < steps or (time.perf_counter() - t0 < min_seconds and done < 4 * steps):
         s.step(1)
         updates += s.n
+        done += 1
+        sweeps.append(s.measurement()["solver_iterations"])
     dt = time.perf_counter() - t0
-    return updates / dt, dt, O.num_threads(), sc.position.shape[0]
+    return updates / dt, dt, O.num_threads(), sc.position.shape[0], done, statistics.mean(sweeps)
 
 
 def main():
@@ -276,20 +296,22 @@ def main():
         n_particles = updates / max(args.steps, 1)
         bytes_per_launch = BYTES_PER_PARTICLE[dom] * n_particles
         achieved = bytes_per_launch / avg_s / 1e9
+        traffic = profiled_traffic(dom)
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                    "traffic": None, "bytes_per_launch": bytes_per_launch,
+                    "traffic": traffic, "bytes_per_launch": bytes_per_launch,
                     "avg_launch_us": round(avg_s * 1e6, 2), "launches": cnt,
                     "kernel_share": {k: round(v[0] / sum(x[0] for x in kernel_times.values()), 4)
                                      for k, v in sorted(kernel_times.items(), key=lambda kv: -kv[1][0])}}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        v, secs, cores, n_cpu = run_cpu(args.cpu_sample_side, args.cpu_steps, 0, args.max_iters, fields)
+        v, secs, cores, n_cpu, done, sweeps = run_cpu(args.cpu_sample_side, args.cpu_steps, 1, args.max_iters,
+                                                      fields, args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{args.cpu_steps} steps of a {n_cpu}-particle ({args.cpu_sample_side}^3) block of "
-                         f"the same configuration, f64 C++ restatement of the reference CPU path, "
-                         f"{secs:.1f} s"}
+               "sample": f"{done} steps (after 1 warm-up step) of a {n_cpu}-particle ({args.cpu_sample_side}^3) "
+                         f"block of the same configuration, {sweeps:.0f} IISPH sweeps per step, f64 C++ "
+                         f"restatement of the reference CPU path on all host threads, {secs:.1f} s"}
 
     if ws > 1:
         dist.barrier()
@@ -324,7 +346,8 @@ def reference_arm(args, ws, rank):
     verts, faces = sc.mesh
     sp = sc.parameters["rest_density_grid_spacing"]
     sdf, vm = O.build_fields(verts, faces, 4 * sp, sc.parameters["kernel_support_radius"], 30)
-    v, secs, cores, n_cpu = run_cpu(args.cpu_sample_side, args.steps, args.warmup, args.max_iters, (sdf, vm))
+    v, secs, cores, n_cpu, done, sweeps = run_cpu(args.cpu_sample_side, args.steps, args.warmup, args.max_iters,
+                                                  (sdf, vm))
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1000.0 / args.steps, "higher_is_better": True,
@@ -333,9 +356,10 @@ def reference_arm(args, ws, rank):
         "config": {"workload": f"IISPH dam break, {args.n_side}^3 particles, 2x1x1 m VolumeMapBoundary box",
                    "sample_particles": n_cpu, "max_solver_iterations": args.max_iters},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} timed steps of a {n_cpu}-particle ({args.cpu_sample_side}^3) "
-                                   f"block of the same configuration (f64 C++ restatement of the reference CPU "
-                                   f"path; the Rust reference cannot be built here)"},
+                         "sample": f"{done} timed steps of a {n_cpu}-particle ({args.cpu_sample_side}^3) block of "
+                                   f"the same configuration, {sweeps:.0f} IISPH sweeps per step (f64 C++ "
+                                   f"restatement of the reference CPU path; the Rust reference cannot be built "
+                                   f"here)"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
