@@ -44,6 +44,11 @@ struct Scalars {
   int status;                      // 0 ok, 2 not converged within the cap
   int iterations_eqs1;             // IISPHwOST first solve sweeps
   int max_bnbrs;                   // largest boundary-sample neighbor count seen
+  // graph-captured stepping (the host reads these once per chunk)
+  double time_acc;                 // simulated time under CFL steps
+  unsigned int trouble;            // bits: 1 neighbor overflow, 2 disabled particles, 4 unconverged
+  int status_any;                  // 2 once any step of the chunk hit the sweep cap
+  unsigned long long loop_sweeps;  // sweeps run by the graph's solver while-loops
 };
 
 // Parameters that are constant over a step (passed by value).

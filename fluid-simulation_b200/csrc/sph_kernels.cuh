@@ -162,8 +162,11 @@ __global__ void __launch_bounds__(kBlock) k_integrate_key(
 
 // Step prologue: active count and the CFL time increment (sph/mod.rs:825-829).
 template <class R>
-__global__ void k_prologue(Scalars* sc, StepParams<R> P) {
+__global__ void k_prologue(Scalars* sc, StepParams<R> P, int accumulate_time) {
   sc->n_active = sc->n - sc->n_below;
+  // simulated time of a CFL step advances by the increment it integrated with
+  // (the one chosen by the previous update); graph-captured steps keep it here
+  if (accumulate_time) sc->time_acc += sc->dt;
   if (P.cfl) {
     const double ms = __longlong_as_double((long long)sc->max_speed);
     const double c = P.cfl_number * P.spacing / ms;  // +inf at rest
@@ -1344,6 +1347,42 @@ __global__ void __launch_bounds__(kBlock) k_sample_volumes(const int* __restrict
   R4<R> o = xi;
   o.w = (R)(gamma_v / (double)sum);
   xb[d] = o;
+}
+
+// ---------------------------------------------------------------------------
+// graph-captured stepping
+// ---------------------------------------------------------------------------
+// Opens a chunk of graph launches: simulated time enters, flags clear.
+__global__ void k_chunk_begin(Scalars* sc, double time) {
+  sc->time_acc = time;
+  sc->trouble = 0;
+  sc->status_any = 0;
+  sc->loop_sweeps = 0;
+}
+
+// Condition of the while-node that runs the Jacobi sweeps of one solve: go on
+// until the sweep kernel sets `converged` or `limit` sweeps have run. Every
+// body execution either finds `converged` set or adds one to `iterations`,
+// so the loop ends after at most `limit` bodies.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const Scalars* __restrict__ sc, int limit) {
+  const unsigned int more = (!sc->converged && sc->iterations < limit) ? 1u : 0u;
+  cudaGraphSetConditional(h, more);
+}
+
+// End of a graph-captured step: records what the per-step host check would
+// have acted on (then the host replays the chunk on the per-step path) and
+// prepares the scalars of the next update exactly as that check does.
+__global__ void k_step_epilogue(Scalars* sc, int K, int solver_loop) {
+  unsigned int t = 0;
+  if (sc->max_nbrs > K) t |= 1u;
+  if (sc->n_below > 0) t |= 2u;
+  if (solver_loop && !sc->converged) t |= 4u;
+  sc->trouble |= t;
+  if (sc->status == 2) sc->status_any = 2;
+  if (solver_loop) sc->loop_sweeps += (unsigned long long)sc->iterations;
+  sc->n = sc->n_active;
+  sc->n_below = 0;
+  sc->max_speed = 0;
 }
 
 }  // namespace sph

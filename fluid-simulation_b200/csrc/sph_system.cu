@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -20,6 +21,7 @@
 
 #include "../../include/sphgpu.h"
 #include "sph_fields.cuh"
+#include "sph_host.hpp"
 #include "sph_kernels.cuh"
 
 namespace sph {
@@ -27,18 +29,7 @@ namespace sph {
 // ---------------------------------------------------------------------------
 // errors and buffers
 // ---------------------------------------------------------------------------
-struct Error : std::runtime_error {
-  int code;
-  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
 thread_local std::string g_last_error;
-
-static void cuda_check(cudaError_t e, const char* what) {
-  if (e == cudaSuccess) return;
-  const int code = (e == cudaErrorMemoryAllocation) ? SPH_ERR_OOM : SPH_ERR_CUDA;
-  throw Error(code, std::string(what) + ": " + cudaGetErrorString(e));
-}
 
 template <class T>
 struct DBuf {
@@ -73,7 +64,9 @@ static size_t round_up(size_t n, size_t m) { return (n + m - 1) / m * m; }
 // serendipity reference node tables (discretization.rs:267-300)
 // ---------------------------------------------------------------------------
 static void upload_serendipity_tables() {
+  static std::mutex mu;
   static bool done_for[64] = {false};
+  std::lock_guard<std::mutex> lock(mu);
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev >= 0 && dev < 64 && done_for[dev]) return;
@@ -100,47 +93,6 @@ static void upload_serendipity_tables() {
   cuda_check(cudaMemcpyToSymbol(c_ser_kind, kind, sizeof kind), "serendipity tables");
   if (dev >= 0 && dev < 64) done_for[dev] = true;
 }
-
-// ---------------------------------------------------------------------------
-// precision-agnostic interface
-// ---------------------------------------------------------------------------
-class SystemBase {
- public:
-  virtual ~SystemBase() = default;
-  virtual SystemBase* clone() const = 0;
-  virtual void upload_fluid(size_t n, const double* x, const double* v, const double* m,
-                            const uint32_t* fid) = 0;
-  virtual int add_sample_boundary(size_t nb, const double* x, const sph_rigid_init* rigid) = 0;
-  virtual int add_volume_map(const sph_grid_desc& sd, const double* sn, const sph_grid_desc& vd,
-                             const double* vn, const sph_rigid_init* rigid) = 0;
-  virtual void initialize() = 0;
-  virtual int step(uint32_t n) = 0;
-  virtual double time() const = 0;
-  virtual uint64_t steps() const = 0;
-  virtual void measurement(sph_measurement* m) = 0;
-  virtual size_t num_particles() const = 0;
-  virtual void download(int field, double* out) = 0;
-  virtual void fluid_ids(uint32_t* out) = 0;
-  virtual void fluid_pos(float* out) = 0;
-  virtual void quantity(int q, float* out) = 0;
-  virtual int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
-  virtual int boundary_neighbors(int bi, uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
-  virtual void boundary_volumes(int bi, double* out) = 0;
-  virtual void vm_samples(int bi, uint8_t* has, double* xb, double* vb, double* vol) = 0;
-  virtual void rigid_state(int bi, double* out) = 0;
-  virtual void set_rigid_state(int bi, const double* in) = 0;
-  virtual uint64_t hash_collisions() = 0;
-  virtual void restore(uint64_t steps, double time, size_t n, const double* x, const double* v,
-                       const double* m, const uint32_t* fid, const double* xi, const double* vi) = 0;
-  virtual int step_host(uint32_t n, const double* xi, const double* vi, double* xo, double* vo) = 0;
-  virtual void* stream() const = 0;
-  virtual void step_stats(sph_step_stats* out) const = 0;
-  virtual uint64_t launches() const = 0;
-  virtual void set_profiling(bool on) = 0;
-  virtual bool kernel_time(const std::string& name, double* ms, uint64_t* count) = 0;
-  virtual size_t device_bytes() const = 0;
-  int device = 0;
-};
 
 // Host-buffer state exchange in reference index order (sph_step_host).
 template <class R>
@@ -199,6 +151,11 @@ class System : public SystemBase {
     upload_serendipity_tables();
   }
   ~System() override {
+    if (chunk_steps_) cudaEventSynchronize(chunk_event_);
+    destroy_graphs();
+    if (chunk_event_) cudaEventDestroy(chunk_event_);
+    if (body_stream_) cudaStreamDestroy(body_stream_);
+    if (h_chunk_sc_) cudaFreeHost(h_chunk_sc_);
     for (auto& kv : prof_) {
       for (auto& e : kv.second.pool) {
         cudaEventDestroy(e.first);
@@ -322,6 +279,21 @@ class System : public SystemBase {
   // ---- stepping ------------------------------------------------------------
   int step(uint32_t nsteps) override {
     if (!initialized_) throw Error(SPH_ERR_STATE, "initialize before stepping");
+    if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
+    if (graph_chunk_ == 0 || profiling_) return step_plain(nsteps);
+    int status = SPH_OK;
+    for (uint32_t left = nsteps; left > 0;) {
+      const uint32_t c = std::min(left, graph_chunk_);
+      chunk_begin(c);
+      const ChunkOutcome o = chunk_finish();
+      if (o.status != SPH_OK) status = o.status;
+      left -= c;
+    }
+    return status;
+  }
+
+  // System::step_forward_in_time (sph/mod.rs:125-144), one host check per step.
+  int step_plain(uint32_t nsteps) {
     int status = SPH_OK;
     for (uint32_t s = 0; s < nsteps; ++s) {
       const auto t0 = std::chrono::steady_clock::now();
@@ -580,8 +552,18 @@ class System : public SystemBase {
     return true;
   }
   size_t device_bytes() const override {
-    size_t b = 0;
-    for (const auto* p : owned_sizes()) b += *p;
+    size_t b = d_sc_.bytes() + d_meas_.bytes();
+    for (const auto* d : {&pos_, &pos2_, &vel_, &vel2_, &xv_, &acc_, &vstar_, &accp_, &xint_, &vint_, &bG_, &bGu_,
+                          &xb_, &xb2_, &vb_, &vb2_, &xbody_, &vmx_, &vmv_, &snap_pos_, &snap_vel_, &snap_acc_,
+                          &snap_xint_, &snap_vint_})
+      b += d->bytes();
+    for (const auto* d : {&press_, &s_, &aii_, &bW_, &rho_pred_}) b += d->bytes();
+    for (const auto* d : {&ref_, &ref2_, &fid_, &fid2_, &key_, &slot_, &perm_, &nbr_, &ncnt_, &count_, &start_,
+                          &tile_sums_, &sbid_, &sbid2_, &sorig_, &sorig2_, &skey_, &sslot_, &sperm_, &scount_,
+                          &sstart_, &snap_ref_, &snap_fid_})
+      b += d->bytes();
+    b += partials_.bytes() + body_partials_.bytes() + stage_x_.bytes() + stage_v_.bytes();
+    b += bodies_d_.bytes() + snap_bodies_.bytes() + snap_sc_.bytes() + ns_d_.bytes() + vms_.bytes();
     for (const auto& f : fields_) b += f->sdf.bytes() + f->vm.bytes();
     return b;
   }
@@ -651,8 +633,6 @@ class System : public SystemBase {
     void clear() { any = false; }
   } bbox_;
   BBox& host_bbox_ = bbox_;
-
-  std::vector<const size_t*> owned_sizes() const { return {}; }
 
   // ---- helpers ---------------------------------------------------------------
   void bbox_add(double x, double y, double z) {
@@ -821,7 +801,7 @@ class System : public SystemBase {
   template <class Kern, class... Args>
   void launch(const char* name, Kern kernel, dim3 g, dim3 b, Args... args) {
     cudaEvent_t e1 = nullptr;
-    if (profiling_) {
+    if (profiling_ && !capturing_) {
       ProfEntry& pe = prof_[name];
       if (pe.used == pe.pool.size()) {
         cudaEvent_t a, c;
@@ -837,7 +817,8 @@ class System : public SystemBase {
     }
     kernel<<<g, b, 0, stream_>>>(args...);
     cuda_check(cudaGetLastError(), name);
-    ++launches_;
+    if (!capturing_) ++launches_;
+    else if (!in_loop_body_) ++capture_kernels_;
     if (e1) cuda_check(cudaEventRecord(e1, stream_), "event");
   }
   void collect_profile() {
@@ -873,10 +854,19 @@ class System : public SystemBase {
     launch("sort", k_gather_particles<R>, dim3(nb), dim3(kBlock), dn, (const uint32_t*)perm_.p,
            (const R4<R>*)pos_.p, (const R4<R>*)vel_.p, (const uint32_t*)ref_.p, (const uint32_t*)fid_.p,
            pos2_.p, vel2_.p, ref2_.p, fid2_.p);
+    swap_particle_buffers();
+  }
+  void swap_particle_buffers() {
     std::swap(pos_.p, pos2_.p);
     std::swap(vel_.p, vel2_.p);
     std::swap(ref_.p, ref2_.p);
     std::swap(fid_.p, fid2_.p);
+  }
+  void swap_sample_buffers() {
+    std::swap(xb_.p, xb2_.p);
+    std::swap(vb_.p, vb2_.p);
+    std::swap(sbid_.p, sbid2_.p);
+    std::swap(sorig_.p, sorig2_.p);
   }
 
   void sort_samples() {
@@ -892,10 +882,7 @@ class System : public SystemBase {
     launch("sample_sort", k_gather_samples<R>, dim3(nb), dim3(kBlock), dn, (const uint32_t*)sperm_.p,
            (const R4<R>*)xb_.p, (const R4<R>*)vb_.p, (const uint32_t*)sbid_.p, (const uint32_t*)sorig_.p,
            xb2_.p, vb2_.p, sbid2_.p, sorig2_.p);
-    std::swap(xb_.p, xb2_.p);
-    std::swap(vb_.p, vb2_.p);
-    std::swap(sbid_.p, sbid2_.p);
-    std::swap(sorig_.p, sorig2_.p);
+    swap_sample_buffers();
   }
 
   SampleGrid<R> sample_grid() const {
@@ -1012,6 +999,10 @@ class System : public SystemBase {
   // device and stop themselves once converged; the host only checks the flag
   // after a batch sized by the previous solve.
   void solve_loop(int after) {
+    if (capturing_ && after < 0) {
+      solve_loop_graph();
+      return;
+    }
     int batch = after >= 0 ? after + 1 : std::max(3, last_iters_);
     if (after < 0 && cfg_.max_solver_iterations) batch = std::min(batch, (int)cfg_.max_solver_iterations);
     for (int k = 0; k < batch; ++k) iisph_iteration(after);
@@ -1091,32 +1082,7 @@ class System : public SystemBase {
   // System::update (sph/mod.rs:674-731); mode 0/1 integrate first (EulerCromer
   // / TakePredicted, euler_cromer.rs:12-25 / take_predicted.rs:14-27), 2 not.
   void update(int mode) {
-    const int nb = blocks_for((long long)n_);
-    const bool sample_dyn = boundary_kind_ == 1 && any_dynamic_;
-    launch("integrate_key", k_integrate_key<R>, dim3(nb), dim3(kBlock), d_sc_.p, pos_.p, vel_.p,
-           (const R4<R>*)acc_.p, (const R4<R>*)xint_.p, (const R4<R>*)vint_.p, mode, key_.p, slot_.p,
-           count_.p, P_);
-    launch("prologue", k_prologue<R>, dim3(1), dim3(1), d_sc_.p, P_);
-    sort_particles();
-    if (sample_dyn) {
-      const int sb = blocks_for((long long)ns_);
-      launch("body_samples", k_body_samples<R>, dim3(sb), dim3(kBlock), (const int*)ns_d_.p,
-             (const Body*)bodies_d_.p, (const R4<R>*)xbody_.p, (const uint32_t*)sorig_.p,
-             (const uint32_t*)sbid_.p, xb_.p, vb_.p);
-      sort_samples();
-    }
-    if (boundary_kind_ == 1)
-      launch("boundary_samples", k_sample_aggregate<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
-             sample_grid(), bW_.p, bG_.p, bGu_.p, P_);
-    else if (boundary_kind_ == 2)
-      launch("boundary_samples", k_vm_sample<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
-             (const VMDesc*)vms_.p, (int)fields_.size(), (const Body*)bodies_d_.p, vmx_.p, vmv_.p, bW_.p,
-             bG_.p, bGu_.p, P_);
-    launch("neighbors_density", k_neighbors_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
-           (const uint32_t*)start_.p, xv_.p, nbr_.p, ncnt_.p, (const R*)bW_.p, boundary_kind_ ? 1 : 0, P_);
-    calc_acceleration();
-    launch("avg_density", k_avg_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
-           (const R4<R>*)vel_.p, partials_.p, P_);
+    issue_update(mode);
     cuda_check(cudaMemcpyAsync(h_sc_, d_sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, stream_), "memcpy");
     sync();
     collect_profile();
@@ -1138,6 +1104,37 @@ class System : public SystemBase {
   }
 
  private:
+  // The kernels of one update, from integration to the average density.
+  void issue_update(int mode) {
+    const int nb = blocks_for((long long)n_);
+    const bool sample_dyn = boundary_kind_ == 1 && any_dynamic_;
+    launch("integrate_key", k_integrate_key<R>, dim3(nb), dim3(kBlock), d_sc_.p, pos_.p, vel_.p,
+           (const R4<R>*)acc_.p, (const R4<R>*)xint_.p, (const R4<R>*)vint_.p, mode, key_.p, slot_.p,
+           count_.p, P_);
+    launch("prologue", k_prologue<R>, dim3(1), dim3(1), d_sc_.p, P_,
+           (capturing_ && cfg_.cfl_time_step) ? 1 : 0);
+    sort_particles();
+    if (sample_dyn) {
+      const int sb = blocks_for((long long)ns_);
+      launch("body_samples", k_body_samples<R>, dim3(sb), dim3(kBlock), (const int*)ns_d_.p,
+             (const Body*)bodies_d_.p, (const R4<R>*)xbody_.p, (const uint32_t*)sorig_.p,
+             (const uint32_t*)sbid_.p, xb_.p, vb_.p);
+      sort_samples();
+    }
+    if (boundary_kind_ == 1)
+      launch("boundary_samples", k_sample_aggregate<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
+             sample_grid(), bW_.p, bG_.p, bGu_.p, P_);
+    else if (boundary_kind_ == 2)
+      launch("boundary_samples", k_vm_sample<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
+             (const VMDesc*)vms_.p, (int)fields_.size(), (const Body*)bodies_d_.p, vmx_.p, vmv_.p, bW_.p,
+             bG_.p, bGu_.p, P_);
+    launch("neighbors_density", k_neighbors_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
+           (const uint32_t*)start_.p, xv_.p, nbr_.p, ncnt_.p, (const R*)bW_.p, boundary_kind_ ? 1 : 0, P_);
+    calc_acceleration();
+    launch("avg_density", k_avg_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
+           (const R4<R>*)vel_.p, partials_.p, P_);
+  }
+
   void zero_body_forces() {
     if (!any_dynamic_) return;
     std::vector<Body> hb = fetch(bodies_d_.p, (size_t)nbodies_);
@@ -1182,6 +1179,229 @@ class System : public SystemBase {
     }
     copy_h2d(d_sc_.p, &next, 1);
     *h_sc_ = next;
+  }
+
+  // ---- graph-captured stepping --------------------------------------------------
+  // One step (body step, update, epilogue) is captured into a CUDA graph; the
+  // IISPH Jacobi loop inside it is a conditional while-node whose body (two
+  // sweep kernels and a condition kernel) repeats until the sweep kernel sets
+  // `converged`. The particle sort ping-pongs between two buffer sets, so two
+  // graphs are captured, one per starting set. A chunk of graph launches
+  // ends with one copy of the step scalars; when any step of it needed host
+  // work the per-step path would have done (neighbor overflow, disabled
+  // particles, a loop that hit its limit), the chunk's starting state is put
+  // back from a device snapshot and the chunk is replayed on that path.
+ public:
+  void set_step_graphs(uint32_t chunk) override {
+    if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
+    graph_chunk_ = chunk;
+    if (!chunk) destroy_graphs();
+    else if (initialized_) prepare_graphs();
+  }
+  uint32_t step_graph_chunk() const override { return graph_chunk_; }
+  uint64_t graph_replays() const override { return graph_replays_; }
+
+  void chunk_begin(uint32_t c) override {
+    if (!initialized_) throw Error(SPH_ERR_STATE, "initialize before stepping");
+    if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
+    if (c == 0) return;
+    prepare_graphs();
+    take_snapshot();
+    chunk_start_sc_ = *h_sc_;
+    chunk_t0_ = std::chrono::steady_clock::now();
+    launch("chunk_begin", k_chunk_begin, dim3(1), dim3(1), d_sc_.p, current_time_);
+    for (uint32_t k = 0; k < c; ++k) {
+      StepGraph& g = graphs_[0].key == (const void*)pos_.p ? graphs_[0] : graphs_[1];
+      if (g.key != (const void*)pos_.p) throw Error(SPH_ERR_STATE, "step graph does not match the buffers");
+      swap_particle_buffers();
+      if (boundary_kind_ == 1 && any_dynamic_) swap_sample_buffers();
+      cuda_check(cudaGraphLaunch(g.exec, stream_), "cudaGraphLaunch");
+    }
+    cuda_check(cudaMemcpyAsync(h_chunk_sc_, d_sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, stream_), "memcpy");
+    cuda_check(cudaEventRecord(chunk_event_, stream_), "cudaEventRecord");
+    chunk_steps_ = c;
+  }
+
+  bool chunk_ready() override {
+    if (!chunk_steps_) return true;
+    return cudaEventQuery(chunk_event_) != cudaErrorNotReady;
+  }
+
+  ChunkOutcome chunk_finish() override {
+    ChunkOutcome o;
+    if (!chunk_steps_) return o;
+    const uint32_t c = chunk_steps_;
+    chunk_steps_ = 0;
+    cuda_check(cudaEventSynchronize(chunk_event_), "chunk");
+    const Scalars s = *h_chunk_sc_;
+    o.steps = c;
+    if (s.trouble) {
+      restore_snapshot();
+      *h_sc_ = chunk_start_sc_;
+      ++graph_replays_;
+      o.replayed = true;
+      o.status = step_plain(c);
+      return o;
+    }
+    *h_sc_ = s;
+    steps_ += c;
+    if (cfg_.cfl_time_step) current_time_ = s.time_acc;
+    avg_density_ = s.avg_density;
+    if (s.iterations > 0) last_iters_ = s.iterations;
+    launches_ += (uint64_t)c * graphs_[0].kernels + 3ull * s.loop_sweeps;
+    wall_ = std::chrono::duration<double>(std::chrono::steady_clock::now() - chunk_t0_).count() / c;
+    o.status = s.status_any == 2 ? SPH_NOT_CONVERGED : SPH_OK;
+    return o;
+  }
+
+ private:
+  struct StepGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const void* key = nullptr;  // position buffer the captured step starts from
+    uint64_t kernels = 0;       // kernel nodes outside the solver loops
+  };
+  static constexpr int kGraphSweepLimit = 10000;  // while-node bound without a sweep cap
+  StepGraph graphs_[2];
+  uint32_t graph_chunk_ = 0, chunk_steps_ = 0;
+  size_t graph_n_ = 0;
+  int graph_K_ = 0;
+  bool capturing_ = false, in_loop_body_ = false;
+  uint64_t capture_kernels_ = 0, graph_replays_ = 0;
+  cudaStream_t body_stream_ = nullptr;
+  cudaEvent_t chunk_event_ = nullptr;
+  Scalars* h_chunk_sc_ = nullptr;
+  Scalars chunk_start_sc_{};
+  std::chrono::steady_clock::time_point chunk_t0_;
+  DBuf<R4<R>> snap_pos_, snap_vel_, snap_acc_, snap_xint_, snap_vint_;
+  DBuf<uint32_t> snap_ref_, snap_fid_;
+  DBuf<Body> snap_bodies_;
+  DBuf<Scalars> snap_sc_;
+
+  void destroy_graphs() {
+    for (auto& g : graphs_) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      if (g.graph) cudaGraphDestroy(g.graph);
+      g = StepGraph{};
+    }
+    graph_n_ = 0;
+    graph_K_ = 0;
+  }
+
+  void prepare_graphs() {
+    if (graphs_[0].exec && graph_n_ == n_ && graph_K_ == K_) return;
+    destroy_graphs();
+    if (!body_stream_) cuda_check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (!chunk_event_) cuda_check(cudaEventCreateWithFlags(&chunk_event_, cudaEventDisableTiming), "cudaEventCreate");
+    if (!h_chunk_sc_) cuda_check(cudaMallocHost((void**)&h_chunk_sc_, sizeof(Scalars)), "cudaMallocHost");
+    alloc_snapshot();
+    // capturing swaps the host-side buffer pointers as a launch would; two
+    // captures in a row bring them back to where they started
+    capture_step(graphs_[0]);
+    capture_step(graphs_[1]);
+    if (graphs_[0].key != (const void*)pos_.p) throw Error(SPH_ERR_STATE, "step graphs out of phase");
+    graph_n_ = n_;
+    graph_K_ = K_;
+  }
+
+  void capture_step(StepGraph& g) {
+    g.key = (const void*)pos_.p;
+    capture_kernels_ = 0;
+    cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    capturing_ = true;
+    try {
+      if (any_dynamic_)
+        launch("body_step", k_body_step, dim3(1), dim3(32), bodies_d_.p, nbodies_, (const Scalars*)d_sc_.p);
+      issue_update(cfg_.integration_scheme == SPH_TAKE_PREDICTED ? 1 : 0);
+      const int loop = cfg_.pressure_solver == SPH_IISPH || cfg_.pressure_solver == SPH_IISPH_W_OST;
+      launch("step_epilogue", k_step_epilogue, dim3(1), dim3(1), d_sc_.p, K_, loop);
+    } catch (...) {
+      capturing_ = false;
+      in_loop_body_ = false;
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(stream_, &junk);
+      if (junk) cudaGraphDestroy(junk);
+      cudaGetLastError();
+      throw;
+    }
+    capturing_ = false;
+    cuda_check(cudaStreamEndCapture(stream_, &g.graph), "cudaStreamEndCapture");
+    cuda_check(cudaGraphInstantiate(&g.exec, g.graph, 0), "cudaGraphInstantiate");
+    g.kernels = capture_kernels_;
+  }
+
+  // resolve_pressure_globally's loop (iisph.rs:419-550) as a while-node.
+  void solve_loop_graph() {
+    cudaStreamCaptureStatus st;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cuda_check(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &graph, &deps, &nd), "cudaStreamGetCaptureInfo");
+    cudaGraphConditionalHandle handle;
+    cuda_check(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault),
+               "cudaGraphConditionalHandleCreate");
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    cuda_check(cudaGraphAddNode(&node, graph, deps, nd, &np), "cudaGraphAddNode");
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    cuda_check(cudaStreamBeginCaptureToGraph(body_stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+               "cudaStreamBeginCaptureToGraph");
+    const int limit = P_.iteration_cap > 0 ? P_.iteration_cap : kGraphSweepLimit;
+    std::swap(stream_, body_stream_);
+    in_loop_body_ = true;
+    try {
+      iisph_iteration(-1);
+      launch("solve_loop", k_loop_cond, dim3(1), dim3(1), handle, (const Scalars*)d_sc_.p, limit);
+    } catch (...) {
+      in_loop_body_ = false;
+      std::swap(stream_, body_stream_);
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(body_stream_, &junk);
+      throw;
+    }
+    in_loop_body_ = false;
+    std::swap(stream_, body_stream_);
+    cudaGraph_t captured = nullptr;
+    cuda_check(cudaStreamEndCapture(body_stream_, &captured), "cudaStreamEndCapture");
+    cuda_check(cudaStreamUpdateCaptureDependencies(stream_, &node, 1, cudaStreamSetCaptureDependencies),
+               "cudaStreamUpdateCaptureDependencies");
+  }
+
+  // State that a chunk of steps reads from the step before it.
+  template <class T>
+  void d2d(T* dst, const T* src, size_t n) {
+    if (n) cuda_check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice, stream_), "D2D");
+  }
+  void alloc_snapshot() {
+    const bool tp = cfg_.integration_scheme == SPH_TAKE_PREDICTED;
+    if (snap_pos_.n < n_ || !snap_pos_.p) {
+      const size_t c = std::max<size_t>(n_, 1);
+      snap_pos_.alloc(c); snap_vel_.alloc(c); snap_acc_.alloc(c); snap_ref_.alloc(c); snap_fid_.alloc(c);
+      if (tp) { snap_xint_.alloc(c); snap_vint_.alloc(c); }
+    }
+    if (!snap_sc_.p) snap_sc_.alloc(1);
+    if (nbodies_ && snap_bodies_.n < (size_t)nbodies_) snap_bodies_.alloc((size_t)nbodies_);
+  }
+  void take_snapshot() {
+    const bool tp = cfg_.integration_scheme == SPH_TAKE_PREDICTED;
+    d2d(snap_pos_.p, pos_.p, n_); d2d(snap_vel_.p, vel_.p, n_); d2d(snap_acc_.p, acc_.p, n_);
+    d2d(snap_ref_.p, ref_.p, n_); d2d(snap_fid_.p, fid_.p, n_);
+    if (tp) { d2d(snap_xint_.p, xint_.p, n_); d2d(snap_vint_.p, vint_.p, n_); }
+    if (nbodies_) d2d(snap_bodies_.p, bodies_d_.p, (size_t)nbodies_);
+    d2d(snap_sc_.p, d_sc_.p, 1);
+  }
+  void restore_snapshot() {
+    const bool tp = cfg_.integration_scheme == SPH_TAKE_PREDICTED;
+    d2d(pos_.p, snap_pos_.p, n_); d2d(vel_.p, snap_vel_.p, n_); d2d(acc_.p, snap_acc_.p, n_);
+    d2d(ref_.p, snap_ref_.p, n_); d2d(fid_.p, snap_fid_.p, n_);
+    if (tp) { d2d(xint_.p, snap_xint_.p, n_); d2d(vint_.p, snap_vint_.p, n_); }
+    if (nbodies_) d2d(bodies_d_.p, snap_bodies_.p, (size_t)nbodies_);
+    d2d(d_sc_.p, snap_sc_.p, 1);
+    sync();
   }
 };
 
@@ -1355,7 +1575,7 @@ void System<R>::restore(uint64_t steps, double time, size_t n, const double* x, 
   update(2);  // continue_from_checkpoint (sph/mod.rs:362-378)
 }
 
-static SystemBase* create_system(const sph_config& c) {
+SystemBase* create_system(const sph_config& c) {
   if (c.precision == SPH_F64) return new System<double>(c);
   return new System<float>(c);
 }
@@ -1739,6 +1959,7 @@ int sph_clone(const sph_system_t* src, sph_system_t** out) {
     }
     h->impl->restore(s->steps(), s->time(), n, x.data(), v.data(), m.data(), fid.data(),
                      xi.empty() ? nullptr : xi.data(), vvi.empty() ? nullptr : vvi.data());
+    h->impl->set_step_graphs(s->step_graph_chunk());
     *out = guard.release();
   });
 }
@@ -1747,6 +1968,19 @@ int sph_launch_count(const sph_system_t* h, uint64_t* out) {
   return guarded([&] {
     if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
     *out = h->impl->launches();
+  });
+}
+int sph_set_step_graphs(sph_system_t* h, uint32_t chunk_steps) {
+  return guarded([&] {
+    if (!h) throw Error(SPH_ERR_INVALID, "null argument");
+    set_device(h);
+    h->impl->set_step_graphs(chunk_steps);
+  });
+}
+int sph_graph_replays(const sph_system_t* h, uint64_t* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    *out = h->impl->graph_replays();
   });
 }
 int sph_set_profiling(sph_system_t* h, int enabled) {

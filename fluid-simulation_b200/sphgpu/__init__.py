@@ -6,7 +6,8 @@ marshals inputs and results.
 """
 from . import _capi as capi
 from ._capi import SPHError
+from .server import SceneServer
 from .system import GpuSystem, RigidInit, find_samples, kernel_function, kernel_gradient, make_config
 
-__all__ = ["capi", "SPHError", "GpuSystem", "RigidInit", "find_samples", "kernel_function",
+__all__ = ["capi", "SPHError", "GpuSystem", "RigidInit", "SceneServer", "find_samples", "kernel_function",
            "kernel_gradient", "make_config"]

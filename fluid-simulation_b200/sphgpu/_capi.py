@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libsphgpu.so")
 
 # status codes
 SPH_OK, SPH_ERR_INVALID, SPH_ERR_OOM, SPH_ERR_CUDA = 0, 1, 2, 3
-SPH_NOT_CONVERGED, SPH_ERR_STATE, SPH_ERR_CAPACITY = 4, 5, 6
+SPH_NOT_CONVERGED, SPH_ERR_STATE, SPH_ERR_CAPACITY, SPH_PENDING = 4, 5, 6, 7
 
 # procedure variants
 CUBIC_BSPLINE_3D = 0
@@ -92,6 +92,40 @@ class SphStepStats(C.Structure):
                 ("not_converged", C.c_int)]
 
 
+class SphServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int), ("memory_budget_bytes", C.c_uint64), ("max_active", C.c_uint32),
+                ("chunk_steps", C.c_uint32)]
+
+
+class SphSampleSet(C.Structure):
+    _fields_ = [("count", C.c_size_t), ("positions", C.c_void_p), ("rigid", C.POINTER(SphRigidInit))]
+
+
+class SphVolumeMapSet(C.Structure):
+    _fields_ = [("sdf", C.POINTER(SphGridDesc)), ("sdf_nodes", C.c_void_p), ("vm", C.POINTER(SphGridDesc)),
+                ("vm_nodes", C.c_void_p), ("rigid", C.POINTER(SphRigidInit))]
+
+
+class SphSceneRequest(C.Structure):
+    _fields_ = [("config", SphConfig), ("n", C.c_size_t), ("position", C.c_void_p), ("velocity", C.c_void_p),
+                ("mass", C.c_void_p), ("fluid_id", C.c_void_p), ("num_sample_sets", C.c_size_t),
+                ("sample_sets", C.POINTER(SphSampleSet)), ("num_volume_maps", C.c_size_t),
+                ("volume_maps", C.POINTER(SphVolumeMapSet)), ("steps", C.c_uint32), ("keep_state", C.c_int)]
+
+
+class SphSceneResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("steps", C.c_uint64), ("time", C.c_double), ("particles", C.c_uint64),
+                ("measurement", SphMeasurement), ("submit_s", C.c_double), ("start_s", C.c_double),
+                ("finish_s", C.c_double), ("device_bytes_reserved", C.c_uint64),
+                ("graph_replays", C.c_uint64), ("kernel_launches", C.c_uint64)]
+
+
+class SphServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in (
+        "submitted", "completed", "queued", "active", "peak_active", "budget_bytes", "reserved_bytes",
+        "peak_reserved_bytes", "graph_replays", "kernel_launches")]
+
+
 class SPHError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"sphgpu error {code}: {msg}")
@@ -154,6 +188,16 @@ SIGNATURES = {
     "sph_set_profiling": (C.c_int, [_vp, C.c_int]),
     "sph_kernel_time": (C.c_int, [_vp, C.c_char_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "sph_device_bytes": (C.c_int, [_vp, C.POINTER(_sz)]),
+    "sph_set_step_graphs": (C.c_int, [_vp, C.c_uint32]),
+    "sph_graph_replays": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "sph_server_create": (C.c_int, [C.POINTER(SphServerConfig), C.POINTER(_vp)]),
+    "sph_server_submit": (C.c_int, [_vp, C.POINTER(SphSceneRequest), C.POINTER(C.c_uint64)]),
+    "sph_server_poll": (C.c_int, [_vp, C.c_uint64, C.POINTER(SphSceneResult)]),
+    "sph_server_wait": (C.c_int, [_vp, C.c_uint64, C.c_double, C.POINTER(SphSceneResult)]),
+    "sph_server_fetch_state": (C.c_int, [_vp, C.c_uint64, _dp, _dp]),
+    "sph_server_release": (C.c_int, [_vp, C.c_uint64]),
+    "sph_server_get_stats": (C.c_int, [_vp, C.POINTER(SphServerStats)]),
+    "sph_server_destroy": (None, [_vp]),
 }
 
 _lib = None

@@ -41,7 +41,10 @@ def transform_mesh(verts, translation=(0, 0, 0), rotation_euler_deg=(0, 0, 0), s
 
 
 def sample_triangle_surface(v0, v1, v2, spacing):
-    """Isotropic raster of one triangle (utilities/sampling.rs:59-106)."""
+    """Isotropic raster of one triangle (utilities/sampling.rs:59-106): grid
+    points (min + i*spacing, min + j*spacing) of the triangle's 2D frame, row
+    j outer, kept when inside or on the triangle (no two edge functions of
+    opposite sign), mapped back as v0 + e_u x + e_v y."""
     e1, e2 = v1 - v0, v2 - v0
     l1 = np.sqrt((e1[0] * e1[0] + e1[1] * e1[1]) + e1[2] * e1[2])
     if l1 < 1e-12:
@@ -58,21 +61,20 @@ def sample_triangle_surface(v0, v1, v2, spacing):
     min_y, max_y = p[:, 1].min(), p[:, 1].max()
     nx = int(np.ceil((max_x - min_x) / spacing))
     ny = int(np.ceil((max_y - min_y) / spacing))
-    out = []
     a, b, c = p
-    for j in range(ny + 1):
-        y = min_y + j * spacing
-        for i in range(nx + 1):
-            x = min_x + i * spacing
-            q = np.array([x, y])
-            d1 = _cross2(b - a, q - a)
-            d2 = _cross2(c - b, q - b)
-            d3 = _cross2(a - c, q - c)
-            has_neg = d1 < 0.0 or d2 < 0.0 or d3 < 0.0
-            has_pos = d1 > 0.0 or d2 > 0.0 or d3 > 0.0
-            if not (has_neg and has_pos):
-                out.append(v0 + eu * x + ev * y)
-    return np.array(out).reshape(-1, 3)
+    y = min_y + np.arange(ny + 1, dtype=np.float64) * spacing
+    x = min_x + np.arange(nx + 1, dtype=np.float64) * spacing
+    Y, X = np.meshgrid(y, x, indexing="ij")
+    X, Y = X.ravel(), Y.ravel()
+
+    def edge(p0, p1):
+        return (p1[0] - p0[0]) * (Y - p0[1]) - (p1[1] - p0[1]) * (X - p0[0])
+    d1, d2, d3 = edge(a, b), edge(b, c), edge(c, a)
+    has_neg = (d1 < 0.0) | (d2 < 0.0) | (d3 < 0.0)
+    has_pos = (d1 > 0.0) | (d2 > 0.0) | (d3 > 0.0)
+    keep = ~(has_neg & has_pos)
+    X, Y = X[keep], Y[keep]
+    return (v0[None, :] + eu[None, :] * X[:, None]) + ev[None, :] * Y[:, None]
 
 
 def _cross2(a, b):
@@ -238,3 +240,70 @@ def floating_cube_scene(n_side=12, spacing=0.02, body_side=0.12, body_density=50
     sc.sample_boundaries.append((samples, rigid))
     sc.description += f", dynamic cube body with {samples.shape[0]} samples"
     return sc
+
+
+def serving_dam_break(n_target, solver="SESPH", stiffness=1000.0, viscosity=0.01, rest_density=1000.0,
+                      spacing=0.02, time_increment=1e-3, seed=0):
+    """Dam break of the scene sweep: an n_side^3 lattice block (n_side =
+    round(n_target^(1/3)), +-1 % jitter) against the -x end of a box
+    container of 2 x 1 x 1.5 block lengths sampled as a StaticSampleBoundary
+    at 0.7 * spacing from the reference's inward cube mesh; support 2h, fixed
+    dt, EulerCromer. IISPH uses omega 0.5, target density error 0.1 % and at
+    most 100 sweeps."""
+    n_side = max(4, int(round(n_target ** (1.0 / 3.0))))
+    h = spacing
+    L = n_side * h
+    half = np.array([L, 0.5 * L, 0.75 * L])
+    verts = transform_mesh(CUBE_VERTICES, scale=tuple(half))
+    samples = sample_triangle_mesh_surface(verts, CUBE_FACES_INWARD, 0.7 * h)
+    pos = lattice_block((n_side, n_side, n_side), h, origin=-half, jitter=0.01, seed=seed)
+    params = {"rest_density_grid_spacing": h, "kernel_support_radius": 2 * h,
+              "disable_particles_below": -50.0, "fluid_viscosity": viscosity,
+              "boundary_viscosity": viscosity, "boundary_pressure_acceleration_weighting": 0.7,
+              "boundary_rest_volume_weighting": 1.0, "time_increment": time_increment}
+    if solver == "SESPH":
+        params["stiffness"] = stiffness
+    else:
+        params.update({"target_density_error": 0.1, "relaxation_factor": 0.5, "min_diagonal_element": 1e-10,
+                       "max_solver_iterations": 100})
+    return Scene(
+        procedures={"kernel_function": "CubicBSpline3D", "integration_scheme": "EulerCromer",
+                    "pressure_solver": solver, "neighbor_search": "SpatialHashing",
+                    "boundary_handling": "StaticSampleBoundary"},
+        parameters=params, cfl_time_step=False, position=pos,
+        mass=np.full(pos.shape[0], rest_density * h ** 3), sample_boundaries=[(samples, None)],
+        mesh=(verts, CUBE_FACES_INWARD),
+        description=f"{solver} dam break {pos.shape[0]} particles, {samples.shape[0]} boundary samples")
+
+
+@dataclass
+class SceneRequest:
+    """One request of the scene sweep."""
+    arrival_s: float
+    n_target: int
+    solver: str
+    stiffness: float
+    viscosity: float
+    rest_density: float
+    steps: int
+    seed: int
+
+    def scene(self) -> Scene:
+        return serving_dam_break(self.n_target, self.solver, self.stiffness, self.viscosity, self.rest_density,
+                                 seed=self.seed)
+
+
+def scene_sweep(count=256, rate_per_s=20.0, n_min=5000, n_max=500000, steps=500, seed=5):
+    """Seeded parameter sweep of dam-break scenes: Poisson arrivals at
+    `rate_per_s`, particle counts log-uniform in [n_min, n_max], SESPH or
+    IISPH with equal probability, stiffness U[500, 5000], viscosity
+    U[0.001, 0.05], rest density U[500, 1500], `steps` time steps each."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate_per_s, count))
+    n = np.exp(rng.uniform(np.log(n_min), np.log(n_max), count))
+    solver = rng.integers(0, 2, count)
+    k = rng.uniform(500.0, 5000.0, count)
+    nu = rng.uniform(0.001, 0.05, count)
+    rho = rng.uniform(500.0, 1500.0, count)
+    return [SceneRequest(float(arrivals[i]), int(n[i]), "SESPH" if solver[i] == 0 else "IISPH", float(k[i]),
+                         float(nu[i]), float(rho[i]), int(steps), int(seed * 100003 + i)) for i in range(count)]

@@ -345,6 +345,15 @@ class GpuSystem:
         A.check(self._L.sph_device_bytes(self._h, C.byref(out)))
         return out.value
 
+    def set_step_graphs(self, chunk_steps: int):
+        """Graph-captured stepping in chunks of `chunk_steps` (0: per-step path)."""
+        A.check(self._L.sph_set_step_graphs(self._h, int(chunk_steps)))
+
+    def graph_replays(self) -> int:
+        out = C.c_uint64()
+        A.check(self._L.sph_graph_replays(self._h, C.byref(out)))
+        return out.value
+
 
 # ---- per-trait shims ------------------------------------------------------------------
 def find_samples(search_range, positions, samples, device=0):

@@ -36,6 +36,7 @@ enum sph_status {
   SPH_NOT_CONVERGED = 4,    /* IISPH hit `max_solver_iterations` (step still completed) */
   SPH_ERR_STATE = 5,        /* call out of order (e.g. step before initialize) */
   SPH_ERR_CAPACITY = 6,     /* a caller buffer is too small; required size returned */
+  SPH_PENDING = 7,          /* a served scene has not finished yet */
 };
 
 /* ---- procedure variants (sph/setup/input.rs:101-134 `Procedures`) ------ */
@@ -299,6 +300,20 @@ int sph_build_volume_map_field(const sph_grid_desc* sdf_grid, const double* sdf_
                                const sph_grid_desc* vm_grid, double kernel_support_radius,
                                int quadrature_degree, double* nodes_out, int device);
 
+/* ---- graph-captured stepping -------------------------------------------- */
+/* With chunk_steps > 0, sph_step captures one time step (with its IISPH
+ * Jacobi loop as a conditional while-node) into a CUDA graph and advances in
+ * chunks of up to chunk_steps graph launches with one host check per chunk
+ * instead of one per step. Results are the same as the per-step path: a
+ * chunk in which a step needed host work (neighbor capacity growth, disabled
+ * particles, a solve still unconverged after 10000 sweeps without a cap) is
+ * put back from a device snapshot and replayed per step. 0 (the default)
+ * selects the per-step path. Profiling (sph_set_profiling) uses the per-step
+ * path. */
+int sph_set_step_graphs(sph_system_t* h, uint32_t chunk_steps);
+/* Chunks replayed on the per-step path since creation. */
+int sph_graph_replays(const sph_system_t* h, uint64_t* out);
+
 /* ---- diagnostics -------------------------------------------------------- */
 /* Scalars of the last completed update, read from the host copy the step
  * already made (no device work). */
@@ -325,6 +340,89 @@ int sph_set_profiling(sph_system_t* h, int enabled);
 int sph_kernel_time(sph_system_t* h, const char* kernel, double* ms, uint64_t* launches);
 /* Device-resident bytes held by the handle. */
 int sph_device_bytes(const sph_system_t* h, size_t* out);
+
+/* ---- scene server: continuous batching of scene solves on one GPU -------- */
+/* The reference runs one scene per backend worker (sci-phi-backend/src/lib.rs:
+ * 190-210 steps a Box<dyn SPHSystem> in a loop). The server is the request
+ * loop form of that worker: scenes are submitted at any time, admitted while
+ * the device has slots and memory for them (an estimate of each scene's
+ * device bytes against a budget), advanced concurrently (each on its own
+ * stream, in chunks of graph-captured steps issued by one scheduler thread)
+ * and retired at their step count. A scene's result does not depend on what
+ * else runs beside it. */
+typedef struct sph_server sph_server_t;
+
+typedef struct sph_server_config {
+  int device;                   /* CUDA device ordinal */
+  uint64_t memory_budget_bytes; /* 0: 90 % of the device memory free at creation */
+  uint32_t max_active;          /* scenes on the device at once; 0: 64 */
+  uint32_t chunk_steps;         /* graph launches per host check; 0: 25 */
+} sph_server_config;
+
+typedef struct sph_sample_set {   /* one sph_add_sample_boundary call */
+  size_t count;
+  const double* positions;        /* 3*count */
+  const sph_rigid_init* rigid;    /* NULL: static */
+} sph_sample_set;
+
+typedef struct sph_volume_map_set {  /* one sph_add_volume_map_boundary call */
+  const sph_grid_desc* sdf;
+  const double* sdf_nodes;
+  const sph_grid_desc* vm;
+  const double* vm_nodes;
+  const sph_rigid_init* rigid;
+} sph_volume_map_set;
+
+typedef struct sph_scene_request {
+  sph_config config;
+  size_t n;                       /* fluid particles */
+  const double* position;         /* 3n */
+  const double* velocity;         /* 3n or NULL */
+  const double* mass;             /* n */
+  const uint32_t* fluid_id;       /* n or NULL */
+  size_t num_sample_sets;
+  const sph_sample_set* sample_sets;
+  size_t num_volume_maps;
+  const sph_volume_map_set* volume_maps;
+  uint32_t steps;                 /* time steps to run */
+  int keep_state;                 /* 1: keep the final positions/velocities */
+} sph_scene_request;
+
+typedef struct sph_scene_result {
+  int status;                     /* SPH_OK, SPH_NOT_CONVERGED or an error code */
+  uint64_t steps;                 /* steps run */
+  double time;                    /* simulated time */
+  uint64_t particles;             /* active particles at the end */
+  sph_measurement measurement;    /* take_measurement at the end */
+  double submit_s, start_s, finish_s;  /* seconds since server creation */
+  uint64_t device_bytes_reserved; /* admission estimate */
+  uint64_t graph_replays;         /* chunks redone on the per-step path */
+  uint64_t kernel_launches;
+} sph_scene_result;
+
+typedef struct sph_server_stats {
+  uint64_t submitted, completed, queued, active, peak_active;
+  uint64_t budget_bytes, reserved_bytes, peak_reserved_bytes;
+  uint64_t graph_replays, kernel_launches;
+} sph_server_stats;
+
+int sph_server_create(const sph_server_config* cfg, sph_server_t** out);
+/* Copies the request (the caller may free its arrays on return). Fails with
+ * SPH_ERR_CAPACITY when the scene alone exceeds the memory budget. */
+int sph_server_submit(sph_server_t* s, const sph_scene_request* req, uint64_t* ticket);
+/* SPH_OK and the result once the scene finished, else SPH_PENDING. */
+int sph_server_poll(sph_server_t* s, uint64_t ticket, sph_scene_result* out);
+/* Blocks up to timeout_s seconds (< 0: no limit); SPH_PENDING on timeout. */
+int sph_server_wait(sph_server_t* s, uint64_t ticket, double timeout_s, sph_scene_result* out);
+/* Final positions and velocities (3*particles doubles each, reference index
+ * order) of a finished scene submitted with keep_state = 1. */
+int sph_server_fetch_state(sph_server_t* s, uint64_t ticket, double* position, double* velocity);
+/* Drops a finished scene's result. */
+int sph_server_release(sph_server_t* s, uint64_t ticket);
+int sph_server_get_stats(sph_server_t* s, sph_server_stats* out);
+/* Cancels queued scenes, stops running ones after their current chunk and
+ * frees everything. */
+void sph_server_destroy(sph_server_t* s);
 
 #ifdef __cplusplus
 }
