@@ -66,7 +66,11 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--profile", action="store_true", help="per-kernel CUDA-event timing (default on)")
+    p.add_argument("--serving-requests", type=int, default=256,
+                   help="scene-sweep requests served batched and one at a time (0: skip)")
+    p.add_argument("--serving-plain-requests", type=int, default=-1,
+                   help="requests of the one-at-a-time arm (-1: all)")
+    p.add_argument("--serving-steps", type=int, default=500)
     return p.parse_args()
 
 
@@ -195,6 +199,76 @@ def run_cpu(n_side, steps, warmup, max_iters, fields, min_seconds=0.0):
     return updates / dt, dt, O.num_threads(), sc.position.shape[0], done, statistics.mean(sweeps)
 
 
+def _pct(values, q):
+    return float(np.percentile(np.asarray(values, np.float64), q)) if len(values) else None
+
+
+def serving_sweep(args, device, rank, ws):
+    """The scene sweep (Poisson arrivals at 20/s, 5k-500k particles, SESPH or
+    IISPH, 500 steps each) served two ways on this GPU: batched by the scene
+    server (continuous admission, concurrent graph-captured scenes) and one
+    scene at a time through the plain single-scene C ABI path, in arrival
+    order. Scenes/s = completed scenes / (last completion - first arrival);
+    latency = completion - arrival. The first requests of both arms keep their
+    final state, which must agree bit for bit."""
+    from sphgpu import scenes
+    from sphgpu.replicas import aggregate, share
+    from sphgpu.server import SceneServer
+    reqs = share(scenes.scene_sweep(count=args.serving_requests, steps=args.serving_steps), rank, ws)
+    built = [r.scene() for r in reqs]
+    n_check = min(4, len(reqs))
+
+    srv = SceneServer(device=device)
+    t0 = time.perf_counter()
+    tickets = []
+    for k, (r, sc) in enumerate(zip(reqs, built)):
+        wait = t0 + r.arrival_s - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        tickets.append(srv.submit(sc, r.steps, keep_state=k < n_check))
+    res = [srv.wait(t, -1) for t in tickets]
+    kept = [srv.fetch_state(t, x["particles"]) for t, x in zip(tickets[:n_check], res[:n_check])]
+    st = srv.stats()
+    srv.close()
+    span = max(x["finish_s"] for x in res) - min(x["submit_s"] for x in res)
+    lat = [x["latency_s"] for x in res]
+    pu = sum(x["particles"] * x["steps"] for x in res)
+    span_ms, done = aggregate(span * 1000.0, len(res), device="cuda")
+    batched = {"scenes_per_s": done / (span_ms / 1000.0), "span_s": span_ms / 1000.0,
+               "p50_s": _pct(lat, 50), "p95_s": _pct(lat, 95), "p99_s": _pct(lat, 99),
+               "particle_updates_per_s": pu / span, "peak_active": st["peak_active"],
+               "graph_replays": st["graph_replays"], "kernel_launches": st["kernel_launches"],
+               "statuses": sorted({x["status"] for x in res})}
+
+    m = len(reqs) if args.serving_plain_requests < 0 else min(len(reqs), args.serving_plain_requests)
+    from sphgpu import capi
+    t0 = time.perf_counter()
+    lat, same = [], 0
+    for k, (r, sc) in enumerate(zip(reqs[:m], built[:m])):
+        ta = t0 + r.arrival_s
+        wait = ta - time.perf_counter()
+        if wait > 0:
+            time.sleep(wait)
+        g = scenes.build_system(sc, device=device)
+        g.step_forward_in_time(r.steps)
+        g.take_measurement()
+        if k < n_check:
+            same += int(np.array_equal(g.download(capi.FIELD_POSITION), kept[k][0]) and
+                        np.array_equal(g.download(capi.FIELD_VELOCITY), kept[k][1]))
+        g.close()
+        lat.append(time.perf_counter() - ta)
+    span = time.perf_counter() - (t0 + reqs[0].arrival_s) if m else 0.0
+    span_ms, done = aggregate(span * 1000.0, m, device="cuda")
+    plain = {"scenes_per_s": done / (span_ms / 1000.0) if span_ms else None, "span_s": span_ms / 1000.0,
+             "requests": m, "p50_s": _pct(lat, 50), "p95_s": _pct(lat, 95), "p99_s": _pct(lat, 99)}
+    return {"metric": "scenes/s (Poisson scene sweep, batched server vs one-at-a-time plain GPU solves)",
+            "requests": args.serving_requests, "arrival_rate_per_s": 20.0, "steps_per_scene": args.serving_steps,
+            "particles_per_scene": "log-uniform 5k-500k (cubic blocks)", "solvers": "SESPH / IISPH 50:50",
+            "batched": batched, "plain": plain,
+            "batched_over_plain": (batched["scenes_per_s"] / plain["scenes_per_s"]) if plain["scenes_per_s"] else None,
+            "identical_final_state": f"{same}/{n_check if m >= n_check else min(m, n_check)}"}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
@@ -245,14 +319,8 @@ def main():
             kernel_times[name] = kt
     sysm.set_profiling(False)
     # whole-job aggregate: sum of updates over ranks / max time over ranks
-    if ws > 1:
-        t = torch.tensor([ms, float(updates)], device="cuda", dtype=torch.float64)
-        tmax = t.clone()
-        dist.all_reduce(tmax[:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-        ms_max, total_updates = float(tmax[0]), float(t[1])
-    else:
-        ms_max, total_updates = ms, float(updates)
+    from sphgpu.replicas import aggregate
+    ms_max, total_updates = aggregate(ms, updates, device="cuda")
     value = total_updates / (ms_max / 1000.0)
 
     # e2e: the plugin call with host buffers (reference order), copies inside
@@ -279,11 +347,7 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)
-        if ws > 1:
-            t = torch.tensor([ems, float(e_updates)], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t[:1], op=dist.ReduceOp.MAX)
-            dist.all_reduce(t[1:], op=dist.ReduceOp.SUM)
-            ems, e_updates = float(t[0]), float(t[1])
+        ems, e_updates = aggregate(ems, e_updates, device="cuda")
         e2e = {"value": e_updates / (ems / 1000.0), "unit": UNIT,
                "h2d_bytes_per_step": 2 * 3 * 8 * n, "d2h_bytes_per_step": 2 * 3 * 8 * n}
 
@@ -313,6 +377,8 @@ def main():
                          f"block of the same configuration, {sweeps:.0f} IISPH sweeps per step, f64 C++ "
                          f"restatement of the reference CPU path on all host threads, {secs:.1f} s"}
 
+    sysm.close()
+    serving = serving_sweep(args, local, rank, ws) if args.serving_requests > 0 else None
     if ws > 1:
         dist.barrier()
     if rank == 0:
@@ -328,6 +394,7 @@ def main():
                        "l2": "working set > L2 (neighbor lists alone exceed 126 MB); no flush needed",
                        "mean_solver_iterations": statistics.mean(iters) if iters else None},
             "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "serving": serving,
         }
         print(json.dumps(line))
     if ws > 1:

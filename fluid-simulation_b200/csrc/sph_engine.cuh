@@ -7,9 +7,12 @@
 //   acc   R4 {ax,ay,az,-}   total acceleration
 //   ref   u32               reference-order index (the row a download writes)
 //   fid   u32               fluid id
-//   nbr   u32 [Np/32][K/4][32][4]  fluid neighbor lists, warp-tiled: lane
-//                           `i%32` of tile `i/32` keeps neighbors 4g..4g+3 in
-//                           one 16-byte group; self is implicit, not stored
+//   nbr   u16 [Np/32][K/4][32][4]  fluid neighbor lists as positions in the
+//                           block's halo, warp-tiled: lane `i%32` of tile
+//                           `i/32` keeps neighbors 4g..4g+3 in one 8-byte
+//                           group; self is implicit, not stored
+//   halo  u32 [blocks][hcap] particle indices of each block's halo (the union
+//                           of its cells' stencil buckets), ascending
 //   ncnt  u32 [N]           neighbor counts
 //   bW, bG, bGu             per-particle boundary aggregates (see kernels)
 //   IISPH scratch: vstar R4, s R, aii R, accp R4, p R
@@ -44,6 +47,7 @@ struct Scalars {
   int status;                      // 0 ok, 2 not converged within the cap
   int iterations_eqs1;             // IISPHwOST first solve sweeps
   int max_bnbrs;                   // largest boundary-sample neighbor count seen
+  int max_halo;                    // largest block halo (particles) seen
   // graph-captured stepping (the host reads these once per chunk)
   double time_acc;                 // simulated time under CFL steps
   unsigned int trouble;            // bits: 1 neighbor overflow, 2 disabled particles, 4 unconverged

@@ -174,6 +174,7 @@ __global__ void k_prologue(Scalars* sc, StepParams<R> P, int accumulate_time) {
   }
   sc->max_nbrs = 0;
   sc->max_bnbrs = 0;
+  sc->max_halo = 0;
   sc->iterations = 0;
   sc->iterations_eqs1 = 0;
   sc->converged = 0;
@@ -350,16 +351,57 @@ __global__ void __launch_bounds__(kBlock) k_gather_samples(
 }
 
 // ---------------------------------------------------------------------------
-// 4. fluid neighbor lists + volume (fused)
+// 4. fluid neighbor lists + volume (fused), block halos
+//
+// The particles of one block (kBlock consecutive particles in bucket order)
+// find their neighbors in the union of the 27-bucket stencils of their
+// cells: the block's halo. Because buckets are contiguous in memory and the
+// halo is kept in ascending bucket key order, the halo is a short list of
+// runs of consecutive particle indices (halo_idx, ascending). Neighbor lists
+// hold 16-bit positions in the block's halo. The passes over neighbors copy
+// the halo's records into shared memory once per launch (ordered loads of
+// those runs) and gather from there; a block whose halo does not fit the
+// shared-memory capacity gathers through halo_idx from global memory.
 //
 // Neighbor-list layout: particle i = 32*t + lane keeps its k-th neighbor at
 //   ((t * K/4 + k/4) * 32 + lane) * 4 + k % 4      (K a multiple of 4)
-// i.e. tile-major, then groups of four neighbors, then lane.
+// i.e. tile-major, then groups of four neighbors, then lane, so a warp reads
+// the next four neighbors of all its lanes as one 256-byte coalesced load.
 __device__ __forceinline__ size_t nbr_slot(int i, int k, int K) {
   const size_t t = (size_t)(i >> 5), lane = (size_t)(i & 31);
   return ((t * (size_t)(K >> 2) + (size_t)(k >> 2)) * 32 + lane) * 4 + (size_t)(k & 3);
 }
-// ---------------------------------------------------------------------------
+
+constexpr int kHaloKeys = 8192;            // >= 27 * kBlock stencil keys, a power of two
+constexpr uint32_t kNoKey = 0xffffffffu;
+constexpr size_t kSearchSmem = kHaloKeys * (sizeof(uint32_t) + sizeof(uint16_t));
+
+// Neighbor lists of one step and the block halos they index.
+struct NbrArgs {
+  const uint16_t* nbr;   // halo positions, layout of nbr_slot
+  const uint32_t* ncnt;  // neighbors per particle (self excluded)
+  const uint32_t* hidx;  // [blocks][hcap] halo particle indices
+  const uint32_t* hn;    // [blocks] halo sizes
+  int K;                 // list capacity per particle
+  int hcap;              // halo table capacity per block
+  int hs;                // halo records a launch stages in shared memory
+};
+
+// The block's halo: its particle indices, its size and whether the launch
+// copies its records to shared memory.
+struct HaloView {
+  const uint32_t* idx;
+  int size;
+  bool staged;
+};
+__device__ __forceinline__ HaloView halo_view(const NbrArgs& N) {
+  HaloView h;
+  h.idx = N.hidx + (size_t)blockIdx.x * (size_t)N.hcap;
+  h.size = min((int)N.hn[blockIdx.x], N.hcap);
+  h.staged = h.size <= N.hs;
+  return h;
+}
+
 template <class R>
 __device__ __forceinline__ void kahan_add(R& s, R& c, R t) {
   const R y = t - c;
@@ -371,46 +413,131 @@ __device__ __forceinline__ void kahan_add(R& s, R& c, R t) {
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_neighbors_density(
     Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, const uint32_t* __restrict__ start,
-    R4<R>* __restrict__ xv, uint32_t* __restrict__ nbr, uint32_t* __restrict__ ncnt,
-    const R* __restrict__ bW, int has_boundary, StepParams<R> P) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    R4<R>* __restrict__ xv, uint16_t* __restrict__ nbr, uint32_t* __restrict__ ncnt,
+    uint32_t* __restrict__ halo_idx, uint32_t* __restrict__ halo_n, const R* __restrict__ bW,
+    int has_boundary, int hcap, StepParams<R> P) {
+  extern __shared__ __align__(32) unsigned char dsm[];
+  uint32_t* skey = reinterpret_cast<uint32_t*>(dsm);                 // sorted stencil keys
+  uint16_t* soff = reinterpret_cast<uint16_t*>(skey + kHaloKeys);    // halo offset of each first key
+  __shared__ int3 s_cell[kBlock];
+  __shared__ uint32_t s_scan[32];
+  const int tid = threadIdx.x;
+  const int i = blockIdx.x * kBlock + tid;
+  const bool active = i < sc->n_active;
+  R4<R> xi = R4<R>{R(0), R(0), R(0), R(0)};
+  int cx = 0, cy = 0, cz = 0;
+  if (active) {
+    xi = pos[i];
+    cx = cell_coord((double)xi.x, P.range);
+    cy = cell_coord((double)xi.y, P.range);
+    cz = cell_coord((double)xi.z, P.range);
+  }
+  s_cell[tid] = make_int3(cx, cy, cz);
+  __syncthreads();
+  // one head per run of particles in the same cell
+  const int3 prev = tid > 0 ? s_cell[tid - 1] : make_int3(0, 0, 0);
+  const bool head = active && (tid == 0 || prev.x != cx || prev.y != cy || prev.z != cz);
+  uint32_t nheads = 0;
+  const uint32_t rank = block_excl_scan_u32(head ? 1u : 0u, s_scan, &nheads);
+  // 1. the heads' stencil keys, bitonic-sorted (duplicates kept)
+  const int nk = 27 * (int)nheads;
+  int S = 32;
+  while (S < nk) S <<= 1;
+  if (head)
+    for (int q = 0; q < 27; ++q)
+      skey[27 * rank + q] = morton_key(cx + q % 3 - 1, cy + (q / 3) % 3 - 1, cz + q / 9 - 1, P.mask);
+  for (int t = nk + tid; t < S; t += kBlock) skey[t] = kNoKey;
+  __syncthreads();
+  for (int k = 2; k <= S; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = tid; t < (S >> 1); t += kBlock) {
+        const int a = (t / j) * 2 * j + (t % j), b = a + j;
+        const uint32_t ka = skey[a], kb = skey[b];
+        if ((ka > kb) == ((a & k) == 0)) {
+          skey[a] = kb;
+          skey[b] = ka;
+        }
+      }
+      __syncthreads();
+    }
+  // 2. distinct buckets in key order -> halo offsets and halo_idx
+  const int per = S >= kBlock ? S / kBlock : 1;
+  const int p0 = tid * per;
+  uint32_t len = 0;
+  for (int q = 0; q < per; ++q) {
+    const int p = p0 + q;
+    if (p >= S) break;
+    const uint32_t k = skey[p];
+    if (k != kNoKey && (p == 0 || skey[p - 1] != k)) len += start[k + 1] - start[k];
+  }
+  uint32_t H = 0;
+  uint32_t run = block_excl_scan_u32(len, s_scan, &H);
+  uint32_t* hidx = halo_idx + (size_t)blockIdx.x * (size_t)hcap;
+  for (int q = 0; q < per; ++q) {
+    const int p = p0 + q;
+    if (p >= S) break;
+    const uint32_t k = skey[p];
+    if (k != kNoKey && (p == 0 || skey[p - 1] != k)) {
+      const uint32_t b = start[k], e = start[k + 1];
+      soff[p] = (uint16_t)min(run, 65535u);
+      for (uint32_t j = b; j < e; ++j)
+        if (run + (j - b) < (uint32_t)hcap) hidx[run + (j - b)] = j;
+      run += e - b;
+    }
+  }
+  if (tid == 0) {
+    halo_n[blockIdx.x] = H;
+    atomicMax(&sc->max_halo, (int)min(H, 0x7fffffffu));
+  }
+  __syncthreads();
+  const uint32_t usable = min(H, (uint32_t)hcap);
+  // 3. neighbors (strict range) and volume, with halo positions
   int cnt = 0;
-  if (i < sc->n_active) {
-    const R4<R> xi = pos[i];
-    const int cx = cell_coord((double)xi.x, P.range), cy = cell_coord((double)xi.y, P.range),
-              cz = cell_coord((double)xi.z, P.range);
+  if (active) {
     R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
     R comp = 0;
     // Visit the 27 stencil buckets in ascending key (= memory) order so every
-    // list comes out sorted by neighbor index: lanes of a warp then gather
-    // their k-th neighbors from nearby addresses in the passes that follow.
+    // list comes out sorted by neighbor index: lanes of a warp then read
+    // their k-th neighbors from nearby halo positions in the passes that follow.
     uint32_t keys[27];
 #pragma unroll
-    for (int s = 0; s < 27; ++s)
-      keys[s] = morton_key(cx + (s % 3) - 1, cy + (s / 3) % 3 - 1, cz + s / 9 - 1, P.mask);
+    for (int q = 0; q < 27; ++q)
+      keys[q] = morton_key(cx + (q % 3) - 1, cy + (q / 3) % 3 - 1, cz + q / 9 - 1, P.mask);
 #pragma unroll
     for (int pass = 0; pass < (P.sorted_lists ? 27 : 0); ++pass) {
 #pragma unroll
-      for (int s = pass & 1; s + 1 < 27; s += 2) {
-        const uint32_t a = keys[s], b = keys[s + 1];
-        keys[s] = min(a, b);
-        keys[s + 1] = max(a, b);
+      for (int q = pass & 1; q + 1 < 27; q += 2) {
+        const uint32_t a = keys[q], b = keys[q + 1];
+        keys[q] = min(a, b);
+        keys[q + 1] = max(a, b);
       }
     }
+    bool miss = false;
 #pragma unroll 1
-    for (int s = 0; s < 27; ++s) {
-          const uint32_t k = keys[s];
-          const uint32_t b = start[k], e = start[k + 1];
-          for (uint32_t j = b; j < e; ++j) {
-            if ((int)j == i) continue;
-            const R4<R> xj = pos[j];
-            if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
-            if (cnt < P.K) nbr[nbr_slot(i, cnt, P.K)] = j;
-            ++cnt;
-            const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-            kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
-          }
+    for (int q = 0; q < 27; ++q) {
+      const uint32_t k = keys[q];
+      int lo = 0, hi = S;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (skey[mid] < k) lo = mid + 1;
+        else hi = mid;
+      }
+      const bool found = lo < S && skey[lo] == k;
+      miss |= !found;
+      const uint32_t off = found ? (uint32_t)soff[lo] : 0u;
+      const uint32_t b = start[k], e = start[k + 1];
+      for (uint32_t j = b; j < e; ++j) {
+        if ((int)j == i) continue;
+        const R4<R> xj = pos[j];
+        if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
+        const uint32_t local = off + (j - b);
+        if (cnt < P.K) nbr[nbr_slot(i, cnt, P.K)] = (uint16_t)(found && local < usable ? local : 0u);
+        ++cnt;
+        const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+        kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
+      }
     }
+    if (miss) atomicMax(&sc->max_halo, 0x7fffffff);  // cannot happen: every stencil bucket is in the halo
     R denom = P.V0 * sum;
     if (has_boundary) denom += bW[i];
     const R V = P.V0 / denom;
@@ -739,34 +866,45 @@ __device__ __forceinline__ void body_accum_flush(double* sh, int nbodies, double
 }
 
 // ---------------------------------------------------------------------------
-// Neighbor gather loop. The stored neighbor indices of NB iterations are
-// fetched first with streaming (evict-first) loads, then the NB gathers are
-// issued, then consumed: NB independent DRAM/L2 round trips in flight per
-// thread instead of one dependent chain per neighbor.
+// Neighbor gather loop. The halo positions of NB neighbors are fetched first
+// (streaming, evict-first 64-bit loads of four 16-bit positions), then the NB
+// records are loaded, then consumed, so NB loads are in flight per thread.
+// Slots past the count read position 0, which every non-empty halo has.
 // ---------------------------------------------------------------------------
 template <int NB, class Load, class Use>
-__device__ __forceinline__ void for_each_neighbor(const uint32_t* __restrict__ nbr, int K, int i,
+__device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ nbr, int K, int i,
                                                   int cnt, Load&& load, Use&& use) {
   static_assert(NB % 4 == 0, "neighbors are read in groups of four");
-  const uint4* base = reinterpret_cast<const uint4*>(nbr) + nbr_slot(i, 0, K) / 4;
+  const uint2* base = reinterpret_cast<const uint2*>(nbr) + nbr_slot(i, 0, K) / 4;
   for (int k0 = 0; k0 < cnt; k0 += NB) {
-    uint32_t j[NB];
+    uint32_t l[NB];
 #pragma unroll
     for (int g = 0; g < NB / 4; ++g) {
-      // group k0/4+g of this lane sits 32 uint4 after the previous group
-      const uint4 q = k0 + 4 * g < cnt ? __ldcs(base + (size_t)(k0 / 4 + g) * 32) : make_uint4(i, i, i, i);
-      j[4 * g + 0] = k0 + 4 * g + 0 < cnt ? q.x : (uint32_t)i;
-      j[4 * g + 1] = k0 + 4 * g + 1 < cnt ? q.y : (uint32_t)i;
-      j[4 * g + 2] = k0 + 4 * g + 2 < cnt ? q.z : (uint32_t)i;
-      j[4 * g + 3] = k0 + 4 * g + 3 < cnt ? q.w : (uint32_t)i;
+      // group k0/4+g of this lane sits 32 uint2 after the previous group
+      const uint2 q = k0 + 4 * g < cnt ? __ldcs(base + (size_t)(k0 / 4 + g) * 32) : make_uint2(0u, 0u);
+      l[4 * g + 0] = k0 + 4 * g + 0 < cnt ? (q.x & 0xffffu) : 0u;
+      l[4 * g + 1] = k0 + 4 * g + 1 < cnt ? (q.x >> 16) : 0u;
+      l[4 * g + 2] = k0 + 4 * g + 2 < cnt ? (q.y & 0xffffu) : 0u;
+      l[4 * g + 3] = k0 + 4 * g + 3 < cnt ? (q.y >> 16) : 0u;
     }
     decltype(load(0u)) d[NB];
 #pragma unroll
-    for (int u = 0; u < NB; ++u) d[u] = load(j[u]);
+    for (int u = 0; u < NB; ++u) d[u] = load(l[u]);
 #pragma unroll
     for (int u = 0; u < NB; ++u)
       if (k0 + u < cnt) use(d[u]);
   }
+}
+
+// Shared-memory layout of staged halo records: arrays of R4 then arrays of R,
+// each `hs` records long.
+template <class R>
+__device__ __forceinline__ R4<R>* staged_vec(unsigned char* dsm, int hs, int which) {
+  return reinterpret_cast<R4<R>*>(dsm) + (size_t)which * hs;
+}
+template <class R>
+__device__ __forceinline__ R* staged_scalar(unsigned char* dsm, int hs, int nvec, int which) {
+  return reinterpret_cast<R*>(reinterpret_cast<R4<R>*>(dsm) + (size_t)nvec * hs) + (size_t)which * hs;
 }
 
 template <class R>
@@ -793,12 +931,22 @@ struct XVM {  // position+volume, one vector and one scalar
 template <class R, int PRESS, int NB>
 __global__ void __launch_bounds__(kBlock) k_accel(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
-    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B,
-    R4<R>* __restrict__ acc, R4<R>* __restrict__ vstar, R* __restrict__ press, int write_vstar,
-    StepParams<R> P) {
+    NbrArgs N, BoundaryArgs<R> B, R4<R>* __restrict__ acc, R4<R>* __restrict__ vstar,
+    R* __restrict__ press, int write_vstar, StepParams<R> P) {
   __shared__ double sh_body[kMaxBodies * 6];
+  extern __shared__ __align__(32) unsigned char dsm[];
   const bool bodies = B.any_dynamic != 0;
   if (bodies) body_accum_init(sh_body, B.nbodies);
+  const HaloView H = halo_view(N);
+  R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
+  R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
+  if (H.staged)
+    for (int l = threadIdx.x; l < H.size; l += kBlock) {
+      const uint32_t g = H.idx[l];
+      s_x[l] = xv[g];
+      s_v[l] = vel[g];
+    }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < sc->n_active) {
     const R4<R> xi = xv[i];
@@ -816,9 +964,14 @@ __global__ void __launch_bounds__(kBlock) k_accel(
     if (PRESS == 1) pi = P.stiffness * fmax(P.V0 / Vi - R(1), R(0));
     R sx = 0, sy = 0, sz = 0;   // viscosity
     R px = 0, py = 0, pz = 0;   // pressure
-    const int cnt = min((int)ncnt[i], P.K);
+    const int cnt = min((int)N.ncnt[i], N.K);
     for_each_neighbor<NB>(
-        nbr, P.K, i, cnt, [&](uint32_t j) { return XV<R>{xv[j], vel[j]}; },
+        N.nbr, N.K, i, cnt,
+        [&](uint32_t l) {
+          if (H.staged) return XV<R>{s_x[l], s_v[l]};
+          const uint32_t g = H.idx[l];
+          return XV<R>{xv[g], vel[g]};
+        },
         [&](const XV<R>& d) {
           const R4<R>& xj = d.x;
           const R4<R>& vj = d.v;
@@ -890,21 +1043,36 @@ __global__ void __launch_bounds__(kBlock) k_accel(
 template <class R, int MODE, int NB>
 __global__ void __launch_bounds__(kBlock) k_pressure_accel(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
-    const R* __restrict__ press, const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt,
-    BoundaryArgs<R> B, R4<R>* __restrict__ out, int mirror, int skip_if_converged,
-    StepParams<R> P) {
+    const R* __restrict__ press, NbrArgs N, BoundaryArgs<R> B, R4<R>* __restrict__ out, int mirror,
+    int skip_if_converged, StepParams<R> P) {
   if (skip_if_converged && sc->converged) return;
   __shared__ double sh_body[kMaxBodies * 6];
+  extern __shared__ __align__(32) unsigned char dsm[];
   const bool bodies = mirror && B.any_dynamic != 0;
   if (bodies) body_accum_init(sh_body, B.nbodies);
+  const HaloView H = halo_view(N);
+  R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
+  R* s_p = staged_scalar<R>(dsm, N.hs, 1, 0);
+  if (H.staged)
+    for (int l = threadIdx.x; l < H.size; l += kBlock) {
+      const uint32_t g = H.idx[l];
+      s_x[l] = xv[g];
+      s_p[l] = press[g];
+    }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < sc->n_active) {
     const R4<R> xi = xv[i];
     const R Vi = xi.w, mi = vel[i].w, pi = press[i];
     R px = 0, py = 0, pz = 0;
-    const int cnt = min((int)ncnt[i], P.K);
+    const int cnt = min((int)N.ncnt[i], N.K);
     for_each_neighbor<NB>(
-        nbr, P.K, i, cnt, [&](uint32_t j) { return XP<R>{xv[j], press[j]}; },
+        N.nbr, N.K, i, cnt,
+        [&](uint32_t l) {
+          if (H.staged) return XP<R>{s_x[l], s_p[l]};
+          const uint32_t g = H.idx[l];
+          return XP<R>{xv[g], press[g]};
+        },
         [&](const XP<R>& d) {
           const R rx = xi.x - d.x.x, ry = xi.y - d.x.y, rz = xi.z - d.x.z;
           const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
@@ -949,9 +1117,21 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
 template <class R, int VP, int NB>
 __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
-    const R4<R>* __restrict__ vstar, const uint32_t* __restrict__ nbr,
-    const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B, R* __restrict__ s_out,
+    const R4<R>* __restrict__ vstar, NbrArgs N, BoundaryArgs<R> B, R* __restrict__ s_out,
     R* __restrict__ aii_out, R* __restrict__ press, StepParams<R> P) {
+  extern __shared__ __align__(32) unsigned char dsm[];
+  const HaloView H = halo_view(N);
+  R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
+  R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
+  R* s_m = staged_scalar<R>(dsm, N.hs, 2, 0);
+  if (H.staged)
+    for (int l = threadIdx.x; l < H.size; l += kBlock) {
+      const uint32_t g = H.idx[l];
+      s_x[l] = xv[g];
+      s_v[l] = vstar[g];
+      s_m[l] = vel[g].w;
+    }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= sc->n_active) return;
   const R dt = (R)sc->dt;
@@ -961,9 +1141,14 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
   R div = 0;                       // sum V_j (v*_i - v*_j) . gradW
   R sfx = 0, sfy = 0, sfz = 0;     // S_f = sum V_j gradW
   R s2 = 0;                        // sum V_j^2 / m_j |gradW|^2
-  const int cnt = min((int)ncnt[i], P.K);
+  const int cnt = min((int)N.ncnt[i], N.K);
   for_each_neighbor<NB>(
-      nbr, P.K, i, cnt, [&](uint32_t j) { return XVM<R>{xv[j], vstar[j], vel[j].w}; },
+      N.nbr, N.K, i, cnt,
+      [&](uint32_t l) {
+        if (H.staged) return XVM<R>{s_x[l], s_v[l], s_m[l]};
+        const uint32_t g = H.idx[l];
+        return XVM<R>{xv[g], vstar[g], vel[g].w};
+      },
       [&](const XVM<R>& d) {
         const R4<R>& xj = d.x;
         const R4<R>& vsj = d.v;
@@ -1001,11 +1186,21 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
 template <class R, int NB>
 __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
     Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ accp,
-    const uint32_t* __restrict__ nbr, const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B,
-    const R* __restrict__ s_in, const R* __restrict__ aii_in, R* __restrict__ press,
-    double* __restrict__ partials, int after, StepParams<R> P) {
+    NbrArgs N, BoundaryArgs<R> B, const R* __restrict__ s_in, const R* __restrict__ aii_in,
+    R* __restrict__ press, double* __restrict__ partials, int after, StepParams<R> P) {
   if (sc->converged) return;
   __shared__ double sh[32];
+  extern __shared__ __align__(32) unsigned char dsm[];
+  const HaloView H = halo_view(N);
+  R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
+  R4<R>* s_a = staged_vec<R>(dsm, N.hs, 1);
+  if (H.staged)
+    for (int l = threadIdx.x; l < H.size; l += kBlock) {
+      const uint32_t g = H.idx[l];
+      s_x[l] = xv[g];
+      s_a[l] = accp[g];
+    }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = sc->n_active;
   double e = 0.0;
@@ -1014,9 +1209,14 @@ __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
     const R4<R> xi = xv[i];
     const R4<R> ai = accp[i];
     R sum = 0;
-    const int cnt = min((int)ncnt[i], P.K);
+    const int cnt = min((int)N.ncnt[i], N.K);
     for_each_neighbor<NB>(
-        nbr, P.K, i, cnt, [&](uint32_t j) { return XV<R>{xv[j], accp[j]}; },
+        N.nbr, N.K, i, cnt,
+        [&](uint32_t l) {
+          if (H.staged) return XV<R>{s_x[l], s_a[l]};
+          const uint32_t g = H.idx[l];
+          return XV<R>{xv[g], accp[g]};
+        },
         [&](const XV<R>& d) {
           const R rx = xi.x - d.x.x, ry = xi.y - d.x.y, rz = xi.z - d.x.z;
           const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
@@ -1098,9 +1298,21 @@ __global__ void __launch_bounds__(kBlock) k_ost_commit(const Scalars* __restrict
 template <class R, int NB>
 __global__ void __launch_bounds__(kBlock) k_split_density(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
-    const R4<R>* __restrict__ vstar, const uint32_t* __restrict__ nbr,
-    const uint32_t* __restrict__ ncnt, BoundaryArgs<R> B, R* __restrict__ press,
+    const R4<R>* __restrict__ vstar, NbrArgs N, BoundaryArgs<R> B, R* __restrict__ press,
     R* __restrict__ rho_pred, StepParams<R> P) {
+  extern __shared__ __align__(32) unsigned char dsm[];
+  const HaloView H = halo_view(N);
+  R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
+  R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
+  R* s_m = staged_scalar<R>(dsm, N.hs, 2, 0);
+  if (H.staged)
+    for (int l = threadIdx.x; l < H.size; l += kBlock) {
+      const uint32_t g = H.idx[l];
+      s_x[l] = xv[g];
+      s_v[l] = vstar[g];
+      s_m[l] = vel[g].w;
+    }
+  __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= sc->n_active) return;
   const R dt = (R)sc->dt;
@@ -1108,9 +1320,14 @@ __global__ void __launch_bounds__(kBlock) k_split_density(
   const R4<R> vsi = vstar[i];
   const R mi = vel[i].w;
   R rho = mi * P.k.cw * R(0.5), comp = 0;  // self term m_i W(0)
-  const int cnt = min((int)ncnt[i], P.K);
+  const int cnt = min((int)N.ncnt[i], N.K);
   for_each_neighbor<NB>(
-      nbr, P.K, i, cnt, [&](uint32_t j) { return XVM<R>{xv[j], vstar[j], vel[j].w}; },
+      N.nbr, N.K, i, cnt,
+      [&](uint32_t l) {
+        if (H.staged) return XVM<R>{s_x[l], s_v[l], s_m[l]};
+        const uint32_t g = H.idx[l];
+        return XVM<R>{xv[g], vstar[g], vel[g].w};
+      },
       [&](const XVM<R>& d) {
         const R4<R>& xj = d.x;
         const R4<R>& vsj = d.v;
@@ -1372,9 +1589,9 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, const Scalars* __restr
 // End of a graph-captured step: records what the per-step host check would
 // have acted on (then the host replays the chunk on the per-step path) and
 // prepares the scalars of the next update exactly as that check does.
-__global__ void k_step_epilogue(Scalars* sc, int K, int solver_loop) {
+__global__ void k_step_epilogue(Scalars* sc, int K, int hcap, int solver_loop) {
   unsigned int t = 0;
-  if (sc->max_nbrs > K) t |= 1u;
+  if (sc->max_nbrs > K || sc->max_halo > hcap) t |= 1u;
   if (sc->n_below > 0) t |= 2u;
   if (solver_loop && !sc->converged) t |= 4u;
   sc->trouble |= t;

@@ -57,6 +57,21 @@ struct DBuf {
   size_t bytes() const { return n * sizeof(T); }
 };
 
+// Opts a kernel into more than 48 KB of dynamic shared memory (once per
+// device and kernel).
+static void allow_smem(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> done;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& have = done[{dev, fn}];
+  if (have >= bytes) return;
+  cuda_check(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+             "cudaFuncSetAttribute");
+  have = bytes;
+}
+
 static int blocks_for(long long n) { return (int)std::max(1LL, (n + kBlock - 1) / kBlock); }
 static size_t round_up(size_t n, size_t m) { return (n + m - 1) / m * m; }
 
@@ -137,6 +152,8 @@ class System : public SystemBase {
   explicit System(const sph_config& c) : cfg_(c) {
     device = c.device;
     if (const char* e = std::getenv("SPHGPU_SORTED_LISTS")) sorted_lists_ = std::atoi(e) != 0;
+    if (const char* e = std::getenv("SPHGPU_HALO_STAGE")) hs_ = std::max(0, std::min(std::atoi(e), 4096));
+    if (const char* e = std::getenv("SPHGPU_HALO_CAPACITY")) hcap_ = std::max(64, std::min(std::atoi(e), 65535));
     if (const char* e = std::getenv("SPHGPU_GATHER_BATCH")) {
       const int v = std::atoi(e);
       nb_ = (v == 4 || v == 8) ? v : 4;
@@ -434,7 +451,8 @@ class System : public SystemBase {
 
   int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) override {
     std::vector<uint32_t> ref = fetch(ref_.p, n_), cnt = fetch(ncnt_.p, n_);
-    std::vector<uint32_t> nb = fetch(nbr_.p, (size_t)K_ * np_);
+    std::vector<uint16_t> nb = fetch(nbr_.p, (size_t)K_ * np_);
+    std::vector<uint32_t> hidx = fetch(halo_idx_.p, (size_t)blocks_for((long long)cap_) * (size_t)hcap_);
     auto slot = [&](size_t i, size_t k) {
       return (((i >> 5) * (size_t)(K_ >> 2) + (k >> 2)) * 32 + (i & 31)) * 4 + (k & 3);
     };
@@ -451,7 +469,8 @@ class System : public SystemBase {
       uint32_t* row = idx + off[r];
       const size_t c = std::min<size_t>(cnt[d], (size_t)K_);
       row[0] = ref[d];
-      for (size_t k = 0; k < c; ++k) row[1 + k] = ref[nb[slot(d, k)]];
+      const uint32_t* h = hidx.data() + (d / kBlock) * (size_t)hcap_;
+      for (size_t k = 0; k < c; ++k) row[1 + k] = ref[h[nb[slot(d, k)]]];
       std::sort(row, row + c + 1);
     }
     return SPH_OK;
@@ -558,7 +577,9 @@ class System : public SystemBase {
                           &snap_xint_, &snap_vint_})
       b += d->bytes();
     for (const auto* d : {&press_, &s_, &aii_, &bW_, &rho_pred_}) b += d->bytes();
-    for (const auto* d : {&ref_, &ref2_, &fid_, &fid2_, &key_, &slot_, &perm_, &nbr_, &ncnt_, &count_, &start_,
+    b += nbr_.bytes();
+    for (const auto* d : {&ref_, &ref2_, &fid_, &fid2_, &key_, &slot_, &perm_, &halo_idx_, &halo_n_, &ncnt_,
+                          &count_, &start_,
                           &tile_sums_, &sbid_, &sbid2_, &sorig_, &sorig2_, &skey_, &sslot_, &sperm_, &scount_,
                           &sstart_, &snap_ref_, &snap_fid_})
       b += d->bytes();
@@ -607,7 +628,10 @@ class System : public SystemBase {
   // particle state
   DBuf<R4<R>> pos_, pos2_, vel_, vel2_, xv_, acc_, vstar_, accp_, xint_, vint_, bG_, bGu_;
   DBuf<R> press_, s_, aii_, bW_, rho_pred_;
-  DBuf<uint32_t> ref_, ref2_, fid_, fid2_, key_, slot_, perm_, nbr_, ncnt_;
+  DBuf<uint32_t> ref_, ref2_, fid_, fid2_, key_, slot_, perm_, ncnt_, halo_idx_, halo_n_;
+  DBuf<uint16_t> nbr_;
+  int hcap_ = 4096;   // halo table capacity per block (grows on overflow, at most 65535)
+  int hs_ = sizeof(R) == 4 ? 1536 : 1024;  // halo records staged in shared memory per block
   DBuf<uint32_t> count_, start_, tile_sums_;
   DBuf<double> partials_, body_partials_, stage_x_, stage_v_;
   // boundaries
@@ -734,6 +758,8 @@ class System : public SystemBase {
     if (cfg_.integration_scheme == SPH_TAKE_PREDICTED) { xint_.alloc(c); vint_.alloc(c); }
     K_ = (int)round_up(cfg_.neighbor_capacity ? cfg_.neighbor_capacity : 64, 4);
     nbr_.alloc((size_t)K_ * np_);
+    halo_n_.alloc((size_t)blocks_for((long long)c));
+    halo_idx_.alloc((size_t)blocks_for((long long)c) * (size_t)hcap_);
     ensure_partials(2 * (size_t)blocks_for((long long)c));
     press_.zero(stream_);
     bW_.zero(stream_); bG_.zero(stream_); bGu_.zero(stream_);
@@ -800,6 +826,26 @@ class System : public SystemBase {
   }
   template <class Kern, class... Args>
   void launch(const char* name, Kern kernel, dim3 g, dim3 b, Args... args) {
+    launch_s(name, kernel, g, b, 0, args...);
+  }
+  // dynamic shared memory of a halo-staging pass: nvec R4 and nscal R arrays
+  size_t smem_of(int nvec, int nscal) const {
+    return (size_t)hs_ * ((size_t)nvec * sizeof(R4<R>) + (size_t)nscal * sizeof(R));
+  }
+  NbrArgs nargs() const {
+    NbrArgs N;
+    N.nbr = nbr_.p;
+    N.ncnt = ncnt_.p;
+    N.hidx = halo_idx_.p;
+    N.hn = halo_n_.p;
+    N.K = K_;
+    N.hcap = hcap_;
+    N.hs = hs_;
+    return N;
+  }
+  template <class Kern, class... Args>
+  void launch_s(const char* name, Kern kernel, dim3 g, dim3 b, size_t smem, Args... args) {
+    if (smem) allow_smem((const void*)kernel, smem);
     cudaEvent_t e1 = nullptr;
     if (profiling_ && !capturing_) {
       ProfEntry& pe = prof_[name];
@@ -815,7 +861,7 @@ class System : public SystemBase {
       cuda_check(cudaEventRecord(pr.first, stream_), "event");
       e1 = pr.second;
     }
-    kernel<<<g, b, 0, stream_>>>(args...);
+    kernel<<<g, b, smem, stream_>>>(args...);
     cuda_check(cudaGetLastError(), name);
     if (!capturing_) ++launches_;
     else if (!in_loop_body_) ++capture_kernels_;
@@ -986,11 +1032,11 @@ class System : public SystemBase {
     const int nb = blocks_for((long long)n_);
     with_nb([&](auto NBc) {
       constexpr int NB = decltype(NBc)::value;
-      launch("iisph_pressure_accel", k_pressure_accel<R, 0, NB>, dim3(nb), dim3(kBlock), (const Scalars*)d_sc_.p,
-             (const R4<R>*)xv_.p, (const R4<R>*)vel_.p, (const R*)press_.p, (const uint32_t*)nbr_.p,
-             (const uint32_t*)ncnt_.p, bargs(), accp_.p, 0, 1, P_);
-      launch("iisph_jacobi", k_iisph_jacobi<R, NB>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
-             (const R4<R>*)accp_.p, (const uint32_t*)nbr_.p, (const uint32_t*)ncnt_.p, bargs(),
+      launch_s("iisph_pressure_accel", k_pressure_accel<R, 0, NB>, dim3(nb), dim3(kBlock), smem_of(1, 1),
+               (const Scalars*)d_sc_.p, (const R4<R>*)xv_.p, (const R4<R>*)vel_.p, (const R*)press_.p, nargs(),
+               bargs(), accp_.p, 0, 1, P_);
+      launch_s("iisph_jacobi", k_iisph_jacobi<R, NB>, dim3(nb), dim3(kBlock), smem_of(2, 0), d_sc_.p,
+               (const R4<R>*)xv_.p, (const R4<R>*)accp_.p, nargs(), bargs(),
              (const R*)s_.p, (const R*)aii_.p, press_.p, partials_.p, after, P_);
     });
   }
@@ -1026,51 +1072,51 @@ class System : public SystemBase {
     const Scalars* csc = d_sc_.p;
     const auto xv = (const R4<R>*)xv_.p;
     const auto vel = (const R4<R>*)vel_.p;
-    const auto nbr = (const uint32_t*)nbr_.p;
-    const auto ncnt = (const uint32_t*)ncnt_.p;
+    const NbrArgs nbr = nargs();
+    const size_t sm_xv = smem_of(2, 0), sm_xp = smem_of(1, 1), sm_xvm = smem_of(2, 1);
     with_nb([&](auto NBc) {
     constexpr int NB = decltype(NBc)::value;
     switch (cfg_.pressure_solver) {
       case SPH_SESPH:
-        launch("accel_sesph", k_accel<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(), acc_.p,
+        launch_s("accel_sesph", k_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(), acc_.p,
                vstar_.p, press_.p, 0, P_);
         body_reduce(nb);
         break;
       case SPH_SESPH_W_SPLITTING:
-        launch("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
+        launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
         body_reduce(nb);
-        launch("split_density", k_split_density<R, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
-               (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), press_.p, rho_pred_.p, P_);
-        launch("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
-               (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
+        launch_s("split_density", k_split_density<R, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
+               (const R4<R>*)vstar_.p, nbr, bargs(), press_.p, rho_pred_.p, P_);
+        launch_s("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
+               (const R*)press_.p, nbr, bargs(), acc_.p, 1, 0, P_);
         body_reduce(nb);
         break;
       case SPH_IISPH:
-        launch("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
+        launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
         body_reduce(nb);
-        launch("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
-               (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), s_.p, aii_.p, press_.p, P_);
+        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
+               (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, P_);
         solve_loop(-1);
-        launch("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
-               (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
+        launch_s("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
+               (const R*)press_.p, nbr, bargs(), acc_.p, 1, 0, P_);
         body_reduce(nb);
         break;
       case SPH_IISPH_W_OST:
-        launch("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), csc, xv, vel, nbr, ncnt, bargs(),
+        launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
-        launch("iisph_source_diag", k_iisph_source_diag<R, 0, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
-               (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), s_.p, aii_.p, press_.p, P_);
+        launch_s("iisph_source_diag", k_iisph_source_diag<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
+               (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, P_);
         solve_loop(3);
-        launch("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
-               (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
+        launch_s("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
+               (const R*)press_.p, nbr, bargs(), acc_.p, 1, 0, P_);
         launch("ost_predict", k_ost_predict<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)acc_.p, vstar_.p);
-        launch("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
-               (const R4<R>*)vstar_.p, nbr, ncnt, bargs(), s_.p, aii_.p, press_.p, P_);
+        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
+               (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, P_);
         solve_loop(-1);
-        launch("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), csc, xv, vel,
-               (const R*)press_.p, nbr, ncnt, bargs(), acc_.p, 1, 0, P_);
+        launch_s("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
+               (const R*)press_.p, nbr, bargs(), acc_.p, 1, 0, P_);
         launch("ost_commit", k_ost_commit<R>, dim3(nb), dim3(kBlock), csc, xv, vel, (const R4<R>*)vstar_.p,
                (const R4<R>*)acc_.p, xint_.p, vint_.p);
         break;
@@ -1088,13 +1134,21 @@ class System : public SystemBase {
     collect_profile();
     avg_density_ = h_sc_->avg_density;
     if (h_sc_->iterations > 0) last_iters_ = h_sc_->iterations;
-    if (h_sc_->max_nbrs > K_) {
-      // Neighbor capacity exceeded: grow it and redo the update on the same
-      // (already integrated) state. Reaction forces gathered so far are
-      // discarded first; they are rebuilt by the redo.
-      K_ = (int)round_up((size_t)h_sc_->max_nbrs + 8, 8);  // multiple of 4 (128-bit groups)
-      P_.K = K_;
-      nbr_.alloc((size_t)K_ * np_);
+    if (h_sc_->max_nbrs > K_ || h_sc_->max_halo > hcap_) {
+      // Neighbor or halo capacity exceeded: grow it and redo the update on
+      // the same (already integrated) state. Reaction forces gathered so far
+      // are discarded first; they are rebuilt by the redo.
+      if (h_sc_->max_nbrs > K_) {
+        K_ = (int)round_up((size_t)h_sc_->max_nbrs + 8, 8);  // multiple of 4 (64-bit groups)
+        P_.K = K_;
+        nbr_.alloc((size_t)K_ * np_);
+      }
+      if (h_sc_->max_halo > hcap_) {
+        if (h_sc_->max_halo > 65535)
+          throw Error(SPH_ERR_CAPACITY, "a block's neighborhood holds more than 65535 particles");
+        hcap_ = (int)std::min<size_t>(65535, round_up((size_t)h_sc_->max_halo * 5 / 4, 256));
+        halo_idx_.alloc((size_t)blocks_for((long long)cap_) * (size_t)hcap_);
+      }
       zero_body_forces();
       finish_disable();
       update(2);
@@ -1128,8 +1182,9 @@ class System : public SystemBase {
       launch("boundary_samples", k_vm_sample<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
              (const VMDesc*)vms_.p, (int)fields_.size(), (const Body*)bodies_d_.p, vmx_.p, vmv_.p, bW_.p,
              bG_.p, bGu_.p, P_);
-    launch("neighbors_density", k_neighbors_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
-           (const uint32_t*)start_.p, xv_.p, nbr_.p, ncnt_.p, (const R*)bW_.p, boundary_kind_ ? 1 : 0, P_);
+    launch_s("neighbors_density", k_neighbors_density<R>, dim3(nb), dim3(kBlock), kSearchSmem, d_sc_.p,
+             (const R4<R>*)pos_.p, (const uint32_t*)start_.p, xv_.p, nbr_.p, ncnt_.p, halo_idx_.p, halo_n_.p,
+             (const R*)bW_.p, boundary_kind_ ? 1 : 0, hcap_, P_);
     calc_acceleration();
     launch("avg_density", k_avg_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
            (const R4<R>*)vel_.p, partials_.p, P_);
@@ -1265,7 +1320,7 @@ class System : public SystemBase {
   StepGraph graphs_[2];
   uint32_t graph_chunk_ = 0, chunk_steps_ = 0;
   size_t graph_n_ = 0;
-  int graph_K_ = 0;
+  int graph_K_ = 0, graph_hcap_ = 0;
   bool capturing_ = false, in_loop_body_ = false;
   uint64_t capture_kernels_ = 0, graph_replays_ = 0;
   cudaStream_t body_stream_ = nullptr;
@@ -1289,7 +1344,7 @@ class System : public SystemBase {
   }
 
   void prepare_graphs() {
-    if (graphs_[0].exec && graph_n_ == n_ && graph_K_ == K_) return;
+    if (graphs_[0].exec && graph_n_ == n_ && graph_K_ == K_ && graph_hcap_ == hcap_) return;
     destroy_graphs();
     if (!body_stream_) cuda_check(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     if (!chunk_event_) cuda_check(cudaEventCreateWithFlags(&chunk_event_, cudaEventDisableTiming), "cudaEventCreate");
@@ -1302,6 +1357,7 @@ class System : public SystemBase {
     if (graphs_[0].key != (const void*)pos_.p) throw Error(SPH_ERR_STATE, "step graphs out of phase");
     graph_n_ = n_;
     graph_K_ = K_;
+    graph_hcap_ = hcap_;
   }
 
   void capture_step(StepGraph& g) {
@@ -1314,7 +1370,7 @@ class System : public SystemBase {
         launch("body_step", k_body_step, dim3(1), dim3(32), bodies_d_.p, nbodies_, (const Scalars*)d_sc_.p);
       issue_update(cfg_.integration_scheme == SPH_TAKE_PREDICTED ? 1 : 0);
       const int loop = cfg_.pressure_solver == SPH_IISPH || cfg_.pressure_solver == SPH_IISPH_W_OST;
-      launch("step_epilogue", k_step_epilogue, dim3(1), dim3(1), d_sc_.p, K_, loop);
+      launch("step_epilogue", k_step_epilogue, dim3(1), dim3(1), d_sc_.p, K_, hcap_, loop);
     } catch (...) {
       capturing_ = false;
       in_loop_body_ = false;
