@@ -7,12 +7,22 @@ sim_lib sph/setup/mod.rs:142-153). Containers are the reference's cube mesh
 (cube_face_normals_inwards.obj: 8 vertices, 12 inward-facing triangles) under
 the reference's mesh transform (utilities/triangle_mesh.rs:314-334: scale,
 then rotate, then translate).
+
+Every fluid block keeps its first particle centers WALL_GAP = 1.5 spacings
+from the container walls. Both boundary handlings add the wall's density
+where a fluid neighbor layer would be: sample boundaries at the wall plane,
+volume maps at max(sd + 1/4 dx, dx) from the particle. A fluid layer closer
+than that is over-dense at rest: at half a spacing, corner particles start
+at up to three times the rest density, and the IISPH solve of such a state
+does not converge and blows the scene apart within a few steps.
 """
 from __future__ import annotations
 
 from dataclasses import dataclass, field
 
 import numpy as np
+
+WALL_GAP = 1.5  # spacings between a container wall and the first fluid particle centers
 
 # Unit cube [-1, 1]^3 with inward-facing triangles, vertex order of the
 # reference's OBJ file.
@@ -118,14 +128,14 @@ class Scene:
 
 def dam_break_sesph_8k(jitter_seed=0, n_side=20):
     """SESPH dam break: a 20^3 lattice (spacing 0.02, +-1 % jitter) in the
-    corner of a 0.6 m cube container of StaticSampleBoundary samples taken at
+    corner (1.5 spacings from the walls) of a 0.6 m cube container of StaticSampleBoundary samples taken at
     0.7 * spacing from the reference's inward cube mesh scaled 0.3; support 2h,
     rest density 1000, stiffness 1000, viscosity 0.01, dt 1e-3, EulerCromer."""
     h = 0.02
     verts = transform_mesh(CUBE_VERTICES, scale=(0.3, 0.3, 0.3))
     samples = sample_triangle_mesh_surface(verts, CUBE_FACES_INWARD, 0.7 * h)
-    pos = lattice_block((n_side, n_side, n_side), h, origin=(-0.3, -0.3, -0.3), jitter=0.01,
-                        seed=jitter_seed)
+    o = -0.3 + (WALL_GAP - 0.5) * h
+    pos = lattice_block((n_side, n_side, n_side), h, origin=(o, o, o), jitter=0.01, seed=jitter_seed)
     return Scene(
         procedures={"kernel_function": "CubicBSpline3D", "integration_scheme": "EulerCromer",
                     "pressure_solver": "SESPH", "neighbor_search": "SpatialHashing",
@@ -141,13 +151,17 @@ def dam_break_sesph_8k(jitter_seed=0, n_side=20):
 
 
 def dam_break_iisph_box(n_side=100, spacing=0.01, jitter_seed=0, box=(2.0, 1.0, 1.0)):
-    """IISPH dam break: an n_side^3 lattice (+-1 % jitter) against the -x end of a
-    box container (the reference's inward cube mesh scaled to `box`) handled as a
+    """IISPH dam break: an n_side^3 lattice (+-1 % jitter) at the -x end of a
+    box container (the reference's inward cube mesh scaled to `box`, each axis
+    widened where needed so the block keeps 1.5 spacings from every wall:
+    100^3 at 0.01 m makes the 2 x 1 x 1 m box 2 x 1.02 x 1.02 m) handled as a
     VolumeMapBoundary with the reference's field spacing dx = 4 * spacing;
     omega 0.5, target density error 0.1 %, CFL 0.4 with dt <= 2e-3."""
     h = spacing
+    need = n_side * h + 2.0 * (WALL_GAP - 0.5) * h
+    box = tuple(max(float(b), need) for b in box)
     verts = transform_mesh(CUBE_VERTICES, scale=(box[0] / 2, box[1] / 2, box[2] / 2))
-    lo = -0.5 * np.asarray(box)
+    lo = -0.5 * np.asarray(box) + (WALL_GAP - 0.5) * h
     pos = lattice_block((n_side, n_side, n_side), h, origin=lo, jitter=0.01, seed=jitter_seed)
     return Scene(
         procedures={"kernel_function": "CubicBSpline3D", "integration_scheme": "EulerCromer",
@@ -245,18 +259,19 @@ def floating_cube_scene(n_side=12, spacing=0.02, body_side=0.12, body_density=50
 def serving_dam_break(n_target, solver="SESPH", stiffness=1000.0, viscosity=0.01, rest_density=1000.0,
                       spacing=0.02, time_increment=1e-3, seed=0):
     """Dam break of the scene sweep: an n_side^3 lattice block (n_side =
-    round(n_target^(1/3)), +-1 % jitter) against the -x end of a box
-    container of 2 x 1 x 1.5 block lengths sampled as a StaticSampleBoundary
+    round(n_target^(1/3)), +-1 % jitter) at the -x end of a box container
+    of 2 x 1 x 1.5 block lengths plus the wall gaps, sampled as a StaticSampleBoundary
     at 0.7 * spacing from the reference's inward cube mesh; support 2h, fixed
     dt, EulerCromer. IISPH uses omega 0.5, target density error 0.1 % and at
     most 100 sweeps."""
     n_side = max(4, int(round(n_target ** (1.0 / 3.0))))
     h = spacing
     L = n_side * h
-    half = np.array([L, 0.5 * L, 0.75 * L])
+    g = (WALL_GAP - 0.5) * h
+    half = np.array([L, 0.5 * L, 0.75 * L]) + g
     verts = transform_mesh(CUBE_VERTICES, scale=tuple(half))
     samples = sample_triangle_mesh_surface(verts, CUBE_FACES_INWARD, 0.7 * h)
-    pos = lattice_block((n_side, n_side, n_side), h, origin=-half, jitter=0.01, seed=seed)
+    pos = lattice_block((n_side, n_side, n_side), h, origin=-half + g, jitter=0.01, seed=seed)
     params = {"rest_density_grid_spacing": h, "kernel_support_radius": 2 * h,
               "disable_particles_below": -50.0, "fluid_viscosity": viscosity,
               "boundary_viscosity": viscosity, "boundary_pressure_acceleration_weighting": 0.7,
@@ -307,3 +322,93 @@ def scene_sweep(count=256, rate_per_s=20.0, n_min=5000, n_max=500000, steps=500,
     rho = rng.uniform(500.0, 1500.0, count)
     return [SceneRequest(float(arrivals[i]), int(n[i]), "SESPH" if solver[i] == 0 else "IISPH", float(k[i]),
                          float(nu[i]), float(rho[i]), int(steps), int(seed * 100003 + i)) for i in range(count)]
+
+
+def two_fluid_ball(radius=1.0, spacing=0.008, seed=0, subdivisions=4):
+    """IISPHwOST two-fluid ball (precision study): a jittered lattice filling
+    the lower half of a sphere container of `radius` (inward icosphere of
+    20*4^subdivisions triangles, handled as a VolumeMapBoundary at the
+    reference's field spacing 4 * spacing), split by a seeded random plane
+    through the center into fluid ids 0 / 1 with rest densities 1000 / 500;
+    viscosity 0.005, TakePredicted, fixed dt 5e-4."""
+    h = spacing
+    rng = np.random.default_rng(seed)
+    n = int(np.ceil(radius / h))
+    g = (np.arange(-n, n) + 0.5) * h
+    Z, Y, X = np.meshgrid(g, g, g, indexing="ij")
+    pos = np.stack([X.ravel(), Y.ravel(), Z.ravel()], axis=1)
+    inside = (np.linalg.norm(pos, axis=1) < radius - WALL_GAP * h) & (pos[:, 2] < 0.0)
+    pos = pos[inside]
+    pos = pos + rng.uniform(-0.01 * h, 0.01 * h, size=pos.shape)
+    pos = pos.astype(np.float32).astype(np.float64)
+    normal = rng.normal(size=3)
+    normal /= np.linalg.norm(normal)
+    side = (pos @ normal) > 0.0
+    verts, faces = icosphere(subdivisions, radius, inward=True)
+    return Scene(
+        procedures={"kernel_function": "CubicBSpline3D", "integration_scheme": "TakePredicted",
+                    "pressure_solver": "IISPHwOST", "neighbor_search": "SpatialHashing",
+                    "boundary_handling": "VolumeMapBoundary"},
+        parameters={"rest_density_grid_spacing": h, "kernel_support_radius": 2 * h,
+                    "disable_particles_below": -50.0, "fluid_viscosity": 0.005, "boundary_viscosity": 0.005,
+                    "boundary_pressure_acceleration_weighting": 0.7, "boundary_rest_volume_weighting": 1.0,
+                    "target_density_error": 0.1, "relaxation_factor": 0.5, "min_diagonal_element": 1e-10,
+                    "time_increment": 5e-4},
+        cfl_time_step=False, position=pos, mass=np.where(side, 500.0, 1000.0) * h ** 3,
+        fluid_id=side.astype(np.uint32), mesh=(verts, faces),
+        description=f"IISPHwOST two-fluid ball, {pos.shape[0]} particles, radius {radius}")
+
+
+def rigid_body_tank(spacing=0.02, tank=(0.8, 0.4, 0.5), fill=0.2, n_cubes=4, n_spheres=4, cube_side=0.15,
+                    sphere_radius=0.08, seed=0):
+    """IISPH rigid-body coupling, all StaticSampleBoundary: a box tank sampled
+    at 0.7 * spacing, a fluid layer of height `fill`, and n_cubes cubes plus
+    n_spheres spheres (two-way coupled RigidBodyMotion bodies sampled at
+    0.7 * spacing) placed above the surface with seeded densities U[300, 1500];
+    CFL time step (0.4, dt <= 2e-3)."""
+    from .system import RigidInit
+    h = spacing
+    rng = np.random.default_rng(seed)
+    half = 0.5 * np.asarray(tank, np.float64)
+    verts = transform_mesh(CUBE_VERTICES, scale=tuple(half))
+    walls = sample_triangle_mesh_surface(verts, CUBE_FACES_INWARD, 0.7 * h)
+    g = (WALL_GAP - 0.5) * h
+    counts = (int(round((tank[0] - 2 * g) / h)), int(round((tank[1] - 2 * g) / h)), int(fill / h))
+    pos = lattice_block(counts, h, origin=-half + g, jitter=0.01, seed=seed)
+    bodies = []
+    nb = n_cubes + n_spheres
+    cols = int(np.ceil(nb / 2))
+    for b in range(nb):
+        cube = b < n_cubes
+        size = cube_side if cube else 2 * sphere_radius
+        cx = -half[0] + (b % cols + 0.5) * (tank[0] / cols)
+        cy = -half[1] + (b // cols + 0.5) * (tank[1] / 2)
+        cz = -half[2] + fill + 0.6 * size + 0.02 * (b % 3)
+        com = (cx + rng.uniform(-0.01, 0.01), cy + rng.uniform(-0.01, 0.01), cz)
+        rho = rng.uniform(300.0, 1500.0)
+        if cube:
+            bv = transform_mesh(CUBE_VERTICES, scale=(cube_side / 2,) * 3)
+            samples = sample_triangle_mesh_surface(bv, CUBE_FACES_OUTWARD, 0.7 * h)
+            mass = rho * cube_side ** 3
+            inertia = box_inertia(mass, cube_side)
+        else:
+            bv, bf = icosphere(2, sphere_radius)
+            samples = sample_triangle_mesh_surface(bv, bf, 0.7 * h)
+            mass = rho * 4.0 / 3.0 * np.pi * sphere_radius ** 3
+            inertia = np.eye(3) * 0.4 * mass * sphere_radius ** 2
+        rigid = RigidInit(mass=mass, inertia_body=inertia, center_of_mass=com,
+                          orientation=tuple(np.r_[np.cos(0.05 * b), np.sin(0.05 * b) * np.array([0.6, 0.0, 0.8])]),
+                          angular_velocity=(0.0, 0.2 * (b % 2), 0.0))
+        bodies.append((samples, rigid))
+    return Scene(
+        procedures={"kernel_function": "CubicBSpline3D", "integration_scheme": "EulerCromer",
+                    "pressure_solver": "IISPH", "neighbor_search": "SpatialHashing",
+                    "boundary_handling": "StaticSampleBoundary"},
+        parameters={"rest_density_grid_spacing": h, "kernel_support_radius": 2 * h,
+                    "disable_particles_below": -50.0, "fluid_viscosity": 0.01, "boundary_viscosity": 0.01,
+                    "boundary_pressure_acceleration_weighting": 0.7, "boundary_rest_volume_weighting": 1.0,
+                    "target_density_error": 0.1, "relaxation_factor": 0.5, "min_diagonal_element": 1e-10,
+                    "max_time_increment": 2e-3, "cfl_number": 0.4, "max_solver_iterations": 100},
+        cfl_time_step=True, position=pos, mass=np.full(pos.shape[0], 1000.0 * h ** 3),
+        sample_boundaries=[(walls, None)] + bodies, mesh=(verts, CUBE_FACES_INWARD),
+        description=f"IISPH tank, {pos.shape[0]} particles, {n_cubes} cubes + {n_spheres} spheres")
