@@ -52,11 +52,20 @@ def build_oracle(scene, fields=None):
     for pts, rigid in scene.sample_boundaries:
         s.add_sample_boundary(pts, None if rigid is None else rigid.to_array32())
     for sdf, vm, rigid in scene.volume_maps:
-        s.add_volume_map_boundary(sdf, vm, None if rigid is None else rigid.to_array32())
+        s.add_volume_map_boundary(_oracle_field(sdf), _oracle_field(vm),
+                                  None if rigid is None else rigid.to_array32())
     if fields is not None:
-        s.add_volume_map_boundary(fields[0], fields[1])
+        s.add_volume_map_boundary(*(_oracle_field(f) for f in fields))
     s.initialize()
     return s
+
+
+def _oracle_field(f):
+    """The oracle's Field for a field built by either side."""
+    import oracle as O
+    if hasattr(f, "desc"):
+        return f
+    return O.Field(f.x_min, f.x_max, f.dx, f.n, f.nodes)
 
 
 def rel_err(a, b, floor):
