@@ -402,6 +402,26 @@ __device__ __forceinline__ HaloView halo_view(const NbrArgs& N) {
   return h;
 }
 
+// Copies the block's halo records to shared memory: copy(l, g) moves the
+// record of particle g to position l. Four positions per thread are in flight
+// (their halo indices first, then the records).
+template <class F>
+__device__ __forceinline__ void stage_halo(const HaloView& H, F&& copy) {
+  for (int l0 = threadIdx.x; l0 < H.size; l0 += 4 * kBlock) {
+    uint32_t g[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int l = l0 + u * kBlock;
+      g[u] = l < H.size ? __ldg(H.idx + l) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int l = l0 + u * kBlock;
+      if (l < H.size) copy(l, g[u]);
+    }
+  }
+}
+
 template <class R>
 __device__ __forceinline__ void kahan_add(R& s, R& c, R t) {
   const R y = t - c;
@@ -491,15 +511,22 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
   }
   __syncthreads();
   const uint32_t usable = min(H, (uint32_t)hcap);
-  // 3. neighbors (strict range) and volume, with halo positions
+  // 3. neighbors (strict range) and volume, with halo positions. Every
+  // candidate lies in the halo; when the halo's positions fit the sort buffer
+  // they are staged there (after the bucket lookups are done) and the
+  // candidate loop reads shared memory instead of global memory.
+  const bool staged = H <= usable && H <= (uint32_t)(kHaloKeys * sizeof(uint32_t) / sizeof(R4<R>));
   int cnt = 0;
+  R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
+  R comp = 0;
+  bool miss = false;
+  // Visit the 27 stencil buckets in ascending key (= memory) order so every
+  // list comes out sorted by neighbor index: lanes of a warp then read their
+  // k-th neighbors from nearby halo positions in the passes that follow.
+  uint32_t keys[27];
+  uint32_t span[27];  // (halo offset << 16) | bucket size, for the staged loop
+  uint32_t own_local = 0xffffffffu;
   if (active) {
-    R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
-    R comp = 0;
-    // Visit the 27 stencil buckets in ascending key (= memory) order so every
-    // list comes out sorted by neighbor index: lanes of a warp then read
-    // their k-th neighbors from nearby halo positions in the passes that follow.
-    uint32_t keys[27];
 #pragma unroll
     for (int q = 0; q < 27; ++q)
       keys[q] = morton_key(cx + (q % 3) - 1, cy + (q / 3) % 3 - 1, cz + q / 9 - 1, P.mask);
@@ -512,7 +539,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
         keys[q + 1] = max(a, b);
       }
     }
-    bool miss = false;
+    const uint32_t own = morton_key(cx, cy, cz, P.mask);
 #pragma unroll 1
     for (int q = 0; q < 27; ++q) {
       const uint32_t k = keys[q];
@@ -523,20 +550,53 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
         else hi = mid;
       }
       const bool found = lo < S && skey[lo] == k;
-      miss |= !found;
+      const uint32_t b = start[k], len = start[k + 1] - b;
+      miss |= !found || len > 0xffffu;
       const uint32_t off = found ? (uint32_t)soff[lo] : 0u;
-      const uint32_t b = start[k], e = start[k + 1];
-      for (uint32_t j = b; j < e; ++j) {
+      span[q] = found && len <= 0xffffu ? (off << 16) | len : 0u;
+      if (k == own && found) own_local = off + ((uint32_t)i - b);
+      keys[q] = b;  // from here on: the bucket's first particle
+    }
+  }
+  if (staged) {
+    __syncthreads();  // every lookup is done: the sort buffer takes the positions
+    R4<R>* s_x = reinterpret_cast<R4<R>*>(dsm);
+    for (uint32_t l = tid; l < H; l += kBlock) s_x[l] = pos[hidx[l]];
+    __syncthreads();
+    if (active) {
+#pragma unroll 1
+      for (int q = 0; q < 27; ++q) {
+        const uint32_t off = span[q] >> 16, len = span[q] & 0xffffu;
+        for (uint32_t r = 0; r < len; ++r) {
+          const uint32_t local = off + r;
+          if (local == own_local) continue;
+          const R4<R> xj = s_x[local];
+          if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
+          if (cnt < P.K) nbr[nbr_slot(i, cnt, P.K)] = (uint16_t)local;
+          ++cnt;
+          const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+          kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
+        }
+      }
+    }
+  } else if (active) {
+#pragma unroll 1
+    for (int q = 0; q < 27; ++q) {
+      const uint32_t b = keys[q], off = span[q] >> 16, len = span[q] & 0xffffu;
+      for (uint32_t r = 0; r < len; ++r) {
+        const uint32_t j = b + r;
         if ((int)j == i) continue;
         const R4<R> xj = pos[j];
         if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
-        const uint32_t local = off + (j - b);
-        if (cnt < P.K) nbr[nbr_slot(i, cnt, P.K)] = (uint16_t)(found && local < usable ? local : 0u);
+        const uint32_t local = off + r;
+        if (cnt < P.K) nbr[nbr_slot(i, cnt, P.K)] = (uint16_t)(local < usable ? local : 0u);
         ++cnt;
         const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
         kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
       }
     }
+  }
+  if (active) {
     if (miss) atomicMax(&sc->max_halo, 0x7fffffff);  // cannot happen: every stencil bucket is in the halo
     R denom = P.V0 * sum;
     if (has_boundary) denom += bW[i];
@@ -941,11 +1001,10 @@ __global__ void __launch_bounds__(kBlock) k_accel(
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
   R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
   if (H.staged)
-    for (int l = threadIdx.x; l < H.size; l += kBlock) {
-      const uint32_t g = H.idx[l];
+    stage_halo(H, [&](int l, uint32_t g) {
       s_x[l] = xv[g];
       s_v[l] = vel[g];
-    }
+    });
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < sc->n_active) {
@@ -1054,11 +1113,10 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
   R* s_p = staged_scalar<R>(dsm, N.hs, 1, 0);
   if (H.staged)
-    for (int l = threadIdx.x; l < H.size; l += kBlock) {
-      const uint32_t g = H.idx[l];
+    stage_halo(H, [&](int l, uint32_t g) {
       s_x[l] = xv[g];
       s_p[l] = press[g];
-    }
+    });
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < sc->n_active) {
@@ -1125,12 +1183,11 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
   R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
   R* s_m = staged_scalar<R>(dsm, N.hs, 2, 0);
   if (H.staged)
-    for (int l = threadIdx.x; l < H.size; l += kBlock) {
-      const uint32_t g = H.idx[l];
+    stage_halo(H, [&](int l, uint32_t g) {
       s_x[l] = xv[g];
       s_v[l] = vstar[g];
       s_m[l] = vel[g].w;
-    }
+    });
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= sc->n_active) return;
@@ -1195,11 +1252,10 @@ __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
   R4<R>* s_a = staged_vec<R>(dsm, N.hs, 1);
   if (H.staged)
-    for (int l = threadIdx.x; l < H.size; l += kBlock) {
-      const uint32_t g = H.idx[l];
+    stage_halo(H, [&](int l, uint32_t g) {
       s_x[l] = xv[g];
       s_a[l] = accp[g];
-    }
+    });
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = sc->n_active;
@@ -1306,12 +1362,11 @@ __global__ void __launch_bounds__(kBlock) k_split_density(
   R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
   R* s_m = staged_scalar<R>(dsm, N.hs, 2, 0);
   if (H.staged)
-    for (int l = threadIdx.x; l < H.size; l += kBlock) {
-      const uint32_t g = H.idx[l];
+    stage_halo(H, [&](int l, uint32_t g) {
       s_x[l] = xv[g];
       s_v[l] = vstar[g];
       s_m[l] = vel[g].w;
-    }
+    });
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= sc->n_active) return;

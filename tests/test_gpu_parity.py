@@ -141,9 +141,9 @@ def test_sesph_multistep_tracks_oracle(A, oracle, sesph_scene):
 # ---------------------------------------------------------------------------------------
 # IISPH with a VolumeMapBoundary box (small, fields built by the oracle)
 # ---------------------------------------------------------------------------------------
-# The reference's volume-map boundary contributes strongly near walls, so an
-# uncapped IISPH solve of this small scene needs hundreds of sweeps; both the
-# engine and the oracle cap it here (the north-star configuration caps at 100).
+# Both the engine and the oracle cap the solve (the north-star configuration
+# caps at 100); with the fluid 1.5 spacings from the walls it converges in a
+# few sweeps, so the cap only bounds the test's run time.
 VM_CAP = 40
 
 
@@ -192,8 +192,7 @@ def test_iisph_volume_map_first_update_matches_oracle(A, oracle, vm_case, precis
 
 @pytest.mark.parametrize("precision", ["f64", "f32"])
 def test_iisph_volume_map_steps_track_oracle(A, oracle, vm_case, precision):
-    # three steps with CFL time increments (the wall-adjacent layer is pushed
-    # away hard in this configuration, so only a short horizon is compared)
+    # three steps with CFL time increments
     from sphgpu import scenes
     sc, fields, _ = vm_case
     g = scenes.build_system(sc, precision=precision, fields=fields)
@@ -206,7 +205,10 @@ def test_iisph_volume_map_steps_track_oracle(A, oracle, vm_case, precision):
         assert abs(mg["time"] - mo["time"]) < tol * mo["time"]
         assert abs(mg["time_step_size"] - mo["time_step_size"]) < tol * mo["time_step_size"]
         assert abs(mg["density"] - mo["density"]) < tol * mo["density"]
-        assert mg["solver_iterations"] == mo["solver_iterations"] == VM_CAP
+        if precision == "f64":
+            assert mg["solver_iterations"] == mo["solver_iterations"] < VM_CAP
+        else:
+            assert abs(mg["solver_iterations"] - mo["solver_iterations"]) <= 1
     x_g, x_o = g.download(A.FIELD_POSITION), o.download(oracle.F_POSITION)
     assert np.max(np.abs(x_g - x_o)) < (1e-9 if precision == "f64" else 1e-5)
 
@@ -217,7 +219,7 @@ def test_iisph_volume_map_steps_track_oracle(A, oracle, vm_case, precision):
 def test_disable_below_threshold_matches_swap_remove_order(A, oracle, sesph_scene):
     from sphgpu import scenes
     sc = scenes.dam_break_sesph_8k()
-    sc.parameters = dict(sc.parameters, disable_particles_below=-0.28)
+    sc.parameters = dict(sc.parameters, disable_particles_below=-0.265)  # below the first layer
     g = scenes.build_system(sc, precision="f64")
     o = build_oracle(sc)
     assert g.n == o.n < 8000
