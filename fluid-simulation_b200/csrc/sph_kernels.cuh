@@ -402,9 +402,30 @@ __device__ __forceinline__ HaloView halo_view(const NbrArgs& N) {
   return h;
 }
 
+// Asynchronous global -> shared copies (cp.async): the records travel without
+// passing through registers, so every copy a thread issues is in flight at
+// once; stage_done() waits for this thread's copies and then for the block.
+template <class T>
+__device__ __forceinline__ void async_copy(T* smem_dst, const T* gsrc) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8 || sizeof(T) % 16 == 0, "cp.async moves 4, 8 or 16 bytes");
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  if constexpr (sizeof(T) % 16 == 0) {
+#pragma unroll
+    for (int o = 0; o < (int)sizeof(T); o += 16)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d + o),
+                   "l"(reinterpret_cast<const char*>(gsrc) + o) : "memory");
+  } else {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gsrc), "n"(sizeof(T)) : "memory");
+  }
+}
+__device__ __forceinline__ void stage_done() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  __syncthreads();
+}
+
 // Copies the block's halo records to shared memory: copy(l, g) moves the
-// record of particle g to position l. Four positions per thread are in flight
-// (their halo indices first, then the records).
+// record of particle g to position l. Four halo indices per thread are read
+// at a time, then their records are requested.
 template <class F>
 __device__ __forceinline__ void stage_halo(const HaloView& H, F&& copy) {
   for (int l0 = threadIdx.x; l0 < H.size; l0 += 4 * kBlock) {
@@ -511,22 +532,23 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
   }
   __syncthreads();
   const uint32_t usable = min(H, (uint32_t)hcap);
-  // 3. neighbors (strict range) and volume, with halo positions. Every
-  // candidate lies in the halo; when the halo's positions fit the sort buffer
-  // they are staged there (after the bucket lookups are done) and the
-  // candidate loop reads shared memory instead of global memory.
+  // 3. The 27 stencil buckets of a cell, in ascending key (= memory) order so
+  // every list comes out sorted by neighbor index (lanes of a warp then read
+  // their k-th neighbors from nearby halo positions in the later passes), as
+  // (halo offset << 16 | size) spans. The first particle of each run of one
+  // cell looks them up and shares them through a table in the offset buffer;
+  // a block with more distinct cells than the table holds looks them up per
+  // particle. The halo's positions then move into the sort buffer when they
+  // fit, and the candidate loop reads shared memory.
+  constexpr int kSpanWords = 28;  // 27 spans + (own bucket offset - its first particle)
+  constexpr int kTableCells = (int)(kHaloKeys * sizeof(uint16_t) / (kSpanWords * sizeof(uint32_t)));
+  const bool table = (int)nheads <= kTableCells;
   const bool staged = H <= usable && H <= (uint32_t)(kHaloKeys * sizeof(uint32_t) / sizeof(R4<R>));
-  int cnt = 0;
-  R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
-  R comp = 0;
+  uint32_t span[27];
+  int own_base = 0;
   bool miss = false;
-  // Visit the 27 stencil buckets in ascending key (= memory) order so every
-  // list comes out sorted by neighbor index: lanes of a warp then read their
-  // k-th neighbors from nearby halo positions in the passes that follow.
-  uint32_t keys[27];
-  uint32_t span[27];  // (halo offset << 16) | bucket size, for the staged loop
-  uint32_t own_local = 0xffffffffu;
-  if (active) {
+  if (table ? head : active) {
+    uint32_t keys[27];
 #pragma unroll
     for (int q = 0; q < 27; ++q)
       keys[q] = morton_key(cx + (q % 3) - 1, cy + (q / 3) % 3 - 1, cz + q / 9 - 1, P.mask);
@@ -554,50 +576,60 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
       miss |= !found || len > 0xffffu;
       const uint32_t off = found ? (uint32_t)soff[lo] : 0u;
       span[q] = found && len <= 0xffffu ? (off << 16) | len : 0u;
-      if (k == own && found) own_local = off + ((uint32_t)i - b);
-      keys[q] = b;  // from here on: the bucket's first particle
+      if (k == own) own_base = (int)off - (int)b;
     }
   }
-  if (staged) {
-    __syncthreads();  // every lookup is done: the sort buffer takes the positions
-    R4<R>* s_x = reinterpret_cast<R4<R>*>(dsm);
+  __syncthreads();  // every lookup is done: the offset and sort buffers are free
+  uint32_t* tab = reinterpret_cast<uint32_t*>(soff);
+  if (table && head) {
+#pragma unroll
+    for (int q = 0; q < 27; ++q) tab[rank * kSpanWords + q] = span[q];
+    tab[rank * kSpanWords + 27] = (uint32_t)own_base;
+  }
+  R4<R>* s_x = reinterpret_cast<R4<R>*>(dsm);
+  if (staged)
     for (uint32_t l = tid; l < H; l += kBlock) s_x[l] = pos[hidx[l]];
-    __syncthreads();
-    if (active) {
+  __syncthreads();
+  int cnt = 0;
+  if (active) {
+    if (miss) atomicMax(&sc->max_halo, 0x7fffffff);  // cannot happen: every stencil bucket is in the halo
+    const int hr = head ? (int)rank : (int)rank - 1;  // this cell's row of the table
+    const uint32_t* row = tab + hr * kSpanWords;
+    if (table) own_base = (int)row[27];
+    const uint32_t own_local = (uint32_t)(own_base + i);
+    uint16_t* list = nbr + nbr_slot(i, 0, P.K);
+    R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
+    R comp = 0;
 #pragma unroll 1
-      for (int q = 0; q < 27; ++q) {
-        const uint32_t off = span[q] >> 16, len = span[q] & 0xffffu;
+    for (int q = 0; q < 27; ++q) {
+      const uint32_t sp = table ? row[q] : span[q];
+      const uint32_t off = sp >> 16, len = sp & 0xffffu;
+      if (staged) {
         for (uint32_t r = 0; r < len; ++r) {
           const uint32_t local = off + r;
           if (local == own_local) continue;
           const R4<R> xj = s_x[local];
           if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
-          if (cnt < P.K) nbr[nbr_slot(i, cnt, P.K)] = (uint16_t)local;
+          if (cnt < P.K) list[(cnt >> 2) * 128 + (cnt & 3)] = (uint16_t)local;
+          ++cnt;
+          const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+          kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
+        }
+      } else {
+        const uint32_t b = len && off < usable ? hidx[off] : 0u;
+        for (uint32_t r = 0; r < len; ++r) {
+          const uint32_t j = b + r;
+          if ((int)j == i) continue;
+          const R4<R> xj = pos[j];
+          if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
+          const uint32_t local = off + r;
+          if (cnt < P.K) list[(cnt >> 2) * 128 + (cnt & 3)] = (uint16_t)(local < usable ? local : 0u);
           ++cnt;
           const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
           kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
         }
       }
     }
-  } else if (active) {
-#pragma unroll 1
-    for (int q = 0; q < 27; ++q) {
-      const uint32_t b = keys[q], off = span[q] >> 16, len = span[q] & 0xffffu;
-      for (uint32_t r = 0; r < len; ++r) {
-        const uint32_t j = b + r;
-        if ((int)j == i) continue;
-        const R4<R> xj = pos[j];
-        if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
-        const uint32_t local = off + r;
-        if (cnt < P.K) nbr[nbr_slot(i, cnt, P.K)] = (uint16_t)(local < usable ? local : 0u);
-        ++cnt;
-        const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-        kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
-      }
-    }
-  }
-  if (active) {
-    if (miss) atomicMax(&sc->max_halo, 0x7fffffff);  // cannot happen: every stencil bucket is in the halo
     R denom = P.V0 * sum;
     if (has_boundary) denom += bW[i];
     const R V = P.V0 / denom;
@@ -935,13 +967,24 @@ template <int NB, class Load, class Use>
 __device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ nbr, int K, int i,
                                                   int cnt, Load&& load, Use&& use) {
   static_assert(NB % 4 == 0, "neighbors are read in groups of four");
+  // group g of this lane sits 32 uint2 after group g-1; the next batch's
+  // groups are requested before the current batch is consumed
   const uint2* base = reinterpret_cast<const uint2*>(nbr) + nbr_slot(i, 0, K) / 4;
+  const int ngroups = (cnt + 3) >> 2;
+  uint2 cur[NB / 4];
+#pragma unroll
+  for (int g = 0; g < NB / 4; ++g) cur[g] = g < ngroups ? __ldcs(base + (size_t)g * 32) : make_uint2(0u, 0u);
   for (int k0 = 0; k0 < cnt; k0 += NB) {
+    uint2 nxt[NB / 4];
+#pragma unroll
+    for (int g = 0; g < NB / 4; ++g) {
+      const int gi = (k0 + NB) / 4 + g;
+      nxt[g] = gi < ngroups ? __ldcs(base + (size_t)gi * 32) : make_uint2(0u, 0u);
+    }
     uint32_t l[NB];
 #pragma unroll
     for (int g = 0; g < NB / 4; ++g) {
-      // group k0/4+g of this lane sits 32 uint2 after the previous group
-      const uint2 q = k0 + 4 * g < cnt ? __ldcs(base + (size_t)(k0 / 4 + g) * 32) : make_uint2(0u, 0u);
+      const uint2 q = cur[g];
       l[4 * g + 0] = k0 + 4 * g + 0 < cnt ? (q.x & 0xffffu) : 0u;
       l[4 * g + 1] = k0 + 4 * g + 1 < cnt ? (q.x >> 16) : 0u;
       l[4 * g + 2] = k0 + 4 * g + 2 < cnt ? (q.y & 0xffffu) : 0u;
@@ -953,6 +996,8 @@ __device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ n
 #pragma unroll
     for (int u = 0; u < NB; ++u)
       if (k0 + u < cnt) use(d[u]);
+#pragma unroll
+    for (int g = 0; g < NB / 4; ++g) cur[g] = nxt[g];
   }
 }
 
@@ -1002,10 +1047,10 @@ __global__ void __launch_bounds__(kBlock) k_accel(
   R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
   if (H.staged)
     stage_halo(H, [&](int l, uint32_t g) {
-      s_x[l] = xv[g];
-      s_v[l] = vel[g];
+      async_copy(&s_x[l], &xv[g]);
+      async_copy(&s_v[l], &vel[g]);
     });
-  __syncthreads();
+  stage_done();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < sc->n_active) {
     const R4<R> xi = xv[i];
@@ -1114,10 +1159,10 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
   R* s_p = staged_scalar<R>(dsm, N.hs, 1, 0);
   if (H.staged)
     stage_halo(H, [&](int l, uint32_t g) {
-      s_x[l] = xv[g];
-      s_p[l] = press[g];
+      async_copy(&s_x[l], &xv[g]);
+      async_copy(&s_p[l], &press[g]);
     });
-  __syncthreads();
+  stage_done();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < sc->n_active) {
     const R4<R> xi = xv[i];
@@ -1184,11 +1229,11 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
   R* s_m = staged_scalar<R>(dsm, N.hs, 2, 0);
   if (H.staged)
     stage_halo(H, [&](int l, uint32_t g) {
-      s_x[l] = xv[g];
-      s_v[l] = vstar[g];
-      s_m[l] = vel[g].w;
+      async_copy(&s_x[l], &xv[g]);
+      async_copy(&s_v[l], &vstar[g]);
+      async_copy(&s_m[l], &vel[g].w);
     });
-  __syncthreads();
+  stage_done();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= sc->n_active) return;
   const R dt = (R)sc->dt;
@@ -1253,10 +1298,10 @@ __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
   R4<R>* s_a = staged_vec<R>(dsm, N.hs, 1);
   if (H.staged)
     stage_halo(H, [&](int l, uint32_t g) {
-      s_x[l] = xv[g];
-      s_a[l] = accp[g];
+      async_copy(&s_x[l], &xv[g]);
+      async_copy(&s_a[l], &accp[g]);
     });
-  __syncthreads();
+  stage_done();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = sc->n_active;
   double e = 0.0;
@@ -1363,11 +1408,11 @@ __global__ void __launch_bounds__(kBlock) k_split_density(
   R* s_m = staged_scalar<R>(dsm, N.hs, 2, 0);
   if (H.staged)
     stage_halo(H, [&](int l, uint32_t g) {
-      s_x[l] = xv[g];
-      s_v[l] = vstar[g];
-      s_m[l] = vel[g].w;
+      async_copy(&s_x[l], &xv[g]);
+      async_copy(&s_v[l], &vstar[g]);
+      async_copy(&s_m[l], &vel[g].w);
     });
-  __syncthreads();
+  stage_done();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= sc->n_active) return;
   const R dt = (R)sc->dt;

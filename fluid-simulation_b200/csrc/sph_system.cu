@@ -1139,7 +1139,8 @@ class System : public SystemBase {
       // the same (already integrated) state. Reaction forces gathered so far
       // are discarded first; they are rebuilt by the redo.
       if (h_sc_->max_nbrs > K_) {
-        K_ = (int)round_up((size_t)h_sc_->max_nbrs + 8, 8);  // multiple of 4 (64-bit groups)
+        // grow with headroom: compressing scenes raise the count step after step
+        K_ = (int)round_up((size_t)h_sc_->max_nbrs * 5 / 4 + 8, 8);  // multiple of 4 (64-bit groups)
         P_.K = K_;
         nbr_.alloc((size_t)K_ * np_);
       }
