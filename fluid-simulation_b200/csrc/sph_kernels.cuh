@@ -451,6 +451,28 @@ __device__ __forceinline__ void kahan_add(R& s, R& c, R t) {
   s = u;
 }
 
+// The 27 stencil bucket keys of cell (cx,cy,cz), ascending (= memory order)
+// when `sorted`, else in stencil order.
+__device__ __forceinline__ void stencil_keys(int cx, int cy, int cz, uint32_t mask, int sorted, uint32_t keys[27]) {
+#pragma unroll
+  for (int q = 0; q < 27; ++q) keys[q] = morton_key(cx + (q % 3) - 1, cy + (q / 3) % 3 - 1, cz + q / 9 - 1, mask);
+  if (sorted) {
+#pragma unroll
+    for (int pass = 0; pass < 27; ++pass) {
+#pragma unroll
+      for (int q = pass & 1; q + 1 < 27; q += 2) {
+        const uint32_t a = keys[q], b = keys[q + 1];
+        keys[q] = min(a, b);
+        keys[q + 1] = max(a, b);
+      }
+    }
+  }
+}
+
+constexpr int kHashSlots = 4096;   // halo bucket set of a block (hash path)
+constexpr int kHashElems = 3072;   // stencil keys the hash path takes (27 per cell)
+__device__ __forceinline__ uint32_t hash_slot(uint32_t k) { return (k * 0x9E3779B1u) >> 20; }  // 12 bits
+
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_neighbors_density(
     Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, const uint32_t* __restrict__ start,
@@ -458,9 +480,8 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
     uint32_t* __restrict__ halo_idx, uint32_t* __restrict__ halo_n, const R* __restrict__ bW,
     int has_boundary, int hcap, StepParams<R> P) {
   extern __shared__ __align__(32) unsigned char dsm[];
-  uint32_t* skey = reinterpret_cast<uint32_t*>(dsm);                 // sorted stencil keys
-  uint16_t* soff = reinterpret_cast<uint16_t*>(skey + kHaloKeys);    // halo offset of each first key
   __shared__ int3 s_cell[kBlock];
+  __shared__ int s_own[kBlock];      // per cell: own bucket's halo offset - its first particle
   __shared__ uint32_t s_scan[32];
   const int tid = threadIdx.x;
   const int i = blockIdx.x * kBlock + tid;
@@ -480,112 +501,167 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
   const bool head = active && (tid == 0 || prev.x != cx || prev.y != cy || prev.z != cz);
   uint32_t nheads = 0;
   const uint32_t rank = block_excl_scan_u32(head ? 1u : 0u, s_scan, &nheads);
-  // 1. the heads' stencil keys, bitonic-sorted (duplicates kept)
   const int nk = 27 * (int)nheads;
-  int S = 32;
-  while (S < nk) S <<= 1;
-  if (head)
-    for (int q = 0; q < 27; ++q)
-      skey[27 * rank + q] = morton_key(cx + q % 3 - 1, cy + (q / 3) % 3 - 1, cz + q / 9 - 1, P.mask);
-  for (int t = nk + tid; t < S; t += kBlock) skey[t] = kNoKey;
-  __syncthreads();
-  for (int k = 2; k <= S; k <<= 1)
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int t = tid; t < (S >> 1); t += kBlock) {
-        const int a = (t / j) * 2 * j + (t % j), b = a + j;
-        const uint32_t ka = skey[a], kb = skey[b];
-        if ((ka > kb) == ((a & k) == 0)) {
-          skey[a] = kb;
-          skey[b] = ka;
-        }
-      }
-      __syncthreads();
-    }
-  // 2. distinct buckets in key order -> halo offsets and halo_idx
-  const int per = S >= kBlock ? S / kBlock : 1;
-  const int p0 = tid * per;
-  uint32_t len = 0;
-  for (int q = 0; q < per; ++q) {
-    const int p = p0 + q;
-    if (p >= S) break;
-    const uint32_t k = skey[p];
-    if (k != kNoKey && (p == 0 || skey[p - 1] != k)) len += start[k + 1] - start[k];
-  }
-  uint32_t H = 0;
-  uint32_t run = block_excl_scan_u32(len, s_scan, &H);
   uint32_t* hidx = halo_idx + (size_t)blockIdx.x * (size_t)hcap;
-  for (int q = 0; q < per; ++q) {
-    const int p = p0 + q;
-    if (p >= S) break;
-    const uint32_t k = skey[p];
-    if (k != kNoKey && (p == 0 || skey[p - 1] != k)) {
-      const uint32_t b = start[k], e = start[k + 1];
-      soff[p] = (uint16_t)min(run, 65535u);
-      for (uint32_t j = b; j < e; ++j)
-        if (run + (j - b) < (uint32_t)hcap) hidx[run + (j - b)] = j;
-      run += e - b;
+  uint32_t H = 0;
+  bool miss = false;
+  // Per cell, the 27 stencil buckets as (halo offset << 16 | size) spans in
+  // ascending key order, in `span_tab` (27 words per cell) when the cells fit,
+  // else per particle in `span`.
+  const bool hashed = nk <= kHashElems;
+  uint32_t* span_tab = nullptr;
+  uint32_t span[27];
+  if (hashed) {
+    // hash path: the set of the cells' stencil buckets in a shared hash table,
+    // halo offsets in slot order
+    uint32_t* hkey = reinterpret_cast<uint32_t*>(dsm);            // kHashSlots
+    uint32_t* hval = hkey + kHashSlots;                            // kHashSlots: offset << 16 | size
+    span_tab = hval + kHashSlots;                                  // kHashElems: keys, then spans
+    for (int t = tid; t < kHashSlots; t += kBlock) hkey[t] = kNoKey;
+    if (head) {
+      uint32_t keys[27];
+      stencil_keys(cx, cy, cz, P.mask, P.sorted_lists, keys);
+#pragma unroll
+      for (int q = 0; q < 27; ++q) span_tab[27 * rank + q] = keys[q];
+    }
+    __syncthreads();
+    for (int e = tid; e < nk; e += kBlock) {
+      const uint32_t k = span_tab[e];
+      uint32_t h = hash_slot(k);
+      for (int probe = 0; probe < kHashSlots; ++probe, h = (h + 1) & (kHashSlots - 1)) {
+        const uint32_t old = atomicCAS(&hkey[h], kNoKey, k);
+        if (old == kNoKey || old == k) break;
+      }
+    }
+    __syncthreads();
+    // sizes of the distinct buckets, offsets by a block scan over the slots
+    constexpr int per = kHashSlots / kBlock;
+    uint32_t len[per], tot = 0;
+#pragma unroll
+    for (int u = 0; u < per; ++u) {
+      const uint32_t k = hkey[tid * per + u];
+      len[u] = k != kNoKey ? start[k + 1] - start[k] : 0u;
+      tot += len[u];
+    }
+    uint32_t run = block_excl_scan_u32(tot, s_scan, &H);
+#pragma unroll
+    for (int u = 0; u < per; ++u) {
+      const uint32_t k = hkey[tid * per + u];
+      miss |= len[u] > 0xffffu;
+      hval[tid * per + u] = (min(run, 65535u) << 16) | min(len[u], 65535u);
+      if (k != kNoKey) {
+        const uint32_t b = start[k];
+        for (uint32_t r = 0; r < len[u]; ++r)
+          if (run + r < (uint32_t)hcap) hidx[run + r] = b + r;
+      }
+      run += len[u];
+    }
+    __syncthreads();
+    // each cell's spans: look its keys up in the table
+    for (int e = tid; e < nk; e += kBlock) {
+      const uint32_t k = span_tab[e];
+      uint32_t h = hash_slot(k), v = 0;
+      bool found = false;
+      for (int probe = 0; probe < kHashSlots; ++probe, h = (h + 1) & (kHashSlots - 1)) {
+        const uint32_t kk = hkey[h];
+        if (kk == k) { v = hval[h]; found = true; break; }
+        if (kk == kNoKey) break;
+      }
+      miss |= !found;
+      span_tab[e] = v;
+    }
+    if (head) {
+      // own bucket: its offset minus its first particle gives the halo position of i
+      const uint32_t own = morton_key(cx, cy, cz, P.mask);
+      uint32_t h = hash_slot(own), v = 0;
+      for (int probe = 0; probe < kHashSlots; ++probe, h = (h + 1) & (kHashSlots - 1)) {
+        const uint32_t kk = hkey[h];
+        if (kk == own) { v = hval[h]; break; }
+        if (kk == kNoKey) break;
+      }
+      s_own[rank] = (int)(v >> 16) - (int)start[own];
+    }
+  } else {
+    // general path: bitonic-sorted stencil keys, halo offsets in key order,
+    // per-particle lookups by binary search
+    uint32_t* skey = reinterpret_cast<uint32_t*>(dsm);                 // sorted stencil keys
+    uint16_t* soff = reinterpret_cast<uint16_t*>(skey + kHaloKeys);    // halo offset of each first key
+    int S = 32;
+    while (S < nk) S <<= 1;
+    if (head) {
+      uint32_t keys[27];
+      stencil_keys(cx, cy, cz, P.mask, 0, keys);
+#pragma unroll
+      for (int q = 0; q < 27; ++q) skey[27 * rank + q] = keys[q];
+    }
+    for (int t = nk + tid; t < S; t += kBlock) skey[t] = kNoKey;
+    __syncthreads();
+    for (int k = 2; k <= S; k <<= 1)
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int t = tid; t < (S >> 1); t += kBlock) {
+          const int a = (t / j) * 2 * j + (t % j), b = a + j;
+          const uint32_t ka = skey[a], kb = skey[b];
+          if ((ka > kb) == ((a & k) == 0)) {
+            skey[a] = kb;
+            skey[b] = ka;
+          }
+        }
+        __syncthreads();
+      }
+    const int per = S >= kBlock ? S / kBlock : 1;
+    const int p0 = tid * per;
+    uint32_t len = 0;
+    for (int q = 0; q < per; ++q) {
+      const int p = p0 + q;
+      if (p >= S) break;
+      const uint32_t k = skey[p];
+      if (k != kNoKey && (p == 0 || skey[p - 1] != k)) len += start[k + 1] - start[k];
+    }
+    uint32_t run = block_excl_scan_u32(len, s_scan, &H);
+    for (int q = 0; q < per; ++q) {
+      const int p = p0 + q;
+      if (p >= S) break;
+      const uint32_t k = skey[p];
+      if (k != kNoKey && (p == 0 || skey[p - 1] != k)) {
+        const uint32_t b = start[k], e = start[k + 1];
+        soff[p] = (uint16_t)min(run, 65535u);
+        for (uint32_t j = b; j < e; ++j)
+          if (run + (j - b) < (uint32_t)hcap) hidx[run + (j - b)] = j;
+        run += e - b;
+      }
+    }
+    __syncthreads();
+    if (active) {
+      uint32_t keys[27];
+      stencil_keys(cx, cy, cz, P.mask, P.sorted_lists, keys);
+      const uint32_t own = morton_key(cx, cy, cz, P.mask);
+#pragma unroll 1
+      for (int q = 0; q < 27; ++q) {
+        const uint32_t k = keys[q];
+        int lo = 0, hi = S;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (skey[mid] < k) lo = mid + 1;
+          else hi = mid;
+        }
+        const bool found = lo < S && skey[lo] == k;
+        const uint32_t b = start[k], len2 = start[k + 1] - b;
+        miss |= !found || len2 > 0xffffu;
+        const uint32_t off = found ? (uint32_t)soff[lo] : 0u;
+        span[q] = found && len2 <= 0xffffu ? (off << 16) | len2 : 0u;
+        if (k == own) s_own[tid] = (int)off - (int)b;
+      }
     }
   }
   if (tid == 0) {
     halo_n[blockIdx.x] = H;
     atomicMax(&sc->max_halo, (int)min(H, 0x7fffffffu));
   }
-  __syncthreads();
+  __syncthreads();  // spans, offsets and halo_idx are complete; the sort / hash buffers are free
   const uint32_t usable = min(H, (uint32_t)hcap);
-  // 3. The 27 stencil buckets of a cell, in ascending key (= memory) order so
-  // every list comes out sorted by neighbor index (lanes of a warp then read
-  // their k-th neighbors from nearby halo positions in the later passes), as
-  // (halo offset << 16 | size) spans. The first particle of each run of one
-  // cell looks them up and shares them through a table in the offset buffer;
-  // a block with more distinct cells than the table holds looks them up per
-  // particle. The halo's positions then move into the sort buffer when they
-  // fit, and the candidate loop reads shared memory.
-  constexpr int kSpanWords = 28;  // 27 spans + (own bucket offset - its first particle)
-  constexpr int kTableCells = (int)(kHaloKeys * sizeof(uint16_t) / (kSpanWords * sizeof(uint32_t)));
-  const bool table = (int)nheads <= kTableCells;
-  const bool staged = H <= usable && H <= (uint32_t)(kHaloKeys * sizeof(uint32_t) / sizeof(R4<R>));
-  uint32_t span[27];
-  int own_base = 0;
-  bool miss = false;
-  if (table ? head : active) {
-    uint32_t keys[27];
-#pragma unroll
-    for (int q = 0; q < 27; ++q)
-      keys[q] = morton_key(cx + (q % 3) - 1, cy + (q / 3) % 3 - 1, cz + q / 9 - 1, P.mask);
-#pragma unroll
-    for (int pass = 0; pass < (P.sorted_lists ? 27 : 0); ++pass) {
-#pragma unroll
-      for (int q = pass & 1; q + 1 < 27; q += 2) {
-        const uint32_t a = keys[q], b = keys[q + 1];
-        keys[q] = min(a, b);
-        keys[q + 1] = max(a, b);
-      }
-    }
-    const uint32_t own = morton_key(cx, cy, cz, P.mask);
-#pragma unroll 1
-    for (int q = 0; q < 27; ++q) {
-      const uint32_t k = keys[q];
-      int lo = 0, hi = S;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (skey[mid] < k) lo = mid + 1;
-        else hi = mid;
-      }
-      const bool found = lo < S && skey[lo] == k;
-      const uint32_t b = start[k], len = start[k + 1] - b;
-      miss |= !found || len > 0xffffu;
-      const uint32_t off = found ? (uint32_t)soff[lo] : 0u;
-      span[q] = found && len <= 0xffffu ? (off << 16) | len : 0u;
-      if (k == own) own_base = (int)off - (int)b;
-    }
-  }
-  __syncthreads();  // every lookup is done: the offset and sort buffers are free
-  uint32_t* tab = reinterpret_cast<uint32_t*>(soff);
-  if (table && head) {
-#pragma unroll
-    for (int q = 0; q < 27; ++q) tab[rank * kSpanWords + q] = span[q];
-    tab[rank * kSpanWords + 27] = (uint32_t)own_base;
-  }
+  // The halo's positions move into the first 32 KB of shared memory when they
+  // fit (the cells' span table lies beyond them).
+  const bool staged = H <= usable && H <= (uint32_t)(2 * kHashSlots * sizeof(uint32_t) / sizeof(R4<R>));
   R4<R>* s_x = reinterpret_cast<R4<R>*>(dsm);
   if (staged)
     for (uint32_t l = tid; l < H; l += kBlock) s_x[l] = pos[hidx[l]];
@@ -593,29 +669,39 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
   int cnt = 0;
   if (active) {
     if (miss) atomicMax(&sc->max_halo, 0x7fffffff);  // cannot happen: every stencil bucket is in the halo
-    const int hr = head ? (int)rank : (int)rank - 1;  // this cell's row of the table
-    const uint32_t* row = tab + hr * kSpanWords;
-    if (table) own_base = (int)row[27];
-    const uint32_t own_local = (uint32_t)(own_base + i);
+    const int hr = head ? (int)rank : (int)rank - 1;  // this cell's row of the span table
+    const uint32_t* row = hashed ? span_tab + 27 * hr : nullptr;
+    const uint32_t own_local = (uint32_t)((hashed ? s_own[hr] : s_own[tid]) + i);
     uint16_t* list = nbr + nbr_slot(i, 0, P.K);
     R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
     R comp = 0;
+    if (staged) {
+      // pass 1: the strict-range test over all candidates builds the list
 #pragma unroll 1
-    for (int q = 0; q < 27; ++q) {
-      const uint32_t sp = table ? row[q] : span[q];
-      const uint32_t off = sp >> 16, len = sp & 0xffffu;
-      if (staged) {
+      for (int q = 0; q < 27; ++q) {
+        const uint32_t sp = hashed ? row[q] : span[q];
+        const uint32_t off = sp >> 16, len = sp & 0xffffu;
         for (uint32_t r = 0; r < len; ++r) {
           const uint32_t local = off + r;
-          if (local == own_local) continue;
           const R4<R> xj = s_x[local];
-          if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
-          if (cnt < P.K) list[(cnt >> 2) * 128 + (cnt & 3)] = (uint16_t)local;
-          ++cnt;
-          const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-          kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
+          if (local != own_local && in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) {
+            if (cnt < P.K) list[(cnt >> 2) * 128 + (cnt & 3)] = (uint16_t)local;
+            ++cnt;
+          }
         }
-      } else {
+      }
+      // pass 2: the kernel sum over the neighbors, in list order
+      const int stored = min(cnt, P.K);
+      for (int k = 0; k < stored; ++k) {
+        const R4<R> xj = s_x[list[(k >> 2) * 128 + (k & 3)]];
+        const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+        kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
+      }
+    } else {
+#pragma unroll 1
+      for (int q = 0; q < 27; ++q) {
+        const uint32_t sp = hashed ? row[q] : span[q];
+        const uint32_t off = sp >> 16, len = sp & 0xffffu;
         const uint32_t b = len && off < usable ? hidx[off] : 0u;
         for (uint32_t r = 0; r < len; ++r) {
           const uint32_t j = b + r;
