@@ -676,11 +676,26 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
     R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
     R comp = 0;
     if (staged) {
-      // pass 1: the strict-range test over all candidates builds the list
+      // pass 1: the strict-range test over all candidates builds the list;
+      // in stencil order, a bucket whose cell lies entirely beyond the
+      // support radius (with a relative margin, so it only skips particles
+      // the test would reject) is passed over
+      const R h = (R)P.range;
+      const R cut2 = (R)(P.range * P.range * (1.0 + 1e-3));
+      const R lox = (R)cx * h, loy = (R)cy * h, loz = (R)cz * h;
 #pragma unroll 1
       for (int q = 0; q < 27; ++q) {
         const uint32_t sp = hashed ? row[q] : span[q];
-        const uint32_t off = sp >> 16, len = sp & 0xffffu;
+        const uint32_t off = sp >> 16;
+        uint32_t len = sp & 0xffffu;
+        if (!P.sorted_lists && len) {
+          const int ox = q % 3 - 1, oy = (q / 3) % 3 - 1, oz = q / 9 - 1;
+          const R ex = ox < 0 ? xi.x - lox : (ox > 0 ? lox + h - xi.x : R(0));
+          const R ey = oy < 0 ? xi.y - loy : (oy > 0 ? loy + h - xi.y : R(0));
+          const R ez = oz < 0 ? xi.z - loz : (oz > 0 ? loz + h - xi.z : R(0));
+          const R dx = fmax(ex, R(0)), dy = fmax(ey, R(0)), dz = fmax(ez, R(0));
+          if (dx * dx + dy * dy + dz * dz > cut2) len = 0;
+        }
         for (uint32_t r = 0; r < len; ++r) {
           const uint32_t local = off + r;
           const R4<R> xj = s_x[local];
@@ -854,7 +869,7 @@ __device__ bool ser_gradient(const DevField& F, double px, double py, double pz,
 // vol = min(VM, 4/3 pi r^3); stored as vmx = {x_b, vol}, vmv = {v_b, kind}
 // where kind 0 = none, 1 = tangent helper x-axis, 2 = helper y-axis.
 template <class R>
-__global__ void __launch_bounds__(kBlock) k_vm_sample(
+__global__ void __launch_bounds__(kBlock, 4) k_vm_sample(
     Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, const VMDesc* __restrict__ vms,
     int nvm, const Body* __restrict__ bodies, R4<R>* __restrict__ vmx, R4<R>* __restrict__ vmv,
     R* __restrict__ bW, R4<R>* __restrict__ bG, R4<R>* __restrict__ bGu, StepParams<R> P) {

@@ -618,7 +618,11 @@ class System : public SystemBase {
   uint64_t time_offset_steps_ = 0;
   int last_iters_ = 3;
   int nb_ = 4;  // neighbor gather batch (prefetch width) of the neighbor passes
-  bool sorted_lists_ = true;   // neighbor lists in ascending index order
+  // Neighbor lists in ascending stencil-key order (1) or in stencil order (0,
+  // the default: neighbor records come from the block's staged halo, so list
+  // order no longer matters for memory locality, and stencil order lets the
+  // search skip buckets whose cell lies beyond the support radius).
+  bool sorted_lists_ = false;
   uint64_t launches_ = 0;
   bool profiling_ = false;
   std::map<std::string, ProfEntry> prof_;
