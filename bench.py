@@ -33,6 +33,9 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# The scene server runs every resident scene on its own stream; more hardware
+# work queues than the default 8 keep their kernels from serializing.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 sys.path.insert(0, os.path.join(ROOT, "fluid-simulation_b200"))
 
 METRIC = "particle-updates/s at 1M IISPH (VolumeMapBoundary dam break)"

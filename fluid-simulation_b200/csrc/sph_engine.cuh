@@ -53,6 +53,8 @@ struct Scalars {
   unsigned int trouble;            // bits: 1 neighbor overflow, 2 disabled particles, 4 unconverged
   int status_any;                  // 2 once any step of the chunk hit the sweep cap
   unsigned long long loop_sweeps;  // sweeps run by the graph's solver while-loops
+  int chunk_max_nbrs;              // largest fluid neighbor count over the chunk
+  int chunk_max_halo;              // largest block halo over the chunk
 };
 
 // Parameters that are constant over a step (passed by value).

@@ -869,7 +869,7 @@ __device__ bool ser_gradient(const DevField& F, double px, double py, double pz,
 // vol = min(VM, 4/3 pi r^3); stored as vmx = {x_b, vol}, vmv = {v_b, kind}
 // where kind 0 = none, 1 = tangent helper x-axis, 2 = helper y-axis.
 template <class R>
-__global__ void __launch_bounds__(kBlock, 4) k_vm_sample(
+__global__ void __launch_bounds__(kBlock) k_vm_sample(
     Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, const VMDesc* __restrict__ vms,
     int nvm, const Body* __restrict__ bodies, R4<R>* __restrict__ vmx, R4<R>* __restrict__ vmv,
     R* __restrict__ bW, R4<R>* __restrict__ bG, R4<R>* __restrict__ bGu, StepParams<R> P) {
@@ -1776,6 +1776,8 @@ __global__ void k_chunk_begin(Scalars* sc, double time) {
   sc->trouble = 0;
   sc->status_any = 0;
   sc->loop_sweeps = 0;
+  sc->chunk_max_nbrs = 0;
+  sc->chunk_max_halo = 0;
 }
 
 // Condition of the while-node that runs the Jacobi sweeps of one solve: go on
@@ -1793,6 +1795,8 @@ __global__ void k_loop_cond(cudaGraphConditionalHandle h, const Scalars* __restr
 __global__ void k_step_epilogue(Scalars* sc, int K, int hcap, int solver_loop) {
   unsigned int t = 0;
   if (sc->max_nbrs > K || sc->max_halo > hcap) t |= 1u;
+  sc->chunk_max_nbrs = max(sc->chunk_max_nbrs, sc->max_nbrs);
+  sc->chunk_max_halo = max(sc->chunk_max_halo, sc->max_halo);
   if (sc->n_below > 0) t |= 2u;
   if (solver_loop && !sc->converged) t |= 4u;
   sc->trouble |= t;

@@ -1142,18 +1142,7 @@ class System : public SystemBase {
       // Neighbor or halo capacity exceeded: grow it and redo the update on
       // the same (already integrated) state. Reaction forces gathered so far
       // are discarded first; they are rebuilt by the redo.
-      if (h_sc_->max_nbrs > K_) {
-        // grow with headroom: compressing scenes raise the count step after step
-        K_ = (int)round_up((size_t)h_sc_->max_nbrs * 5 / 4 + 8, 8);  // multiple of 4 (64-bit groups)
-        P_.K = K_;
-        nbr_.alloc((size_t)K_ * np_);
-      }
-      if (h_sc_->max_halo > hcap_) {
-        if (h_sc_->max_halo > 65535)
-          throw Error(SPH_ERR_CAPACITY, "a block's neighborhood holds more than 65535 particles");
-        hcap_ = (int)std::min<size_t>(65535, round_up((size_t)h_sc_->max_halo * 5 / 4, 256));
-        halo_idx_.alloc((size_t)blocks_for((long long)cap_) * (size_t)hcap_);
-      }
+      grow_capacity(h_sc_->max_nbrs, h_sc_->max_halo);
       zero_body_forces();
       finish_disable();
       update(2);
@@ -1193,6 +1182,27 @@ class System : public SystemBase {
     calc_acceleration();
     launch("avg_density", k_avg_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
            (const R4<R>*)vel_.p, partials_.p, P_);
+  }
+
+  // Grows the neighbor-list and halo capacities past the counts a step
+  // needed (with headroom: compressing scenes raise them step after step).
+  // Returns whether anything grew.
+  bool grow_capacity(int max_nbrs, int max_halo) {
+    bool grew = false;
+    if (max_nbrs > K_) {
+      K_ = (int)round_up((size_t)max_nbrs * 5 / 4 + 8, 8);  // multiple of 4 (64-bit groups)
+      P_.K = K_;
+      nbr_.alloc((size_t)K_ * np_);
+      grew = true;
+    }
+    if (max_halo > hcap_) {
+      if (max_halo > 65535)
+        throw Error(SPH_ERR_CAPACITY, "a block's neighborhood holds more than 65535 particles");
+      hcap_ = (int)std::min<size_t>(65535, round_up((size_t)max_halo * 5 / 4, 256));
+      halo_idx_.alloc((size_t)blocks_for((long long)cap_) * (size_t)hcap_);
+      grew = true;
+    }
+    return grew;
   }
 
   void zero_body_forces() {
@@ -1300,6 +1310,12 @@ class System : public SystemBase {
       *h_sc_ = chunk_start_sc_;
       ++graph_replays_;
       o.replayed = true;
+      if (s.trouble == 1u && grow_capacity(s.chunk_max_nbrs, s.chunk_max_halo)) {
+        // only the neighbor or halo capacity ran out: grow it past what the
+        // chunk needed and run the chunk again as graphs (recaptured)
+        chunk_begin(c);
+        return chunk_finish();
+      }
       o.status = step_plain(c);
       return o;
     }

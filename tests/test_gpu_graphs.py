@@ -129,3 +129,15 @@ def test_graph_chunk_with_disabled_particles_is_replayed(A):
     assert plain["n"] < pos.shape[0]
     _assert_same(plain, graph)
     assert graph["replays"] >= 1
+
+
+def test_graph_chunk_that_outgrows_the_neighbor_capacity_is_rerun(A):
+    """A soft SESPH dam break compresses, so its neighbor counts outgrow the
+    capacity sized at the first update: the chunk is rerun as graphs after
+    the capacity grows, and the results stay those of the per-step path."""
+    from sphgpu import scenes
+    sc = scenes.serving_dam_break(8000, "SESPH", stiffness=500.0, viscosity=0.01, rest_density=1000.0, seed=9)
+    plain = _run(A, sc, 150, 0)
+    graph = _run(A, sc, 150, 25)
+    _assert_same(plain, graph)
+    assert graph["replays"] >= 1
