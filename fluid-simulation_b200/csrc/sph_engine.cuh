@@ -48,6 +48,7 @@ struct Scalars {
   int iterations_eqs1;             // IISPHwOST first solve sweeps
   int max_bnbrs;                   // largest boundary-sample neighbor count seen
   int max_halo;                    // largest block halo (particles) seen
+  unsigned int vm_near;            // particles within the support radius of a volume map
   // graph-captured stepping (the host reads these once per chunk)
   double time_acc;                 // simulated time under CFL steps
   unsigned int trouble;            // bits: 1 neighbor overflow, 2 disabled particles, 4 unconverged

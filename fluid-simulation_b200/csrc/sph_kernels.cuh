@@ -175,6 +175,7 @@ __global__ void k_prologue(Scalars* sc, StepParams<R> P, int accumulate_time) {
   sc->max_nbrs = 0;
   sc->max_bnbrs = 0;
   sc->max_halo = 0;
+  sc->vm_near = 0;
   sc->iterations = 0;
   sc->iterations_eqs1 = 0;
   sc->converged = 0;
@@ -868,13 +869,52 @@ __device__ bool ser_gradient(const DevField& F, double px, double py, double pz,
 // One volume-map boundary sample per (particle, boundary): x_b = x - n d with
 // vol = min(VM, 4/3 pi r^3); stored as vmx = {x_b, vol}, vmv = {v_b, kind}
 // where kind 0 = none, 1 = tangent helper x-axis, 2 = helper y-axis.
+// Volume-map samples in two kernels: k_vm_near evaluates every particle's
+// signed distance (the cheap, light first test of find_boundary_samples) and
+// lists the particles within the support radius of some boundary, writing
+// the empty result for all others; k_vm_sample then does the full sampling
+// for the listed particles only.
 template <class R>
-__global__ void __launch_bounds__(kBlock) k_vm_sample(
-    Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, const VMDesc* __restrict__ vms,
-    int nvm, const Body* __restrict__ bodies, R4<R>* __restrict__ vmx, R4<R>* __restrict__ vmv,
-    R* __restrict__ bW, R4<R>* __restrict__ bG, R4<R>* __restrict__ bGu, StepParams<R> P) {
+__global__ void __launch_bounds__(kBlock) k_vm_near(
+    Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, const VMDesc* __restrict__ vms, int nvm,
+    const Body* __restrict__ bodies, uint32_t* __restrict__ near_list, R4<R>* __restrict__ vmx,
+    R4<R>* __restrict__ vmv, R* __restrict__ bW, R4<R>* __restrict__ bG, R4<R>* __restrict__ bGu,
+    StepParams<R> P) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= sc->n_active) return;
+  const R4<R> xr = pos[i];
+  const double p[3] = {(double)xr.x, (double)xr.y, (double)xr.z};
+  bool near = false;
+  for (int b = 0; b < nvm && !near; ++b) {
+    const VMDesc& D = vms[b];
+    double pl[3] = {p[0], p[1], p[2]};
+    if (D.body >= 0) body_world_to_local(bodies[D.body], p, pl);
+    double sd;
+    near = ser_function(D.sdf, pl[0], pl[1], pl[2], sd) && sd < P.range;
+  }
+  if (near) {
+    near_list[atomicAdd(&sc->vm_near, 1u)] = (uint32_t)i;
+    return;
+  }
+  for (int b = 0; b < nvm; ++b) {
+    const size_t o = (size_t)b * P.Np + i;
+    vmx[o] = R4<R>{R(0), R(0), R(0), R(0)};
+    vmv[o] = R4<R>{R(0), R(0), R(0), R(0)};
+  }
+  bW[i] = R(0);
+  bG[i] = R4<R>{R(0), R(0), R(0), R(0)};
+  bGu[i] = R4<R>{R(0), R(0), R(0), R(0)};
+}
+
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_vm_sample(
+    Scalars* __restrict__ sc, const uint32_t* __restrict__ near_list, const R4<R>* __restrict__ pos,
+    const VMDesc* __restrict__ vms, int nvm, const Body* __restrict__ bodies, R4<R>* __restrict__ vmx,
+    R4<R>* __restrict__ vmv, R* __restrict__ bW, R4<R>* __restrict__ bG, R4<R>* __restrict__ bGu,
+    StepParams<R> P) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (int)sc->vm_near) return;
+  const int i = (int)near_list[t];
   const R4<R> xr = pos[i];
   const double p[3] = {(double)xr.x, (double)xr.y, (double)xr.z};
   const double range = P.range;

@@ -578,7 +578,7 @@ class System : public SystemBase {
       b += d->bytes();
     for (const auto* d : {&press_, &s_, &aii_, &bW_, &rho_pred_}) b += d->bytes();
     b += nbr_.bytes();
-    for (const auto* d : {&ref_, &ref2_, &fid_, &fid2_, &key_, &slot_, &perm_, &halo_idx_, &halo_n_, &ncnt_,
+    for (const auto* d : {&ref_, &ref2_, &fid_, &fid2_, &key_, &slot_, &perm_, &halo_idx_, &halo_n_, &vm_near_, &ncnt_,
                           &count_, &start_,
                           &tile_sums_, &sbid_, &sbid2_, &sorig_, &sorig2_, &skey_, &sslot_, &sperm_, &scount_,
                           &sstart_, &snap_ref_, &snap_fid_})
@@ -654,6 +654,7 @@ class System : public SystemBase {
   std::vector<std::unique_ptr<FieldPair>> fields_;
   DBuf<VMDesc> vms_;
   DBuf<R4<R>> vmx_, vmv_;
+  DBuf<uint32_t> vm_near_;  // particles near a volume map this step
   // bounding box of the scene (cells chosen from it)
   struct BBox {
     double mn[3], mx[3];
@@ -1003,6 +1004,7 @@ class System : public SystemBase {
     copy_h2d(vms_.p, h.data(), (size_t)nvm);
     vmx_.alloc((size_t)nvm * np_);
     vmv_.alloc((size_t)nvm * np_);
+    vm_near_.alloc(std::max<size_t>(cap_, 1));
     vmv_.zero(stream_);
   }
 
@@ -1172,10 +1174,14 @@ class System : public SystemBase {
     if (boundary_kind_ == 1)
       launch("boundary_samples", k_sample_aggregate<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
              sample_grid(), bW_.p, bG_.p, bGu_.p, P_);
-    else if (boundary_kind_ == 2)
-      launch("boundary_samples", k_vm_sample<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
-             (const VMDesc*)vms_.p, (int)fields_.size(), (const Body*)bodies_d_.p, vmx_.p, vmv_.p, bW_.p,
-             bG_.p, bGu_.p, P_);
+    else if (boundary_kind_ == 2) {
+      launch("vm_near", k_vm_near<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)pos_.p,
+             (const VMDesc*)vms_.p, (int)fields_.size(), (const Body*)bodies_d_.p, vm_near_.p, vmx_.p, vmv_.p,
+             bW_.p, bG_.p, bGu_.p, P_);
+      launch("boundary_samples", k_vm_sample<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const uint32_t*)vm_near_.p,
+             (const R4<R>*)pos_.p, (const VMDesc*)vms_.p, (int)fields_.size(), (const Body*)bodies_d_.p, vmx_.p,
+             vmv_.p, bW_.p, bG_.p, bGu_.p, P_);
+    }
     launch_s("neighbors_density", k_neighbors_density<R>, dim3(nb), dim3(kBlock), kSearchSmem, d_sc_.p,
              (const R4<R>*)pos_.p, (const uint32_t*)start_.p, xv_.p, nbr_.p, ncnt_.p, halo_idx_.p, halo_n_.p,
              (const R*)bW_.p, boundary_kind_ ? 1 : 0, hcap_, P_);
