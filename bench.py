@@ -50,6 +50,7 @@ BYTES_PER_PARTICLE = {
     "accel_nonpressure": 60,     # R x,v,V,m, boundary samples             W a, v*
     "pressure_accel": 64,        # R x,V,m,p,a, boundary agg.              W a
     "neighbors_density": 32,     # R x, boundary agg.                      W V
+    "vm_near": 20,               # R x                                     W near list (wall particles)
     "boundary_samples": 28,      # R x                                     W samples
     "integrate_key": 60,         # R x,v,a                                 W x,v
     "sort": 84,                  # R x,key,idx; permute x,v,ids
@@ -155,7 +156,8 @@ def peaks():
 
 # ncu summaries of the dominant kernels (committed under profiles/): DRAM
 # read + write bytes of one launch of the bench workload.
-TRAFFIC_PROFILES = {"iisph_jacobi": "profiles/iisph_jacobi_1M_volume_map.md"}
+TRAFFIC_PROFILES = {"iisph_jacobi": "profiles/iisph_jacobi_1M_volume_map.md",
+                    "neighbors_density": "profiles/neighbors_density_1M_volume_map.md"}
 
 
 def profiled_traffic(kernel):
