@@ -3,16 +3,21 @@
 
 Workload (one "step" = one SPH time step, sim_lib sph/mod.rs:125-144, of the
 whole scene): a 100^3 lattice (spacing 0.01 m, +-1 % seeded jitter, rest
-density 1000) against the -x end of a 2 x 1 x 1 m box handled as a
-VolumeMapBoundary (fields at the reference's dx = 4 * spacing, built on the
-GPU before timing), IISPH with omega 0.5, target density error 0.1 %, at most
-100 sweeps per solve, CFL time step (0.4, dt <= 2e-3), viscosity 0.01, f32
-state. Inputs are synthetic and seeded.
+density 1000) at the -x end of a 2 x 1 x 1 m box, widened to 1.02 m so the
+block keeps 1.5 spacings from every wall, handled as a VolumeMapBoundary
+(fields at the reference's dx = 4 * spacing, built on the GPU before timing),
+IISPH with omega 0.5, target density error 0.1 %, at most 100 sweeps per
+solve, CFL time step (0.4, dt <= 2e-3), viscosity 0.01, f32 state. Inputs
+are synthetic and seeded.
 
 Arms:
   default          the CUDA engine through the C ABI; `value` is device time
                    (CUDA events on the engine's stream), `e2e` runs the same
                    steps through sph_step_host with host buffers in and out.
+                   The line's `serving` object is the scene sweep (256
+                   Poisson-arrival dam breaks of 5k-500k particles, 500
+                   steps each) served batched by the scene server and, for
+                   its first 64 requests, one at a time on the plain path.
   --impl reference the reference's CPU algorithm (the f64 C++ restatement in
                    oracle/, all host threads) on a bounded sample of the same
                    configuration (a 50^3 block), same metric.
@@ -72,8 +77,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--serving-requests", type=int, default=256,
                    help="scene-sweep requests served batched and one at a time (0: skip)")
-    p.add_argument("--serving-plain-requests", type=int, default=-1,
-                   help="requests of the one-at-a-time arm (-1: all)")
+    p.add_argument("--serving-plain-requests", type=int, default=64,
+                   help="requests of the one-at-a-time arm, the first ones of the sweep (-1: all)")
     p.add_argument("--serving-steps", type=int, default=500)
     return p.parse_args()
 
@@ -391,7 +396,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice + jitter)",
-            "config": {"workload": f"IISPH dam break, {args.n_side}^3 particles, 2x1x1 m VolumeMapBoundary box",
+            "config": {"workload": f"IISPH dam break, {args.n_side}^3 particles, 2 x 1.02 x 1.02 m VolumeMapBoundary box (1.5-spacing wall gap)",
                        "particles_per_gpu": args.n_side ** 3, "solver": "IISPH", "omega": 0.5,
                        "target_density_error_pct": 0.1, "max_solver_iterations": args.max_iters,
                        "cfl": 0.4, "max_dt": 2e-3, "precision": "f32 state, f64 reductions",
@@ -425,7 +430,7 @@ def reference_arm(args, ws, rank):
         "warmup": args.warmup, "ms_per_step": secs * 1000.0 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice + jitter)",
         "impl": "reference",
-        "config": {"workload": f"IISPH dam break, {args.n_side}^3 particles, 2x1x1 m VolumeMapBoundary box",
+        "config": {"workload": f"IISPH dam break, {args.n_side}^3 particles, 2 x 1.02 x 1.02 m VolumeMapBoundary box (1.5-spacing wall gap)",
                    "sample_particles": n_cpu, "max_solver_iterations": args.max_iters},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{done} timed steps of a {n_cpu}-particle ({args.cpu_sample_side}^3) block of "
