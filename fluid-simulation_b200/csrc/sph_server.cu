@@ -77,8 +77,8 @@ static size_t field_nodes(const sph_grid_desc& g) {
 static uint64_t estimate_bytes(const SceneJob& j) {
   const double w = j.cfg.precision == SPH_F64 ? 8.0 : 4.0;
   const int ps = j.cfg.pressure_solver;
-  const double K = std::max<double>(j.cfg.neighbor_capacity ? j.cfg.neighbor_capacity : 64, 64) * 1.5;
-  double per = 4 * w * 8 + 4 * 8 + w * 2 + 4 * K;      // state, sort, pressure/bW, neighbor lists
+  const double K = std::max<double>(j.cfg.neighbor_capacity ? j.cfg.neighbor_capacity : 128, 128) * 1.5;
+  double per = 4 * w * 8 + 4 * 8 + w * 2 + 2 * K + 4 * 8192.0 / 256;  // state, sort, p/bW, lists, halo table
   if (ps != SPH_SESPH) per += 4 * w;                    // predicted velocity
   if (ps == SPH_IISPH || ps == SPH_IISPH_W_OST) per += 2 * w + 4 * w;
   if (ps == SPH_SESPH_W_SPLITTING) per += w;

@@ -634,7 +634,7 @@ class System : public SystemBase {
   DBuf<R> press_, s_, aii_, bW_, rho_pred_;
   DBuf<uint32_t> ref_, ref2_, fid_, fid2_, key_, slot_, perm_, ncnt_, halo_idx_, halo_n_;
   DBuf<uint16_t> nbr_;
-  int hcap_ = 4096;   // halo table capacity per block (grows on overflow, at most 65535)
+  int hcap_ = 8192;   // halo table capacity per block (grows on overflow, at most 65535)
   int hs_ = sizeof(R) == 4 ? 1536 : 1024;  // halo records staged in shared memory per block
   DBuf<uint32_t> count_, start_, tile_sums_;
   DBuf<double> partials_, body_partials_, stage_x_, stage_v_;
@@ -761,7 +761,7 @@ class System : public SystemBase {
     }
     if (cfg_.pressure_solver == SPH_SESPH_W_SPLITTING) rho_pred_.alloc(c);
     if (cfg_.integration_scheme == SPH_TAKE_PREDICTED) { xint_.alloc(c); vint_.alloc(c); }
-    K_ = (int)round_up(cfg_.neighbor_capacity ? cfg_.neighbor_capacity : 64, 4);
+    K_ = (int)round_up(cfg_.neighbor_capacity ? cfg_.neighbor_capacity : 128, 4);
     nbr_.alloc((size_t)K_ * np_);
     halo_n_.alloc((size_t)blocks_for((long long)c));
     halo_idx_.alloc((size_t)blocks_for((long long)c) * (size_t)hcap_);
@@ -1196,7 +1196,7 @@ class System : public SystemBase {
   bool grow_capacity(int max_nbrs, int max_halo) {
     bool grew = false;
     if (max_nbrs > K_) {
-      K_ = (int)round_up((size_t)max_nbrs * 5 / 4 + 8, 8);  // multiple of 4 (64-bit groups)
+      K_ = (int)round_up((size_t)max_nbrs * 3 / 2 + 8, 8);  // multiple of 4 (64-bit groups)
       P_.K = K_;
       nbr_.alloc((size_t)K_ * np_);
       grew = true;
@@ -1204,7 +1204,7 @@ class System : public SystemBase {
     if (max_halo > hcap_) {
       if (max_halo > 65535)
         throw Error(SPH_ERR_CAPACITY, "a block's neighborhood holds more than 65535 particles");
-      hcap_ = (int)std::min<size_t>(65535, round_up((size_t)max_halo * 5 / 4, 256));
+      hcap_ = (int)std::min<size_t>(65535, round_up((size_t)max_halo * 3 / 2, 256));
       halo_idx_.alloc((size_t)blocks_for((long long)cap_) * (size_t)hcap_);
       grew = true;
     }
@@ -1730,7 +1730,7 @@ void sph_config_default(sph_config* c) {
   c->max_time_increment = 0.01;
   c->cfl_number = 0.4;
   c->max_solver_iterations = 0;
-  c->neighbor_capacity = 64;
+  c->neighbor_capacity = 128;
   c->device = 0;
 }
 

@@ -86,7 +86,8 @@ typedef struct sph_config {
   double gravity_center[3];                         /* radial gravity */
   uint32_t max_solver_iterations; /* 0 = unbounded like the reference; else a cap
                                      that ends the solve with SPH_NOT_CONVERGED */
-  uint32_t neighbor_capacity;     /* fluid neighbors stored per particle; 0 = 64 */
+  uint32_t neighbor_capacity;     /* fluid neighbors stored per particle (16-bit entries);
+                                     0 = 128; grows when a step needs more */
   int device;                     /* CUDA device ordinal */
 } sph_config;
 

@@ -137,7 +137,8 @@ def test_graph_chunk_that_outgrows_the_neighbor_capacity_is_rerun(A):
     the capacity grows, and the results stay those of the per-step path."""
     from sphgpu import scenes
     sc = scenes.serving_dam_break(8000, "SESPH", stiffness=500.0, viscosity=0.01, rest_density=1000.0, seed=9)
-    plain = _run(A, sc, 150, 0)
-    graph = _run(A, sc, 150, 25)
+    # start from a small capacity so that it is outgrown during the run
+    plain = _run(A, sc, 150, 0, extra={"neighbor_capacity": 8})
+    graph = _run(A, sc, 150, 25, extra={"neighbor_capacity": 8})
     _assert_same(plain, graph)
     assert graph["replays"] >= 1
