@@ -374,6 +374,7 @@ __device__ __forceinline__ size_t nbr_slot(int i, int k, int K) {
 }
 
 constexpr int kHaloKeys = 8192;            // >= 27 * kBlock stencil keys, a power of two
+static_assert(kHaloKeys >= 27 * kBlock, "the sort buffer must hold the stencil keys of a full block");
 constexpr uint32_t kNoKey = 0xffffffffu;
 constexpr size_t kSearchSmem = kHaloKeys * (sizeof(uint32_t) + sizeof(uint16_t));
 

@@ -122,3 +122,19 @@ def test_destroy_with_queued_and_running_scenes_returns(A):
     t0 = time.time()
     srv.close()
     assert time.time() - t0 < 60
+
+
+def test_a_scene_that_fails_to_build_reports_its_error(A):
+    """IISPHwOST only pairs with TakePredicted (sph/setup/mod.rs:229-231): the
+    request is accepted, its build fails on the setup thread, and its result
+    carries the error status while other scenes still complete."""
+    from sphgpu import scenes
+    from sphgpu.server import SceneServer
+    bad = scenes.serving_dam_break(5000, "IISPH", seed=11)
+    bad.procedures = dict(bad.procedures, pressure_solver="IISPHwOST")  # EulerCromer stays
+    good = scenes.serving_dam_break(5000, "SESPH", seed=12)
+    with SceneServer() as srv:
+        tb, tg = srv.submit(bad, 10), srv.submit(good, 10)
+        rb, rg = srv.wait(tb, 120), srv.wait(tg, 120)
+    assert rb["status"] == A.SPH_ERR_INVALID and rb["steps"] == 0
+    assert rg["status"] == A.SPH_OK and rg["steps"] == 10
