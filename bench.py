@@ -83,11 +83,17 @@ def parse():
     return p.parse_args()
 
 
-def scene(n_side, max_iters):
+def scene(n_side, max_iters, box=(2.0, 1.0, 1.0)):
     from sphgpu import scenes
-    sc = scenes.dam_break_iisph_box(n_side=n_side)
+    sc = scenes.dam_break_iisph_box(n_side=n_side, box=box)
     sc.parameters = dict(sc.parameters, max_solver_iterations=max_iters)
     return sc
+
+
+def workload_box(args):
+    """Container of the benchmark scene (widened for the wall gap); the CPU
+    samples run in the same container with the same fields."""
+    return scene(args.n_side, args.max_iters).container
 
 
 class ClockSampler:
@@ -175,7 +181,7 @@ def profiled_traffic(kernel):
     return None
 
 
-def run_cpu(n_side, steps, warmup, max_iters, fields, min_seconds=0.0):
+def run_cpu(n_side, steps, warmup, max_iters, fields, min_seconds=0.0, box=(2.0, 1.0, 1.0)):
     """The reference's CPU algorithm (oracle restatement, all host threads) on
     a bounded n_side^3 sample of the workload: `steps` timed steps, more while
     less than `min_seconds` of CPU work has been timed (at most 4x `steps`).
@@ -183,7 +189,7 @@ def run_cpu(n_side, steps, warmup, max_iters, fields, min_seconds=0.0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from sphgpu.system import PROCEDURES
-    sc = scene(n_side, max_iters)
+    sc = scene(n_side, max_iters, box)
     cfg = dict(sc.parameters)
     cfg.update(integration_scheme=PROCEDURES["integration_scheme"][sc.procedures["integration_scheme"]],
                pressure_solver=PROCEDURES["pressure_solver"][sc.procedures["pressure_solver"]],
@@ -302,8 +308,11 @@ def main():
     stream = torch.cuda.ExternalStream(sysm.stream(), device=local)
     for _ in range(args.warmup):
         sysm.step_forward_in_time(1)
+    # Copies of the warmed-up state: the kernel shares and the end-to-end
+    # number run exactly the steps the device-timed region runs.
+    sys_prof = sysm.clone()
+    sys_e2e = None if args.no_e2e else sysm.clone()
     launches0 = sysm.launch_count()
-    sysm.set_profiling(True)
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
@@ -322,12 +331,16 @@ def main():
     clk = clocks.stop()
     ms = ev0.elapsed_time(ev1)
     launches = sysm.launch_count() - launches0
+    # per-kernel CUDA-event times of the same steps on the first copy
+    sys_prof.set_profiling(True)
+    for _ in range(args.steps):
+        sys_prof.step_forward_in_time(1)
     kernel_times = {}
     for name in BYTES_PER_PARTICLE:
-        kt = sysm.kernel_time(name)
+        kt = sys_prof.kernel_time(name)
         if kt:
             kernel_times[name] = kt
-    sysm.set_profiling(False)
+    sys_prof.close()
     # whole-job aggregate: sum of updates over ranks / max time over ranks
     from sphgpu.replicas import aggregate
     ms_max, total_updates = aggregate(ms, updates, device="cuda")
@@ -335,28 +348,30 @@ def main():
 
     # e2e: the plugin call with host buffers (reference order), copies inside
     e2e = None
-    if not args.no_e2e:
-        n = sysm.n
+    if sys_e2e is not None:
+        n = sys_e2e.n
+        e_stream = torch.cuda.ExternalStream(sys_e2e.stream(), device=local)
         xin = torch.empty((n, 3), dtype=torch.float64).pin_memory()
         vin = torch.empty((n, 3), dtype=torch.float64).pin_memory()
         xout = torch.empty((n, 3), dtype=torch.float64).pin_memory()
         vout = torch.empty((n, 3), dtype=torch.float64).pin_memory()
-        xin.numpy()[:] = sysm.download(capi.FIELD_POSITION)
-        vin.numpy()[:] = sysm.download(capi.FIELD_VELOCITY)
+        xin.numpy()[:] = sys_e2e.download(capi.FIELD_POSITION)
+        vin.numpy()[:] = sys_e2e.download(capi.FIELD_VELOCITY)
         torch.cuda.synchronize()
         if ws > 1:
             dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        e0.record(e_stream)
         e_updates = 0
         for _ in range(args.steps):
-            sysm.step_host(1, xin, vin, xout, vout)
-            e_updates += sysm.n
+            sys_e2e.step_host(1, xin, vin, xout, vout)
+            e_updates += sys_e2e.n
             xin, xout = xout, xin
             vin, vout = vout, vin
-        e1.record(stream)
+        e1.record(e_stream)
         torch.cuda.synchronize()
         ems = e0.elapsed_time(e1)
+        sys_e2e.close()
         ems, e_updates = aggregate(ems, e_updates, device="cuda")
         e2e = {"value": e_updates / (ems / 1000.0), "unit": UNIT,
                "h2d_bytes_per_step": 2 * 3 * 8 * n, "d2h_bytes_per_step": 2 * 3 * 8 * n}
@@ -381,7 +396,7 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         v, secs, cores, n_cpu, done, sweeps = run_cpu(args.cpu_sample_side, args.cpu_steps, 1, args.max_iters,
-                                                      fields, args.cpu_seconds)
+                                                      fields, args.cpu_seconds, box=sc.container)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{done} steps (after 1 warm-up step) of a {n_cpu}-particle ({args.cpu_sample_side}^3) "
                          f"block of the same configuration, {sweeps:.0f} IISPH sweeps per step, f64 C++ "
@@ -419,12 +434,13 @@ def reference_arm(args, ws, rank):
     # is available (bounded: coarse box fields, once)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    sc = scene(args.cpu_sample_side, args.max_iters)
+    box = workload_box(args)
+    sc = scene(args.cpu_sample_side, args.max_iters, box)
     verts, faces = sc.mesh
     sp = sc.parameters["rest_density_grid_spacing"]
     sdf, vm = O.build_fields(verts, faces, 4 * sp, sc.parameters["kernel_support_radius"], 30)
     v, secs, cores, n_cpu, done, sweeps = run_cpu(args.cpu_sample_side, args.steps, args.warmup, args.max_iters,
-                                                  (sdf, vm))
+                                                  (sdf, vm), box=box)
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1000.0 / args.steps, "higher_is_better": True,

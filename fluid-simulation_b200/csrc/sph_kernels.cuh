@@ -1105,9 +1105,25 @@ __device__ __forceinline__ void body_accum_flush(double* sh, int nbodies, double
 // records are loaded, then consumed, so NB loads are in flight per thread.
 // Slots past the count read position 0, which every non-empty halo has.
 // ---------------------------------------------------------------------------
+// The first batch of a particle's list, requested ahead of use (a kernel can
+// issue it before it waits for its halo staging).
+template <int NB>
+struct ListHead {
+  uint2 g[NB / 4];
+};
+template <int NB>
+__device__ __forceinline__ ListHead<NB> list_head(const uint16_t* __restrict__ nbr, int K, int i, int cnt) {
+  ListHead<NB> h;
+  const uint2* base = reinterpret_cast<const uint2*>(nbr) + nbr_slot(i, 0, K) / 4;
+  const int ngroups = (cnt + 3) >> 2;
+#pragma unroll
+  for (int g = 0; g < NB / 4; ++g) h.g[g] = g < ngroups ? __ldcs(base + (size_t)g * 32) : make_uint2(0u, 0u);
+  return h;
+}
+
 template <int NB, class Load, class Use>
-__device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ nbr, int K, int i,
-                                                  int cnt, Load&& load, Use&& use) {
+__device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ nbr, int K, int i, int cnt,
+                                                  const ListHead<NB>& head, Load&& load, Use&& use) {
   static_assert(NB % 4 == 0, "neighbors are read in groups of four");
   // group g of this lane sits 32 uint2 after group g-1; the next batch's
   // groups are requested before the current batch is consumed
@@ -1115,7 +1131,7 @@ __device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ n
   const int ngroups = (cnt + 3) >> 2;
   uint2 cur[NB / 4];
 #pragma unroll
-  for (int g = 0; g < NB / 4; ++g) cur[g] = g < ngroups ? __ldcs(base + (size_t)g * 32) : make_uint2(0u, 0u);
+  for (int g = 0; g < NB / 4; ++g) cur[g] = head.g[g];
   for (int k0 = 0; k0 < cnt; k0 += NB) {
     uint2 nxt[NB / 4];
 #pragma unroll
@@ -1141,6 +1157,11 @@ __device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ n
 #pragma unroll
     for (int g = 0; g < NB / 4; ++g) cur[g] = nxt[g];
   }
+}
+template <int NB, class Load, class Use>
+__device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ nbr, int K, int i, int cnt,
+                                                  Load&& load, Use&& use) {
+  for_each_neighbor<NB>(nbr, K, i, cnt, list_head<NB>(nbr, K, i, cnt), load, use);
 }
 
 // Shared-memory layout of staged halo records: arrays of R4 then arrays of R,
@@ -1297,6 +1318,20 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
   const bool bodies = mirror && B.any_dynamic != 0;
   if (bodies) body_accum_init(sh_body, B.nbodies);
   const HaloView H = halo_view(N);
+  // this particle's own data and first list batch travel while the halo stages
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < sc->n_active;
+  int cnt = 0;
+  ListHead<NB> head{};
+  R4<R> xi{};
+  R mi = 1, pi = 0;
+  if (act) {
+    cnt = min((int)N.ncnt[i], N.K);
+    head = list_head<NB>(N.nbr, N.K, i, cnt);
+    xi = xv[i];
+    mi = vel[i].w;
+    pi = press[i];
+  }
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
   R* s_p = staged_scalar<R>(dsm, N.hs, 1, 0);
   if (H.staged)
@@ -1305,14 +1340,11 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
       async_copy(&s_p[l], &press[g]);
     });
   stage_done();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < sc->n_active) {
-    const R4<R> xi = xv[i];
-    const R Vi = xi.w, mi = vel[i].w, pi = press[i];
+  if (act) {
+    const R Vi = xi.w;
     R px = 0, py = 0, pz = 0;
-    const int cnt = min((int)N.ncnt[i], N.K);
     for_each_neighbor<NB>(
-        N.nbr, N.K, i, cnt,
+        N.nbr, N.K, i, cnt, head,
         [&](uint32_t l) {
           if (H.staged) return XP<R>{s_x[l], s_p[l]};
           const uint32_t g = H.idx[l];
@@ -1436,6 +1468,24 @@ __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
   __shared__ double sh[32];
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
+  // this particle's own data and first list batch travel while the halo stages
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = sc->n_active;
+  const bool act = i < n;
+  int cnt = 0;
+  ListHead<NB> head{};
+  R4<R> xi{}, ai{}, bg{};
+  R aii = 0, s = 0, p0 = 0;
+  if (act) {
+    cnt = min((int)N.ncnt[i], N.K);
+    head = list_head<NB>(N.nbr, N.K, i, cnt);
+    xi = xv[i];
+    ai = accp[i];
+    aii = aii_in[i];
+    s = s_in[i];
+    p0 = press[i];
+    if (B.kind != 0) bg = B.bG[i];
+  }
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
   R4<R>* s_a = staged_vec<R>(dsm, N.hs, 1);
   if (H.staged)
@@ -1444,17 +1494,12 @@ __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
       async_copy(&s_a[l], &accp[g]);
     });
   stage_done();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = sc->n_active;
   double e = 0.0;
-  if (i < n) {
+  if (act) {
     const R dt = (R)sc->dt;
-    const R4<R> xi = xv[i];
-    const R4<R> ai = accp[i];
     R sum = 0;
-    const int cnt = min((int)N.ncnt[i], N.K);
     for_each_neighbor<NB>(
-        N.nbr, N.K, i, cnt,
+        N.nbr, N.K, i, cnt, head,
         [&](uint32_t l) {
           if (H.staged) return XV<R>{s_x[l], s_a[l]};
           const uint32_t g = H.idx[l];
@@ -1465,13 +1510,9 @@ __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
           const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
           sum += d.x.w * f * ((ai.x - d.v.x) * rx + (ai.y - d.v.y) * ry + (ai.z - d.v.z) * rz);
         });
-    if (B.kind != 0) {
-      const R4<R> g = B.bG[i];
-      sum += ai.x * g.x + ai.y * g.y + ai.z * g.z;
-    }
+    if (B.kind != 0) sum += ai.x * bg.x + ai.y * bg.y + ai.z * bg.z;
     const R A = dt * dt * sum;
-    const R aii = aii_in[i], s = s_in[i];
-    if (aii < -P.min_diag) press[i] = fmax(press[i] + P.omega * (s - A) / aii, R(0));
+    if (aii < -P.min_diag) press[i] = fmax(p0 + P.omega * (s - A) / aii, R(0));
     if (s < R(0)) e = fabs((double)A - (double)s);
   }
   const double bs = block_sum(e, sh);

@@ -124,6 +124,7 @@ class Scene:
     volume_maps: list = field(default_factory=list)         # [(sdf, vm, RigidInit|None)]
     mesh: tuple | None = None                               # (verts, faces) of the container
     description: str = ""
+    container: tuple | None = None                          # box extents of a box container
 
 
 def dam_break_sesph_8k(jitter_seed=0, n_side=20):
@@ -174,7 +175,7 @@ def dam_break_iisph_box(n_side=100, spacing=0.01, jitter_seed=0, box=(2.0, 1.0, 
                     "relaxation_factor": 0.5, "min_diagonal_element": 1e-10,
                     "max_time_increment": 2e-3, "cfl_number": 0.4},
         cfl_time_step=True, position=pos, mass=np.full(pos.shape[0], 1000.0 * h ** 3),
-        mesh=(verts, CUBE_FACES_INWARD),
+        mesh=(verts, CUBE_FACES_INWARD), container=box,
         description=f"IISPH dam break {pos.shape[0]} particles in a {box} box volume map")
 
 
