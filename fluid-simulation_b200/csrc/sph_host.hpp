@@ -53,6 +53,7 @@ class SystemBase {
   virtual void fluid_ids(uint32_t* out) = 0;
   virtual void fluid_pos(float* out) = 0;
   virtual void quantity(int q, float* out) = 0;
+  virtual void quantity_at(int q, size_t n, const float* pos, float* out) = 0;
   virtual int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
   virtual int boundary_neighbors(int bi, uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
   virtual void boundary_volumes(int bi, double* out) = 0;

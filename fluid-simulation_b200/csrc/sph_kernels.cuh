@@ -20,6 +20,7 @@
 //   k_iisph_*            pressure_solver/iisph.rs:117-560,
 //                        iisph_optimized_source_term.rs:53-217
 //   k_body_*             boundary_handling/rigid_body_motion.rs:135-201
+//   k_quantity_at        sph/mod.rs:241-341, sph/quantities.rs:14-330
 #pragma once
 
 #include <cfloat>
@@ -907,6 +908,37 @@ __global__ void __launch_bounds__(kBlock) k_vm_near(
   bGu[i] = R4<R>{R(0), R(0), R(0), R(0)};
 }
 
+// Normal-mode sample of volume map D for the world-frame point p
+// (volume_map_boundary.rs:1287-1330): the signed distance (in the body frame
+// for a dynamic map) must be below the search range, the gradient norm inside
+// (0.5, 2) and the volume-map value positive (then clamped to the volume of
+// the support ball); the sample sits at max(sd + spacing/4, spacing) against
+// the normalized gradient, moving with the body's velocity there. Returns
+// false, leaving the outputs untouched, when the point has no sample.
+__device__ __forceinline__ bool vm_normal_sample(const VMDesc& D, const Body* body, const double p[3],
+                                                 double range, double ball, double spacing,
+                                                 double xb[3], double vb[3], double& vol) {
+  double pl[3] = {p[0], p[1], p[2]};
+  if (body) body_world_to_local(*body, p, pl);
+  double sd;
+  if (!ser_function(D.sdf, pl[0], pl[1], pl[2], sd) || !(sd < range)) return false;
+  double g[3];
+  if (!ser_gradient(D.sdf, pl[0], pl[1], pl[2], g)) return false;
+  if (body) {
+    double gw[3];
+    qrot(body->q, g, gw);
+    g[0] = gw[0]; g[1] = gw[1]; g[2] = gw[2];
+  }
+  const double gn = __dsqrt_rn(add_(add_(mul_(g[0], g[0]), mul_(g[1], g[1])), mul_(g[2], g[2])));
+  double vm;
+  if (!(gn > 0.5 && gn < 2.0) || !ser_function(D.vm, pl[0], pl[1], pl[2], vm) || !(vm > 0.0)) return false;
+  vol = vm < ball ? vm : ball;
+  const double d = fmax(add_(sd, mul_(0.25, spacing)), spacing);
+  for (int c = 0; c < 3; ++c) xb[c] = sub_(p[c], mul_(div_(g[c], gn), d));
+  if (body) body_velocity_at(*body, xb, vb);
+  return true;
+}
+
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_vm_sample(
     Scalars* __restrict__ sc, const uint32_t* __restrict__ near_list, const R4<R>* __restrict__ pos,
@@ -924,46 +956,27 @@ __global__ void __launch_bounds__(kBlock) k_vm_sample(
   for (int b = 0; b < nvm; ++b) {
     const VMDesc& D = vms[b];
     const Body* body = D.body >= 0 ? &bodies[D.body] : nullptr;
-    double pl[3] = {p[0], p[1], p[2]};
-    if (body) body_world_to_local(*body, p, pl);
     int kind = 0;
     double xb[3] = {0, 0, 0}, vb[3] = {0, 0, 0}, vol = 0;
-    double sd;
-    if (ser_function(D.sdf, pl[0], pl[1], pl[2], sd) && sd < range) {
-      double g[3];
-      if (ser_gradient(D.sdf, pl[0], pl[1], pl[2], g)) {
-        if (body) {
-          double gw[3];
-          qrot(body->q, g, gw);
-          g[0] = gw[0]; g[1] = gw[1]; g[2] = gw[2];
-        }
-        const double gn = __dsqrt_rn(add_(add_(mul_(g[0], g[0]), mul_(g[1], g[1])), mul_(g[2], g[2])));
-        double vm;
-        if (gn > 0.5 && gn < 2.0 && ser_function(D.vm, pl[0], pl[1], pl[2], vm) && vm > 0.0) {
-          vol = vm < ball ? vm : ball;
-          const double d = fmax(add_(sd, mul_(0.25, P.spacing)), P.spacing);
-          for (int c = 0; c < 3; ++c) xb[c] = sub_(p[c], mul_(div_(g[c], gn), d));
-          if (body) body_velocity_at(*body, xb, vb);
-          const double u[3] = {xb[0] - p[0], xb[1] - p[1], xb[2] - p[2]};
-          const double un = sqrt((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]);
-          kind = fabs(u[0] / un) > 0.9 ? 2 : 1;
-          // aggregates in f64 from the exact sample position
-          const double rx = p[0] - xb[0], ry = p[1] - xb[1], rz = p[2] - xb[2];
-          const double r2 = (rx * rx + ry * ry) + rz * rz;
-          const double rn = sqrt(r2), q = rn / range;
-          const double a1 = q < 1.0 ? 1.0 - q : 0.0, a2 = q < 0.5 ? 0.5 - q : 0.0;
-          const double alpha = 16.0 / 3.14159265358979323846;
-          const double kw = alpha / (range * range * range) * (a1 * a1 * a1 - 4.0 * (a2 * a2 * a2));
-          const double f = rn > 0.0 ? alpha / (range * range * range * range) *
-                                          (-3.0 * a1 * a1 + 12.0 * a2 * a2) / rn
-                                    : 0.0;
-          w += (R)(vol * kw);
-          const double vf = vol * f;
-          gx += (R)(vf * rx); gy += (R)(vf * ry); gz += (R)(vf * rz);
-          gv += (R)(vf * (vb[0] * rx + vb[1] * ry + vb[2] * rz));
-          ux += (R)(f * rx); uy += (R)(f * ry); uz += (R)(f * rz);
-        }
-      }
+    if (vm_normal_sample(D, body, p, range, ball, P.spacing, xb, vb, vol)) {
+      const double u[3] = {xb[0] - p[0], xb[1] - p[1], xb[2] - p[2]};
+      const double un = sqrt((u[0] * u[0] + u[1] * u[1]) + u[2] * u[2]);
+      kind = fabs(u[0] / un) > 0.9 ? 2 : 1;
+      // aggregates in f64 from the exact sample position
+      const double rx = p[0] - xb[0], ry = p[1] - xb[1], rz = p[2] - xb[2];
+      const double r2 = (rx * rx + ry * ry) + rz * rz;
+      const double rn = sqrt(r2), q = rn / range;
+      const double a1 = q < 1.0 ? 1.0 - q : 0.0, a2 = q < 0.5 ? 0.5 - q : 0.0;
+      const double alpha = 16.0 / 3.14159265358979323846;
+      const double kw = alpha / (range * range * range) * (a1 * a1 * a1 - 4.0 * (a2 * a2 * a2));
+      const double f = rn > 0.0 ? alpha / (range * range * range * range) *
+                                      (-3.0 * a1 * a1 + 12.0 * a2 * a2) / rn
+                                : 0.0;
+      w += (R)(vol * kw);
+      const double vf = vol * f;
+      gx += (R)(vf * rx); gy += (R)(vf * ry); gz += (R)(vf * rz);
+      gv += (R)(vf * (vb[0] * rx + vb[1] * ry + vb[2] * rz));
+      ux += (R)(f * rx); uy += (R)(f * ry); uz += (R)(f * rz);
     }
     const size_t o = (size_t)b * P.Np + i;
     vmx[o] = R4<R>{(R)xb[0], (R)xb[1], (R)xb[2], (R)vol};
@@ -972,6 +985,102 @@ __global__ void __launch_bounds__(kBlock) k_vm_sample(
   bW[i] = w;
   bG[i] = R4<R>{gx, gy, gz, gv};
   bGu[i] = R4<R>{ux, uy, uz, R(0)};
+}
+
+// ScalarQuantity at evaluation positions (sph/mod.rs:241-341 with the sums
+// of quantities.rs:14-330), for sensor planes: one thread per position walks
+// the 27 buckets of the fluid grid of the last update (sorted positions and
+// volumes `xv`, velocities and masses `vel`, pressures), keeps the
+// reference's exact neighbor predicate and sums in f64 whatever the state
+// precision. Speed and volume also take the position's boundary samples
+// (RequestMode::Normal): the sorted sample grid, or one sample per volume
+// map. Quantities: 0 speed |sum v V W|, 1 volume V0 / sum V0 W, 2 density
+// sum m W, 3 density error 100 sum_{m < V0} (V0/m - 1) m W (the reference
+// passes the masses where the sum takes volumes), 4 pressure sum p V W,
+// 5 kinetic energy sum m |v|^2 V W / 2. The result is cast to f32.
+template <class R>
+__global__ void __launch_bounds__(kBlock) k_quantity_at(
+    int quantity, int n_eval, const float* __restrict__ eval, float* __restrict__ out,
+    const uint32_t* __restrict__ start, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
+    const R* __restrict__ press, SampleGrid<R> G, const VMDesc* __restrict__ vms, int nvm,
+    const Body* __restrict__ bodies, KernelConst<double> kd, double V0, StepParams<R> P) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_eval) return;
+  const double p[3] = {(double)eval[3 * t], (double)eval[3 * t + 1], (double)eval[3 * t + 2]};
+  const double h = P.range;
+  const int cx = cell_coord(p[0], h), cy = cell_coord(p[1], h), cz = cell_coord(p[2], h);
+  double s = 0, sx = 0, sy = 0, sz = 0;
+  if (start) {
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const uint32_t k = morton_key(cx + dx, cy + dy, cz + dz, P.mask);
+          const uint32_t e = start[k + 1];
+          for (uint32_t j = start[k]; j < e; ++j) {
+            const R4<R> xj = xv[j];
+            const double qx = (double)xj.x, qy = (double)xj.y, qz = (double)xj.z;
+            if (!in_range_exact(p[0], p[1], p[2], qx, qy, qz, h)) continue;
+            const double rx = p[0] - qx, ry = p[1] - qy, rz = p[2] - qz;
+            const double w = kernel_w_r2<double>((rx * rx + ry * ry) + rz * rz, kd);
+            const double V = (double)xj.w;
+            if (quantity == 1) { s += V0 * w; continue; }
+            const R4<R> vj = vel[j];
+            const double vx = (double)vj.x, vy = (double)vj.y, vz = (double)vj.z, m = (double)vj.w;
+            switch (quantity) {
+              case 0: sx += vx * V * w; sy += vy * V * w; sz += vz * V * w; break;
+              case 2: s += m * w; break;
+              case 3: if (m < V0) s += (V0 / m - 1.0) * m * w; break;
+              case 4: s += (double)press[j] * V * w; break;
+              default: s += 0.5 * m * ((vx * vx + vy * vy) + vz * vz) * V * w; break;
+            }
+          }
+        }
+  }
+  if (quantity <= 1) {
+    if (G.start) {
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            const uint32_t k = morton_key(cx + dx, cy + dy, cz + dz, G.mask);
+            const uint32_t e = G.start[k + 1];
+            for (uint32_t j = G.start[k]; j < e; ++j) {
+              const R4<R> xs = G.xb[j];
+              const double qx = (double)xs.x, qy = (double)xs.y, qz = (double)xs.z;
+              if (!in_range_exact(p[0], p[1], p[2], qx, qy, qz, h)) continue;
+              const double rx = p[0] - qx, ry = p[1] - qy, rz = p[2] - qz;
+              const double vw = (double)xs.w * kernel_w_r2<double>((rx * rx + ry * ry) + rz * rz, kd);
+              if (quantity == 1) {
+                s += vw;
+              } else {
+                const R4<R> vs = G.vb[j];
+                sx += (double)vs.x * vw; sy += (double)vs.y * vw; sz += (double)vs.z * vw;
+              }
+            }
+          }
+    }
+    const double ball = 4.0 / 3.0 * 3.14159265358979323846 * (h * h * h);
+    for (int b = 0; b < nvm; ++b) {
+      const VMDesc& D = vms[b];
+      double xb[3] = {0, 0, 0}, vb[3] = {0, 0, 0}, vol = 0;
+      if (!vm_normal_sample(D, D.body >= 0 ? &bodies[D.body] : nullptr, p, h, ball, P.spacing, xb, vb, vol))
+        continue;
+      const double rx = p[0] - xb[0], ry = p[1] - xb[1], rz = p[2] - xb[2];
+      const double vw = vol * kernel_w_r2<double>((rx * rx + ry * ry) + rz * rz, kd);
+      if (quantity == 1) {
+        s += vw;
+      } else {
+        sx += vb[0] * vw; sy += vb[1] * vw; sz += vb[2] * vw;
+      }
+    }
+  }
+  double val;
+  switch (quantity) {
+    case 0: val = sqrt((sx * sx + sy * sy) + sz * sz); break;
+    case 1: val = V0 / s; break;
+    case 3: val = 100.0 * s; break;
+    default: val = s; break;
+  }
+  out[t] = (float)val;
 }
 
 // ---------------------------------------------------------------------------

@@ -449,6 +449,31 @@ class System : public SystemBase {
     }
   }
 
+  // sph/mod.rs:241-341: quantity at n host positions (3n floats) into n
+  // floats, from the state of the last update; the system's state is not
+  // changed.
+  void quantity_at(int q, size_t n, const float* pos, float* out) override {
+    if (q < SPH_Q_SPEED || q > SPH_Q_KINETIC_ENERGY) throw Error(SPH_ERR_INVALID, "unknown quantity");
+    if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
+    if (n == 0) return;
+    if (n > (size_t)INT32_MAX / 3) throw Error(SPH_ERR_CAPACITY, "too many evaluation positions");
+    if (eval_pos_.n < 3 * n) eval_pos_.alloc(3 * n);
+    if (eval_out_.n < n) eval_out_.alloc(n);
+    cuda_check(cudaMemcpyAsync(eval_pos_.p, pos, 3 * n * sizeof(float), cudaMemcpyHostToDevice, stream_),
+               "cudaMemcpyAsync");
+    const double h = cfg_.kernel_support_radius, sp = cfg_.rest_density_grid_spacing;
+    SampleGrid<R> G = sample_grid();
+    if (boundary_kind_ != 1 || ns_ == 0) G.start = nullptr;
+    const int nvm = boundary_kind_ == 2 ? (int)fields_.size() : 0;
+    launch("quantity_at", k_quantity_at<R>, dim3(blocks_for((long long)n)), dim3(kBlock), q, (int)n,
+           (const float*)eval_pos_.p, eval_out_.p, n_ ? (const uint32_t*)start_.p : (const uint32_t*)nullptr,
+           (const R4<R>*)xv_.p, (const R4<R>*)vel_.p, (const R*)press_.p, G, (const VMDesc*)vms_.p, nvm,
+           (const Body*)bodies_d_.p, make_kernel_const<double>(h), sp * sp * sp, P_);
+    cuda_check(cudaMemcpyAsync(out, eval_out_.p, n * sizeof(float), cudaMemcpyDeviceToHost, stream_),
+               "cudaMemcpyAsync");
+    cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
+  }
+
   int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) override {
     std::vector<uint32_t> ref = fetch(ref_.p, n_), cnt = fetch(ncnt_.p, n_);
     std::vector<uint16_t> nb = fetch(nbr_.p, (size_t)K_ * np_);
@@ -584,6 +609,7 @@ class System : public SystemBase {
                           &sstart_, &snap_ref_, &snap_fid_})
       b += d->bytes();
     b += partials_.bytes() + body_partials_.bytes() + stage_x_.bytes() + stage_v_.bytes();
+    b += eval_pos_.bytes() + eval_out_.bytes();
     b += bodies_d_.bytes() + snap_bodies_.bytes() + snap_sc_.bytes() + ns_d_.bytes() + vms_.bytes();
     for (const auto& f : fields_) b += f->sdf.bytes() + f->vm.bytes();
     return b;
@@ -655,6 +681,7 @@ class System : public SystemBase {
   DBuf<VMDesc> vms_;
   DBuf<R4<R>> vmx_, vmv_;
   DBuf<uint32_t> vm_near_;  // particles near a volume map this step
+  DBuf<float> eval_pos_, eval_out_;  // quantity evaluation positions and values
   // bounding box of the scene (cells chosen from it)
   struct BBox {
     double mn[3], mx[3];
@@ -1905,6 +1932,14 @@ int sph_get_quantity_of_fluid_samples(sph_system_t* h, int q, float* out) {
     if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
     set_device(h);
     h->impl->quantity(q, out);
+  });
+}
+int sph_get_quantity_at_positions(sph_system_t* h, int q, size_t n, const float* positions, float* out) {
+  return guarded([&] {
+    if (!h || (n && (!positions || !out))) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->quantity_at(q, n, positions, out);
   });
 }
 int sph_download(sph_system_t* h, int field, double* out) {

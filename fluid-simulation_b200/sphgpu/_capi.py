@@ -161,6 +161,7 @@ SIGNATURES = {
     "sph_get_fluid_ids": (C.c_int, [_vp, _u32p]),
     "sph_get_fluid_pos": (C.c_int, [_vp, _fp]),
     "sph_get_quantity_of_fluid_samples": (C.c_int, [_vp, C.c_int, _fp]),
+    "sph_get_quantity_at_positions": (C.c_int, [_vp, C.c_int, _sz, _fp, _fp]),
     "sph_download": (C.c_int, [_vp, C.c_int, _dp]),
     "sph_get_fluid_neighbors": (C.c_int, [_vp, _vp, _vp, _sz, C.POINTER(_sz)]),
     "sph_get_boundary_neighbors": (C.c_int, [_vp, C.c_int, _vp, _vp, _sz, C.POINTER(_sz)]),

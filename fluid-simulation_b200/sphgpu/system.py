@@ -243,6 +243,16 @@ class GpuSystem:
         A.check(self._L.sph_get_quantity_of_fluid_samples(self._h, int(quantity), out))
         return out
 
+    def get_quantity_at_positions(self, quantity: int, positions) -> np.ndarray:
+        """SPHSystem::get_quantity_at_positions (sph/mod.rs:241-341): the
+        quantity at arbitrary positions (n x 3, taken as f32 like the
+        reference's `&[[f32; 3]]`), e.g. the points of a sensor plane."""
+        pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        out = np.zeros(pos.shape[0], np.float32)
+        A.check(self._L.sph_get_quantity_at_positions(self._h, int(quantity), pos.shape[0],
+                                                      pos.reshape(-1), out))
+        return out
+
     def download(self, field: int) -> np.ndarray:
         n = self.n
         shape = (n, 3) if field in A.VECTOR_FIELDS else (n,)

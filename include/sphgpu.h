@@ -218,6 +218,17 @@ int sph_num_particles(const sph_system_t* h, size_t* out);
 int sph_get_fluid_ids(sph_system_t* h, uint32_t* out);                    /* :186-188 */
 int sph_get_fluid_pos(sph_system_t* h, float* out);                       /* :190-196 */
 int sph_get_quantity_of_fluid_samples(sph_system_t* h, int quantity, float* out); /* :202-239 */
+/* SPHSystem::get_quantity_at_positions (sph/mod.rs:241-341, sums of
+ * sph/quantities.rs:14-330): `quantity` (sph_quantity) at n positions
+ * (3n floats, e.g. a sensor plane) into out[n], from the state of the last
+ * update. Speed and volume include the boundary samples of each position.
+ * Unlike the reference, which searches the boundary samples of the
+ * positions in place of the fluid's until the next update, the system's
+ * state is left unchanged. n == 0 is a no-op. Rejects an unknown quantity
+ * (SPH_ERR_INVALID) and a call while a chunk of graph steps is in flight
+ * (SPH_ERR_STATE). */
+int sph_get_quantity_at_positions(sph_system_t* h, int quantity, size_t n, const float* positions,
+                                  float* out);
 int sph_download(sph_system_t* h, int field, double* out);
 /* Fluid neighbor lists in reference index space, self included, each row
  * sorted ascending (NeighborList, neighbor_search/mod.rs:49-161).

@@ -65,6 +65,7 @@ def lib():
     u32p = np.ctypeslib.ndpointer(np.uint32, flags="C")
     i64p = np.ctypeslib.ndpointer(np.int64, flags="C")
     u8p = np.ctypeslib.ndpointer(np.uint8, flags="C")
+    f32p = np.ctypeslib.ndpointer(np.float32, flags="C")
     sig = {
         "oracle_system_create": (vp, [C.POINTER(OracleConfig)]),
         "oracle_destroy": (None, [vp]),
@@ -80,6 +81,7 @@ def lib():
         "oracle_steps": (C.c_ulonglong, [vp]),
         "oracle_hash_duplicates": (sz, [vp]),
         "oracle_download": (i, [vp, i, dp]),
+        "oracle_quantity_at_positions": (i, [vp, i, sz, f32p, f32p]),
         "oracle_fluid_neighbor_total": (sz, [vp]),
         "oracle_fluid_neighbors": (None, [vp, u64p, u64p]),
         "oracle_boundary_neighbor_total": (sz, [vp, sz]),
@@ -358,6 +360,15 @@ class OracleSystem:
         if rc:
             raise RuntimeError(f"oracle field {field} unavailable")
         return out.reshape(shape)
+
+    def quantity_at_positions(self, quantity, positions):
+        """ScalarQuantity `quantity` at positions (n x 3, cast to f32 like the
+        reference's `&[[f32; 3]]`), f32 values."""
+        pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        out = np.zeros(pos.shape[0], np.float32)
+        if lib().oracle_quantity_at_positions(self.h, int(quantity), pos.shape[0], pos.reshape(-1), out):
+            raise ValueError(f"unknown quantity {quantity}")
+        return out
 
     def fluid_neighbors(self):
         tot = lib().oracle_fluid_neighbor_total(self.h)

@@ -174,6 +174,18 @@ double oracle_time(void* hh) { return ((OracleHandle*)hh)->sys.time(); }
 unsigned long long oracle_steps(void* hh) { return ((OracleHandle*)hh)->sys.time_steps_propagated; }
 size_t oracle_hash_duplicates(void* hh) { return ((OracleHandle*)hh)->sys.hash_duplicates; }
 
+// ScalarQuantity at n positions (3n floats) into out (n floats); 0 on
+// success, 1 for an unknown quantity code.
+int oracle_quantity_at_positions(void* hh, int quantity, size_t n, const float* pos, float* out) {
+  System& s = ((OracleHandle*)hh)->sys;
+  if (quantity < 0 || quantity > 5) return 1;
+  std::vector<V3> eval(n);
+  for (size_t i = 0; i < n; ++i) eval[i] = V3{(double)pos[3 * i], (double)pos[3 * i + 1], (double)pos[3 * i + 2]};
+  std::vector<float> q = s.quantity_at_positions(quantity, eval);
+  for (size_t i = 0; i < n; ++i) out[i] = q[i];
+  return 0;
+}
+
 // field ids: 0 position, 1 velocity, 2 acceleration, 3 mass, 4 volume,
 // 5 pressure, 6 fluid_id, 7 origin, 8 s_f, 9 a_ff, 10 solver velocity slot 0,
 // 11 integrator position slot 0, 12 integrator velocity slot 0

@@ -892,6 +892,69 @@ parallel_for((size_t)(n), [&](size_t b__, size_t e__) {
   });
 }
 
+// sph/mod.rs:241-341 (get_quantity_at_positions) with the sums of
+// quantities.rs:14-330: fluid samples of each evaluation position by the
+// system's spatial hashing, boundary samples searched for the evaluation
+// positions (Normal mode; speed and volume only), f64 sums cast to f32.
+// Quantity codes follow ScalarQuantity: 0 speed, 1 volume, 2 density,
+// 3 density error, 4 pressure, 5 kinetic energy. As in the reference, the
+// boundary's per-particle sample lists then describe the evaluation
+// positions until the next update rebuilds them.
+std::vector<float> System::quantity_at_positions(int q, const std::vector<V3>& eval) {
+  if (q < 0 || q > 5) throw std::invalid_argument("unknown quantity");
+  const double h = params.kernel_support_radius, V0 = params.rest_volume;
+  NeighborList nl;
+  ns.find_samples(h, eval, fluid.position, nl);
+  boundary->find_boundary_samples(h, eval, params.rest_density_grid_spacing);
+  std::vector<float> out(eval.size());
+  parallel_for(eval.size(), [&](size_t b__, size_t e__) {
+    for (size_t id = b__; id < e__; ++id) {
+      const V3 x = eval[id];
+      double s = 0.;
+      V3 sv{0., 0., 0.};
+      for (const size_t* it = nl.begin(id); it != nl.end(id); ++it) {
+        const size_t j = *it;
+        const double w = kernel_function(x - fluid.position[j], h);
+        switch (q) {
+          case 0: sv += fluid.velocity[j] * fluid.volume[j] * w; break;       // :89-99
+          case 1: s += V0 * w; break;                                         // :33-40
+          case 2: s += fluid.mass[j] * w; break;                              // :139-148
+          case 3: {                                                           // :195-211
+            // called with the fluid MASSES in the volume slot (sph/mod.rs:302-311)
+            const double m = fluid.mass[j];
+            if (m < V0) s += (V0 / m - 1.) * m * w;
+            break;
+          }
+          case 4: s += fluid.pressure[j] * fluid.volume[j] * w; break;        // :255-264
+          case 5:                                                             // :309-319
+            s += 0.5 * fluid.mass[j] * norm_squared(fluid.velocity[j]) * fluid.volume[j] * w;
+            break;
+        }
+      }
+      if (q == 0 || q == 1) {
+        for (size_t bi = 0; bi < boundary->count(); ++bi) {
+          const Boundary& b = boundary->at(bi);
+          auto r = b.get_neighbors(id, RequestMode::Normal);
+          for (const size_t* it = r.first; it != r.second; ++it) {
+            const double w = kernel_function(x - b.position(*it), h);
+            if (q == 0) sv += b.velocity(*it) * b.volume(*it) * w;
+            else s += b.volume(*it) * w;
+          }
+        }
+      }
+      double val;
+      switch (q) {
+        case 0: val = norm(sv); break;
+        case 1: val = V0 / s; break;
+        case 3: val = 100. * s; break;
+        default: val = s;
+      }
+      out[id] = (float)val;
+    }
+  });
+  return out;
+}
+
 // non_pressure_accelerations.rs:64-103
 void System::add_gravity_acceleration() {
   const double g = 9.81;

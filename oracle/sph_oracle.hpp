@@ -375,6 +375,8 @@ struct System {
 
   // pieces
   void get_volume();
+  // ScalarQuantity at arbitrary positions (sensor planes), f32 in and out.
+  std::vector<float> quantity_at_positions(int quantity, const std::vector<V3>& eval);
   void add_gravity_acceleration();
   void add_viscosity_acceleration();
   void set_pred_vel_by_applying_acc(bool to_pred_vel);

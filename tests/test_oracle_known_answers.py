@@ -6,6 +6,7 @@ against the oracle (sim_lib = simulation_lib):
   kernel      tests/sph/kernel/cubic_spline.rs:17-232
   hashing     src/neighbor_search/spatial_hashing.rs:173-390
   volume      src/sph/quantities.rs:437-633
+  quantities  src/sph/quantities.rs:437-800 through sph/mod.rs:241-341
   IISPH       tests/sph/pressure_solver/iisph.rs:429-490
   IISPHwOST   src/sph/pressure_solver/iisph_optimized_source_term.rs:530-582
   EulerCromer tests/sph/integration_schemes/euler_cromer.rs:91-300
@@ -331,3 +332,112 @@ def test_mesh_signed_distance_cube(oracle):
     # outside near an edge: euclidean distance to the edge, negative for the container
     d = oracle.mesh_signed_distance(v, inw, [1.3, 1.4, 0.0])
     assert abs(d + math.hypot(0.3, 0.4)) < 1e-12
+
+
+# ---- quantities at arbitrary positions (sensor planes) ------------------------------------
+Q_SPEED, Q_VOLUME, Q_DENSITY, Q_DENSITY_ERROR, Q_PRESSURE, Q_KINETIC_ENERGY = range(6)
+
+
+def _manual(oracle, s, eval_pts, h, term):
+    """Sum of term(j) * W(x - x_j) over the fluid samples within h of each
+    evaluation point (f64, the point taken as f32 like the reference)."""
+    pos = s.download(oracle.F_POSITION)
+    out = []
+    for x in np.asarray(eval_pts, np.float32).astype(np.float64):
+        acc = 0.0
+        for j in range(len(pos)):
+            if np.linalg.norm(x - pos[j]) < h:
+                acc += term(j) * oracle.kernel_function(x - pos[j], h)
+        out.append(acc)
+    return np.array(out)
+
+
+def test_quantity_volume_matches_formula_at_and_between_samples(oracle):
+    # quantities.rs:437-535: V0 / sum V0 W, at the samples and at a point between them
+    h, dx = 1.0, 0.3
+    pos = [[0.0, 0.0, 0.0], [0.3, 0.0, 0.0], [0.0, 0.3, 0.0]]
+    s = _isolated_system(oracle, pos, h=h, spacing=dx)
+    ev = pos + [[0.15, 0.0, 0.0]]
+    got = s.quantity_at_positions(Q_VOLUME, ev)
+    V0 = dx ** 3
+    want = V0 / _manual(oracle, s, ev, h, lambda j: V0)
+    assert np.array_equal(got, want.astype(np.float32))
+
+
+def test_quantity_volume_of_an_isolated_point_is_infinite(oracle):
+    # quantities.rs:476-504: zero neighbor sum -> +inf
+    s = _isolated_system(oracle, [[1000.0, 1000.0, 1000.0]], h=0.1, spacing=0.05)
+    v = s.quantity_at_positions(Q_VOLUME, [[0.0, 0.0, 0.0]])
+    assert np.isinf(v[0]) and v[0] > 0
+    for q in (Q_SPEED, Q_DENSITY, Q_DENSITY_ERROR, Q_PRESSURE, Q_KINETIC_ENERGY):
+        assert s.quantity_at_positions(q, [[0.0, 0.0, 0.0]])[0] == 0.0
+
+
+def test_quantity_on_empty_input(oracle):
+    # quantities.rs:542-561
+    s = _isolated_system(oracle, [[0.0, 0.0, 0.0]])
+    for q in range(6):
+        assert s.quantity_at_positions(q, np.zeros((0, 3))).shape == (0,)
+    with pytest.raises(ValueError):
+        s.quantity_at_positions(6, [[0.0, 0.0, 0.0]])
+
+
+def test_quantity_lattice_recovers_rest_density_and_volume(oracle):
+    # quantities.rs:564-633: a lattice at rest spacing, h / dx = 4, evaluated at its center
+    h, dx = 0.2, 0.05
+    k = int(round(h / dx))
+    g = np.arange(-k, k + 1) * dx
+    pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    s = _isolated_system(oracle, pos, h=h, spacing=dx, mass=1000.0 * dx ** 3)
+    rho = s.quantity_at_positions(Q_DENSITY, [[0.0, 0.0, 0.0]])[0]
+    vol = s.quantity_at_positions(Q_VOLUME, [[0.0, 0.0, 0.0]])[0]
+    assert abs(rho - 1000.0) / 1000.0 < 0.15
+    assert abs(vol - dx ** 3) / dx ** 3 < 0.15
+
+
+def test_quantity_speed_pressure_kinetic_energy_match_formulas(oracle):
+    # quantities.rs:637-800, with the system's own volumes, velocities, masses and pressures
+    h, dx = 1.0, 0.3
+    pos = [[0.0, 0.0, 0.0], [0.4, 0.0, 0.0], [0.0, 0.4, 0.0]]
+    vel = [[1.0, 0.0, 0.0], [0.0, 2.0, 0.0], [0.0, 0.0, 3.0]]
+    s = _isolated_system(oracle, pos, vel=vel, h=h, spacing=dx, mass=[0.5, 0.6, 0.7])
+    V = s.download(oracle.F_VOLUME)
+    v = s.download(oracle.F_VELOCITY)
+    m = s.download(oracle.F_MASS)
+    p = s.download(oracle.F_PRESSURE)
+    ev = pos + [[0.1, 0.2, 0.05], [0.9, 0.9, 0.9]]
+    x = np.asarray(ev, np.float32).astype(np.float64)
+    P = s.download(oracle.F_POSITION)
+    sv = np.zeros((len(ev), 3))
+    for i in range(len(ev)):
+        for j in range(3):
+            if np.linalg.norm(x[i] - P[j]) < h:
+                sv[i] += v[j] * V[j] * oracle.kernel_function(x[i] - P[j], h)
+    speed = s.quantity_at_positions(Q_SPEED, ev)
+    assert np.allclose(speed, np.linalg.norm(sv, axis=1), rtol=1e-6, atol=0)
+    pres = s.quantity_at_positions(Q_PRESSURE, ev)
+    assert np.allclose(pres, _manual(oracle, s, ev, h, lambda j: p[j] * V[j]), rtol=1e-6, atol=1e-12)
+    ke = s.quantity_at_positions(Q_KINETIC_ENERGY, ev)
+    want = _manual(oracle, s, ev, h, lambda j: 0.5 * m[j] * (v[j] @ v[j]) * V[j])
+    assert np.allclose(ke, want, rtol=1e-6, atol=0)
+    rho = s.quantity_at_positions(Q_DENSITY, ev)
+    assert np.allclose(rho, _manual(oracle, s, ev, h, lambda j: m[j]), rtol=1e-6, atol=0)
+
+
+def test_quantity_density_error_takes_masses_in_the_volume_slot(oracle):
+    # quantities.rs:682-718 with sph/mod.rs:302-311, which passes the fluid
+    # MASSES as `sample_volumes`: neighbors whose mass is at or above the rest
+    # volume are skipped, the others add (V0 / m - 1) m W
+    h, dx = 1.0, 0.3
+    V0 = dx ** 3
+    pos = [[0.0, 0.0, 0.0], [0.2, 0.0, 0.0], [0.0, 0.2, 0.0]]
+    masses = [V0, 1.5 * V0, 0.5 * V0]
+    s = _isolated_system(oracle, pos, h=h, spacing=dx, mass=masses)
+    got = s.quantity_at_positions(Q_DENSITY_ERROR, pos)
+    want = 100.0 * _manual(oracle, s, pos, h, lambda j: (V0 / masses[j] - 1.0) * masses[j]
+                           if masses[j] < V0 else 0.0)
+    assert np.allclose(got, want, rtol=1e-6, atol=0)
+    assert got[0] > 0
+    # water-like masses (rest density 1000) are never below the rest volume: zero everywhere
+    s2 = _isolated_system(oracle, pos, h=h, spacing=dx)
+    assert np.all(s2.quantity_at_positions(Q_DENSITY_ERROR, pos) == 0.0)
