@@ -57,6 +57,7 @@ class SystemBase {
   virtual int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
   virtual int boundary_neighbors(int bi, uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
   virtual void boundary_volumes(int bi, double* out) = 0;
+  virtual void boundary_positions(int bi, double* out) = 0;  // world frame, upload order
   virtual void vm_samples(int bi, uint8_t* has, double* xb, double* vb, double* vol) = 0;
   virtual void rigid_state(int bi, double* out) = 0;
   virtual void set_rigid_state(int bi, const double* in) = 0;

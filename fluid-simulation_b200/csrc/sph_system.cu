@@ -21,6 +21,7 @@
 
 #include "../../include/sphgpu.h"
 #include "sph_fields.cuh"
+#include "sph_formats.hpp"
 #include "sph_host.hpp"
 #include "sph_kernels.cuh"
 
@@ -511,6 +512,19 @@ class System : public SystemBase {
       const size_t g = o[s];
       if (g >= sample_offsets_[bi] && g < sample_offsets_[bi] + sample_counts_[bi])
         out[g - sample_offsets_[bi]] = (double)x[s].w;
+    }
+  }
+  void boundary_positions(int bi, double* out) override {
+    if (boundary_kind_ != 1 || bi < 0 || bi >= (int)sample_counts_.size())
+      throw Error(SPH_ERR_INVALID, "not a sample boundary");
+    std::vector<R4<R>> x = fetch(xb_.p, ns_);
+    std::vector<uint32_t> o = fetch(sorig_.p, ns_);
+    for (size_t s = 0; s < ns_; ++s) {
+      const size_t g = o[s];
+      if (g >= sample_offsets_[bi] && g < sample_offsets_[bi] + sample_counts_[bi]) {
+        double* d = out + 3 * (g - sample_offsets_[bi]);
+        d[0] = (double)x[s].x; d[1] = (double)x[s].y; d[2] = (double)x[s].z;
+      }
     }
   }
   void vm_samples(int bi, uint8_t* has, double* xbo, double* vbo, double* vol) override {
@@ -1979,6 +1993,14 @@ int sph_get_boundary_volumes(sph_system_t* h, int bi, double* out) {
     h->impl->boundary_volumes(bi, out);
   });
 }
+int sph_get_boundary_positions(sph_system_t* h, int bi, double* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->boundary_positions(bi, out);
+  });
+}
 int sph_get_volume_map_samples(sph_system_t* h, int bi, uint8_t* has, double* xb, double* vb, double* vol) {
   return guarded([&] {
     if (!h || !has || !xb || !vb || !vol) throw Error(SPH_ERR_INVALID, "null argument");
@@ -2018,6 +2040,146 @@ int sph_continue_from_checkpoint(sph_system_t* h, uint64_t steps, double t, size
     if (!h || (n && (!x || !v || !m))) throw Error(SPH_ERR_INVALID, "null argument");
     set_device(h);
     h->impl->restore(steps, t, n, x, v, m, fid, xi, vi);
+  });
+}
+
+// SystemCheckpoint::from_sph_system (sph/mod.rs:849-856): step counter,
+// time, the fluid in reference order (fluid.rs:351-371, integrator slots
+// included) and one entry per boundary (Some for dynamic ones).
+int sph_get_checkpoint(sph_system_t* h, sph_checkpoint_t** out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    SystemBase* s = h->impl.get();
+    const size_t n = s->num_particles();
+    sph::fmt::Checkpoint c;
+    c.time_steps_propagated = s->steps();
+    c.current_time = s->time();
+    c.position.resize(3 * n);
+    c.velocity.resize(3 * n);
+    c.mass.resize(n);
+    c.fluid_id.resize(n);
+    s->download(SPH_FIELD_POSITION, c.position.data());
+    s->download(SPH_FIELD_VELOCITY, c.velocity.data());
+    s->download(SPH_FIELD_MASS, c.mass.data());
+    s->fluid_ids(c.fluid_id.data());
+    if (h->cfg.integration_scheme == SPH_TAKE_PREDICTED) {  // take_predicted.rs:9-10: one slot each
+      c.integrator_position.emplace_back(3 * n);
+      c.integrator_velocity.emplace_back(3 * n);
+      s->download(SPH_FIELD_INTEGRATOR_POSITION, c.integrator_position[0].data());
+      s->download(SPH_FIELD_INTEGRATOR_VELOCITY, c.integrator_velocity[0].data());
+    }
+    size_t si = 0, vi = 0;
+    for (size_t b = 0; b < h->order.size(); ++b) {
+      const bool dyn = h->order[b] == 0 ? h->samples[si++].dyn : h->vms[vi++].dyn;
+      sph::fmt::RigidState r;
+      if (dyn) {
+        s->rigid_state((int)b, r.s.data());
+        r.dynamic = true;
+      }
+      c.boundaries.push_back(r);
+    }
+    *out = sph::fmt::new_checkpoint(std::move(c));
+  });
+}
+
+// SPHSystem::continue_from_checkpoint (sph/mod.rs:362-378). As in the
+// reference, the integrator slots start from zero (Fluid::resize_slots,
+// fluid.rs:113-129, replaces them) and are rewritten by the update; the
+// boundary entries are applied only when their count matches the system's
+// boundaries, each only where both sides are dynamic
+// (static_sample_boundary.rs:263-277, :561-572).
+int sph_restore_checkpoint(sph_system_t* h, const sph_checkpoint_t* ck) {
+  return guarded([&] {
+    if (!h || !ck) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    const sph::fmt::Checkpoint& c = ck->c;
+    c.check();
+    set_device(h);
+    if (c.boundaries.size() == h->order.size()) {
+      size_t si = 0, vi = 0;
+      for (size_t b = 0; b < h->order.size(); ++b) {
+        const bool dyn = h->order[b] == 0 ? h->samples[si++].dyn : h->vms[vi++].dyn;
+        if (dyn && c.boundaries[b].dynamic) h->impl->set_rigid_state((int)b, c.boundaries[b].s.data());
+      }
+    }
+    const size_t n = c.n();
+    h->impl->restore(c.time_steps_propagated, c.current_time, n, c.position.data(), c.velocity.data(),
+                     c.mass.data(), c.fluid_id.data(), nullptr, nullptr);
+  });
+}
+
+// TimeStepInfo::from_system (render_info.rs:83-92, :110-158, :179-194) and
+// the boundary's Samples visualization (static_sample_boundary.rs:221-249;
+// a volume-map system has no samples and reports an empty, uniformly
+// colored set, volume_map_boundary.rs:1484-1490), encoded as bincode.
+int sph_encode_time_step_info(sph_system_t* h, const sph_frame_selector* sel, sph_bytes_t** out) {
+  return guarded([&] {
+    if (!h || !sel || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    SystemBase* s = h->impl.get();
+    sph_frame_view f;
+    std::memset(&f, 0, sizeof f);
+    f.time_step_number = s->steps();
+    s->measurement(&f.measurement);
+    f.fluid = sel->fluid;
+    f.fluid_coloring = sel->fluid_coloring;
+    f.quantity = sel->quantity;
+    std::vector<float> pos, data;
+    std::vector<uint32_t> ids;
+    std::vector<sph_sensor_plane> planes;
+    std::vector<std::vector<float>> plane_data;
+    if (sel->fluid == SPH_FLUID_SAMPLES) {
+      const size_t n = s->num_particles();
+      pos.resize(3 * n);
+      s->fluid_pos(pos.data());
+      f.n = n;
+      f.fluid_positions = pos.data();
+      if (sel->fluid_coloring == SPH_COLORING_ID) {
+        ids.resize(n);
+        s->fluid_ids(ids.data());
+        f.fluid_ids = ids.data();
+      } else if (sel->fluid_coloring == SPH_COLORING_QUANTITY) {
+        data.resize(n);
+        s->quantity(sel->quantity, data.data());
+        f.fluid_data = data.data();
+      }
+    } else if (sel->fluid == SPH_FLUID_SENSOR_PLANE) {
+      if (sel->num_planes && !sel->planes) throw Error(SPH_ERR_INVALID, "null planes");
+      planes.resize(sel->num_planes);
+      plane_data.resize(sel->num_planes);
+      for (size_t k = 0; k < sel->num_planes; ++k) {
+        const sph_sensor_plane& p = sel->planes[k];
+        const size_t np = p.rows * p.cols;
+        if (np && !p.positions) throw Error(SPH_ERR_INVALID, "null plane positions");
+        plane_data[k].resize(np);
+        s->quantity_at(sel->quantity, np, p.positions, plane_data[k].data());
+        planes[k] = sph_sensor_plane{p.positions, plane_data[k].data(), p.rows, p.cols};
+      }
+      f.num_planes = planes.size();
+      f.planes = planes.data();
+    }
+    std::vector<float> bpos;
+    std::vector<uint32_t> bids;
+    f.boundary_coloring = SPH_COLORING_UNIFORM;
+    if (h->cfg.boundary_handling == SPH_STATIC_SAMPLE_BOUNDARY) {
+      f.boundary_coloring = sel->boundary_coloring;
+      size_t si = 0;
+      for (size_t b = 0; b < h->order.size(); ++b) {
+        if (h->order[b] != 0) continue;
+        const size_t nb = h->samples[si++].x.size() / 3;
+        std::vector<double> x(3 * nb);
+        if (nb) s->boundary_positions((int)b, x.data());
+        for (double v : x) bpos.push_back((float)v);
+        bids.insert(bids.end(), nb, sel->render_mesh_ids ? sel->render_mesh_ids[b] : (uint32_t)b);
+      }
+      f.num_boundary_samples = bpos.size() / 3;
+      f.boundary_positions = bpos.data();
+      f.boundary_ids = bids.data();
+    }
+    *out = sph::fmt::new_bytes(sph::fmt::time_step_info_to_bincode(f));
   });
 }
 

@@ -126,6 +126,45 @@ class SphServerStats(C.Structure):
         "peak_reserved_bytes", "graph_replays", "kernel_launches")]
 
 
+# checkpoint / recording formats
+FORMAT_RON, FORMAT_BINCODE = 0, 1
+FLUID_SAMPLES, FLUID_SENSOR_PLANE = 1, 2
+COLORING_UNIFORM, COLORING_ID, COLORING_QUANTITY = 0, 1, 2
+
+
+class SphCheckpointView(C.Structure):
+    _fields_ = [
+        ("time_steps_propagated", C.c_uint64), ("current_time", C.c_double), ("n", C.c_size_t),
+        ("fluid_id", C.c_void_p), ("position", C.c_void_p), ("velocity", C.c_void_p), ("mass", C.c_void_p),
+        ("integrator_position_slots", C.c_size_t), ("integrator_position", C.c_void_p),
+        ("integrator_velocity_slots", C.c_size_t), ("integrator_velocity", C.c_void_p),
+        ("num_boundaries", C.c_size_t), ("dynamic", C.c_void_p), ("rigid_state", C.c_void_p),
+    ]
+
+
+class SphSensorPlane(C.Structure):
+    _fields_ = [("positions", C.c_void_p), ("data", C.c_void_p), ("rows", C.c_size_t), ("cols", C.c_size_t)]
+
+
+class SphFrameSelector(C.Structure):
+    _fields_ = [
+        ("fluid", C.c_int), ("fluid_coloring", C.c_int), ("quantity", C.c_int),
+        ("num_planes", C.c_size_t), ("planes", C.POINTER(SphSensorPlane)),
+        ("boundary_coloring", C.c_int), ("render_mesh_ids", C.c_void_p),
+    ]
+
+
+class SphFrameView(C.Structure):
+    _fields_ = [
+        ("time_step_number", C.c_uint64), ("measurement", SphMeasurement),
+        ("fluid", C.c_int), ("fluid_coloring", C.c_int), ("quantity", C.c_int),
+        ("n", C.c_size_t), ("fluid_positions", C.c_void_p), ("fluid_ids", C.c_void_p), ("fluid_data", C.c_void_p),
+        ("num_planes", C.c_size_t), ("planes", C.POINTER(SphSensorPlane)),
+        ("boundary_coloring", C.c_int), ("num_boundary_samples", C.c_size_t),
+        ("boundary_positions", C.c_void_p), ("boundary_ids", C.c_void_p),
+    ]
+
+
 class SPHError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"sphgpu error {code}: {msg}")
@@ -199,6 +238,18 @@ SIGNATURES = {
     "sph_server_release": (C.c_int, [_vp, C.c_uint64]),
     "sph_server_get_stats": (C.c_int, [_vp, C.POINTER(SphServerStats)]),
     "sph_server_destroy": (None, [_vp]),
+    "sph_get_boundary_positions": (C.c_int, [_vp, C.c_int, _dp]),
+    "sph_bytes_get": (C.c_int, [_vp, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(_sz)]),
+    "sph_bytes_free": (None, [_vp]),
+    "sph_checkpoint_from_view": (C.c_int, [C.POINTER(SphCheckpointView), C.POINTER(_vp)]),
+    "sph_checkpoint_view_of": (C.c_int, [_vp, C.POINTER(SphCheckpointView)]),
+    "sph_checkpoint_free": (None, [_vp]),
+    "sph_checkpoint_encode": (C.c_int, [_vp, C.c_int, C.POINTER(_vp)]),
+    "sph_checkpoint_decode": (C.c_int, [C.c_char_p, _sz, C.c_int, C.POINTER(_vp)]),
+    "sph_get_checkpoint": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "sph_restore_checkpoint": (C.c_int, [_vp, _vp]),
+    "sph_frame_encode": (C.c_int, [C.POINTER(SphFrameView), C.POINTER(_vp)]),
+    "sph_encode_time_step_info": (C.c_int, [_vp, C.POINTER(SphFrameSelector), C.POINTER(_vp)]),
 }
 
 _lib = None

@@ -314,6 +314,62 @@ class GpuSystem:
         A.check(self._L.sph_get_boundary_volumes(self._h, bi, out))
         return out
 
+    def boundary_positions(self, bi: int, nb: int) -> np.ndarray:
+        out = np.zeros(3 * nb)
+        A.check(self._L.sph_get_boundary_positions(self._h, bi, out))
+        return out.reshape(-1, 3)
+
+    # ---- checkpoints and recording frames ------------------------------------
+    def get_checkpoint(self):
+        """SystemCheckpoint::from_sph_system (sph/mod.rs:849-856)."""
+        from .formats import _from_handle
+        h = C.c_void_p()
+        A.check(self._L.sph_get_checkpoint(self._h, C.byref(h)))
+        try:
+            return _from_handle(h)
+        finally:
+            self._L.sph_checkpoint_free(h)
+
+    def restore_checkpoint(self, ck):
+        """SPHSystem::continue_from_checkpoint (sph/mod.rs:362-378) from a
+        `formats.Checkpoint` (fluid, rigid states, step counter and time)."""
+        from .formats import _to_handle
+        h = _to_handle(ck)
+        try:
+            A.check(self._L.sph_restore_checkpoint(self._h, h))
+        finally:
+            self._L.sph_checkpoint_free(h)
+
+    def encode_time_step_info(self, fluid="samples", fluid_coloring="uniform", quantity=A.Q_SPEED,
+                              planes=(), boundary_coloring="uniform", render_mesh_ids=None) -> bytes:
+        """TimeStepInfo::from_system (render_info.rs:83-92) as bincode bytes.
+        fluid: "samples" or "sensor_plane"; fluid_coloring: "uniform", "id" or
+        "quantity"; planes: [(positions, rows, cols)]; boundary_coloring:
+        "uniform" or "id"."""
+        from .formats import _bytes
+        keep = []
+        sel = A.SphFrameSelector()
+        sel.fluid = A.FLUID_SAMPLES if fluid == "samples" else A.FLUID_SENSOR_PLANE
+        sel.fluid_coloring = {"uniform": A.COLORING_UNIFORM, "id": A.COLORING_ID,
+                              "quantity": A.COLORING_QUANTITY}[fluid_coloring]
+        sel.quantity = int(quantity)
+        arr = (A.SphSensorPlane * max(1, len(planes)))()
+        for k, (pos, rows, cols) in enumerate(planes):
+            p = np.ascontiguousarray(np.asarray(pos, np.float32).reshape(-1))
+            keep.append(p)
+            arr[k].positions = p.ctypes.data if p.size else None
+            arr[k].rows, arr[k].cols = int(rows), int(cols)
+        sel.num_planes = len(planes)
+        sel.planes = arr
+        sel.boundary_coloring = A.COLORING_ID if boundary_coloring == "id" else A.COLORING_UNIFORM
+        if render_mesh_ids is not None:
+            ids = np.ascontiguousarray(render_mesh_ids, np.uint32)
+            keep.append(ids)
+            sel.render_mesh_ids = ids.ctypes.data
+        out = C.c_void_p()
+        A.check(self._L.sph_encode_time_step_info(self._h, C.byref(sel), C.byref(out)))
+        return _bytes(out)
+
     def volume_map_samples(self, bi: int):
         n = self.n
         has = np.zeros(n, np.uint8)

@@ -241,6 +241,10 @@ int sph_get_boundary_neighbors(sph_system_t* h, int bi, uint64_t* offsets, uint3
                                size_t capacity, size_t* total);
 /* Pseudo volumes of the samples of sample boundary `bi` (upload order). */
 int sph_get_boundary_volumes(sph_system_t* h, int bi, double* out);
+/* World positions (3 doubles each) of the samples of sample boundary `bi`
+ * at the last update, upload order (Boundary::positions,
+ * static_sample_boundary.rs:311-321). */
+int sph_get_boundary_positions(sph_system_t* h, int bi, double* out);
 /* Volume-map samples of boundary `bi` per particle: has[n] (0/1),
  * x_b[3n], v_b[3n], vol[n] (volume_map_boundary.rs:1287-1342). */
 int sph_get_volume_map_samples(sph_system_t* h, int bi, uint8_t* has, double* xb, double* vb,
@@ -435,6 +439,105 @@ int sph_server_get_stats(sph_server_t* s, sph_server_stats* out);
 /* Cancels queued scenes, stops running ones after their current chunk and
  * frees everything. */
 void sph_server_destroy(sph_server_t* s);
+
+/* ---- checkpoint and recording formats ----------------------------------- */
+/* The readback formats either side of the step: the system checkpoint
+ * (SerSystemCheckpoint, sph/mod.rs:883-915) that sci-phi-backend writes as
+ * RON (recording.rs:37-61) and the `--state` path reads back
+ * (sph/setup/mod.rs:142-153), also in its bincode form (its Encode/Decode
+ * derive), and the recording frame (TimeStepInfo, render_info.rs:71-106) in
+ * bincode's standard configuration, each record of a recording file being a
+ * little-endian u64 length and these bytes (recording.rs:146-210). */
+enum sph_format { SPH_FORMAT_RON = 0, SPH_FORMAT_BINCODE = 1 };
+
+/* An owned byte string; `data` stays valid until sph_bytes_free. */
+typedef struct sph_bytes sph_bytes_t;
+int sph_bytes_get(const sph_bytes_t* b, const uint8_t** data, size_t* len);
+void sph_bytes_free(sph_bytes_t* b);
+
+/* SystemCheckpoint as plain arrays (fluid.rs:351-421, reference index order;
+ * boundary_handling/mod.rs:135-170, one entry per boundary in add order). */
+typedef struct sph_checkpoint_view {
+  uint64_t time_steps_propagated;
+  double current_time;
+  size_t n;                          /* fluid samples */
+  const uint32_t* fluid_id;          /* n */
+  const double* position;            /* 3n */
+  const double* velocity;            /* 3n */
+  const double* mass;                /* n */
+  size_t integrator_position_slots;  /* slots of 3n doubles each, back to back */
+  const double* integrator_position;
+  size_t integrator_velocity_slots;
+  const double* integrator_velocity;
+  size_t num_boundaries;
+  const uint8_t* dynamic;            /* per boundary: 1 = rigid state present */
+  const double* rigid_state;         /* 19 per boundary, sph_get_rigid_state layout */
+} sph_checkpoint_view;
+
+/* An owned checkpoint. */
+typedef struct sph_checkpoint sph_checkpoint_t;
+int sph_checkpoint_from_view(const sph_checkpoint_view* view, sph_checkpoint_t** out);
+/* Fills `view` with pointers into `c` (valid until sph_checkpoint_free). */
+int sph_checkpoint_view_of(const sph_checkpoint_t* c, sph_checkpoint_view* view);
+void sph_checkpoint_free(sph_checkpoint_t* c);
+/* SerSystemCheckpoint -> RON text (ron::to_string) or bincode bytes. */
+int sph_checkpoint_encode(const sph_checkpoint_t* c, int format, sph_bytes_t** out);
+/* RON text (any whitespace, comments, struct names, field order) or bincode
+ * bytes -> checkpoint; SPH_ERR_INVALID with the position of a syntax error. */
+int sph_checkpoint_decode(const uint8_t* data, size_t len, int format, sph_checkpoint_t** out);
+/* SystemCheckpoint::from_sph_system (sph/mod.rs:849-856). */
+int sph_get_checkpoint(sph_system_t* h, sph_checkpoint_t** out);
+/* SPHSystem::continue_from_checkpoint (sph/mod.rs:362-378): fluid, rigid
+ * states, step counter and time, then update(). The boundaries must match
+ * the system's in number and static/dynamic kind, and the integrator slots
+ * its integration scheme (TakePredicted: 1 each, else none). */
+int sph_restore_checkpoint(sph_system_t* h, const sph_checkpoint_t* c);
+
+/* Recording frames: the TimeStepInfo variants that need no triangle meshes,
+ * FluidVisualization::Samples / ::SensorPlane and
+ * BoundaryVisualization::Samples (render_info.rs:110-245). */
+enum sph_fluid_visualization { SPH_FLUID_SAMPLES = 1, SPH_FLUID_SENSOR_PLANE = 2 };
+enum sph_sample_coloring { SPH_COLORING_UNIFORM = 0, SPH_COLORING_ID = 1, SPH_COLORING_QUANTITY = 2 };
+
+typedef struct sph_sensor_plane {  /* SensorPlaneData (render_info.rs:196-202) */
+  const float* positions;          /* 3 * rows * cols */
+  const float* data;               /* rows * cols (frame views only) */
+  size_t rows, cols;
+} sph_sensor_plane;
+
+/* What a frame shows (the selector TimeStepInfo::from_system takes). */
+typedef struct sph_frame_selector {
+  int fluid;                       /* sph_fluid_visualization */
+  int fluid_coloring;              /* Samples: UNIFORM, ID (fluid id) or QUANTITY */
+  int quantity;                    /* sph_quantity for QUANTITY and SENSOR_PLANE */
+  size_t num_planes;
+  const sph_sensor_plane* planes;  /* positions, rows, cols (data unused) */
+  int boundary_coloring;           /* UNIFORM or ID (render mesh id) */
+  const uint32_t* render_mesh_ids; /* per boundary; NULL = the boundary index */
+} sph_frame_selector;
+
+/* A frame's contents (TimeStepInfo itself). */
+typedef struct sph_frame_view {
+  uint64_t time_step_number;
+  sph_measurement measurement;
+  int fluid, fluid_coloring, quantity;
+  size_t n;                        /* Samples */
+  const float* fluid_positions;    /* 3n */
+  const uint32_t* fluid_ids;       /* n, ID coloring */
+  const float* fluid_data;         /* n, QUANTITY coloring */
+  size_t num_planes;
+  const sph_sensor_plane* planes;  /* SensorPlane, with data */
+  int boundary_coloring;
+  size_t num_boundary_samples;
+  const float* boundary_positions; /* 3 * num_boundary_samples */
+  const uint32_t* boundary_ids;    /* per sample, ID coloring */
+} sph_frame_view;
+
+/* TimeStepInfo -> bincode bytes (render_info.rs:101-106). */
+int sph_frame_encode(const sph_frame_view* frame, sph_bytes_t** out);
+/* TimeStepInfo::from_system (render_info.rs:83-92) on the device state,
+ * encoded; sensor planes are evaluated with sph_get_quantity_at_positions. */
+int sph_encode_time_step_info(sph_system_t* h, const sph_frame_selector* sel, sph_bytes_t** out);
 
 #ifdef __cplusplus
 }

@@ -8,9 +8,10 @@ covers all six ScalarQuantity values: speed and volume with sample
 boundaries (static and a rotating body) and with volume maps (static and a
 rotating body), and the fluid-only sums. The f64 engine is held to 1e-6 of
 the oracle (the sums run in f64 in both, in different orders, and are cast
-to f32); the f32 engine to 1e-4, the size of its state's rounding, except
-for IISPH pressures, which its f32 solve sets within the target density
-error (2e-2 of the largest pressure).
+to f32); the f32 engine to 1e-4, the size of its state's rounding (for
+volumes: of their kernel sums), except for pressures: near rest they are
+small differences of densities, and the IISPH solve in f32 stops within the
+target density error, so they are held to 2e-2 of the largest pressure.
 """
 import numpy as np
 import pytest
@@ -20,6 +21,8 @@ from conftest import build_oracle
 pytestmark = pytest.mark.gpu
 
 QUANTITIES = range(6)
+QUANTITY_VOLUME = 1
+QUANTITY_PRESSURE = 4
 
 
 @pytest.fixture(scope="module")
@@ -64,9 +67,31 @@ def _compare(got, want, rtol):
     assert err.max() < rtol, (err.max(), int(err.argmax()))
 
 
-def _check_all(g, o, pts, rtol, quantities=QUANTITIES):
+def _compare_volume_sums(got, want, V0, atol):
+    """Volumes through their kernel sums sum V0 W / V0 (about 1 inside the
+    fluid, 0 where the volume is infinite). An f32 state moves positions by
+    an ulp, which changes W of a neighbor at the support's edge by a large
+    factor but by little in absolute terms: where such a neighbor is a
+    point's only one, the volume's relative error is large while its sum's
+    absolute error stays at the rounding level."""
+    sg = V0 / np.asarray(got, np.float64)
+    sw = V0 / np.asarray(want, np.float64)
+    err = np.abs(sg - sw)
+    assert err.max() < atol, (err.max(), int(err.argmax()))
+
+
+def _check_all(g, o, pts, rtol, quantities=QUANTITIES, precision="f64", spacing=None):
     for q in quantities:
-        _compare(g.get_quantity_at_positions(q, pts), o.quantity_at_positions(q, pts), rtol)
+        got, want = g.get_quantity_at_positions(q, pts), o.quantity_at_positions(q, pts)
+        if q == QUANTITY_VOLUME and precision == "f32":
+            _compare_volume_sums(got, want, spacing ** 3, rtol)
+        elif q == QUANTITY_PRESSURE and precision == "f32":
+            # near rest, SESPH pressures are k (rho / rho0 - 1) with rho / rho0 - 1
+            # of a few 1e-3, so the f32 state's density rounding (~1e-5) moves
+            # them by ~1e-2 of their largest value
+            _compare(got, want, 2e-2)
+        else:
+            _compare(got, want, rtol)
 
 
 def _with_velocity(sc, seed=1, scale=0.5):
@@ -84,7 +109,7 @@ def test_sample_boundary_scene_at_initialization(A, oracle, precision, rtol):
     pts = _eval_points(sc)
     # a plane through the container's wall samples as well
     pts = np.concatenate([pts, _plane((-0.32,) * 3, (0.32,) * 3, 0, -0.295, 40).astype(np.float32)])
-    _check_all(g, o, pts, rtol)
+    _check_all(g, o, pts, rtol, precision=precision, spacing=0.02)
     g.close()
 
 
@@ -114,7 +139,7 @@ def test_rotating_sample_body(A, oracle, precision, rtol):
     pts = np.concatenate([_eval_points(sc, n=32),
                           _plane(c - 0.1, c + 0.1, 0, c[0], 40),
                           _plane(c - 0.1, c + 0.1, 2, c[2] - 0.05, 40)]).astype(np.float32)
-    _check_all(g, o, pts, rtol)
+    _check_all(g, o, pts, rtol, precision=precision, spacing=0.02)
     # the body's samples move: speed near it includes their velocities
     near = _plane(c - 0.07, c + 0.07, 0, c[0], 20).astype(np.float32)
     assert g.get_quantity_at_positions(A.Q_SPEED, near).max() > 0
@@ -149,7 +174,8 @@ def test_volume_maps_static_and_rotating(A, oracle, precision, rtol):
     pts = np.concatenate([_eval_points(sc, n=32),
                           _plane((-0.3, -0.16, -0.16), (0.3, 0.16, 0.16), 1, 0.0, 48),
                           _plane(c - 0.09, c + 0.09, 2, 0.01, 40)]).astype(np.float32)
-    _check_all(g, o, pts, rtol, quantities=[q for q in QUANTITIES if q != A.Q_PRESSURE])
+    _check_all(g, o, pts, rtol, quantities=[q for q in QUANTITIES if q != A.Q_PRESSURE],
+               precision=precision, spacing=0.02)
     # IISPH pressures: the f32 Jacobi solve stops within the target density
     # error of the f64 one, not at its rounding
     _compare(g.get_quantity_at_positions(A.Q_PRESSURE, pts), o.quantity_at_positions(A.Q_PRESSURE, pts),
