@@ -74,6 +74,8 @@ def lib():
         "oracle_add_sample_boundary": (i, [vp, sz, dp, vp]),
         "oracle_add_volume_map_boundary": (i, [vp, dp, i64p, dp, dp, i64p, dp, vp]),
         "oracle_initialize": (i, [vp]),
+        "oracle_set_vm_aabb": (i, [vp, sz, dp, dp]),
+        "oracle_contact_probe": (i, [vp, d, dp, dp, C.POINTER(sz), C.POINTER(C.c_uint)]),
         "oracle_step": (i, [vp, i]),
         "oracle_num_particles": (sz, [vp]),
         "oracle_measure": (None, [vp, dp]),
@@ -327,6 +329,19 @@ class OracleSystem:
         r = None if keep is None else keep.ctypes.data_as(C.c_void_p)
         assert lib().oracle_add_volume_map_boundary(self.h, sdf.desc, sdf.n, sdf.nodes, vm.desc,
                                                     vm.n, vm.nodes, r) == 0
+
+    def set_vm_aabb(self, bi, center, half_extents):
+        """Body-frame mesh bounding box of volume-map boundary `bi` (enables
+        its rigid-rigid contact)."""
+        assert lib().oracle_set_vm_aabb(self.h, int(bi), _f64(center), _f64(half_extents)) == 0
+
+    def contact_probe(self, dt, nb):
+        """One contact solve on the current state, not applied:
+        (force[nb,3], torque[nb,3], cells, sweeps)."""
+        f, t = np.zeros(3 * nb), np.zeros(3 * nb)
+        cells, its = C.c_size_t(), C.c_uint()
+        assert lib().oracle_contact_probe(self.h, float(dt), f, t, C.byref(cells), C.byref(its)) == 0
+        return f.reshape(nb, 3), t.reshape(nb, 3), cells.value, its.value
 
     def initialize(self):
         assert lib().oracle_initialize(self.h) == 0

@@ -140,6 +140,34 @@ int oracle_add_volume_map_boundary(void* hh, const double* sdf_desc, const long 
   return 0;
 }
 
+// Mesh bounding box (body frame) of volume-map boundary `bi`, which makes it
+// take part in rigid-rigid contact.
+int oracle_set_vm_aabb(void* hh, size_t bi, const double* center, const double* half) {
+  auto* vb = dynamic_cast<VolumeMapBoundary*>(((OracleHandle*)hh)->sys.boundary.get());
+  if (!vb || bi >= vb->boundaries.size()) return 1;
+  VMBoundary& b = vb->boundaries[bi];
+  b.has_aabb = true;
+  b.aabb_center = V3{center[0], center[1], center[2]};
+  b.aabb_half = V3{half[0], half[1], half[2]};
+  return 0;
+}
+
+// One contact solve on the current state without applying it: per-boundary
+// force and torque (3 doubles each), the number of contact cells and sweeps.
+int oracle_contact_probe(void* hh, double dt, double* force, double* torque, size_t* cells,
+                         unsigned* iterations) {
+  auto* vb = dynamic_cast<VolumeMapBoundary*>(((OracleHandle*)hh)->sys.boundary.get());
+  if (!vb) return 1;
+  ContactResult r = vb->solve_contacts(dt, false);
+  for (size_t b = 0; b < r.force.size(); ++b) {
+    force[3 * b] = r.force[b].x; force[3 * b + 1] = r.force[b].y; force[3 * b + 2] = r.force[b].z;
+    torque[3 * b] = r.torque[b].x; torque[3 * b + 1] = r.torque[b].y; torque[3 * b + 2] = r.torque[b].z;
+  }
+  *cells = r.cells;
+  *iterations = r.iterations;
+  return 0;
+}
+
 int oracle_initialize(void* hh) {
   auto* h = (OracleHandle*)hh;
   try {

@@ -3,6 +3,7 @@
 #include "sph_oracle.hpp"
 
 #include <algorithm>
+#include <limits>
 #include <chrono>
 #include <cstring>
 #include <stdexcept>
@@ -490,7 +491,420 @@ parallel_for((size_t)(n), [&](size_t b__, size_t e__) {
     }
   }
 }
+// ---------------------------------------------------------------------------
+// Rigid-rigid contact of VolumeMapBoundary (volume_map_boundary.rs:55-1102):
+// broad phase on world AABBs, contact cells from the overlap boxes, the
+// contact volume of each cell by 8^3 Gauss-Legendre quadrature of the
+// product of both bodies' cubic extension functions of the signed distance,
+// and a projected Jacobi iteration with nonlinear conjugate-gradient
+// acceleration (NNCG) for the contact pressures p_c >= 0 and the friction
+// impulses lambda_c inside the Coulomb cone.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr double kContactCellSizeFactor = 0.5;   // :60
+constexpr int kContactQuadratureDegree = 8;       // :57
+constexpr double kFrictionCoefficient = 0.5;      // :62
+constexpr double kRelaxation = 0.5;               // :64
+constexpr double kMinDiagonal = 1e-35;            // :65
+constexpr double kFbTolPressure = 1e-6;           // :67
+constexpr double kFbTolFriction = 1e-3;           // :68
+
+M3 m3_identity() {
+  M3 m;
+  m.m[0][0] = m.m[1][1] = m.m[2][2] = 1.0;
+  return m;
+}
+M3 m3_add(const M3& a, const M3& b) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.m[i][j] = a.m[i][j] + b.m[i][j];
+  return r;
+}
+M3 m3_sub(const M3& a, const M3& b) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.m[i][j] = a.m[i][j] - b.m[i][j];
+  return r;
+}
+M3 m3_scale(const M3& a, double s) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.m[i][j] = a.m[i][j] * s;
+  return r;
+}
+M3 m3_outer(V3 a, V3 b) {
+  const double x[3] = {a.x, a.y, a.z}, y[3] = {b.x, b.y, b.z};
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.m[i][j] = x[i] * y[j];
+  return r;
+}
+M3 m3_cross_matrix(V3 v) {
+  M3 r;
+  r.m[0][1] = -v.z; r.m[0][2] = v.y;
+  r.m[1][0] = v.z;  r.m[1][2] = -v.x;
+  r.m[2][0] = -v.y; r.m[2][1] = v.x;
+  return r;
+}
+M3 m3_abs(const M3& a) {
+  M3 r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r.m[i][j] = std::fabs(a.m[i][j]);
+  return r;
+}
+
+struct WorldBox {
+  V3 min, max;
+};
+
+// BoundaryType::world_aabb (:2122-2151): |R| applied to the local half extents.
+WorldBox world_aabb(const VMBoundary& b) {
+  if (!b.dynamic) return {b.aabb_center - b.aabb_half, b.aabb_center + b.aabb_half};
+  const M3 r = qto_matrix(b.state.orientation);
+  const V3 he = mul(m3_abs(r), b.aabb_half);
+  const V3 c = b.state.local_to_world(b.aabb_center);
+  return {c - he, c + he};
+}
+bool boxes_overlap(const WorldBox& a, const WorldBox& b) {  // :1783-1790
+  return a.min.x <= b.max.x && a.max.x >= b.min.x && a.min.y <= b.max.y && a.max.y >= b.min.y &&
+         a.min.z <= b.max.z && a.max.z >= b.min.z;
+}
+bool boxes_intersection(const WorldBox& a, const WorldBox& b, WorldBox& out) {  // :1792-1805
+  out.min = {std::max(a.min.x, b.min.x), std::max(a.min.y, b.min.y), std::max(a.min.z, b.min.z)};
+  out.max = {std::min(a.max.x, b.max.x), std::min(a.max.y, b.max.y), std::min(a.max.z, b.max.z)};
+  return out.min.x <= out.max.x && out.min.y <= out.max.y && out.min.z <= out.max.z;
+}
+
+// cubic_extension_fn and its derivative (:1717-1745): W(x)/W(0) on (0, h).
+double cubic_extension(double x, double h) {
+  if (x >= h) return 0.;
+  if (x <= 0.) return 1.;
+  return kernel_function(V3{x, 0., 0.}, h) / kernel_function(V3{0., 0., 0.}, h);
+}
+double cubic_extension_derivative(double x, double h) {
+  if (x >= h || x <= 0.0) return 0.0;
+  return kernel_gradient(V3{x, 0., 0.}, h).x / kernel_function(V3{0., 0., 0.}, h);
+}
+
+struct QuadPoint {  // QuadPointData (:784-793)
+  V3 pos;
+  double weight;
+  V3 grad_a, grad_b;
+  double s_a, s_b, sp_a, sp_b;
+};
+struct Cell {  // ContactCell (:678-697)
+  size_t a, b;
+  std::vector<QuadPoint> q;
+  double volume;
+  V3 center, f_a, tau_a, f_b, tau_b;
+  M3 tproj;
+  double acc_p = 0, acc_f = 0;
+};
+
+const RigidBodyMotion* motion_of(const VMBoundary& b) { return b.dynamic ? &b.state : nullptr; }
+
+// build_contact_cell (:700-782) with quadrature_points (:805-833).
+bool build_cell(size_t ia, size_t ib, V3 from, V3 to, const std::vector<VMBoundary>& bs, double h,
+                const std::vector<double>& gx, const std::vector<double>& gw, Cell& cell) {
+  const V3 half = (to - from) * 0.5;
+  const V3 center = from + half;
+  const double scaling = 2.0;
+  double v_c = 0.0;
+  cell.q.clear();
+  const int n = (int)gx.size();
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j)
+      for (int k = 0; k < n; ++k) {
+        const V3 pos = center + V3{gx[i] * half.x, gx[j] * half.y, gx[k] * half.z};
+        const double w = gw[i] * gw[j] * gw[k] * half.x * half.y * half.z;
+        double phi_a, phi_b;
+        if (!bs[ia].signed_distance(pos, phi_a)) continue;
+        if (!bs[ib].signed_distance(pos, phi_b)) continue;
+        const double s_a = cubic_extension(scaling * phi_a + h, h);
+        const double s_b = cubic_extension(scaling * phi_b + h, h);
+        if (s_a <= 0.0 || s_b <= 0.0) continue;
+        V3 ga, gb;
+        if (!bs[ia].signed_distance_gradient(pos, ga)) continue;
+        if (!bs[ib].signed_distance_gradient(pos, gb)) continue;
+        v_c += w * s_a * s_b;
+        cell.q.push_back(QuadPoint{pos, w, ga, gb, s_a, s_b,
+                                   scaling * cubic_extension_derivative(scaling * phi_a + h, h),
+                                   scaling * cubic_extension_derivative(scaling * phi_b + h, h)});
+      }
+  if (v_c <= 0.0 || cell.q.empty()) return false;
+  cell.a = ia;
+  cell.b = ib;
+  cell.volume = v_c;
+  return true;
+}
+
+// compute_diagonal (:835-926).
+void compute_diagonal(Cell& c, const std::vector<VMBoundary>& bs, double dt) {
+  const RigidBodyMotion* ma = motion_of(bs[c.a]);
+  const RigidBodyMotion* mb = motion_of(bs[c.b]);
+  V3 xv{0, 0, 0}, f_a{0, 0, 0}, t_a{0, 0, 0}, f_b{0, 0, 0}, t_b{0, 0, 0};
+  for (const QuadPoint& q : c.q) {
+    const double w_g = q.weight * q.s_a * q.s_b;
+    xv += w_g * q.pos;
+    const double w_a = q.weight * q.sp_a * q.s_b;
+    f_a += w_a * q.grad_a;
+    if (ma) t_a += w_a * cross(q.pos - ma->center_of_mass, q.grad_a);
+    const double w_b = q.weight * q.sp_b * q.s_a;
+    f_b += w_b * q.grad_b;
+    if (mb) t_b += w_b * cross(q.pos - mb->center_of_mass, q.grad_b);
+  }
+  c.center = xv / c.volume;
+  c.f_a = f_a;
+  c.tau_a = t_a;
+  c.f_b = f_b;
+  c.tau_b = t_b;
+  const V3 n = c.f_a / std::max(norm(c.f_a), 1e-15);
+  c.tproj = m3_sub(m3_identity(), m3_outer(n, n));
+  auto pressure_term = [](const RigidBodyMotion* m, V3 f, V3 t) {
+    return m ? dot(f, f) / m->mass + dot(t, mul(m->inertia_tensor_inv_world, t)) : 0.0;
+  };
+  c.acc_p = dt * dt * (pressure_term(ma, f_a, t_a) + pressure_term(mb, f_b, t_b));
+  auto friction_term = [&](const RigidBodyMotion* m) {
+    if (!m) return M3{};
+    const M3 rx = m3_cross_matrix(c.center - m->center_of_mass);
+    return m3_sub(m3_scale(m3_identity(), 1.0 / m->mass), mul(mul(rx, m->inertia_tensor_inv_world), rx));
+  };
+  const M3 k = mul(m3_scale(c.tproj, dt), m3_add(friction_term(ma), friction_term(mb)));
+  c.acc_f = 1. / 3. * ((k.m[0][0] + k.m[1][1]) + k.m[2][2]);
+}
+
+// mean_fischer_burmeister (utilities/mod.rs:27-41).
+double mean_fischer_burmeister(const std::vector<double>& a, const std::vector<double>& b) {
+  double sum = 0.0;
+  for (size_t i = 0; i < a.size(); ++i) sum += std::fabs(a[i] + b[i] - std::sqrt(a[i] * a[i] + b[i] * b[i]));
+  return sum / (double)a.size();
+}
+
+}  // namespace
+
+ContactResult VolumeMapBoundary::solve_contacts(double dt, bool commit) {
+  ContactResult res;
+  const size_t nb = boundaries.size();
+  res.force.assign(nb, V3{0, 0, 0});
+  res.torque.assign(nb, V3{0, 0, 0});
+  const double h = kernel_support_radius;
+  // broad_phase (:70-96) and generate_contact_cells (:98-161)
+  std::vector<WorldBox> boxes(nb);
+  for (size_t i = 0; i < nb; ++i)
+    if (boundaries[i].has_aabb) boxes[i] = world_aabb(boundaries[i]);
+  std::vector<double> gx, gw;
+  gauss_legendre(kContactQuadratureDegree, gx, gw);
+  std::vector<Cell> cells;
+  for (size_t i = 0; i < nb; ++i) {
+    if (!boundaries[i].has_aabb) continue;
+    for (size_t j = i + 1; j < nb; ++j) {
+      if (!boundaries[j].has_aabb) continue;
+      if (!boundaries[i].dynamic && !boundaries[j].dynamic) continue;
+      if (!boxes_overlap(boxes[i], boxes[j])) continue;
+      WorldBox ov;
+      if (!boxes_intersection(boxes[i], boxes[j], ov)) continue;
+      // subdivide_overlap (:1813-1844)
+      const double target = h * kContactCellSizeFactor;
+      const V3 ext = ov.max - ov.min;
+      const size_t n[3] = {std::max<size_t>((size_t)std::ceil(ext.x / target), 1),
+                           std::max<size_t>((size_t)std::ceil(ext.y / target), 1),
+                           std::max<size_t>((size_t)std::ceil(ext.z / target), 1)};
+      const V3 cs{ext.x / (double)n[0], ext.y / (double)n[1], ext.z / (double)n[2]};
+      for (size_t iz = 0; iz < n[2]; ++iz)
+        for (size_t iy = 0; iy < n[1]; ++iy)
+          for (size_t ix = 0; ix < n[0]; ++ix) {
+            const V3 from = ov.min + V3{(double)ix * cs.x, (double)iy * cs.y, (double)iz * cs.z};
+            const V3 to = from + cs;
+            const V3 center = from + (to - from) * 0.5;
+            const double bound = 2.0 * (norm(to - from) * 0.5);
+            double pa, pb;
+            if (!boundaries[i].signed_distance(center, pa) || !boundaries[j].signed_distance(center, pb)) continue;
+            if (!(pa - bound < 0. && pb - bound < 0.)) continue;
+            Cell c;
+            if (build_cell(i, j, from, to, boundaries, h, gx, gw, c)) cells.push_back(std::move(c));
+          }
+    }
+  }
+  const size_t n = cells.size();
+  res.cells = n;
+  if (n == 0) return res;
+  // solve_for_p_c (:186-645)
+  for (Cell& c : cells) compute_diagonal(c, boundaries, dt);
+  std::vector<std::vector<std::pair<size_t, bool>>> touching(nb);  // BodyCellIndex (:647-676)
+  for (size_t c = 0; c < n; ++c) {
+    touching[cells[c].a].push_back({c, true});
+    touching[cells[c].b].push_back({c, false});
+  }
+  std::vector<double> p(n, 0.0), v_err(n, 0.0), s_p(n, 0.0);
+  std::vector<V3> lambda(n, V3{0, 0, 0}), v_tang(n, V3{0, 0, 0}), s_l(n, V3{0, 0, 0});
+  std::vector<V3> ef(nb), et(nb), vt(nb), wt(nb);
+  auto accumulate = [&]() {  // accumulate_extra_forces (:928-965)
+    for (size_t b = 0; b < nb; ++b) {
+      V3 f{0, 0, 0}, t{0, 0, 0};
+      for (auto [ci, is_a] : touching[b]) {
+        const Cell& c = cells[ci];
+        const RigidBodyMotion* ma = motion_of(boundaries[c.a]);
+        const RigidBodyMotion* mb = motion_of(boundaries[c.b]);
+        if (is_a) {
+          f += p[ci] * c.f_a + lambda[ci];
+          if (ma) t += p[ci] * c.tau_a + cross(c.center - ma->center_of_mass, lambda[ci]);
+        } else {
+          f += p[ci] * c.f_b - lambda[ci];
+          if (mb) t += p[ci] * c.tau_b - cross(c.center - mb->center_of_mass, lambda[ci]);
+        }
+      }
+      ef[b] = f;
+      et[b] = t;
+    }
+  };
+  auto predict = [&]() {
+    for (size_t b = 0; b < nb; ++b) {  // compute_trial_velocities (:967-994)
+      const RigidBodyMotion* m = motion_of(boundaries[b]);
+      if (!m) {
+        vt[b] = wt[b] = V3{0, 0, 0};
+        continue;
+      }
+      vt[b] = m->linear_velocity + dt / m->mass * (m->force + ef[b]);
+      wt[b] = mul(m->inertia_tensor_inv_world, m->angular_momentum + dt * (m->torque + et[b]));
+    }
+    for (size_t c = 0; c < n; ++c) {
+      const Cell& k = cells[c];
+      // predicted_volume_error (:996-1009)
+      v_err[c] = -k.volume + dt * (((dot(vt[k.a], k.f_a) + dot(wt[k.a], k.tau_a)) + dot(vt[k.b], k.f_b)) +
+                                   dot(wt[k.b], k.tau_b));
+      // predicted_tangential_velocity (:1011-1033)
+      const RigidBodyMotion* ma = motion_of(boundaries[k.a]);
+      const RigidBodyMotion* mb = motion_of(boundaries[k.b]);
+      if (ma && mb) {
+        const V3 v_rel = ((vt[k.a] + cross(wt[k.a], k.center - ma->center_of_mass)) - vt[k.b]) -
+                         cross(wt[k.b], k.center - mb->center_of_mass);
+        v_tang[c] = mul(k.tproj, v_rel);
+      } else {
+        v_tang[c] = V3{0, 0, 0};
+      }
+    }
+  };
+  // projected_jacobi (:1035-1102)
+  auto jacobi = [&](std::vector<double>& p_out, std::vector<V3>& l_out) {
+    std::vector<uint32_t> active(nb, 0);
+    for (size_t b = 0; b < nb; ++b)
+      for (auto [ci, is_a] : touching[b])
+        if (v_err[ci] < 0.0 || p[ci] > 0.0) ++active[b];
+    p_out.resize(n);
+    l_out.resize(n);
+    for (size_t c = 0; c < n; ++c) {
+      const Cell& k = cells[c];
+      const double n_max = (double)std::max<uint32_t>(std::max(active[k.a], active[k.b]), 1);
+      const double alpha = kRelaxation / n_max / std::max(k.acc_p, kMinDiagonal);
+      p_out[c] = std::max(p[c] - alpha * v_err[c], 0.0);
+      const double lmax = kFrictionCoefficient * p[c] * norm(k.f_a);
+      V3 star = -v_tang[c] / std::max(k.acc_f, kMinDiagonal);
+      const double sn = norm(star);
+      if (sn > lmax) star = lmax * star / sn;
+      V3 ln = lambda[c] + kRelaxation / n_max * star;
+      const double lnn = norm(ln);
+      l_out[c] = lnn > lmax ? lmax * ln / lnn : ln;
+    }
+  };
+  std::vector<double> pp(n), vtn(n), dev(n);
+  auto merits = [&]() {
+    for (size_t c = 0; c < n; ++c) {
+      pp[c] = p[c] * std::max(cells[c].acc_p, kMinDiagonal);
+      vtn[c] = norm(v_tang[c]);
+      dev[c] = std::max(cells[c].acc_f, kMinDiagonal) *
+               (kFrictionCoefficient * p[c] * norm(cells[c].f_a) - norm(lambda[c]));
+    }
+  };
+  accumulate();
+  predict();
+  std::vector<double> pj, gp(n);
+  std::vector<V3> lj, gl(n);
+  jacobi(pj, lj);
+  double prev_gp = 0, prev_gl = 0;
+  for (size_t c = 0; c < n; ++c) {
+    gp[c] = -(pj[c] - p[c]);
+    gl[c] = -(lj[c] - lambda[c]);
+    s_p[c] = -gp[c];
+    s_l[c] = -gl[c];
+    prev_gp += gp[c] * gp[c];
+    prev_gl += dot(gl[c], gl[c]);
+  }
+  p = pj;
+  lambda = lj;
+  accumulate();
+  predict();
+  merits();
+  uint32_t it = 0;
+  while (!(mean_fischer_burmeister(pp, v_err) < kFbTolPressure &&
+           mean_fischer_burmeister(vtn, dev) < kFbTolFriction) &&
+         it < contact_iteration_cap) {
+    jacobi(pj, lj);
+    double gpn = 0, gln = 0;
+    for (size_t c = 0; c < n; ++c) {
+      gp[c] = -(pj[c] - p[c]);
+      gl[c] = -(lj[c] - lambda[c]);
+      gpn += gp[c] * gp[c];
+      gln += dot(gl[c], gl[c]);
+    }
+    const double beta = (gpn + gln) / std::max(prev_gp + prev_gl, std::numeric_limits<double>::min());
+    if (beta > 1.0) {
+      std::fill(s_p.begin(), s_p.end(), 0.0);
+      std::fill(s_l.begin(), s_l.end(), V3{0, 0, 0});
+      p = pj;
+      lambda = lj;
+    } else {
+      std::vector<double> p_out(n), sp_out(n);
+      std::vector<V3> l_out(n), sl_out(n);
+      for (size_t c = 0; c < n; ++c) {
+        const double p_nncg = pj[c] + beta * s_p[c];
+        if (p_nncg < 0.0) {
+          p_out[c] = pj[c];
+          sp_out[c] = 0.0;
+        } else {
+          p_out[c] = p_nncg;
+          sp_out[c] = beta * s_p[c] - gp[c];
+        }
+        // the friction cone of the iterate before this update (:452-467)
+        const V3 l_nncg = lj[c] + beta * s_l[c];
+        const V3 tp = mul(cells[c].tproj, l_nncg);
+        const double lmax = kFrictionCoefficient * p[c] * norm(cells[c].f_a);
+        if (norm(tp) > lmax) {
+          l_out[c] = lj[c];
+          sl_out[c] = V3{0, 0, 0};
+        } else {
+          l_out[c] = tp;
+          sl_out[c] = beta * s_l[c] - gl[c];
+        }
+      }
+      p = p_out;
+      s_p = sp_out;
+      lambda = l_out;
+      s_l = sl_out;
+    }
+    prev_gp = gpn;
+    prev_gl = gln;
+    accumulate();
+    predict();
+    merits();
+    ++it;
+  }
+  res.iterations = it;
+  accumulate();
+  for (size_t b = 0; b < nb; ++b) {
+    res.force[b] = ef[b];
+    res.torque[b] = et[b];
+    if (commit && boundaries[b].dynamic) {  // add_force_and_torque (rigid_body_motion.rs:156-159)
+      boundaries[b].state.force += ef[b];
+      boundaries[b].state.torque += et[b];
+    }
+  }
+  return res;
+}
+
+// :1440-1453: contact forces first, then every body integrates.
 void VolumeMapBoundary::step_forward_in_time(double dt) {
+  solve_contacts(dt, true);
   for (auto& b : boundaries)
     if (b.dynamic) b.state.step_forward_in_time(dt);
 }

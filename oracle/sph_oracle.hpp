@@ -265,6 +265,11 @@ struct VMBoundary : Boundary {
   bool dynamic = false;
   Serendipity sdf, vm;
   RigidBodyMotion state;
+  // Mesh bounding box in the body frame (trimesh.local_aabb(),
+  // volume_map_boundary.rs:1137-1150); boundaries without one take no part
+  // in rigid-rigid contact.
+  bool has_aabb = false;
+  V3 aabb_center, aabb_half;
   // flattened samples: Normal entries [0, n_normal), viscosity after
   std::vector<V3> spos, svel;
   std::vector<double> svol;
@@ -285,9 +290,23 @@ struct VMBoundary : Boundary {
   V3 velocity_at_point_on_boundary(V3 p) const;
 };
 
+// Result of one rigid-rigid contact solve (volume_map_boundary.rs:186-645).
+struct ContactResult {
+  size_t cells = 0;
+  uint32_t iterations = 0;
+  std::vector<V3> force, torque;  // per boundary, added to the dynamic ones
+};
+
 struct VolumeMapBoundary : BoundaryHandling {
   std::vector<VMBoundary> boundaries;
-  void initialize(double, double) override {}
+  double kernel_support_radius = 0;
+  // Sweep cap of the contact solve; the reference loops until converged.
+  uint32_t contact_iteration_cap = 100000;
+  void initialize(double ksr, double) override { kernel_support_radius = ksr; }
+  // Contact cells, NNCG-accelerated projected Jacobi for the contact
+  // pressures and frictions, and the resulting forces and torques; with
+  // `commit` they are added to the bodies.
+  ContactResult solve_contacts(double dt, bool commit);
   void find_boundary_samples(double search_range, const std::vector<V3>& positions,
                              double spacing) override;
   size_t count() const override { return boundaries.size(); }
