@@ -111,7 +111,40 @@ struct DevField {
 
 struct VMDesc {
   DevField sdf, vm;
-  int body;  // index into the body table, -1 for static
+  int body;                     // index into the body table, -1 for static
+  int has_aabb;                 // 1: takes part in rigid-rigid contact
+  double aabb_c[3], aabb_h[3];  // mesh bounding box in the body frame
+};
+
+// Rigid-rigid contact of volume-map bodies (volume_map_boundary.rs:55-1102).
+// A pair of overlapping world bounding boxes is cut into sub-cells (tasks);
+// a task whose quadrature finds both bodies' solids becomes a contact cell.
+constexpr int kContactQuad = 8;  // Gauss-Legendre points per axis (:57)
+// Sweeps of one contact solve at most; the reference iterates until its
+// merits converge (it only warns beyond 100 sweeps, :63, :163-176).
+constexpr int kContactSweepCap = 10000;
+struct ContactGL {
+  double x[kContactQuad], w[kContactQuad];
+};
+struct ContactPair {
+  int a, b;
+  int n[3];       // sub-cells per axis
+  int first;      // first task of the pair
+  double min[3];  // overlap box corner
+  double cs[3];   // sub-cell size
+};
+struct ContactCell {  // ContactCell after compute_diagonal (:678-697, 835-926)
+  int valid, a, b, pad;
+  double volume, center[3], f_a[3], tau_a[3], f_b[3], tau_b[3], tproj[9], acc_p, acc_f;
+};
+struct ContactState {  // per compacted cell, the solver's iterates
+  double p, s_p, v_err, pj, gp;
+  double lambda[3], s_l[3], v_tang[3], lj[3], gl[3];
+};
+struct ContactScalars {
+  int npairs, ntasks, ncells, iterations;
+  int overflow;  // tasks beyond the capacity were dropped
+  int capped;    // the solve stopped at the sweep cap
 };
 
 // Sample-boundary grid (all sample boundaries of a scene in one sorted set).

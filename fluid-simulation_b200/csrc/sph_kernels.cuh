@@ -1998,4 +1998,567 @@ __global__ void k_step_epilogue(Scalars* sc, int K, int hcap, int solver_loop) {
   sc->max_speed = 0;
 }
 
+// ---------------------------------------------------------------------------
+// Rigid-rigid contact of volume-map bodies (volume_map_boundary.rs:55-1102,
+// 1440-1453), run before the body step. k_contact_tasks cuts the overlap of
+// every pair of world bounding boxes (at least one body dynamic) into
+// sub-cells; k_contact_build evaluates one sub-cell per block, one 8^3
+// Gauss-Legendre point per thread, and reduces the contact cell's volume,
+// center and unit force/torque sensitivities (build_contact_cell and
+// compute_diagonal); k_contact_solve runs the NNCG-accelerated projected
+// Jacobi iteration for all cells in one block and adds the contact forces
+// and torques to the bodies. Everything is f64.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool vm_phi(const VMDesc& D, const Body* bodies, const double p[3], double& phi) {
+  double pl[3] = {p[0], p[1], p[2]};
+  if (D.body >= 0) body_world_to_local(bodies[D.body], p, pl);
+  return ser_function(D.sdf, pl[0], pl[1], pl[2], phi);
+}
+__device__ __forceinline__ bool vm_phi_grad(const VMDesc& D, const Body* bodies, const double p[3], double g[3]) {
+  double pl[3] = {p[0], p[1], p[2]};
+  if (D.body >= 0) body_world_to_local(bodies[D.body], p, pl);
+  if (!ser_gradient(D.sdf, pl[0], pl[1], pl[2], g)) return false;
+  if (D.body >= 0) {
+    double gw[3];
+    qrot(bodies[D.body].q, g, gw);
+    g[0] = gw[0]; g[1] = gw[1]; g[2] = gw[2];
+  }
+  return true;
+}
+
+// cubic_extension_fn and its derivative (:1717-1745): the cubic spline's
+// W(x) / W(0) on (0, h), 1 below and 0 above.
+__device__ __forceinline__ double cubic_ext(double x, double h) {
+  if (x >= h) return 0.;
+  if (x <= 0.) return 1.;
+  const double q = x / h, a = fmax(1. - q, 0.), b = fmax(0.5 - q, 0.);
+  const double c = 16. / 3.14159265358979323846 / (h * h * h);
+  return (c * (a * a * a - 4. * (b * b * b))) / (c * 0.5);
+}
+__device__ __forceinline__ double cubic_ext_derivative(double x, double h) {
+  if (x >= h || x <= 0.) return 0.;
+  const double q = x / h, a = fmax(1. - q, 0.), b = fmax(0.5 - q, 0.);
+  const double alpha = 16. / 3.14159265358979323846;
+  const double c4 = alpha / (h * h * h * h);
+  return (((c4 * x) / x) * (-3. * (a * a) + 12. * (b * b))) / (alpha / (h * h * h) * 0.5);
+}
+
+// World bounding box (BoundaryType::world_aabb, :2122-2151).
+__device__ void vm_world_box(const VMDesc& D, const Body* bodies, double lo[3], double hi[3]) {
+  if (D.body < 0) {
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = D.aabb_c[d] - D.aabb_h[d];
+      hi[d] = D.aabb_c[d] + D.aabb_h[d];
+    }
+    return;
+  }
+  const Body& B = bodies[D.body];
+  double Rm[9], c[3];
+  mat_rot(B.q, Rm);
+  qrot(B.q, D.aabb_c, c);
+  for (int d = 0; d < 3; ++d) {
+    const double he = (fabs(Rm[d * 3]) * D.aabb_h[0] + fabs(Rm[d * 3 + 1]) * D.aabb_h[1]) +
+                      fabs(Rm[d * 3 + 2]) * D.aabb_h[2];
+    const double cw = c[d] + B.com[d];
+    lo[d] = cw - he;
+    hi[d] = cw + he;
+  }
+}
+
+// broad_phase (:70-96) and the task list of generate_contact_cells
+// (:98-117) with subdivide_overlap (:1813-1844); one thread.
+__global__ void k_contact_tasks(const VMDesc* __restrict__ vms, const Body* __restrict__ bodies, int nb,
+                                double target, ContactPair* __restrict__ pairs, ContactScalars* __restrict__ cs,
+                                int task_cap) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int np = 0, nt = 0, overflow = 0;
+  for (int i = 0; i < nb; ++i) {
+    if (!vms[i].has_aabb) continue;
+    double li[3], hi_[3];
+    vm_world_box(vms[i], bodies, li, hi_);
+    for (int j = i + 1; j < nb; ++j) {
+      if (!vms[j].has_aabb) continue;
+      if (vms[i].body < 0 && vms[j].body < 0) continue;
+      double lj[3], hj[3];
+      vm_world_box(vms[j], bodies, lj, hj);
+      bool overlap = true;
+      for (int d = 0; d < 3; ++d) overlap = overlap && li[d] <= hj[d] && hi_[d] >= lj[d];
+      if (!overlap) continue;
+      double mn[3], mx[3];
+      bool inter = true;
+      for (int d = 0; d < 3; ++d) {
+        mn[d] = fmax(li[d], lj[d]);
+        mx[d] = fmin(hi_[d], hj[d]);
+        inter = inter && mn[d] <= mx[d];
+      }
+      if (!inter) continue;
+      ContactPair P;
+      P.a = i;
+      P.b = j;
+      double cnt = 1.0;
+      for (int d = 0; d < 3; ++d) {
+        const double ext = mx[d] - mn[d];
+        const double nd = fmax(ceil(ext / target), 1.0);
+        cnt *= nd;
+        P.n[d] = nd < 1e7 ? (int)nd : 10000000;
+        P.min[d] = mn[d];
+      }
+      if (cnt > (double)(task_cap - nt)) {
+        overflow = 1;
+        continue;
+      }
+      for (int d = 0; d < 3; ++d) P.cs[d] = (mx[d] - mn[d]) / (double)P.n[d];
+      P.first = nt;
+      pairs[np++] = P;
+      nt += P.n[0] * P.n[1] * P.n[2];
+    }
+  }
+  cs->npairs = np;
+  cs->ntasks = nt;
+  cs->ncells = 0;
+  cs->iterations = 0;
+  cs->overflow = overflow;
+  cs->capped = 0;
+}
+
+// build_contact_cell (:700-782) and compute_diagonal (:835-926): block per
+// sub-cell, thread per quadrature point (x slowest, z fastest as
+// quadrature_points orders them).
+constexpr int kContactThreads = kContactQuad * kContactQuad * kContactQuad;
+__global__ void __launch_bounds__(kContactThreads) k_contact_build(
+    const VMDesc* __restrict__ vms, const Body* __restrict__ bodies, const ContactPair* __restrict__ pairs,
+    const ContactScalars* __restrict__ cs, ContactCell* __restrict__ cells, ContactGL gl, double h,
+    const Scalars* __restrict__ sc) {
+  __shared__ double red[kContactThreads / 32][17];
+  __shared__ double tot[17];
+  __shared__ int go;
+  const int ntasks = cs->ntasks, npairs = cs->npairs;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int t = blockIdx.x; t < ntasks; t += gridDim.x) {
+    int pi = 0;
+    while (pi + 1 < npairs && pairs[pi + 1].first <= t) ++pi;
+    const ContactPair P = pairs[pi];
+    const int local = t - P.first;
+    const int idx[3] = {local % P.n[0], (local / P.n[0]) % P.n[1], local / (P.n[0] * P.n[1])};
+    double from[3], dd[3], half[3], center[3];
+    for (int d = 0; d < 3; ++d) {
+      from[d] = P.min[d] + (double)idx[d] * P.cs[d];
+      dd[d] = (from[d] + P.cs[d]) - from[d];
+      half[d] = dd[d] * 0.5;
+      center[d] = from[d] + half[d];
+    }
+    const VMDesc& A = vms[P.a];
+    const VMDesc& B = vms[P.b];
+    if (threadIdx.x == 0) {
+      // pruning (:128-159): both solids within twice the half diagonal
+      const double bound = 2.0 * (sqrt((dd[0] * dd[0] + dd[1] * dd[1]) + dd[2] * dd[2]) * 0.5);
+      double pa, pb;
+      const bool oka = vm_phi(A, bodies, center, pa);
+      const bool okb = vm_phi(B, bodies, center, pb);
+      go = oka && okb && pa - bound < 0. && pb - bound < 0.;
+      if (!go) cells[t].valid = 0;
+    }
+    __syncthreads();
+    if (!go) {
+      __syncthreads();
+      continue;
+    }
+    const int q = threadIdx.x;
+    const int i = q >> 6, j = (q >> 3) & 7, k = q & 7;
+    const double pos[3] = {center[0] + gl.x[i] * half[0], center[1] + gl.x[j] * half[1],
+                           center[2] + gl.x[k] * half[2]};
+    const double w = gl.w[i] * gl.w[j] * gl.w[k] * half[0] * half[1] * half[2];
+    // 0 count, 1 volume, 2-4 x V, 5-7 f_a, 8-10 tau_a, 11-13 f_b, 14-16 tau_b
+    double v[17];
+    for (int c = 0; c < 17; ++c) v[c] = 0.0;
+    double pa, pb, ga[3], gb[3];
+    if (vm_phi(A, bodies, pos, pa) && vm_phi(B, bodies, pos, pb)) {
+      const double sa = cubic_ext(2.0 * pa + h, h), sb = cubic_ext(2.0 * pb + h, h);
+      if (sa > 0.0 && sb > 0.0 && vm_phi_grad(A, bodies, pos, ga) && vm_phi_grad(B, bodies, pos, gb)) {
+        const double spa = 2.0 * cubic_ext_derivative(2.0 * pa + h, h);
+        const double spb = 2.0 * cubic_ext_derivative(2.0 * pb + h, h);
+        const double wg = w * sa * sb, wa = w * spa * sb, wb = w * spb * sa;
+        v[0] = 1.0;
+        v[1] = wg;
+        for (int d = 0; d < 3; ++d) {
+          v[2 + d] = wg * pos[d];
+          v[5 + d] = wa * ga[d];
+          v[11 + d] = wb * gb[d];
+        }
+        if (A.body >= 0) {
+          const double* c = bodies[A.body].com;
+          const double r[3] = {pos[0] - c[0], pos[1] - c[1], pos[2] - c[2]};
+          v[8] = wa * (r[1] * ga[2] - r[2] * ga[1]);
+          v[9] = wa * (r[2] * ga[0] - r[0] * ga[2]);
+          v[10] = wa * (r[0] * ga[1] - r[1] * ga[0]);
+        }
+        if (B.body >= 0) {
+          const double* c = bodies[B.body].com;
+          const double r[3] = {pos[0] - c[0], pos[1] - c[1], pos[2] - c[2]};
+          v[14] = wb * (r[1] * gb[2] - r[2] * gb[1]);
+          v[15] = wb * (r[2] * gb[0] - r[0] * gb[2]);
+          v[16] = wb * (r[0] * gb[1] - r[1] * gb[0]);
+        }
+      }
+    }
+    for (int c = 0; c < 17; ++c) {
+      const double s = warp_sum(v[c]);
+      if (lane == 0) red[warp][c] = s;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      for (int c = 0; c < 17; ++c) {
+        double s = lane < kContactThreads / 32 ? red[lane][c] : 0.0;
+        s = warp_sum(s);
+        if (lane == 0) tot[c] = s;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      ContactCell& C = cells[t];
+      const double vol = tot[1];
+      if (!(vol > 0.0) || tot[0] == 0.0) {
+        C.valid = 0;
+      } else {
+        const double dt = sc->dt;
+        C.valid = 1;
+        C.a = P.a;
+        C.b = P.b;
+        C.volume = vol;
+        for (int d = 0; d < 3; ++d) {
+          C.center[d] = tot[2 + d] / vol;
+          C.f_a[d] = tot[5 + d];
+          C.tau_a[d] = tot[8 + d];
+          C.f_b[d] = tot[11 + d];
+          C.tau_b[d] = tot[14 + d];
+        }
+        const double fn = fmax(sqrt((C.f_a[0] * C.f_a[0] + C.f_a[1] * C.f_a[1]) + C.f_a[2] * C.f_a[2]), 1e-15);
+        const double nrm[3] = {C.f_a[0] / fn, C.f_a[1] / fn, C.f_a[2] / fn};
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) C.tproj[r * 3 + c] = (r == c ? 1.0 : 0.0) - nrm[r] * nrm[c];
+        double acc_p = 0.0, T[9];
+        for (int e = 0; e < 9; ++e) T[e] = 0.0;
+        for (int side = 0; side < 2; ++side) {
+          const VMDesc& D = side ? B : A;
+          if (D.body < 0) continue;
+          const Body& M = bodies[D.body];
+          const double* f = side ? C.f_b : C.f_a;
+          const double* tq = side ? C.tau_b : C.tau_a;
+          const double* I = M.inv_inertia_world;
+          double It[3];
+          for (int r = 0; r < 3; ++r) It[r] = (I[r * 3] * tq[0] + I[r * 3 + 1] * tq[1]) + I[r * 3 + 2] * tq[2];
+          acc_p += ((f[0] * f[0] + f[1] * f[1]) + f[2] * f[2]) / M.mass + ((tq[0] * It[0] + tq[1] * It[1]) + tq[2] * It[2]);
+          // I / m - [r]x I^-1 [r]x with r = center - com
+          const double r[3] = {C.center[0] - M.com[0], C.center[1] - M.com[1], C.center[2] - M.com[2]};
+          const double X[9] = {0.0, -r[2], r[1], r[2], 0.0, -r[0], -r[1], r[0], 0.0};
+          double XI[9], XIX[9];
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+              XI[a * 3 + b] = (X[a * 3] * I[b] + X[a * 3 + 1] * I[3 + b]) + X[a * 3 + 2] * I[6 + b];
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+              XIX[a * 3 + b] = (XI[a * 3] * X[b] + XI[a * 3 + 1] * X[3 + b]) + XI[a * 3 + 2] * X[6 + b];
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) T[a * 3 + b] += (a == b ? 1.0 / M.mass : 0.0) - XIX[a * 3 + b];
+        }
+        C.acc_p = dt * dt * acc_p;
+        double tr = 0.0;
+        for (int a = 0; a < 3; ++a) {
+          const double row = ((dt * C.tproj[a * 3]) * T[a] + (dt * C.tproj[a * 3 + 1]) * T[3 + a]) +
+                             (dt * C.tproj[a * 3 + 2]) * T[6 + a];
+          tr += row;
+        }
+        C.acc_f = 1. / 3. * tr;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ double block_sum_all(double v, double* sh, double* out) {
+  const double t = block_sum(v, sh);
+  if (threadIdx.x == 0) *out = t;
+  __syncthreads();
+  const double r = *out;
+  __syncthreads();
+  return r;
+}
+
+// solve_for_p_c (:186-645) with accumulate_extra_forces (:928-965),
+// compute_trial_velocities (:967-994), predicted_volume_error (:996-1009),
+// predicted_tangential_velocity (:1011-1033), projected_jacobi (:1035-1102)
+// and mean_fischer_burmeister (utilities/mod.rs:27-41); one block of 1024
+// threads, warp b gathering body b's cells. The reference iterates until the
+// merits converge; here at most `sweep_cap` sweeps run (`capped` is set).
+constexpr int kContactSolveThreads = 1024;
+__global__ void __launch_bounds__(kContactSolveThreads) k_contact_solve(
+    Body* __restrict__ bodies, int nb, const ContactCell* __restrict__ cells, ContactScalars* __restrict__ cs,
+    int* __restrict__ cell_idx, ContactState* __restrict__ st, const Scalars* __restrict__ sc, int sweep_cap) {
+  constexpr double kMu = 0.5, kOmega = 0.5, kMinDiag = 1e-35, kTolP = 1e-6, kTolF = 1e-3;
+  __shared__ double sh[32];
+  __shared__ double bc;
+  __shared__ int scan[32];
+  __shared__ int base;
+  __shared__ double ef[kMaxBodies][3], et[kMaxBodies][3], vt[kMaxBodies][3], wt[kMaxBodies][3];
+  __shared__ int nact[kMaxBodies];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthreads = blockDim.x;
+  const double dt = sc->dt;
+  const int ntasks = cs->ntasks;
+  // valid cells in task order
+  if (tid == 0) base = 0;
+  __syncthreads();
+  for (int c0 = 0; c0 < ntasks; c0 += nthreads) {
+    const int t = c0 + tid;
+    const int f = (t < ntasks && cells[t].valid) ? 1 : 0;
+    int x = f;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) scan[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int y = lane < nthreads / 32 ? scan[lane] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int z = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= o) y += z;
+      }
+      scan[lane] = y;
+    }
+    __syncthreads();
+    const int before = (warp ? scan[warp - 1] : 0) + x - f;
+    if (f) cell_idx[base + before] = t;
+    __syncthreads();
+    if (tid == 0) base += scan[nthreads / 32 - 1];
+    __syncthreads();
+  }
+  const int n = base;
+  if (n == 0) {
+    if (tid == 0) cs->ncells = 0;
+    return;
+  }
+  for (int c = tid; c < n; c += nthreads) {
+    ContactState& S = st[c];
+    S.p = S.s_p = S.v_err = S.pj = S.gp = 0.0;
+    for (int d = 0; d < 3; ++d) S.lambda[d] = S.s_l[d] = S.v_tang[d] = S.lj[d] = S.gl[d] = 0.0;
+  }
+  __syncthreads();
+
+  auto accumulate = [&]() {
+    if (warp < nb) {
+      const int b = warp;
+      const bool dyn = bodies[b].dynamic != 0;
+      double f[3] = {0.0, 0.0, 0.0}, tq[3] = {0.0, 0.0, 0.0};
+      for (int c = lane; c < n; c += 32) {
+        const ContactCell& C = cells[cell_idx[c]];
+        const ContactState& S = st[c];
+        if (C.a != b && C.b != b) continue;
+        const bool is_a = C.a == b;
+        const double sgn = is_a ? 1.0 : -1.0;
+        const double* fv = is_a ? C.f_a : C.f_b;
+        const double* tv = is_a ? C.tau_a : C.tau_b;
+        for (int d = 0; d < 3; ++d) f[d] += S.p * fv[d] + sgn * S.lambda[d];
+        if (dyn) {
+          const double* com = bodies[b].com;
+          const double r[3] = {C.center[0] - com[0], C.center[1] - com[1], C.center[2] - com[2]};
+          const double* l = S.lambda;
+          const double cr[3] = {r[1] * l[2] - r[2] * l[1], r[2] * l[0] - r[0] * l[2], r[0] * l[1] - r[1] * l[0]};
+          for (int d = 0; d < 3; ++d) tq[d] += S.p * tv[d] + sgn * cr[d];
+        }
+      }
+      for (int d = 0; d < 3; ++d) {
+        const double fs = warp_sum(f[d]), ts = warp_sum(tq[d]);
+        if (lane == 0) {
+          ef[b][d] = fs;
+          et[b][d] = ts;
+        }
+      }
+    }
+    __syncthreads();
+  };
+  auto predict = [&]() {
+    if (tid < nb) {
+      const Body& M = bodies[tid];
+      if (!M.dynamic) {
+        for (int d = 0; d < 3; ++d) vt[tid][d] = wt[tid][d] = 0.0;
+      } else {
+        double l[3];
+        for (int d = 0; d < 3; ++d) {
+          vt[tid][d] = M.v[d] + dt / M.mass * (M.F[d] + ef[tid][d]);
+          l[d] = M.L[d] + dt * (M.T[d] + et[tid][d]);
+        }
+        const double* I = M.inv_inertia_world;
+        for (int r = 0; r < 3; ++r) wt[tid][r] = (I[r * 3] * l[0] + I[r * 3 + 1] * l[1]) + I[r * 3 + 2] * l[2];
+      }
+    }
+    __syncthreads();
+    for (int c = tid; c < n; c += nthreads) {
+      const ContactCell& C = cells[cell_idx[c]];
+      ContactState& S = st[c];
+      const int a = C.a, b = C.b;
+      auto dot3 = [](const double* x, const double* y) { return (x[0] * y[0] + x[1] * y[1]) + x[2] * y[2]; };
+      S.v_err = -C.volume + dt * (((dot3(vt[a], C.f_a) + dot3(wt[a], C.tau_a)) + dot3(vt[b], C.f_b)) +
+                                  dot3(wt[b], C.tau_b));
+      if (bodies[a].dynamic && bodies[b].dynamic) {
+        double vr[3];
+        const double ra[3] = {C.center[0] - bodies[a].com[0], C.center[1] - bodies[a].com[1],
+                              C.center[2] - bodies[a].com[2]};
+        const double rb[3] = {C.center[0] - bodies[b].com[0], C.center[1] - bodies[b].com[1],
+                              C.center[2] - bodies[b].com[2]};
+        const double* wa = wt[a];
+        const double* wb = wt[b];
+        const double ca[3] = {wa[1] * ra[2] - wa[2] * ra[1], wa[2] * ra[0] - wa[0] * ra[2], wa[0] * ra[1] - wa[1] * ra[0]};
+        const double cb[3] = {wb[1] * rb[2] - wb[2] * rb[1], wb[2] * rb[0] - wb[0] * rb[2], wb[0] * rb[1] - wb[1] * rb[0]};
+        for (int d = 0; d < 3; ++d) vr[d] = ((vt[a][d] + ca[d]) - vt[b][d]) - cb[d];
+        for (int r = 0; r < 3; ++r)
+          S.v_tang[r] = (C.tproj[r * 3] * vr[0] + C.tproj[r * 3 + 1] * vr[1]) + C.tproj[r * 3 + 2] * vr[2];
+      } else {
+        S.v_tang[0] = S.v_tang[1] = S.v_tang[2] = 0.0;
+      }
+    }
+    __syncthreads();
+  };
+  auto norm3 = [](const double* x) { return sqrt((x[0] * x[0] + x[1] * x[1]) + x[2] * x[2]); };
+  auto jacobi = [&]() {
+    if (warp < nb) {
+      int cnt = 0;
+      for (int c = lane; c < n; c += 32) {
+        const ContactCell& C = cells[cell_idx[c]];
+        if ((C.a == warp || C.b == warp) && (st[c].v_err < 0.0 || st[c].p > 0.0)) ++cnt;
+      }
+      for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+      if (lane == 0) nact[warp] = cnt;
+    }
+    __syncthreads();
+    for (int c = tid; c < n; c += nthreads) {
+      const ContactCell& C = cells[cell_idx[c]];
+      ContactState& S = st[c];
+      const double n_max = (double)max(max(nact[C.a], nact[C.b]), 1);
+      const double alpha = kOmega / n_max / fmax(C.acc_p, kMinDiag);
+      S.pj = fmax(S.p - alpha * S.v_err, 0.0);
+      const double lmax = kMu * S.p * norm3(C.f_a);
+      double star[3];
+      const double af = fmax(C.acc_f, kMinDiag);
+      for (int d = 0; d < 3; ++d) star[d] = -S.v_tang[d] / af;
+      const double sn = norm3(star);
+      if (sn > lmax)
+        for (int d = 0; d < 3; ++d) star[d] = lmax * star[d] / sn;
+      double ln[3];
+      for (int d = 0; d < 3; ++d) ln[d] = S.lambda[d] + kOmega / n_max * star[d];
+      const double lnn = norm3(ln);
+      for (int d = 0; d < 3; ++d) S.lj[d] = lnn > lmax ? lmax * ln[d] / lnn : ln[d];
+    }
+    __syncthreads();
+  };
+  auto converged = [&]() {
+    double fp = 0.0, ff = 0.0;
+    for (int c = tid; c < n; c += nthreads) {
+      const ContactCell& C = cells[cell_idx[c]];
+      const ContactState& S = st[c];
+      const double pp = S.p * fmax(C.acc_p, kMinDiag);
+      fp += fabs(pp + S.v_err - sqrt(pp * pp + S.v_err * S.v_err));
+      const double vtn = norm3(S.v_tang);
+      const double dev = fmax(C.acc_f, kMinDiag) * (kMu * S.p * norm3(C.f_a) - norm3(S.lambda));
+      ff += fabs(vtn + dev - sqrt(vtn * vtn + dev * dev));
+    }
+    fp = block_sum_all(fp, sh, &bc);
+    ff = block_sum_all(ff, sh, &bc);
+    return fp / (double)n < kTolP && ff / (double)n < kTolF;
+  };
+
+  accumulate();
+  predict();
+  jacobi();
+  double prev = 0.0;
+  {
+    double g2 = 0.0;
+    for (int c = tid; c < n; c += nthreads) {
+      ContactState& S = st[c];
+      S.gp = -(S.pj - S.p);
+      S.s_p = -S.gp;
+      g2 += S.gp * S.gp;
+      double gl2 = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        S.gl[d] = -(S.lj[d] - S.lambda[d]);
+        S.s_l[d] = -S.gl[d];
+      }
+      gl2 = (S.gl[0] * S.gl[0] + S.gl[1] * S.gl[1]) + S.gl[2] * S.gl[2];
+      g2 += gl2;
+      S.p = S.pj;
+      for (int d = 0; d < 3; ++d) S.lambda[d] = S.lj[d];
+    }
+    prev = block_sum_all(g2, sh, &bc);
+  }
+  accumulate();
+  predict();
+  int it = 0;
+  bool done = converged();
+  while (!done && it < sweep_cap) {
+    jacobi();
+    double g2 = 0.0;
+    for (int c = tid; c < n; c += nthreads) {
+      ContactState& S = st[c];
+      S.gp = -(S.pj - S.p);
+      g2 += S.gp * S.gp;
+      for (int d = 0; d < 3; ++d) S.gl[d] = -(S.lj[d] - S.lambda[d]);
+      g2 += (S.gl[0] * S.gl[0] + S.gl[1] * S.gl[1]) + S.gl[2] * S.gl[2];
+    }
+    const double gsum = block_sum_all(g2, sh, &bc);
+    const double beta = gsum / fmax(prev, DBL_MIN);
+    for (int c = tid; c < n; c += nthreads) {
+      const ContactCell& C = cells[cell_idx[c]];
+      ContactState& S = st[c];
+      if (beta > 1.0) {
+        S.s_p = 0.0;
+        for (int d = 0; d < 3; ++d) S.s_l[d] = 0.0;
+        S.p = S.pj;
+        for (int d = 0; d < 3; ++d) S.lambda[d] = S.lj[d];
+        continue;
+      }
+      // the friction cone of the iterate before this update (:452-467)
+      const double lmax = kMu * S.p * norm3(C.f_a);
+      const double p_nncg = S.pj + beta * S.s_p;
+      if (p_nncg < 0.0) {
+        S.p = S.pj;
+        S.s_p = 0.0;
+      } else {
+        S.p = p_nncg;
+        S.s_p = beta * S.s_p - S.gp;
+      }
+      double ln[3], tp[3];
+      for (int d = 0; d < 3; ++d) ln[d] = S.lj[d] + beta * S.s_l[d];
+      for (int r = 0; r < 3; ++r) tp[r] = (C.tproj[r * 3] * ln[0] + C.tproj[r * 3 + 1] * ln[1]) + C.tproj[r * 3 + 2] * ln[2];
+      if (norm3(tp) > lmax) {
+        for (int d = 0; d < 3; ++d) {
+          S.lambda[d] = S.lj[d];
+          S.s_l[d] = 0.0;
+        }
+      } else {
+        for (int d = 0; d < 3; ++d) {
+          S.lambda[d] = tp[d];
+          S.s_l[d] = beta * S.s_l[d] - S.gl[d];
+        }
+      }
+    }
+    __syncthreads();
+    prev = gsum;
+    accumulate();
+    predict();
+    done = converged();
+    ++it;
+  }
+  accumulate();
+  if (tid < nb && bodies[tid].dynamic) {  // add_force_and_torque (rigid_body_motion.rs:156-159)
+    for (int d = 0; d < 3; ++d) {
+      bodies[tid].F[d] += ef[tid][d];
+      bodies[tid].T[d] += et[tid][d];
+    }
+  }
+  if (tid == 0) {
+    cs->ncells = n;
+    cs->iterations = it;
+    cs->capped = done ? 0 : 1;
+  }
+}
+
 }  // namespace sph

@@ -278,7 +278,10 @@ class System : public SystemBase {
     // boundaries
     if (cfg_.boundary_handling == SPH_STATIC_SAMPLE_BOUNDARY && !h_sample_bid_.empty())
       init_sample_boundaries();
-    if (cfg_.boundary_handling == SPH_VOLUME_MAP_BOUNDARY && !fields_.empty()) init_volume_maps();
+    if (cfg_.boundary_handling == SPH_VOLUME_MAP_BOUNDARY && !fields_.empty()) {
+      init_volume_maps();
+      init_contacts();
+    }
     boundary_kind_ = !h_sample_bid_.empty() ? 1 : (!fields_.empty() ? 2 : 0);
     // scalars
     Scalars s{};
@@ -319,6 +322,7 @@ class System : public SystemBase {
       // integrate happens inside update(mode) fused with the cell keys; the
       // rigid-body step must come between it and the neighbor search, and
       // only needs the time increment, so it is issued first on the stream.
+      issue_contacts();
       if (any_dynamic_) launch("body_step", k_body_step, dim3(1), dim3(32), bodies_d_.p, nbodies_, (const Scalars*)d_sc_.p);
       ++steps_;
       if (cfg_.cfl_time_step) current_time_ += dt_used;
@@ -624,6 +628,8 @@ class System : public SystemBase {
       b += d->bytes();
     b += partials_.bytes() + body_partials_.bytes() + stage_x_.bytes() + stage_v_.bytes();
     b += eval_pos_.bytes() + eval_out_.bytes();
+    b += contact_pairs_.bytes() + contact_cells_.bytes() + contact_state_.bytes() + contact_idx_.bytes() +
+         contact_scalars_.bytes();
     b += bodies_d_.bytes() + snap_bodies_.bytes() + snap_sc_.bytes() + ns_d_.bytes() + vms_.bytes();
     for (const auto& f : fields_) b += f->sdf.bytes() + f->vm.bytes();
     return b;
@@ -634,6 +640,8 @@ class System : public SystemBase {
   struct FieldPair {
     sph_grid_desc sdf_desc, vm_desc;
     DBuf<double> sdf, vm;
+    bool has_aabb = false;  // mesh bounding box (body frame) for rigid-rigid contact
+    double aabb_c[3] = {0, 0, 0}, aabb_h[3] = {0, 0, 0};
   };
   struct ProfEntry {
     double ms = 0;
@@ -693,6 +701,15 @@ class System : public SystemBase {
   DBuf<int> ns_d_;
   std::vector<std::unique_ptr<FieldPair>> fields_;
   DBuf<VMDesc> vms_;
+  // rigid-rigid contact of volume-map bodies
+  bool contact_ = false;
+  int contact_task_cap_ = 0;
+  ContactGL contact_gl_{};
+  DBuf<ContactPair> contact_pairs_;
+  DBuf<ContactCell> contact_cells_;
+  DBuf<ContactState> contact_state_;
+  DBuf<int> contact_idx_;
+  DBuf<ContactScalars> contact_scalars_;
   DBuf<R4<R>> vmx_, vmv_;
   DBuf<uint32_t> vm_near_;  // particles near a volume map this step
   DBuf<float> eval_pos_, eval_out_;  // quantity evaluation positions and values
@@ -1022,6 +1039,84 @@ class System : public SystemBase {
     copy_h2d(xb_.p, cur.data(), ns_);
   }
 
+  void set_volume_map_aabb(int bi, const double* c, const double* hext) override {
+    if (initialized_) throw Error(SPH_ERR_STATE, "bounding boxes are set before initialize");
+    if (bi < 0 || bi >= (int)fields_.size()) throw Error(SPH_ERR_INVALID, "not a volume-map boundary");
+    for (int d = 0; d < 3; ++d)
+      if (!std::isfinite(c[d]) || !std::isfinite(hext[d]) || hext[d] < 0.0)
+        throw Error(SPH_ERR_INVALID, "bad bounding box");
+    FieldPair& f = *fields_[bi];
+    f.has_aabb = true;
+    for (int d = 0; d < 3; ++d) {
+      f.aabb_c[d] = c[d];
+      f.aabb_h[d] = hext[d];
+    }
+  }
+
+  // Contact runs when some pair of boxed boundaries has a dynamic body. Its
+  // task capacity bounds the sub-cells of every such pair: an overlap is no
+  // wider than either box, and a rotated box no wider than twice the norm of
+  // its half extents.
+  void init_contacts() {
+    const int nb = (int)fields_.size();
+    const double target = cfg_.kernel_support_radius * 0.5;  // CONTACT_CELL_SIZE_FACTOR (:60)
+    double total = 0.0;
+    for (int i = 0; i < nb; ++i)
+      for (int j = i + 1; j < nb; ++j) {
+        const FieldPair &a = *fields_[i], &b = *fields_[j];
+        if (!a.has_aabb || !b.has_aabb || (!bodies_[i].dynamic && !bodies_[j].dynamic)) continue;
+        const double ra = 2.0 * std::sqrt(a.aabb_h[0] * a.aabb_h[0] + a.aabb_h[1] * a.aabb_h[1] + a.aabb_h[2] * a.aabb_h[2]);
+        const double rb = 2.0 * std::sqrt(b.aabb_h[0] * b.aabb_h[0] + b.aabb_h[1] * b.aabb_h[1] + b.aabb_h[2] * b.aabb_h[2]);
+        double cnt = 1.0;
+        for (int d = 0; d < 3; ++d) {
+          const double ea = bodies_[i].dynamic ? ra : 2.0 * a.aabb_h[d];
+          const double eb = bodies_[j].dynamic ? rb : 2.0 * b.aabb_h[d];
+          cnt *= std::floor(std::min(ea, eb) / target) + 2.0;
+        }
+        total += cnt;
+      }
+    contact_ = total > 0.0;
+    if (!contact_) return;
+    if (total > 4.0e6) throw Error(SPH_ERR_CAPACITY, "rigid-rigid contact would need more than 4M sub-cells");
+    contact_task_cap_ = (int)total;
+    contact_pairs_.alloc((size_t)kMaxBodies * (kMaxBodies - 1) / 2);
+    contact_cells_.alloc((size_t)contact_task_cap_);
+    contact_state_.alloc((size_t)contact_task_cap_);
+    contact_idx_.alloc((size_t)contact_task_cap_);
+    contact_scalars_.alloc(1);
+    contact_scalars_.zero(stream_);
+    std::vector<double> gx, gw;
+    gauss_legendre_nodes(kContactQuad, gx, gw);
+    for (int k = 0; k < kContactQuad; ++k) {
+      contact_gl_.x[k] = gx[k];
+      contact_gl_.w[k] = gw[k];
+    }
+  }
+
+  // VolumeMapBoundary::step_forward_in_time (volume_map_boundary.rs:1440-1453):
+  // contact forces first; the body step that follows integrates them.
+  void issue_contacts() {
+    if (!contact_) return;
+    const double h = cfg_.kernel_support_radius;
+    launch("contact_tasks", k_contact_tasks, dim3(1), dim3(32), (const VMDesc*)vms_.p, (const Body*)bodies_d_.p,
+           nbodies_, h * 0.5, contact_pairs_.p, contact_scalars_.p, contact_task_cap_);
+    launch("contact_build", k_contact_build, dim3(std::min(contact_task_cap_, 2 * 148)), dim3(kContactThreads),
+           (const VMDesc*)vms_.p, (const Body*)bodies_d_.p, (const ContactPair*)contact_pairs_.p,
+           (const ContactScalars*)contact_scalars_.p, contact_cells_.p, contact_gl_, h, (const Scalars*)d_sc_.p);
+    launch("contact_solve", k_contact_solve, dim3(1), dim3(kContactSolveThreads), bodies_d_.p, nbodies_,
+           (const ContactCell*)contact_cells_.p, contact_scalars_.p, contact_idx_.p, contact_state_.p,
+           (const Scalars*)d_sc_.p, kContactSweepCap);
+  }
+
+  void contact_stats(uint32_t* out) override {
+    ContactScalars c{};
+    if (contact_) c = fetch(contact_scalars_.p, 1)[0];
+    out[0] = (uint32_t)c.ncells;
+    out[1] = (uint32_t)c.iterations;
+    out[2] = (uint32_t)c.overflow;
+    out[3] = (uint32_t)c.capped;
+  }
+
   void init_volume_maps() {
     const int nvm = (int)fields_.size();
     std::vector<VMDesc> h(nvm);
@@ -1040,6 +1135,11 @@ class System : public SystemBase {
       fill(h[b].sdf, fields_[b]->sdf_desc, fields_[b]->sdf.p);
       fill(h[b].vm, fields_[b]->vm_desc, fields_[b]->vm.p);
       h[b].body = bodies_[b].dynamic ? b : -1;
+      h[b].has_aabb = fields_[b]->has_aabb ? 1 : 0;
+      for (int d = 0; d < 3; ++d) {
+        h[b].aabb_c[d] = fields_[b]->aabb_c[d];
+        h[b].aabb_h[d] = fields_[b]->aabb_h[d];
+      }
     }
     vms_.alloc(nvm);
     copy_h2d(vms_.p, h.data(), (size_t)nvm);
@@ -1434,6 +1534,7 @@ class System : public SystemBase {
     cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     capturing_ = true;
     try {
+      issue_contacts();
       if (any_dynamic_)
         launch("body_step", k_body_step, dim3(1), dim3(32), bodies_d_.p, nbodies_, (const Scalars*)d_sc_.p);
       issue_update(cfg_.integration_scheme == SPH_TAKE_PREDICTED ? 1 : 0);
@@ -1718,7 +1819,14 @@ struct sph_system {
   // Replay log for sph_clone: the inputs that built the system.
   struct Fluid { std::vector<double> x, v, m; std::vector<uint32_t> fid; } fluid;
   struct SampleB { std::vector<double> x; bool dyn; sph_rigid_init rigid; };
-  struct VMB { sph_grid_desc sd, vd; std::vector<double> sn, vn; bool dyn; sph_rigid_init rigid; };
+  struct VMB {
+    sph_grid_desc sd, vd;
+    std::vector<double> sn, vn;
+    bool dyn;
+    sph_rigid_init rigid;
+    bool has_aabb = false;
+    double aabb[6] = {0, 0, 0, 0, 0, 0};
+  };
   std::vector<int> order;  // 0 sample, 1 vm
   std::vector<SampleB> samples;
   std::vector<VMB> vms;
@@ -1856,6 +1964,38 @@ int sph_add_volume_map_boundary(sph_system_t* h, const sph_grid_desc* sdf, const
     if (rigid) b.rigid = *rigid;
     h->vms.push_back(std::move(b));
     h->order.push_back(1);
+  });
+}
+
+int sph_set_volume_map_aabb(sph_system_t* h, int bi, const double* center, const double* half_extents) {
+  return guarded([&] {
+    if (!h || !center || !half_extents) throw Error(SPH_ERR_INVALID, "null argument");
+    if (h->initialized) throw Error(SPH_ERR_STATE, "bounding boxes are set before initialize");
+    set_device(h);
+    h->impl->set_volume_map_aabb(bi, center, half_extents);
+    // the replay log of sph_clone: boundary bi is the bi-th volume map
+    int k = -1;
+    for (size_t j = 0, seen = 0; j < h->order.size(); ++j)
+      if (h->order[j] == 1) {
+        if ((int)j == bi) k = (int)seen;
+        ++seen;
+      }
+    if (k >= 0) {
+      h->vms[(size_t)k].has_aabb = true;
+      for (int d = 0; d < 3; ++d) {
+        h->vms[(size_t)k].aabb[d] = center[d];
+        h->vms[(size_t)k].aabb[3 + d] = half_extents[d];
+      }
+    }
+  });
+}
+
+int sph_get_contact_stats(sph_system_t* h, uint32_t* out4) {
+  return guarded([&] {
+    if (!h || !out4) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    h->impl->contact_stats(out4);
   });
 }
 
@@ -2205,8 +2345,10 @@ int sph_clone(const sph_system_t* src, sph_system_t** out) {
         rc = sph_add_sample_boundary(h, s.x.size() / 3, s.x.data(), s.dyn ? &s.rigid : nullptr, nullptr);
       } else {
         const auto& b = src->vms[vi++];
+        int bi = -1;
         rc = sph_add_volume_map_boundary(h, &b.sd, b.sn.data(), &b.vd, b.vn.data(), b.dyn ? &b.rigid : nullptr,
-                                         nullptr);
+                                         &bi);
+        if (rc == SPH_OK && b.has_aabb) rc = sph_set_volume_map_aabb(h, bi, b.aabb, b.aabb + 3);
       }
       if (rc) throw Error(rc, sph_last_error());
     }

@@ -239,6 +239,8 @@ SIGNATURES = {
     "sph_server_get_stats": (C.c_int, [_vp, C.POINTER(SphServerStats)]),
     "sph_server_destroy": (None, [_vp]),
     "sph_get_boundary_positions": (C.c_int, [_vp, C.c_int, _dp]),
+    "sph_set_volume_map_aabb": (C.c_int, [_vp, C.c_int, _dp, _dp]),
+    "sph_get_contact_stats": (C.c_int, [_vp, _u32p]),
     "sph_bytes_get": (C.c_int, [_vp, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(_sz)]),
     "sph_bytes_free": (None, [_vp]),
     "sph_checkpoint_from_view": (C.c_int, [C.POINTER(SphCheckpointView), C.POINTER(_vp)]),

@@ -121,7 +121,7 @@ class Scene:
     velocity: np.ndarray | None = None
     fluid_id: np.ndarray | None = None
     sample_boundaries: list = field(default_factory=list)   # [(positions, RigidInit|None)]
-    volume_maps: list = field(default_factory=list)         # [(sdf, vm, RigidInit|None)]
+    volume_maps: list = field(default_factory=list)         # [(sdf, vm, RigidInit|None[, (center, half)])]
     mesh: tuple | None = None                               # (verts, faces) of the container
     description: str = ""
     container: tuple | None = None                          # box extents of a box container
@@ -193,8 +193,8 @@ def build_system(scene: Scene, precision="f32", device=0, fields=None, extra_par
     s.upload_fluid(scene.position, scene.velocity, scene.mass, scene.fluid_id)
     for pts, rigid in scene.sample_boundaries:
         s.add_sample_boundary(pts, rigid)
-    for sdf, vm, rigid in scene.volume_maps:
-        s.add_volume_map_boundary(sdf, vm, rigid)
+    for sdf, vm, rigid, *aabb in scene.volume_maps:
+        s.add_volume_map_boundary(sdf, vm, rigid, aabb[0] if aabb else None)
     if fields is not None:
         s.add_volume_map_boundary(fields[0], fields[1])
     s.initialize()

@@ -93,7 +93,9 @@ class SceneServer:
         req.num_sample_sets = len(scene.sample_boundaries)
         req.sample_sets = sets
         vsets = (A.SphVolumeMapSet * max(1, len(scene.volume_maps)))()
-        for k, (sdf, vm, rigid) in enumerate(scene.volume_maps):
+        # a request carries no bounding boxes: served volume-map scenes run without
+        # rigid-rigid contact
+        for k, (sdf, vm, rigid, *_) in enumerate(scene.volume_maps):
             d1 = grid_desc(sdf.x_min, sdf.x_max, sdf.dx, sdf.n)
             d2 = grid_desc(vm.x_min, vm.x_max, vm.dx, vm.n)
             keep += [d1, d2]

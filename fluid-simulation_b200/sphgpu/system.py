@@ -161,8 +161,10 @@ class GpuSystem:
         self._boundaries.append(("samples", p.shape[0]))
         return bi.value
 
-    def add_volume_map_boundary(self, sdf, vm, rigid: RigidInit | None = None) -> int:
-        """sdf / vm: objects with x_min, x_max, dx, n, nodes (dense lattice, NaN absent)."""
+    def add_volume_map_boundary(self, sdf, vm, rigid: RigidInit | None = None, aabb=None) -> int:
+        """sdf / vm: objects with x_min, x_max, dx, n, nodes (dense lattice, NaN absent).
+        aabb: (center, half_extents) of the mesh in the body frame; boundaries
+        with one take part in rigid-rigid contact."""
         bi = C.c_int()
         r = C.byref(rigid.to_c()) if rigid is not None else None
         sd = grid_desc(sdf.x_min, sdf.x_max, sdf.dx, sdf.n)
@@ -171,7 +173,18 @@ class GpuSystem:
             self._h, C.byref(sd), np.ascontiguousarray(sdf.nodes, np.float64).ravel(), C.byref(vd),
             np.ascontiguousarray(vm.nodes, np.float64).ravel(), r, C.byref(bi)))
         self._boundaries.append(("volume_map", 0))
+        if aabb is not None:
+            c = np.ascontiguousarray(aabb[0], np.float64).reshape(3)
+            h = np.ascontiguousarray(aabb[1], np.float64).reshape(3)
+            A.check(self._L.sph_set_volume_map_aabb(self._h, bi.value, c, h))
         return bi.value
+
+    def contact_stats(self) -> dict:
+        """Rigid-rigid contact of the last step: cells, solver sweeps, whether
+        sub-cells were dropped for capacity, whether the sweep cap stopped it."""
+        out = np.zeros(4, np.uint32)
+        A.check(self._L.sph_get_contact_stats(self._h, out))
+        return dict(zip(("cells", "sweeps", "overflow", "capped"), out.tolist()))
 
     def initialize(self):
         A.check(self._L.sph_initialize(self._h))

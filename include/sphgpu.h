@@ -190,6 +190,18 @@ int sph_add_volume_map_boundary(sph_system_t* h, const sph_grid_desc* sdf, const
                                 const sph_grid_desc* vm, const double* vm_nodes,
                                 const sph_rigid_init* rigid, int* boundary_index);
 
+/* The mesh's bounding box in the body frame (center, half extents) of
+ * volume-map boundary `bi`, as VolumeMapBoundary keeps it
+ * (volume_map_boundary.rs:1137-1150, 1209-1222). Boundaries with a box take
+ * part in rigid-rigid contact: before each body step, every pair of
+ * overlapping boxes with a dynamic body is cut into contact cells and the
+ * contact pressures and frictions are solved (volume_map_boundary.rs:55-1102,
+ * 1440-1453). Without boxes there is no contact. Call before initialize. */
+int sph_set_volume_map_aabb(sph_system_t* h, int bi, const double* center, const double* half_extents);
+/* Contact cells, solver sweeps, whether sub-cells were dropped for capacity,
+ * and whether the sweep cap (10000) stopped the solve, for the last step. */
+int sph_get_contact_stats(sph_system_t* h, uint32_t* out4);
+
 /* BoundaryHandling::initialize (boundary_handling/mod.rs:62-67) followed by
  * the first update() of System::new_boxed (sph/mod.rs:418-419). */
 int sph_initialize(sph_system_t* h);

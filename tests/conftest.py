@@ -49,11 +49,15 @@ def build_oracle(scene, fields=None):
     import oracle as O
     s = O.OracleSystem(oracle_config(scene))
     s.upload_fluid(scene.position, scene.velocity, scene.mass, scene.fluid_id)
+    boxes = []
     for pts, rigid in scene.sample_boundaries:
         s.add_sample_boundary(pts, None if rigid is None else rigid.to_array32())
-    for sdf, vm, rigid in scene.volume_maps:
+    for sdf, vm, rigid, *aabb in scene.volume_maps:
         s.add_volume_map_boundary(_oracle_field(sdf), _oracle_field(vm),
                                   None if rigid is None else rigid.to_array32())
+        if aabb:
+            s.set_vm_aabb(len(boxes), *aabb[0])
+        boxes.append(bool(aabb))
     if fields is not None:
         s.add_volume_map_boundary(*(_oracle_field(f) for f in fields))
     s.initialize()

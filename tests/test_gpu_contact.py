@@ -1,0 +1,127 @@
+"""Rigid-rigid contact of volume-map bodies on the device against the oracle
+(VolumeMapBoundary::step_forward_in_time, volume_map_boundary.rs:55-1102,
+1440-1453).
+
+Two dynamic balls overlap inside a volume-map box while one slides into the
+other. The fluid sits in the far corner, so the bodies feel only gravity
+and contact. (The container takes part in the broad phase, but as in the
+reference its bounding box ends at its walls while its solid lies outside
+them, so it makes no contact cells.) The f64 engine follows the oracle's
+body states step by step; both solve the same contact problem, in different
+summation orders, to the same merit tolerances, so the states agree to
+1e-5 of their scale. Without bounding boxes there is no contact, and the
+balls fall as the oracle's do. Graph-captured steps reproduce the per-step
+path bit for bit.
+"""
+import numpy as np
+import pytest
+
+from conftest import build_oracle
+
+pytestmark = pytest.mark.gpu
+
+SPACING = 0.02
+
+
+@pytest.fixture(scope="module")
+def A():
+    from sphgpu import _capi
+    _capi.load()
+    return _capi
+
+
+@pytest.fixture(scope="module")
+def fields():
+    from sphgpu import scenes
+    from sphgpu.fields import build_volume_map_fields
+    box = np.array([0.6, 0.32, 0.32])
+    verts = scenes.transform_mesh(scenes.CUBE_VERTICES, scale=tuple(box / 2))
+    container = build_volume_map_fields(verts, scenes.CUBE_FACES_INWARD, 4 * SPACING, 2 * SPACING)
+    bv, bf = scenes.icosphere(2, 0.06)
+    ball = build_volume_map_fields(bv, bf, 4 * SPACING, 2 * SPACING)
+    return {"container": container, "ball": ball, "box_half": box / 2,
+            "ball_aabb": (0.5 * (bv.min(0) + bv.max(0)), 0.5 * (bv.max(0) - bv.min(0)))}
+
+
+def _scene(fields, boxes=True):
+    from sphgpu import scenes
+    from sphgpu.system import RigidInit
+    pos = scenes.lattice_block((6, 6, 6), SPACING, origin=(-0.27, -0.13, -0.13), jitter=0.01, seed=3)
+    sc = scenes.Scene(
+        procedures={"kernel_function": "CubicBSpline3D", "integration_scheme": "EulerCromer",
+                    "pressure_solver": "SESPH", "neighbor_search": "SpatialHashing",
+                    "boundary_handling": "VolumeMapBoundary"},
+        parameters={"rest_density_grid_spacing": SPACING, "kernel_support_radius": 2 * SPACING,
+                    "disable_particles_below": -50.0, "fluid_viscosity": 0.01, "boundary_viscosity": 0.01,
+                    "boundary_pressure_acceleration_weighting": 0.7, "boundary_rest_volume_weighting": 1.0,
+                    "stiffness": 1000.0, "time_increment": 1e-3},
+        cfl_time_step=False, position=pos, mass=np.full(pos.shape[0], 1000.0 * SPACING ** 3))
+    floor = -fields["box_half"][2]
+    mass = 700.0 * 4.0 / 3.0 * np.pi * 0.06 ** 3
+    inertia = np.eye(3) * 0.4 * mass * 0.06 ** 2
+    b1 = RigidInit(mass=mass, inertia_body=inertia, center_of_mass=(0.12, 0.0, floor + 0.08),
+                   orientation=(np.cos(0.1), 0.0, np.sin(0.1), 0.0), linear_velocity=(0.0, 0.0, -0.05))
+    b2 = RigidInit(mass=mass, inertia_body=inertia, center_of_mass=(0.12 - 0.112, 0.01, floor + 0.095),
+                   linear_velocity=(0.2, 0.0, 0.0), angular_velocity=(0.0, 0.0, 1.0))
+    cbox = ((0.0, 0.0, 0.0), tuple(fields["box_half"]))
+    extra = (cbox,) if boxes else ()
+    bextra = (fields["ball_aabb"],) if boxes else ()
+    sc.volume_maps = [(*fields["container"], None, *extra), (*fields["ball"], b1, *bextra),
+                      (*fields["ball"], b2, *bextra)]
+    return sc
+
+
+def _bodies(s):
+    return np.stack([s.rigid_state(bi) for bi in (1, 2)])
+
+
+def _assert_close(g, o):
+    # com, q, v, L; forces are reset by the step
+    for sl, scale in ((slice(0, 3), 0.3), (slice(3, 7), 1.0), (slice(7, 10), 0.5), (slice(10, 13), 1e-4)):
+        err = np.abs(g[:, sl] - o[:, sl]).max()
+        assert err < 1e-5 * (scale + np.abs(o[:, sl]).max()), (sl, err)
+
+
+@pytest.mark.parametrize("boxes", [True, False])
+def test_bodies_follow_the_oracle(A, oracle, fields, boxes):
+    from sphgpu import scenes
+    sc = _scene(fields, boxes)
+    g = scenes.build_system(sc, precision="f64")
+    o = build_oracle(sc)
+    for step in range(6):
+        g.step_forward_in_time(1)
+        o.step(1)
+        _assert_close(_bodies(g), _bodies(o))
+        st = g.contact_stats()
+        if boxes:
+            assert st["cells"] > 0 and st["overflow"] == 0 and st["capped"] == 0, st
+        else:
+            assert st["cells"] == 0
+    g.close()
+
+
+def test_contact_pushes_bodies_apart(A, fields):
+    from sphgpu import scenes
+    with_c = scenes.build_system(_scene(fields, True), precision="f64")
+    without = scenes.build_system(_scene(fields, False), precision="f64")
+    with_c.step_forward_in_time(3)
+    without.step_forward_in_time(3)
+    a, b = _bodies(with_c), _bodies(without)
+    # the struck ball (at +x) is pushed along +x, the sliding one is slowed
+    assert a[0, 7] > b[0, 7] + 0.01
+    assert a[1, 7] < b[1, 7] - 0.01
+    with_c.close()
+    without.close()
+
+
+def test_graph_steps_equal_per_step_with_contact(A, fields):
+    from sphgpu import scenes
+    plain = scenes.build_system(_scene(fields, True))
+    graph = scenes.build_system(_scene(fields, True))
+    graph.set_step_graphs(5)
+    plain.step_forward_in_time(10)
+    graph.step_forward_in_time(10)
+    assert np.array_equal(_bodies(plain), _bodies(graph))
+    assert np.array_equal(plain.download(A.FIELD_POSITION), graph.download(A.FIELD_POSITION))
+    plain.close()
+    graph.close()
