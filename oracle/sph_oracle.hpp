@@ -258,9 +258,8 @@ struct Serendipity {
   bool gradient(V3 p, V3& out) const;
 };
 
-// VolumeMapBoundary per-step sampling (volume_map_boundary.rs:1259-1424).
-// Rigid-rigid contact (volume_map_boundary.rs:70-1102) is not restated; it only
-// acts when bodies touch.
+// VolumeMapBoundary per-step sampling (volume_map_boundary.rs:1259-1424) and
+// rigid-rigid contact (volume_map_boundary.rs:55-1102, solve_contacts below).
 struct VMBoundary : Boundary {
   bool dynamic = false;
   Serendipity sdf, vm;
