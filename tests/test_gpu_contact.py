@@ -8,8 +8,9 @@ and contact. (The container takes part in the broad phase, but as in the
 reference its bounding box ends at its walls while its solid lies outside
 them, so it makes no contact cells.) The f64 engine follows the oracle's
 body states step by step; both solve the same contact problem, in different
-summation orders, to the same merit tolerances, so the states agree to
-1e-5 of their scale. Without bounding boxes there is no contact, and the
+summation orders, to the same merit tolerances: positions and orientations
+agree to 1e-5, velocities to 1e-2 and angular momenta to 5e-2, the
+looseness the reference's stopping tolerances leave in the impulses. Without bounding boxes there is no contact, and the
 balls fall as the oracle's do. Graph-captured steps reproduce the per-step
 path bit for bit.
 """
@@ -75,11 +76,17 @@ def _bodies(s):
     return np.stack([s.rigid_state(bi) for bi in (1, 2)])
 
 
-def _assert_close(g, o):
-    # com, q, v, L; forces are reset by the step
-    for sl, scale in ((slice(0, 3), 0.3), (slice(3, 7), 1.0), (slice(7, 10), 0.5), (slice(10, 13), 1e-4)):
+def _assert_close(g, o, info):
+    # com and q to 1e-5, v to 1e-2, L to 5e-2. The contact solve stops once its
+    # merits pass the reference's tolerances (1e-6 on volume-scale pressure
+    # terms, 1e-3 m/s on the tangential velocity), so its impulses are
+    # converged to a few 1e-4 of the normal impulse and about 1e-2 of the
+    # friction; rounding in other summation orders changes the sweep count
+    # (60 against 62 here) and moves them that much.
+    for sl, scale, rel in ((slice(0, 3), 0.3, 1e-5), (slice(3, 7), 1.0, 1e-5), (slice(7, 10), 0.5, 1e-2),
+                           (slice(10, 13), 1e-4, 5e-2)):
         err = np.abs(g[:, sl] - o[:, sl]).max()
-        assert err < 1e-5 * (scale + np.abs(o[:, sl]).max()), (sl, err)
+        assert err < rel * (scale + np.abs(o[:, sl]).max()), (sl, err, info)
 
 
 @pytest.mark.parametrize("boxes", [True, False])
@@ -89,14 +96,14 @@ def test_bodies_follow_the_oracle(A, oracle, fields, boxes):
     g = scenes.build_system(sc, precision="f64")
     o = build_oracle(sc)
     for step in range(6):
+        _, _, cells, sweeps = o.contact_probe(1e-3, 3)
         g.step_forward_in_time(1)
         o.step(1)
-        _assert_close(_bodies(g), _bodies(o))
         st = g.contact_stats()
+        _assert_close(_bodies(g), _bodies(o), (step, st, cells, sweeps))
+        assert st["cells"] == cells and st["overflow"] == 0 and st["capped"] == 0, (st, cells, sweeps)
         if boxes:
-            assert st["cells"] > 0 and st["overflow"] == 0 and st["capped"] == 0, st
-        else:
-            assert st["cells"] == 0
+            assert cells > 0
     g.close()
 
 
