@@ -76,6 +76,7 @@ def lib():
         "oracle_initialize": (i, [vp]),
         "oracle_set_vm_aabb": (i, [vp, sz, dp, dp]),
         "oracle_contact_probe": (i, [vp, d, dp, dp, C.POINTER(sz), C.POINTER(C.c_uint)]),
+        "oracle_sesph_probe": (i, [dp, sz, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp, dp]),
         "oracle_step": (i, [vp, i]),
         "oracle_num_particles": (sz, [vp]),
         "oracle_measure": (None, [vp, dp]),
@@ -268,6 +269,26 @@ def iisph_probe(pos, vel, mass, volume, dt, h, spacing, gamma_p, omega, eps, bpo
                              None if keep is None else keep.ctypes.data_as(C.c_void_p),
                              float(bvol), int(after), out)
     return out[0], out[1], out[2], int(out[3])
+
+
+def sesph_probe(h, spacing, stiffness, weighting, pos, mass, vol, acc=None, fluid_neighbors=True,
+                boundary_pos=None, boundary_vol=None, body_com=None):
+    """SESPH pressure and pressure acceleration on given fluid volumes (the
+    setting of the reference's SESPH unit tests): (pressure[n], acc[n,3],
+    body force[3], body torque[3])."""
+    pos = _f64(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    acc = np.zeros((n, 3)) if acc is None else _f64(acc).reshape(-1, 3)
+    bp = None if boundary_pos is None else _f64(boundary_pos).reshape(-1, 3)
+    nb = 0 if bp is None else bp.shape[0]
+    bv = None if boundary_vol is None else _f64(boundary_vol)
+    com = None if body_com is None else _f64(body_com)
+    p, a, ft = np.zeros(n), np.zeros(3 * n), np.zeros(6)
+    lib().oracle_sesph_probe(_f64([h, spacing, stiffness, weighting]), n, pos.ravel(), _f64(mass), _f64(vol),
+                             acc.ravel(), 1 if fluid_neighbors else 0, nb,
+                             None if bp is None else bp.ctypes.data, None if bv is None else bv.ctypes.data,
+                             None if com is None else com.ctypes.data, p, a, ft)
+    return p, a.reshape(n, 3), ft[:3], ft[3:]
 
 
 def set_num_threads(n):

@@ -168,6 +168,87 @@ int oracle_contact_probe(void* hh, double dt, double* force, double* torque, siz
   return 0;
 }
 
+// SESPH::solve_and_add_acceleration (sesph.rs:31-67) on given fluid volumes,
+// the shape of the reference's SESPH unit tests
+// (tests/sph/pressure_solver/sesph.rs:309-633). prm = {h, spacing,
+// stiffness, boundary pressure weighting}. Fluid neighbors come from the
+// spatial hashing, or are empty (with_fluid_neighbors = 0); the nb boundary
+// samples (positions, volumes) form one sample boundary, dynamic with its
+// center of mass at body_com when that is given. Writes the pressures, the
+// accelerations (starting from acc) and the body's force and torque.
+int oracle_sesph_probe(const double* prm, size_t n, const double* pos, const double* mass, const double* vol,
+                       const double* acc, int with_fluid_neighbors, size_t nb, const double* bpos,
+                       const double* bvol, const double* body_com, double* p_out, double* acc_out,
+                       double* body_force_torque) {
+  System s;
+  s.solver = Solver::SESPH;
+  SystemParameters& P = s.params;
+  P.kernel_support_radius = prm[0];
+  P.rest_density_grid_spacing = prm[1];
+  P.rest_volume = prm[1] * prm[1] * prm[1];
+  s.sp.stiffness = prm[2];
+  P.boundary_pressure_acceleration_weighting = prm[3];
+  auto sb = std::make_unique<StaticSampleBoundary>();
+  sb->cell_size = prm[0];
+  if (nb) {
+    SampleBoundary b;
+    for (size_t k = 0; k < nb; ++k) {
+      b.xb.push_back(V3{bpos[3 * k], bpos[3 * k + 1], bpos[3 * k + 2]});
+      b.vb.push_back(V3{0, 0, 0});
+      b.vol.push_back(bvol[k]);
+    }
+    b.dynamic = body_com != nullptr;
+    if (b.dynamic) {
+      M3 eye;
+      eye.m[0][0] = eye.m[1][1] = eye.m[2][2] = 1.0;
+      b.state = RigidBodyMotion(1.0, eye, eye, V3{body_com[0], body_com[1], body_com[2]}, Quat{}, V3{}, V3{});
+    }
+    sb->boundaries.push_back(std::move(b));
+  }
+  s.boundary = std::move(sb);
+  Fluid& f = s.fluid;
+  f.num_active = n;
+  f.fluid_id.assign(n, 0);
+  f.origin.assign(n, 0);
+  f.position.resize(n);
+  f.velocity.assign(n, V3{0, 0, 0});
+  f.acceleration.resize(n);
+  f.mass.assign(mass, mass + n);
+  f.volume.assign(vol, vol + n);
+  f.pressure.assign(n, 0.0);
+  for (size_t i = 0; i < n; ++i) {
+    f.position[i] = V3{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    f.acceleration[i] = V3{acc[3 * i], acc[3 * i + 1], acc[3 * i + 2]};
+  }
+  f.resize_slots(0, 0, 0, 0);
+  if (with_fluid_neighbors) {
+    s.ns = SpatialHashing(prm[0]);
+    s.ns.find_samples(prm[0], f.position, f.position, s.fluid_nl);
+  } else {
+    s.fluid_nl.indices.clear();
+    s.fluid_nl.offsets.assign(n + 1, 0);
+  }
+  s.boundary->find_boundary_samples(prm[0], f.position, prm[1]);
+  s.sesph();
+  for (size_t i = 0; i < n; ++i) {
+    p_out[i] = f.pressure[i];
+    acc_out[3 * i] = f.acceleration[i].x;
+    acc_out[3 * i + 1] = f.acceleration[i].y;
+    acc_out[3 * i + 2] = f.acceleration[i].z;
+  }
+  for (int k = 0; k < 6; ++k) body_force_torque[k] = 0.0;
+  if (nb && body_com) {
+    const RigidBodyMotion& m = static_cast<StaticSampleBoundary&>(*s.boundary).boundaries[0].state;
+    const V3 v[2] = {m.force, m.torque};
+    for (int k = 0; k < 2; ++k) {
+      body_force_torque[3 * k] = v[k].x;
+      body_force_torque[3 * k + 1] = v[k].y;
+      body_force_torque[3 * k + 2] = v[k].z;
+    }
+  }
+  return 0;
+}
+
 int oracle_initialize(void* hh) {
   auto* h = (OracleHandle*)hh;
   try {
