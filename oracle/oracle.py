@@ -77,6 +77,7 @@ def lib():
         "oracle_set_vm_aabb": (i, [vp, sz, dp, dp]),
         "oracle_contact_probe": (i, [vp, d, dp, dp, C.POINTER(sz), C.POINTER(C.c_uint)]),
         "oracle_sesph_probe": (i, [dp, sz, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp, dp]),
+        "oracle_nonpressure_probe": (i, [dp, i, sz, dp, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp]),
         "oracle_step": (i, [vp, i]),
         "oracle_num_particles": (sz, [vp]),
         "oracle_measure": (None, [vp, dp]),
@@ -289,6 +290,30 @@ def sesph_probe(h, spacing, stiffness, weighting, pos, mass, vol, acc=None, flui
                              None if bp is None else bp.ctypes.data, None if bv is None else bv.ctypes.data,
                              None if com is None else com.ctypes.data, p, a, ft)
     return p, a.reshape(n, 3), ft[:3], ft[3:]
+
+
+def nonpressure_probe(h, spacing, pos, vel, mass, vol, fluid_viscosity=0.0, boundary_viscosity=0.0,
+                      gravity=None, viscosity=True, acc=None, fluid_neighbors=True, boundary_pos=None,
+                      boundary_vol=None, body_com=None):
+    """Gravity (gravity = "uniform" or a radial center) and/or viscosity
+    accelerations on given fluid arrays: (acc[n,3], body force[3], torque[3])."""
+    pos = _f64(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    acc = np.zeros((n, 3)) if acc is None else _f64(acc).reshape(-1, 3)
+    bp = None if boundary_pos is None else _f64(boundary_pos).reshape(-1, 3)
+    nb = 0 if bp is None else bp.shape[0]
+    bv = None if boundary_vol is None else _f64(boundary_vol)
+    com = None if body_com is None else _f64(body_com)
+    radial = gravity is not None and not isinstance(gravity, str)
+    center = gravity if radial else (0.0, 0.0, 0.0)
+    prm = _f64([h, spacing, fluid_viscosity, boundary_viscosity, 1.0 if radial else 0.0, *center])
+    which = (1 if gravity is not None else 0) | (2 if viscosity else 0)
+    a, ft = np.zeros(3 * n), np.zeros(6)
+    lib().oracle_nonpressure_probe(prm, which, n, pos.ravel(), _f64(vel).reshape(-1), _f64(mass), _f64(vol),
+                                   acc.ravel(), 1 if fluid_neighbors else 0, nb,
+                                   None if bp is None else bp.ctypes.data, None if bv is None else bv.ctypes.data,
+                                   None if com is None else com.ctypes.data, a, ft)
+    return a.reshape(n, 3), ft[:3], ft[3:]
 
 
 def set_num_threads(n):

@@ -168,28 +168,20 @@ int oracle_contact_probe(void* hh, double dt, double* force, double* torque, siz
   return 0;
 }
 
-// SESPH::solve_and_add_acceleration (sesph.rs:31-67) on given fluid volumes,
-// the shape of the reference's SESPH unit tests
-// (tests/sph/pressure_solver/sesph.rs:309-633). prm = {h, spacing,
-// stiffness, boundary pressure weighting}. Fluid neighbors come from the
-// spatial hashing, or are empty (with_fluid_neighbors = 0); the nb boundary
-// samples (positions, volumes) form one sample boundary, dynamic with its
-// center of mass at body_com when that is given. Writes the pressures, the
-// accelerations (starting from acc) and the body's force and torque.
-int oracle_sesph_probe(const double* prm, size_t n, const double* pos, const double* mass, const double* vol,
-                       const double* acc, int with_fluid_neighbors, size_t nb, const double* bpos,
-                       const double* bvol, const double* body_com, double* p_out, double* acc_out,
-                       double* body_force_torque) {
-  System s;
-  s.solver = Solver::SESPH;
+// A System around given fluid arrays for the solver-level probes below (the
+// shape of the reference's solver unit tests): fluid neighbors from the
+// spatial hashing, or none (with_nl = 0); the nb boundary samples
+// (positions, volumes) form one sample boundary, dynamic (unit mass and
+// inertia) with its center of mass at body_com when that is given.
+static void probe_system(System& s, double h, double spacing, size_t n, const double* pos, const double* vel,
+                         const double* mass, const double* vol, const double* acc, int with_nl, size_t nb,
+                         const double* bpos, const double* bvol, const double* body_com) {
   SystemParameters& P = s.params;
-  P.kernel_support_radius = prm[0];
-  P.rest_density_grid_spacing = prm[1];
-  P.rest_volume = prm[1] * prm[1] * prm[1];
-  s.sp.stiffness = prm[2];
-  P.boundary_pressure_acceleration_weighting = prm[3];
+  P.kernel_support_radius = h;
+  P.rest_density_grid_spacing = spacing;
+  P.rest_volume = spacing * spacing * spacing;
   auto sb = std::make_unique<StaticSampleBoundary>();
-  sb->cell_size = prm[0];
+  sb->cell_size = h;
   if (nb) {
     SampleBoundary b;
     for (size_t k = 0; k < nb; ++k) {
@@ -211,41 +203,82 @@ int oracle_sesph_probe(const double* prm, size_t n, const double* pos, const dou
   f.fluid_id.assign(n, 0);
   f.origin.assign(n, 0);
   f.position.resize(n);
-  f.velocity.assign(n, V3{0, 0, 0});
+  f.velocity.resize(n);
   f.acceleration.resize(n);
   f.mass.assign(mass, mass + n);
   f.volume.assign(vol, vol + n);
   f.pressure.assign(n, 0.0);
   for (size_t i = 0; i < n; ++i) {
     f.position[i] = V3{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    f.velocity[i] = vel ? V3{vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]} : V3{0, 0, 0};
     f.acceleration[i] = V3{acc[3 * i], acc[3 * i + 1], acc[3 * i + 2]};
   }
   f.resize_slots(0, 0, 0, 0);
-  if (with_fluid_neighbors) {
-    s.ns = SpatialHashing(prm[0]);
-    s.ns.find_samples(prm[0], f.position, f.position, s.fluid_nl);
+  if (with_nl) {
+    s.ns = SpatialHashing(h);
+    s.ns.find_samples(h, f.position, f.position, s.fluid_nl);
   } else {
     s.fluid_nl.indices.clear();
     s.fluid_nl.offsets.assign(n + 1, 0);
   }
-  s.boundary->find_boundary_samples(prm[0], f.position, prm[1]);
-  s.sesph();
-  for (size_t i = 0; i < n; ++i) {
-    p_out[i] = f.pressure[i];
+  s.boundary->find_boundary_samples(h, f.position, spacing);
+}
+
+static void probe_outputs(System& s, size_t nb, const double* body_com, double* acc_out, double* body_ft) {
+  const Fluid& f = s.fluid;
+  for (size_t i = 0; i < f.len(); ++i) {
     acc_out[3 * i] = f.acceleration[i].x;
     acc_out[3 * i + 1] = f.acceleration[i].y;
     acc_out[3 * i + 2] = f.acceleration[i].z;
   }
-  for (int k = 0; k < 6; ++k) body_force_torque[k] = 0.0;
+  for (int k = 0; k < 6; ++k) body_ft[k] = 0.0;
   if (nb && body_com) {
     const RigidBodyMotion& m = static_cast<StaticSampleBoundary&>(*s.boundary).boundaries[0].state;
     const V3 v[2] = {m.force, m.torque};
     for (int k = 0; k < 2; ++k) {
-      body_force_torque[3 * k] = v[k].x;
-      body_force_torque[3 * k + 1] = v[k].y;
-      body_force_torque[3 * k + 2] = v[k].z;
+      body_ft[3 * k] = v[k].x;
+      body_ft[3 * k + 1] = v[k].y;
+      body_ft[3 * k + 2] = v[k].z;
     }
   }
+}
+
+// SESPH::solve_and_add_acceleration (sesph.rs:31-67) on given fluid volumes
+// (tests/sph/pressure_solver/sesph.rs:309-633). prm = {h, spacing,
+// stiffness, boundary pressure weighting}.
+int oracle_sesph_probe(const double* prm, size_t n, const double* pos, const double* mass, const double* vol,
+                       const double* acc, int with_fluid_neighbors, size_t nb, const double* bpos,
+                       const double* bvol, const double* body_com, double* p_out, double* acc_out,
+                       double* body_force_torque) {
+  System s;
+  s.solver = Solver::SESPH;
+  probe_system(s, prm[0], prm[1], n, pos, nullptr, mass, vol, acc, with_fluid_neighbors, nb, bpos, bvol, body_com);
+  s.sp.stiffness = prm[2];
+  s.params.boundary_pressure_acceleration_weighting = prm[3];
+  s.sesph();
+  for (size_t i = 0; i < n; ++i) p_out[i] = s.fluid.pressure[i];
+  probe_outputs(s, nb, body_com, acc_out, body_force_torque);
+  return 0;
+}
+
+// add_gravity_acceleration and add_viscosity_acceleration
+// (non_pressure_accelerations.rs:64-185) on given fluid arrays
+// (non_pressure_accelerations.rs:473-964 tests). prm = {h, spacing, fluid
+// viscosity, boundary viscosity, gravity mode (0 uniform, 1 radial), center
+// x, y, z}; which: bit 0 gravity, bit 1 viscosity.
+int oracle_nonpressure_probe(const double* prm, int which, size_t n, const double* pos, const double* vel,
+                             const double* mass, const double* vol, const double* acc, int with_fluid_neighbors,
+                             size_t nb, const double* bpos, const double* bvol, const double* body_com,
+                             double* acc_out, double* body_force_torque) {
+  System s;
+  probe_system(s, prm[0], prm[1], n, pos, vel, mass, vol, acc, with_fluid_neighbors, nb, bpos, bvol, body_com);
+  s.params.fluid_viscosity = prm[2];
+  s.params.boundary_viscosity = prm[3];
+  s.params.gravity = prm[4] != 0.0 ? Gravity::Radial : Gravity::Uniform;
+  s.params.gravity_center = V3{prm[5], prm[6], prm[7]};
+  if (which & 1) s.add_gravity_acceleration();
+  if (which & 2) s.add_viscosity_acceleration();
+  probe_outputs(s, nb, body_com, acc_out, body_force_torque);
   return 0;
 }
 

@@ -1,6 +1,7 @@
 """Pins the oracle's pressure solvers to the reference's solver unit tests,
 restated against the oracle (paths under simulation_lib/):
-  SESPH  tests/sph/pressure_solver/sesph.rs:309-633
+  SESPH      tests/sph/pressure_solver/sesph.rs:309-633
+  gravity, viscosity  src/sph/non_pressure_accelerations.rs:473-964
 The tests build the solver's inputs directly (positions, masses and volumes,
 an empty or hashed fluid neighbor list, one boundary sample) and check the
 pressures, the pressure accelerations and the reaction on a dynamic body.
@@ -75,3 +76,107 @@ def test_sesph_boundary_term_reacts_on_a_dynamic_body(oracle):
     assert np.linalg.norm(f - (-force_on_fluid)) < 1e-9
     # applied at the sample: the torque about the center of mass
     assert np.linalg.norm(t - np.cross(bpos - com, f)) < 1e-12
+
+
+# ---- gravity and viscosity (non_pressure_accelerations.rs:473-964) ------------------
+G = 9.81
+
+
+def _np(oracle, pos, vel=None, **kw):
+    pos = np.asarray(pos, np.float64).reshape(-1, 3)
+    n = pos.shape[0]
+    vel = np.zeros((n, 3)) if vel is None else vel
+    return oracle.nonpressure_probe(H, SPACING, pos, vel, kw.pop("mass", np.full(n, 0.5)),
+                                    kw.pop("vol", np.full(n, 0.02)), **kw)
+
+
+def test_radial_gravity_pulls_toward_the_center(oracle):
+    acc, _, _ = _np(oracle, [[2.0, 0, 0]], gravity=(0.0, 0.0, 0.0), viscosity=False)
+    d = np.array([-2.0, 0.0, 0.0])
+    assert np.linalg.norm(acc[0] - G * d / np.sqrt(d @ d + 1e-4)) < 1e-9
+
+
+def test_radial_gravity_adds_onto_the_existing_acceleration(oracle):
+    only, _, _ = _np(oracle, [[1.0, 0, 0]], gravity=(0.0, 0.0, 0.0), viscosity=False)
+    both, _, _ = _np(oracle, [[1.0, 0, 0]], gravity=(0.0, 0.0, 0.0), viscosity=False, acc=[[3.0, -2.0, 1.0]])
+    assert np.linalg.norm(both[0] - (np.array([3.0, -2.0, 1.0]) + only[0])) < 1e-9
+
+
+def test_radial_gravity_is_finite_at_the_center(oracle):
+    acc, _, _ = _np(oracle, [[0.0, 0, 0]], gravity=(0.0, 0.0, 0.0), viscosity=False)
+    assert np.array_equal(acc[0], [0.0, 0.0, 0.0])
+
+
+def test_radial_gravity_acts_on_each_particle(oracle):
+    acc, _, _ = _np(oracle, [[1.0, 0, 0], [0, 2.0, 0]], gravity=(0.0, 0.0, 0.0), viscosity=False)
+    assert acc[0, 0] < 0 and acc[1, 1] < 0
+
+
+def test_radial_gravity_pulls_dynamic_bodies_and_skips_static_ones(oracle):
+    _, f, _ = _np(oracle, [[50.0, 50, 50]], gravity=(0.0, 0.0, 0.0), viscosity=False,
+                  boundary_pos=[[60.0, 60, 60]], boundary_vol=[0.01], body_com=[3.0, 0.0, 0.0])
+    assert f[0] < 0 and abs(f[1]) < 1e-12 and abs(f[2]) < 1e-12
+    _, f, _ = _np(oracle, [[50.0, 50, 50]], gravity=(0.0, 0.0, 0.0), viscosity=False,
+                  boundary_pos=[[60.0, 60, 60]], boundary_vol=[0.01])
+    assert not f.any()
+
+
+def test_uniform_gravity_is_constant(oracle):
+    acc, f, _ = _np(oracle, [[5.0, 0, 0], [-3.0, 7.0, 2.0]], gravity="uniform", viscosity=False,
+                    boundary_pos=[[100.0, 0, 0]], boundary_vol=[0.01], body_com=[100.0, 0.0, 0.0])
+    assert np.array_equal(acc[0], [0.0, 0.0, -G]) and np.array_equal(acc[1], [0.0, 0.0, -G])
+    assert np.array_equal(f, [0.0, 0.0, -G])  # unit body mass
+
+
+def _visc_term(oracle, nu, vol_j, xi, xj, vi, vj):
+    r = np.asarray(xi) - np.asarray(xj)
+    return nu * 2.0 * (3.0 + 2.0) * vol_j * (np.asarray(vi) - np.asarray(vj)) @ r / (
+        r @ r + 0.01 * SPACING ** 2) * _grad(oracle, r)
+
+
+def test_fluid_viscosity_matches_the_formula(oracle):
+    pos = np.array([[0.0, 0, 0], [0.3, 0, 0], [0, 0.3, 0]])
+    vel = np.eye(3)
+    vol = np.array([0.02, 0.025, 0.03])
+    acc, _, _ = _np(oracle, pos, vel, vol=vol, fluid_viscosity=5.0, boundary_viscosity=5.0)
+    for i in range(3):
+        want = sum(_visc_term(oracle, 5.0, vol[j], pos[i], pos[j], vel[i], vel[j]) for j in range(3))
+        assert np.linalg.norm(acc[i] - want) < 1e-9
+
+
+def test_fluid_viscosity_vanishes_for_equal_velocities(oracle):
+    v = np.array([[2.0, -1.0, 0.5]] * 2)
+    acc, _, _ = _np(oracle, [[0.0, 0, 0], [0.3, 0, 0]], v, fluid_viscosity=5.0, boundary_viscosity=5.0)
+    assert np.abs(acc).max() < 1e-12
+
+
+def test_fluid_viscosity_is_linear_in_the_viscosity(oracle):
+    v = np.array([[1.0, 0, 0], [-1.0, 0, 0]])
+    a1, _, _ = _np(oracle, [[0.0, 0, 0], [0.3, 0, 0]], v, fluid_viscosity=2.0, boundary_viscosity=2.0)
+    a2, _, _ = _np(oracle, [[0.0, 0, 0], [0.3, 0, 0]], v, fluid_viscosity=4.0, boundary_viscosity=4.0)
+    assert np.linalg.norm(a2[0] - 2.0 * a1[0]) < 1e-9
+
+
+def test_viscosity_without_neighbors_is_zero(oracle):
+    acc, _, _ = _np(oracle, [[0.0, 0, 0]], [[1.0, 0, 0]], fluid_viscosity=5.0, boundary_viscosity=5.0,
+                    fluid_neighbors=False)
+    assert np.array_equal(acc[0], [0.0, 0.0, 0.0])
+
+
+def test_boundary_viscosity_static_and_dynamic(oracle):
+    bpos = np.array([0.2, 0.0, 0.0])
+    want = _visc_term(oracle, 5.0, 0.01, [0, 0, 0], bpos, [1.0, 0, 0], [0, 0, 0])
+    acc, f, _ = _np(oracle, [[0.0, 0, 0]], [[1.0, 0, 0]], boundary_viscosity=5.0, fluid_neighbors=False,
+                    boundary_pos=[bpos], boundary_vol=[0.01])
+    assert np.linalg.norm(acc[0] - want) < 1e-9 and not f.any()
+    acc, f, t = _np(oracle, [[0.0, 0, 0]], [[1.0, 0, 0]], boundary_viscosity=5.0, fluid_neighbors=False,
+                    boundary_pos=[bpos], boundary_vol=[0.01], body_com=[5.0, 0.0, 0.0])
+    assert np.linalg.norm(f - (-0.5 * acc[0])) < 1e-9
+    assert np.linalg.norm(t - np.cross(bpos - np.array([5.0, 0, 0]), f)) < 1e-12
+
+
+def test_boundary_viscosity_acts_per_particle(oracle):
+    acc, f, _ = _np(oracle, [[0.0, 0, 0], [0.0, 1.0, 0]], [[1.0, 0, 0], [0, 1.0, 0]], boundary_viscosity=5.0,
+                    fluid_neighbors=False, boundary_pos=[[0.2, 0, 0], [0.0, 1.2, 0]], boundary_vol=[0.01, 0.01],
+                    body_com=[10.0, 0.0, 0.0])
+    assert abs(acc[0, 0]) > 1e-12 and abs(acc[1, 1]) > 1e-12
