@@ -78,6 +78,8 @@ def lib():
         "oracle_contact_probe": (i, [vp, d, dp, dp, C.POINTER(sz), C.POINTER(C.c_uint)]),
         "oracle_sesph_probe": (i, [dp, sz, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp, dp]),
         "oracle_nonpressure_probe": (i, [dp, i, sz, dp, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp]),
+        "oracle_iisph_terms_probe": (i, [dp, i, sz, dp, dp, dp, dp, i, sz, vp, vp, dp, dp]),
+        "oracle_iisph_initialize_probe": (i, [sz, dp, dp, d, d, i, dp]),
         "oracle_step": (i, [vp, i]),
         "oracle_num_particles": (sz, [vp]),
         "oracle_measure": (None, [vp, dp]),
@@ -314,6 +316,31 @@ def nonpressure_probe(h, spacing, pos, vel, mass, vol, fluid_viscosity=0.0, boun
                                    None if bp is None else bp.ctypes.data, None if bv is None else bv.ctypes.data,
                                    None if com is None else com.ctypes.data, a, ft)
     return a.reshape(n, 3), ft[:3], ft[3:]
+
+
+def iisph_terms_probe(h, spacing, dt, weighting, which, pos, vel, mass, vol, fluid_neighbors=True,
+                      boundary_pos=None, boundary_vol=None):
+    """IISPH source term (which "vde" or "vp") or diagonal ("diag") on given
+    arrays, vel being the predicted velocities: (s_f[n], a_ff[n])."""
+    pos = _f64(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    bp = None if boundary_pos is None else _f64(boundary_pos).reshape(-1, 3)
+    nb = 0 if bp is None else bp.shape[0]
+    bv = None if boundary_vol is None else _f64(boundary_vol)
+    code = {"vde": 1, "vp": 2, "diag": 4}[which]
+    s_f, a_ff = np.zeros(n), np.zeros(n)
+    lib().oracle_iisph_terms_probe(_f64([h, spacing, dt, weighting]), code, n, pos.ravel(), _f64(vel).reshape(-1),
+                                   _f64(mass), _f64(vol), 1 if fluid_neighbors else 0, nb,
+                                   None if bp is None else bp.ctypes.data, None if bv is None else bv.ctypes.data,
+                                   s_f, a_ff)
+    return s_f, a_ff
+
+
+def iisph_initialize_probe(s_f, a_ff, omega, eps, clamp):
+    s_f, a_ff = _f64(s_f), _f64(a_ff)
+    p = np.zeros(s_f.shape[0])
+    lib().oracle_iisph_initialize_probe(s_f.shape[0], s_f, a_ff, float(omega), float(eps), 1 if clamp else 0, p)
+    return p
 
 
 def set_num_threads(n):

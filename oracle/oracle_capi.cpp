@@ -282,6 +282,49 @@ int oracle_nonpressure_probe(const double* prm, int which, size_t n, const doubl
   return 0;
 }
 
+// IISPH's source terms and diagonal element (iisph.rs:117-342) on given
+// fluid arrays, vel being the solver's predicted velocities
+// (iisph.rs:714-1017 tests). prm = {h, spacing, dt, boundary pressure
+// weighting}; which: 1 set_source_term_vde, 2 set_source_term_vp, 4
+// set_diagonal_element.
+int oracle_iisph_terms_probe(const double* prm, int which, size_t n, const double* pos, const double* vel,
+                             const double* mass, const double* vol, int with_fluid_neighbors, size_t nb,
+                             const double* bpos, const double* bvol, double* s_out, double* a_out) {
+  System s;
+  std::vector<double> acc(3 * n, 0.0);
+  probe_system(s, prm[0], prm[1], n, pos, nullptr, mass, vol, acc.data(), with_fluid_neighbors, nb, bpos, bvol,
+               nullptr);
+  s.params.time_increment = prm[2];
+  s.params.boundary_pressure_acceleration_weighting = prm[3];
+  s.fluid.resize_slots(0, 0, 1, 1);
+  for (size_t i = 0; i < n; ++i) s.fluid.solver_velocity_slots[0][i] = V3{vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]};
+  s.iisph.s_f.assign(n, 0.0);
+  s.iisph.a_ff.assign(n, 0.0);
+  if (which & 1) s.set_source_term_vde();
+  if (which & 2) s.set_source_term_vp();
+  if (which & 4) s.set_diagonal_element();
+  for (size_t i = 0; i < n; ++i) {
+    s_out[i] = s.iisph.s_f[i];
+    a_out[i] = s.iisph.a_ff[i];
+  }
+  return 0;
+}
+
+// IISPH::initialize (iisph.rs:344-376) on given source terms and diagonals.
+int oracle_iisph_initialize_probe(size_t n, const double* s_f, const double* a_ff, double omega, double eps,
+                                  int clamp, double* p_out) {
+  System s;
+  s.fluid.num_active = n;
+  s.fluid.pressure.assign(n, 0.0);
+  s.iisph.s_f.assign(s_f, s_f + n);
+  s.iisph.a_ff.assign(a_ff, a_ff + n);
+  s.sp.relaxation_factor = omega;
+  s.sp.min_diagonal_element = eps;
+  s.iisph_initialize(clamp != 0);
+  for (size_t i = 0; i < n; ++i) p_out[i] = s.fluid.pressure[i];
+  return 0;
+}
+
 int oracle_initialize(void* hh) {
   auto* h = (OracleHandle*)hh;
   try {

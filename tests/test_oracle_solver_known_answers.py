@@ -2,6 +2,7 @@
 restated against the oracle (paths under simulation_lib/):
   SESPH      tests/sph/pressure_solver/sesph.rs:309-633
   gravity, viscosity  src/sph/non_pressure_accelerations.rs:473-964
+  IISPH      src/sph/pressure_solver/iisph.rs:714-1081
 The tests build the solver's inputs directly (positions, masses and volumes,
 an empty or hashed fluid neighbor list, one boundary sample) and check the
 pressures, the pressure accelerations and the reaction on a dynamic body.
@@ -180,3 +181,54 @@ def test_boundary_viscosity_acts_per_particle(oracle):
                     fluid_neighbors=False, boundary_pos=[[0.2, 0, 0], [0.0, 1.2, 0]], boundary_vol=[0.01, 0.01],
                     body_com=[10.0, 0.0, 0.0])
     assert abs(acc[0, 0]) > 1e-12 and abs(acc[1, 1]) > 1e-12
+
+
+# ---- IISPH source terms, diagonal, initialization (pressure_solver/iisph.rs:714-1081) ----
+DT = 0.05
+
+
+def test_iisph_vde_source_term_is_zero_without_neighbors(oracle):
+    s_f, _ = oracle.iisph_terms_probe(H, SPACING, DT, 0.0, "vde", [[0, 0, 0]], [[1.0, 0, 0]], [0.5], [0.02],
+                                      fluid_neighbors=False)
+    assert s_f[0] == 0.0
+
+
+def test_iisph_vde_source_term_matches_the_formula(oracle):
+    pos = np.array([[0.0, 0, 0], [0.3, 0, 0]])
+    vel = np.array([[1.0, 0, 0], [-1.0, 0, 0]])
+    vol = np.array([0.02, 0.02])
+    s_f, _ = oracle.iisph_terms_probe(H, SPACING, DT, 0.0, "vde", pos, vel, [0.5, 0.5], vol)
+    want = -sum(DT * vol[j] * (vel[0] - vel[j]) @ _grad(oracle, pos[0] - pos[j]) for j in range(2))
+    assert abs(s_f[0] - want) < 1e-9
+
+
+def test_iisph_vp_source_term_keeps_the_volume_deviation(oracle):
+    s_f, _ = oracle.iisph_terms_probe(H, SPACING, DT, 0.0, "vp", [[0, 0, 0]], [[0.0, 0, 0]], [0.5], [0.5 * RV],
+                                      fluid_neighbors=False)
+    assert abs(s_f[0] - (1.0 - RV / (0.5 * RV))) < 1e-9
+
+
+def test_iisph_diagonal_is_zero_for_an_isolated_particle(oracle):
+    _, a = oracle.iisph_terms_probe(H, SPACING, DT, 0.0, "diag", [[0, 0, 0]], [[0.0, 0, 0]], [0.5], [RV],
+                                    fluid_neighbors=False)
+    assert a[0] == 0.0
+
+
+def test_iisph_diagonal_with_a_boundary_neighbor(oracle):
+    w, bpos, bvol = 0.5, np.array([0.2, 0.0, 0.0]), 0.01
+    _, a = oracle.iisph_terms_probe(H, SPACING, DT, w, "diag", [[0, 0, 0]], [[0.0, 0, 0]], [0.5], [RV],
+                                    fluid_neighbors=False, boundary_pos=[bpos], boundary_vol=[bvol])
+    sum_b = bvol * _grad(oracle, -bpos)
+    c_f = -RV / 0.5 * (2.0 * w * sum_b)
+    want = DT * DT * (c_f @ sum_b)
+    assert abs(a[0] - want) < 1e-9 and a[0] <= 0.0
+
+
+def test_iisph_initialize_cases(oracle):
+    # near-zero diagonal -> 0; clamped negative -> 0; unclamped negative kept; positive formula
+    assert oracle.iisph_initialize_probe([-5.0], [0.0], 0.5, 1e-6, True)[0] == 0.0
+    assert oracle.iisph_initialize_probe([1.0], [-2.0], 0.5, 1e-9, True)[0] == 0.0
+    p = oracle.iisph_initialize_probe([1.0], [-2.0], 0.5, 1e-9, False)[0]
+    assert abs(p - 0.5 * 1.0 / -2.0) < 1e-9 and p < 0.0
+    p = oracle.iisph_initialize_probe([-1.0], [-2.0], 0.5, 1e-9, True)[0]
+    assert abs(p - 0.5 * -1.0 / -2.0) < 1e-9 and p > 0.0
