@@ -79,6 +79,7 @@ def lib():
         "oracle_sesph_probe": (i, [dp, sz, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp, dp]),
         "oracle_nonpressure_probe": (i, [dp, i, sz, dp, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp]),
         "oracle_iisph_terms_probe": (i, [dp, i, sz, dp, dp, dp, dp, i, sz, vp, vp, dp, dp]),
+        "oracle_splitting_probe": (i, [dp, sz, dp, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp, dp, dp]),
         "oracle_iisph_initialize_probe": (i, [sz, dp, dp, d, d, i, dp]),
         "oracle_step": (i, [vp, i]),
         "oracle_num_particles": (sz, [vp]),
@@ -334,6 +335,26 @@ def iisph_terms_probe(h, spacing, dt, weighting, which, pos, vel, mass, vol, flu
                                    None if bp is None else bp.ctypes.data, None if bv is None else bv.ctypes.data,
                                    s_f, a_ff)
     return s_f, a_ff
+
+
+def splitting_probe(h, spacing, dt, stiffness, weighting, pos, vel, mass, vol=None, acc=None,
+                    fluid_neighbors=True, boundary_pos=None, boundary_vol=None, body_com=None):
+    """SESPHwSplitting on given arrays (the predicted velocities are
+    vel + dt acc): (density_pred[n], pressure[n], acc[n,3], body force, torque)."""
+    pos = _f64(pos).reshape(-1, 3)
+    n = pos.shape[0]
+    vol = np.full(n, spacing ** 3) if vol is None else _f64(vol)
+    acc = np.zeros((n, 3)) if acc is None else _f64(acc).reshape(-1, 3)
+    bp = None if boundary_pos is None else _f64(boundary_pos).reshape(-1, 3)
+    nb = 0 if bp is None else bp.shape[0]
+    bv = None if boundary_vol is None else _f64(boundary_vol)
+    com = None if body_com is None else _f64(body_com)
+    rho, p, a, ft = np.zeros(n), np.zeros(n), np.zeros(3 * n), np.zeros(6)
+    lib().oracle_splitting_probe(_f64([h, spacing, dt, stiffness, weighting]), n, pos.ravel(),
+                                 _f64(vel).reshape(-1), _f64(mass), vol, acc.ravel(), 1 if fluid_neighbors else 0,
+                                 nb, None if bp is None else bp.ctypes.data, None if bv is None else bv.ctypes.data,
+                                 None if com is None else com.ctypes.data, rho, p, a, ft)
+    return rho, p, a.reshape(n, 3), ft[:3], ft[3:]
 
 
 def iisph_initialize_probe(s_f, a_ff, omega, eps, clamp):

@@ -282,6 +282,31 @@ int oracle_nonpressure_probe(const double* prm, int which, size_t n, const doubl
   return 0;
 }
 
+// SESPHwSplitting::solve_and_add_acceleration (sesph_with_splitting.rs:
+// 33-152) on given fluid arrays (sesph_with_splitting.rs:428-660 tests).
+// prm = {h, spacing, dt, stiffness, boundary pressure weighting}. Writes the
+// predicted densities, pressures, accelerations and the body's force and
+// torque.
+int oracle_splitting_probe(const double* prm, size_t n, const double* pos, const double* vel, const double* mass,
+                           const double* vol, const double* acc, int with_fluid_neighbors, size_t nb,
+                           const double* bpos, const double* bvol, const double* body_com, double* rho_out,
+                           double* p_out, double* acc_out, double* body_force_torque) {
+  System s;
+  s.solver = Solver::SESPHwSplitting;
+  probe_system(s, prm[0], prm[1], n, pos, vel, mass, vol, acc, with_fluid_neighbors, nb, bpos, bvol, body_com);
+  s.params.time_increment = prm[2];
+  s.sp.stiffness = prm[3];
+  s.params.boundary_pressure_acceleration_weighting = prm[4];
+  s.fluid.resize_slots(0, 0, 0, 1);
+  s.sesph_w_splitting();
+  for (size_t i = 0; i < n; ++i) {
+    rho_out[i] = s.density_pred[i];
+    p_out[i] = s.fluid.pressure[i];
+  }
+  probe_outputs(s, nb, body_com, acc_out, body_force_torque);
+  return 0;
+}
+
 // IISPH's source terms and diagonal element (iisph.rs:117-342) on given
 // fluid arrays, vel being the solver's predicted velocities
 // (iisph.rs:714-1017 tests). prm = {h, spacing, dt, boundary pressure

@@ -3,6 +3,7 @@ restated against the oracle (paths under simulation_lib/):
   SESPH      tests/sph/pressure_solver/sesph.rs:309-633
   gravity, viscosity  src/sph/non_pressure_accelerations.rs:473-964
   IISPH      src/sph/pressure_solver/iisph.rs:714-1081
+  SESPHwSplitting  src/sph/pressure_solver/sesph_with_splitting.rs:428-660
 The tests build the solver's inputs directly (positions, masses and volumes,
 an empty or hashed fluid neighbor list, one boundary sample) and check the
 pressures, the pressure accelerations and the reaction on a dynamic body.
@@ -232,3 +233,46 @@ def test_iisph_initialize_cases(oracle):
     assert abs(p - 0.5 * 1.0 / -2.0) < 1e-9 and p < 0.0
     p = oracle.iisph_initialize_probe([-1.0], [-2.0], 0.5, 1e-9, True)[0]
     assert abs(p - 0.5 * -1.0 / -2.0) < 1e-9 and p > 0.0
+
+
+# ---- SESPHwSplitting (pressure_solver/sesph_with_splitting.rs:428-660) ----------------
+def test_splitting_predicted_density_of_an_isolated_particle_is_zero(oracle):
+    rho, p, acc, _, _ = oracle.splitting_probe(H, SPACING, DT, 100.0, 0.0, [[0, 0, 0]], [[1.0, 0, 0]], [0.5],
+                                               fluid_neighbors=False, acc=[[0.0, 0.0, -9.81]])
+    # density_pred = 0 -> volume = inf -> max(V0 / inf - 1, 0) = 0
+    assert rho[0] == 0.0 and p[0] == 0.0
+    assert np.array_equal(acc[0], [0.0, 0.0, -9.81])
+
+
+def test_splitting_predicted_density_with_fluid_neighbors(oracle):
+    pos = np.array([[0.0, 0, 0], [0.3, 0, 0]])
+    vel = np.array([[1.0, 0, 0], [-1.0, 0, 0]])
+    mass = np.array([0.5, 0.6])
+    rho, _, _, _, _ = oracle.splitting_probe(H, SPACING, DT, 100.0, 0.0, pos, vel, mass)
+    want = sum(mass[j] * oracle.kernel_function(pos[0] - pos[j], H)
+               + DT * (vel[0] - vel[j]) @ _grad(oracle, pos[0] - pos[j]) for j in range(2))
+    assert abs(rho[0] - want) < 1e-9
+
+
+def test_splitting_predicted_density_with_a_boundary_neighbor(oracle):
+    bpos, bvol = np.array([0.2, 0.0, 0.0]), 0.01
+    rho, _, _, _, _ = oracle.splitting_probe(H, SPACING, DT, 100.0, 0.0, [[0, 0, 0]], [[1.0, 0, 0]], [0.5],
+                                             fluid_neighbors=False, boundary_pos=[bpos], boundary_vol=[bvol])
+    want = bvol * (0.5 / RV) * oracle.kernel_function(-bpos, H) + DT * np.array([1.0, 0, 0]) @ _grad(oracle, -bpos)
+    assert abs(rho[0] - want) < 1e-9
+
+
+def test_splitting_pressures_of_a_compressed_pair(oracle):
+    pos = np.array([[0.0, 0, 0], [0.3, 0, 0]])
+    mass = np.array([0.5, 0.5])
+    rho, p, _, _, _ = oracle.splitting_probe(H, SPACING, DT, 500.0, 0.0, pos, np.zeros((2, 3)), mass)
+    for i in range(2):
+        want_rho = sum(mass[j] * oracle.kernel_function(pos[i] - pos[j], H) for j in range(2))
+        assert abs(p[i] - 500.0 * max(RV / (mass[i] / want_rho) - 1.0, 0.0)) < 1e-9
+
+
+def test_splitting_reaction_on_a_dynamic_body(oracle):
+    _, _, acc, f, _ = oracle.splitting_probe(H, SPACING, DT, 500.0, 1.0, [[0, 0, 0]], [[0.0, 0, 0]], [0.5],
+                                             vol=[0.5 * RV], fluid_neighbors=False, boundary_pos=[[0.2, 0, 0]],
+                                             boundary_vol=[0.01], body_com=[5.0, 0.0, 0.0])
+    assert np.linalg.norm(f - (-0.5 * acc[0])) < 1e-9
