@@ -572,7 +572,23 @@ std::vector<uint8_t> time_step_info_to_bincode(const sph_frame_view& f) {
     if (q < SPH_Q_SPEED || q > SPH_Q_KINETIC_ENERGY) throw Error(SPH_ERR_INVALID, "unknown quantity");
     w.varint((uint64_t)q);  // ScalarQuantity variant index
   };
-  if (f.fluid == SPH_FLUID_SAMPLES) {
+  if (f.fluid == SPH_FLUID_TRIANGLE_MESH) {
+    // TriangleMesh { meshes: Vec<(u32, RenderMesh)>, max_fluid_id, coloring }
+    w.varint(0);
+    const size_t nm = f.meshes ? f.meshes->m.size() : 0;
+    w.varint(nm);
+    for (size_t k = 0; k < nm; ++k) {
+      const SurfaceMeshOut& m = f.meshes->m[k];
+      w.varint(m.fluid_id);
+      w.varint(m.vertices.size() / 6);  // RenderVertex { position, normal }
+      for (double x : m.vertices) w.f64(x);
+      w.vec_u32(m.indices.data(), m.indices.size());
+    }
+    w.varint(f.max_fluid_id);
+    if (f.fluid_coloring != SPH_COLORING_UNIFORM && f.fluid_coloring != SPH_COLORING_ID)
+      throw Error(SPH_ERR_INVALID, "unknown fluid mesh coloring");
+    w.varint(f.fluid_coloring == SPH_COLORING_ID ? 1 : 0);  // FluidMeshColoring
+  } else if (f.fluid == SPH_FLUID_SAMPLES) {
     w.varint(1);
     if (f.n && !f.fluid_positions) throw Error(SPH_ERR_INVALID, "null fluid positions");
     w.vec3_f32(f.fluid_positions, f.n);
@@ -608,7 +624,7 @@ std::vector<uint8_t> time_step_info_to_bincode(const sph_frame_view& f) {
       w.varint(pl.cols);
     }
   } else {
-    throw Error(SPH_ERR_INVALID, "fluid visualization must be Samples or SensorPlane (meshes are not built)");
+    throw Error(SPH_ERR_INVALID, "unknown fluid visualization");
   }
   // BoundaryVisualization::Samples
   w.varint(1);

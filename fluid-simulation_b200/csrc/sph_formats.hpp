@@ -57,8 +57,7 @@ Checkpoint checkpoint_from_ron(const char* text, size_t len);
 std::vector<uint8_t> checkpoint_to_bincode(const Checkpoint& c);
 Checkpoint checkpoint_from_bincode(const uint8_t* data, size_t len);
 
-// TimeStepInfo (render_info.rs:71-81) with the variants that need no
-// triangle meshes.
+// TimeStepInfo (render_info.rs:71-81).
 std::vector<uint8_t> time_step_info_to_bincode(const sph_frame_view& f);
 
 // Rust's `Display` of an f64, the float syntax of RON's writer.

@@ -9,6 +9,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/sphgpu.h"
 
@@ -34,6 +35,13 @@ struct ChunkOutcome {
   bool replayed = false;      // the chunk was redone on the per-step path
 };
 
+// One reconstructed fluid surface: 6 doubles per vertex (position, normal).
+struct SurfaceMeshOut {
+  uint32_t fluid_id = 0;
+  std::vector<double> vertices;
+  std::vector<uint32_t> indices;
+};
+
 class SystemBase {
  public:
   virtual ~SystemBase() = default;
@@ -54,6 +62,7 @@ class SystemBase {
   virtual void fluid_pos(float* out) = 0;
   virtual void quantity(int q, float* out) = 0;
   virtual void quantity_at(int q, size_t n, const float* pos, float* out) = 0;
+  virtual void reconstruct_surfaces(std::vector<SurfaceMeshOut>& out) = 0;
   virtual int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
   virtual int boundary_neighbors(int bi, uint64_t* off, uint32_t* idx, size_t cap, size_t* total) = 0;
   virtual void boundary_volumes(int bi, double* out) = 0;
@@ -92,3 +101,8 @@ class SystemBase {
 SystemBase* create_system(const sph_config& c);
 
 }  // namespace sph
+
+// The C ABI's owned mesh list (sph_reconstruct_surfaces).
+struct sph_meshes {
+  std::vector<sph::SurfaceMeshOut> m;
+};

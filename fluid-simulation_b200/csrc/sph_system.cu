@@ -24,6 +24,7 @@
 #include "sph_formats.hpp"
 #include "sph_host.hpp"
 #include "sph_kernels.cuh"
+#include "sph_surface.cuh"
 
 namespace sph {
 
@@ -479,6 +480,103 @@ class System : public SystemBase {
     cuda_check(cudaStreamSynchronize(stream_), "cudaStreamSynchronize");
   }
 
+  // Fluid::reconstruct_surfaces (fluid.rs:212-347): one mesh per fluid id in
+  // ascending order, each group's rest density from its first particle's mass
+  // (reference index order); groups without triangles are left out.
+  void reconstruct_surfaces(std::vector<SurfaceMeshOut>& out) override {
+    out.clear();
+    if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
+    const size_t n = n_;
+    if (n == 0) return;
+    std::vector<uint32_t> ids(n);
+    fluid_ids(ids.data());
+    std::vector<double> mass(n);
+    download(SPH_FIELD_MASS, mass.data());
+    std::map<uint32_t, double> groups;
+    for (size_t i = 0; i < n; ++i)
+      if (!groups.count(ids[i])) groups[ids[i]] = mass[i];
+    static const SurfaceCases cases = surface_case_table();
+    const double h = cfg_.kernel_support_radius, sp = cfg_.rest_density_grid_spacing;
+    const double V0 = sp * sp * sp, r = 0.5 * sp, cube = 0.75 * r;
+    auto grow = [](auto& buf, size_t cnt) {
+      if (buf.n < cnt) buf.alloc(cnt);
+    };
+    grow(surf_vol_, n);
+    grow(surf_bounds_, 7);
+    const int nb = blocks_for((long long)n);
+    auto blocks = [](long long m) { return dim3((unsigned)((m + kBlock - 1) / kBlock)); };
+    auto scan_u32 = [&](uint32_t* count, long long m, uint32_t* outp) {
+      const long long tiles = (m + kScanTile - 1) / kScanTile;
+      grow(surf_tiles_, (size_t)tiles);
+      launch("surface_scan", k_scan_tiles, dim3((unsigned)tiles), dim3(kBlock), (const uint32_t*)count, (int)m,
+             surf_tiles_.p);
+      launch("surface_scan", k_scan_tile_sums, dim3(1), dim3(1024), surf_tiles_.p, (int)tiles);
+      launch("surface_scan", k_scan_apply, dim3((unsigned)tiles), dim3(kBlock), count, (int)m,
+             (const uint32_t*)surf_tiles_.p, outp);
+    };
+    for (const auto& g : groups) {
+      const uint32_t group = g.first;
+      const double rest_density = g.second / V0;
+      const double m = rest_density * (4.0 / 3.0 * 3.14159265358979323846 * (r * r * r));
+      launch("surface_density", k_surf_density<R>, dim3(nb), dim3(kBlock), (int)n, (const uint32_t*)start_.p,
+             (const R4<R>*)xv_.p, (const uint32_t*)fid_.p, group, m, h, mask_, surf_vol_.p);
+      const unsigned long long init[7] = {~0ull, ~0ull, ~0ull, 0ull, 0ull, 0ull, 0ull};
+      copy_h2d(surf_bounds_.p, init, 7);
+      launch("surface_bounds", k_surf_bounds<R>, dim3(nb), dim3(kBlock), (int)n, (const R4<R>*)xv_.p,
+             (const uint32_t*)fid_.p, group, surf_bounds_.p);
+      std::vector<unsigned long long> bk = fetch(surf_bounds_.p, 7);
+      SurfaceLattice L;
+      L.cube = cube;
+      double npts = 1.0;
+      for (int d = 0; d < 3; ++d) {
+        const double lo = surf_unkey(bk[d]), hi = surf_unkey(bk[3 + d]);
+        const long long a = (long long)std::floor((lo - h) / cube) - 1;
+        const long long b = (long long)std::floor((hi + h) / cube) + 1;
+        L.k0[d] = a;
+        L.n[d] = b - a + 1;
+        npts *= (double)L.n[d];
+      }
+      if (npts > 6.0e8) throw Error(SPH_ERR_CAPACITY, "surface lattice larger than 6e8 points");
+      const long long np = (long long)npts;
+      const long long nc = (L.n[0] - 1) * (L.n[1] - 1) * (L.n[2] - 1);
+      grow(surf_phi_, (size_t)np);
+      grow(surf_flag_, (size_t)(3 * np + 1));
+      grow(surf_vid_, (size_t)(3 * np + 1));
+      grow(surf_tris_, (size_t)(nc + 1));
+      grow(surf_toff_, (size_t)(nc + 1));
+      launch("surface_levelset", k_surf_levelset<R>, blocks(np), dim3(kBlock), L, np, (const uint32_t*)start_.p,
+             (const R4<R>*)xv_.p, (const uint32_t*)fid_.p, group, (const double*)surf_vol_.p, h, mask_,
+             surf_phi_.p);
+      launch("surface_edges", k_surf_edges, blocks(np), dim3(kBlock), L, np, (const double*)surf_phi_.p,
+             surf_flag_.p);
+      cuda_check(cudaMemsetAsync(surf_flag_.p + 3 * np, 0, sizeof(uint32_t), stream_), "cudaMemsetAsync");
+      scan_u32(surf_flag_.p, 3 * np + 1, surf_vid_.p);
+      launch("surface_cells", k_surf_cells, blocks(nc), dim3(kBlock), L, nc, (const double*)surf_phi_.p, cases,
+             surf_tris_.p);
+      cuda_check(cudaMemsetAsync(surf_tris_.p + nc, 0, sizeof(uint32_t), stream_), "cudaMemsetAsync");
+      scan_u32(surf_tris_.p, nc + 1, surf_toff_.p);
+      uint32_t nv = 0, nt = 0;
+      cuda_check(cudaMemcpyAsync(&nv, surf_vid_.p + 3 * np, sizeof nv, cudaMemcpyDeviceToHost, stream_), "D2H");
+      cuda_check(cudaMemcpyAsync(&nt, surf_toff_.p + nc, sizeof nt, cudaMemcpyDeviceToHost, stream_), "D2H");
+      sync();
+      if (nt == 0) continue;
+      grow(surf_vtx_, (size_t)nv * 6);
+      grow(surf_idx_, (size_t)nt * 3);
+      launch("surface_vertices", k_surf_vertices, blocks(3 * np), dim3(kBlock), L, 3 * np,
+             (const double*)surf_phi_.p, (const uint32_t*)surf_vid_.p, surf_vtx_.p);
+      launch("surface_triangles", k_surf_triangles, blocks(nc), dim3(kBlock), L, nc, (const double*)surf_phi_.p,
+             cases, (const uint32_t*)surf_toff_.p, (const uint32_t*)surf_vid_.p, surf_idx_.p);
+      launch("surface_normals", k_surf_normals, blocks(nt), dim3(kBlock), (long long)nt,
+             (const uint32_t*)surf_idx_.p, surf_vtx_.p);
+      launch("surface_normals", k_surf_normalize, blocks(nv), dim3(kBlock), (long long)nv, surf_vtx_.p);
+      SurfaceMeshOut mo;
+      mo.fluid_id = group;
+      mo.vertices = fetch(surf_vtx_.p, (size_t)nv * 6);
+      mo.indices = fetch(surf_idx_.p, (size_t)nt * 3);
+      out.push_back(std::move(mo));
+    }
+  }
+
   int fluid_neighbors(uint64_t* off, uint32_t* idx, size_t cap, size_t* total) override {
     std::vector<uint32_t> ref = fetch(ref_.p, n_), cnt = fetch(ncnt_.p, n_);
     std::vector<uint16_t> nb = fetch(nbr_.p, (size_t)K_ * np_);
@@ -628,6 +726,8 @@ class System : public SystemBase {
       b += d->bytes();
     b += partials_.bytes() + body_partials_.bytes() + stage_x_.bytes() + stage_v_.bytes();
     b += eval_pos_.bytes() + eval_out_.bytes();
+    b += surf_vol_.bytes() + surf_phi_.bytes() + surf_vtx_.bytes() + surf_flag_.bytes() + surf_vid_.bytes() +
+         surf_tris_.bytes() + surf_toff_.bytes() + surf_idx_.bytes() + surf_tiles_.bytes() + surf_bounds_.bytes();
     b += contact_pairs_.bytes() + contact_cells_.bytes() + contact_state_.bytes() + contact_idx_.bytes() +
          contact_scalars_.bytes();
     b += bodies_d_.bytes() + snap_bodies_.bytes() + snap_sc_.bytes() + ns_d_.bytes() + vms_.bytes();
@@ -713,6 +813,10 @@ class System : public SystemBase {
   DBuf<R4<R>> vmx_, vmv_;
   DBuf<uint32_t> vm_near_;  // particles near a volume map this step
   DBuf<float> eval_pos_, eval_out_;  // quantity evaluation positions and values
+  // surface reconstruction scratch (grown on demand, render frames only)
+  DBuf<double> surf_vol_, surf_phi_, surf_vtx_;
+  DBuf<uint32_t> surf_flag_, surf_vid_, surf_tris_, surf_toff_, surf_idx_, surf_tiles_;
+  DBuf<unsigned long long> surf_bounds_;
   // bounding box of the scene (cells chosen from it)
   struct BBox {
     double mn[3], mx[3];
@@ -2271,7 +2375,15 @@ int sph_encode_time_step_info(sph_system_t* h, const sph_frame_selector* sel, sp
     std::vector<uint32_t> ids;
     std::vector<sph_sensor_plane> planes;
     std::vector<std::vector<float>> plane_data;
-    if (sel->fluid == SPH_FLUID_SAMPLES) {
+    sph_meshes meshes;
+    if (sel->fluid == SPH_FLUID_TRIANGLE_MESH) {  // render_info.rs:128-133
+      s->reconstruct_surfaces(meshes.m);
+      f.meshes = &meshes;
+      const size_t n = s->num_particles();
+      std::vector<uint32_t> all(n);
+      if (n) s->fluid_ids(all.data());
+      for (uint32_t id : all) f.max_fluid_id = std::max(f.max_fluid_id, id);
+    } else if (sel->fluid == SPH_FLUID_SAMPLES) {
       const size_t n = s->num_particles();
       pos.resize(3 * n);
       s->fluid_pos(pos.data());
@@ -2322,6 +2434,37 @@ int sph_encode_time_step_info(sph_system_t* h, const sph_frame_selector* sel, sp
     *out = sph::fmt::new_bytes(sph::fmt::time_step_info_to_bincode(f));
   });
 }
+
+int sph_reconstruct_surfaces(sph_system_t* h, sph_meshes_t** out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
+    set_device(h);
+    auto m = std::make_unique<sph_meshes>();
+    h->impl->reconstruct_surfaces(m->m);
+    *out = m.release();
+  });
+}
+int sph_meshes_count(const sph_meshes_t* m, size_t* out) {
+  return guarded([&] {
+    if (!m || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    *out = m->m.size();
+  });
+}
+int sph_meshes_get(const sph_meshes_t* m, size_t k, uint32_t* fluid_id, size_t* nv, const double** vertices,
+                   size_t* ni, const uint32_t** indices) {
+  return guarded([&] {
+    if (!m || !fluid_id || !nv || !vertices || !ni || !indices) throw Error(SPH_ERR_INVALID, "null argument");
+    if (k >= m->m.size()) throw Error(SPH_ERR_INVALID, "mesh index out of range");
+    const sph::SurfaceMeshOut& s = m->m[k];
+    *fluid_id = s.fluid_id;
+    *nv = s.vertices.size() / 6;
+    *vertices = s.vertices.data();
+    *ni = s.indices.size();
+    *indices = s.indices.data();
+  });
+}
+void sph_meshes_free(sph_meshes_t* m) { delete m; }
 
 // Deep copy: rebuild from the recorded inputs, then restore the source's
 // current dynamic state (fluid, rigid bodies, step counter and time).

@@ -128,7 +128,7 @@ class SphServerStats(C.Structure):
 
 # checkpoint / recording formats
 FORMAT_RON, FORMAT_BINCODE = 0, 1
-FLUID_SAMPLES, FLUID_SENSOR_PLANE = 1, 2
+FLUID_TRIANGLE_MESH, FLUID_SAMPLES, FLUID_SENSOR_PLANE = 0, 1, 2
 COLORING_UNIFORM, COLORING_ID, COLORING_QUANTITY = 0, 1, 2
 
 
@@ -162,6 +162,7 @@ class SphFrameView(C.Structure):
         ("num_planes", C.c_size_t), ("planes", C.POINTER(SphSensorPlane)),
         ("boundary_coloring", C.c_int), ("num_boundary_samples", C.c_size_t),
         ("boundary_positions", C.c_void_p), ("boundary_ids", C.c_void_p),
+        ("meshes", C.c_void_p), ("max_fluid_id", C.c_uint32),
     ]
 
 
@@ -240,6 +241,12 @@ SIGNATURES = {
     "sph_server_destroy": (None, [_vp]),
     "sph_get_boundary_positions": (C.c_int, [_vp, C.c_int, _dp]),
     "sph_set_volume_map_aabb": (C.c_int, [_vp, C.c_int, _dp, _dp]),
+    "sph_reconstruct_surfaces": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "sph_meshes_count": (C.c_int, [_vp, C.POINTER(_sz)]),
+    "sph_meshes_get": (C.c_int, [_vp, _sz, C.POINTER(C.c_uint32), C.POINTER(_sz),
+                                 C.POINTER(C.POINTER(C.c_double)), C.POINTER(_sz),
+                                 C.POINTER(C.POINTER(C.c_uint32))]),
+    "sph_meshes_free": (None, [_vp]),
     "sph_get_contact_stats": (C.c_int, [_vp, _u32p]),
     "sph_bytes_get": (C.c_int, [_vp, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(_sz)]),
     "sph_bytes_free": (None, [_vp]),

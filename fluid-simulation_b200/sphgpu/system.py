@@ -332,6 +332,29 @@ class GpuSystem:
         A.check(self._L.sph_get_boundary_positions(self._h, bi, out))
         return out.reshape(-1, 3)
 
+    # ---- surfaces, checkpoints and recording frames ------------------------------
+    def reconstruct_surfaces(self):
+        """Fluid::reconstruct_surfaces (sph/fluid.rs:212-347): [(fluid_id,
+        vertices (n, 6): position and unit normal, indices (3 per triangle))]."""
+        h = C.c_void_p()
+        A.check(self._L.sph_reconstruct_surfaces(self._h, C.byref(h)))
+        try:
+            cnt = C.c_size_t()
+            A.check(self._L.sph_meshes_count(h, C.byref(cnt)))
+            out = []
+            for k in range(cnt.value):
+                fid, nv, ni = C.c_uint32(), C.c_size_t(), C.c_size_t()
+                vp, ip = C.POINTER(C.c_double)(), C.POINTER(C.c_uint32)()
+                A.check(self._L.sph_meshes_get(h, k, C.byref(fid), C.byref(nv), C.byref(vp), C.byref(ni),
+                                               C.byref(ip)))
+                v = np.ctypeslib.as_array(vp, shape=(6 * nv.value,)).reshape(-1, 6).copy() if nv.value else \
+                    np.zeros((0, 6))
+                i = np.ctypeslib.as_array(ip, shape=(ni.value,)).copy() if ni.value else np.zeros(0, np.uint32)
+                out.append((fid.value, v, i))
+            return out
+        finally:
+            self._L.sph_meshes_free(h)
+
     # ---- checkpoints and recording frames ------------------------------------
     def get_checkpoint(self):
         """SystemCheckpoint::from_sph_system (sph/mod.rs:849-856)."""
@@ -356,13 +379,14 @@ class GpuSystem:
     def encode_time_step_info(self, fluid="samples", fluid_coloring="uniform", quantity=A.Q_SPEED,
                               planes=(), boundary_coloring="uniform", render_mesh_ids=None) -> bytes:
         """TimeStepInfo::from_system (render_info.rs:83-92) as bincode bytes.
-        fluid: "samples" or "sensor_plane"; fluid_coloring: "uniform", "id" or
-        "quantity"; planes: [(positions, rows, cols)]; boundary_coloring:
-        "uniform" or "id"."""
+        fluid: "samples", "sensor_plane" or "triangle_mesh"; fluid_coloring:
+        "uniform", "id" or "quantity" (samples); planes: [(positions, rows,
+        cols)]; boundary_coloring: "uniform" or "id"."""
         from .formats import _bytes
         keep = []
         sel = A.SphFrameSelector()
-        sel.fluid = A.FLUID_SAMPLES if fluid == "samples" else A.FLUID_SENSOR_PLANE
+        sel.fluid = {"samples": A.FLUID_SAMPLES, "sensor_plane": A.FLUID_SENSOR_PLANE,
+                     "triangle_mesh": A.FLUID_TRIANGLE_MESH}[fluid]
         sel.fluid_coloring = {"uniform": A.COLORING_UNIFORM, "id": A.COLORING_ID,
                               "quantity": A.COLORING_QUANTITY}[fluid_coloring]
         sel.quantity = int(quantity)

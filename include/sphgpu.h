@@ -505,10 +505,25 @@ int sph_get_checkpoint(sph_system_t* h, sph_checkpoint_t** out);
  * its integration scheme (TakePredicted: 1 each, else none). */
 int sph_restore_checkpoint(sph_system_t* h, const sph_checkpoint_t* c);
 
-/* Recording frames: the TimeStepInfo variants that need no triangle meshes,
- * FluidVisualization::Samples / ::SensorPlane and
+/* Recording frames: TimeStepInfo with FluidVisualization::TriangleMesh
+ * (reconstructed surfaces), ::Samples or ::SensorPlane, and
  * BoundaryVisualization::Samples (render_info.rs:110-245). */
-enum sph_fluid_visualization { SPH_FLUID_SAMPLES = 1, SPH_FLUID_SENSOR_PLANE = 2 };
+enum sph_fluid_visualization {
+  SPH_FLUID_TRIANGLE_MESH = 0, SPH_FLUID_SAMPLES = 1, SPH_FLUID_SENSOR_PLANE = 2
+};
+
+/* Fluid::reconstruct_surfaces (sph/fluid.rs:212-347): one triangle mesh per
+ * fluid id (ascending), each vertex 6 doubles (position, area-weighted unit
+ * normal), from the device state. The surface is the 0.6 level of
+ * phi(x) = sum_i (m / rho_i) W(x - x_i) on a lattice of 0.75 r (r = half the
+ * rest spacing), the method of the third-party splashsurf_lib 0.14.1 that
+ * the reference calls, restated. */
+typedef struct sph_meshes sph_meshes_t;
+int sph_reconstruct_surfaces(sph_system_t* h, sph_meshes_t** out);
+int sph_meshes_count(const sph_meshes_t* m, size_t* out);
+int sph_meshes_get(const sph_meshes_t* m, size_t k, uint32_t* fluid_id, size_t* num_vertices,
+                   const double** vertices, size_t* num_indices, const uint32_t** indices);
+void sph_meshes_free(sph_meshes_t* m);
 enum sph_sample_coloring { SPH_COLORING_UNIFORM = 0, SPH_COLORING_ID = 1, SPH_COLORING_QUANTITY = 2 };
 
 typedef struct sph_sensor_plane {  /* SensorPlaneData (render_info.rs:196-202) */
@@ -520,7 +535,8 @@ typedef struct sph_sensor_plane {  /* SensorPlaneData (render_info.rs:196-202) *
 /* What a frame shows (the selector TimeStepInfo::from_system takes). */
 typedef struct sph_frame_selector {
   int fluid;                       /* sph_fluid_visualization */
-  int fluid_coloring;              /* Samples: UNIFORM, ID (fluid id) or QUANTITY */
+  int fluid_coloring;              /* Samples: UNIFORM, ID (fluid id) or QUANTITY;
+                                      TriangleMesh: UNIFORM or ID */
   int quantity;                    /* sph_quantity for QUANTITY and SENSOR_PLANE */
   size_t num_planes;
   const sph_sensor_plane* planes;  /* positions, rows, cols (data unused) */
@@ -543,6 +559,8 @@ typedef struct sph_frame_view {
   size_t num_boundary_samples;
   const float* boundary_positions; /* 3 * num_boundary_samples */
   const uint32_t* boundary_ids;    /* per sample, ID coloring */
+  const sph_meshes_t* meshes;      /* TriangleMesh */
+  uint32_t max_fluid_id;           /* TriangleMesh: the largest fluid id */
 } sph_frame_view;
 
 /* TimeStepInfo -> bincode bytes (render_info.rs:101-106). */

@@ -79,6 +79,13 @@ def lib():
         "oracle_sesph_probe": (i, [dp, sz, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp, dp]),
         "oracle_nonpressure_probe": (i, [dp, i, sz, dp, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp]),
         "oracle_iisph_terms_probe": (i, [dp, i, sz, dp, dp, dp, dp, i, sz, vp, vp, dp, dp]),
+        "oracle_surfaces_from": (vp, [sz, dp, u32p, dp, d, d, d]),
+        "oracle_surfaces": (vp, [vp]),
+        "oracle_surfaces_count": (sz, [vp]),
+        "oracle_surface_sizes": (None, [vp, sz, C.POINTER(C.c_uint32), C.POINTER(sz), C.POINTER(sz)]),
+        "oracle_surface_copy": (None, [vp, sz, dp, dp, u32p]),
+        "oracle_surfaces_free": (None, [vp]),
+        "oracle_surface_grid": (None, [sz, dp, d, d, i64p, i64p]),
         "oracle_splitting_probe": (i, [dp, sz, dp, dp, dp, dp, dp, i, sz, vp, vp, vp, dp, dp, dp, dp]),
         "oracle_iisph_initialize_probe": (i, [sz, dp, dp, d, d, i, dp]),
         "oracle_step": (i, [vp, i]),
@@ -337,6 +344,39 @@ def iisph_terms_probe(h, spacing, dt, weighting, which, pos, vel, mass, vol, flu
     return s_f, a_ff
 
 
+def _meshes(m):
+    L = lib()
+    try:
+        out = []
+        for k in range(L.oracle_surfaces_count(m)):
+            fid, nv, ni = C.c_uint32(), C.c_size_t(), C.c_size_t()
+            L.oracle_surface_sizes(m, k, C.byref(fid), C.byref(nv), C.byref(ni))
+            pos, nrm = np.zeros(3 * nv.value), np.zeros(3 * nv.value)
+            idx = np.zeros(max(ni.value, 1), np.uint32)
+            L.oracle_surface_copy(m, k, pos, nrm, idx)
+            out.append((fid.value, pos.reshape(-1, 3), nrm.reshape(-1, 3), idx[:ni.value]))
+        return out
+    finally:
+        L.oracle_surfaces_free(m)
+
+
+def reconstruct_surfaces(positions, fluid_ids, masses, spacing, rest_volume, h):
+    """Fluid::reconstruct_surfaces on given particles: [(fluid_id, positions,
+    normals, indices)] in ascending fluid id."""
+    pos = _f64(positions).reshape(-1, 3)
+    n = pos.shape[0]
+    ids = np.ascontiguousarray(fluid_ids, np.uint32).reshape(n)
+    return _meshes(lib().oracle_surfaces_from(n, pos.ravel(), ids, _f64(masses).reshape(n), float(spacing),
+                                              float(rest_volume), float(h)))
+
+
+def surface_grid(positions, h, cube):
+    pos = _f64(positions).reshape(-1, 3)
+    k0, n = np.zeros(3, np.int64), np.zeros(3, np.int64)
+    lib().oracle_surface_grid(pos.shape[0], pos.ravel(), float(h), float(cube), k0, n)
+    return k0, n
+
+
 def splitting_probe(h, spacing, dt, stiffness, weighting, pos, vel, mass, vol=None, acc=None,
                     fluid_neighbors=True, boundary_pos=None, boundary_vol=None, body_com=None):
     """SESPHwSplitting on given arrays (the predicted velocities are
@@ -428,6 +468,10 @@ class OracleSystem:
         """Body-frame mesh bounding box of volume-map boundary `bi` (enables
         its rigid-rigid contact)."""
         assert lib().oracle_set_vm_aabb(self.h, int(bi), _f64(center), _f64(half_extents)) == 0
+
+    def reconstruct_surfaces(self):
+        """Fluid::reconstruct_surfaces on the current fluid."""
+        return _meshes(lib().oracle_surfaces(self.h))
 
     def contact_probe(self, dt, nb):
         """One contact solve on the current state, not applied:

@@ -350,6 +350,51 @@ int oracle_iisph_initialize_probe(size_t n, const double* s_f, const double* a_f
   return 0;
 }
 
+// Fluid::reconstruct_surfaces (fluid.rs:212-347) on n particles given as
+// positions (3n), fluid ids and masses; returns an owned mesh list.
+void* oracle_surfaces_from(size_t n, const double* pos, const uint32_t* ids, const double* mass, double spacing,
+                           double rest_volume, double h) {
+  Fluid f;
+  f.num_active = n;
+  f.position.resize(n);
+  for (size_t i = 0; i < n; ++i) f.position[i] = V3{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  f.fluid_id.assign(ids, ids + n);
+  f.mass.assign(mass, mass + n);
+  return new std::vector<SurfaceMesh>(reconstruct_surfaces(f, spacing, rest_volume, h));
+}
+// The same on an oracle system's current fluid.
+void* oracle_surfaces(void* hh) {
+  System& s = ((OracleHandle*)hh)->sys;
+  return new std::vector<SurfaceMesh>(reconstruct_surfaces(s.fluid, s.params.rest_density_grid_spacing,
+                                                           s.params.rest_volume, s.params.kernel_support_radius));
+}
+size_t oracle_surfaces_count(void* m) { return ((std::vector<SurfaceMesh>*)m)->size(); }
+void oracle_surface_sizes(void* m, size_t k, uint32_t* id, size_t* nv, size_t* ni) {
+  const SurfaceMesh& s = (*(std::vector<SurfaceMesh>*)m)[k];
+  *id = s.fluid_id;
+  *nv = s.position.size();
+  *ni = s.indices.size();
+}
+void oracle_surface_copy(void* m, size_t k, double* pos, double* nrm, uint32_t* idx) {
+  const SurfaceMesh& s = (*(std::vector<SurfaceMesh>*)m)[k];
+  for (size_t v = 0; v < s.position.size(); ++v) {
+    pos[3 * v] = s.position[v].x; pos[3 * v + 1] = s.position[v].y; pos[3 * v + 2] = s.position[v].z;
+    nrm[3 * v] = s.normal[v].x; nrm[3 * v + 1] = s.normal[v].y; nrm[3 * v + 2] = s.normal[v].z;
+  }
+  for (size_t t = 0; t < s.indices.size(); ++t) idx[t] = s.indices[t];
+}
+void oracle_surfaces_free(void* m) { delete (std::vector<SurfaceMesh>*)m; }
+// The marching-cubes lattice of a point set: k0[3], n[3], cube.
+void oracle_surface_grid(size_t n, const double* pos, double h, double cube, long long* k0, long long* np) {
+  std::vector<V3> p(n);
+  for (size_t i = 0; i < n; ++i) p[i] = V3{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  SurfaceGrid g = surface_grid(p, h, cube);
+  for (int d = 0; d < 3; ++d) {
+    k0[d] = g.k0[d];
+    np[d] = g.n[d];
+  }
+}
+
 int oracle_initialize(void* hh) {
   auto* h = (OracleHandle*)hh;
   try {

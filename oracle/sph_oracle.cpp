@@ -1723,4 +1723,224 @@ void System::iisph_w_ost() {
   std::swap(fluid.integrator_velocity_slots[0], fluid.solver_velocity_slots[0]);
 }
 
+
+// ---------------------------------------------------------------------------
+// Surface reconstruction (fluid.rs:212-347; splashsurf_lib 0.14.1 restated)
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr double kIsoSurfaceThreshold = 0.6;  // fluid.rs:265
+
+// Cube corners c = bx + 2 by + 4 bz; local edge e = 4 * dir + rank of its
+// lower corner among the corners whose bit `dir` is 0.
+int corner_bit(int c, int d) { return (c >> d) & 1; }
+int edge_of(int a, int b) {
+  const int x = a ^ b;
+  const int d = x == 1 ? 0 : (x == 2 ? 1 : 2);
+  const int lo = a < b ? a : b;
+  int rank = 0;
+  for (int c = 0; c < lo; ++c)
+    if (!corner_bit(c, d)) ++rank;
+  return 4 * d + rank;
+}
+int edge_lower_corner(int e) {
+  const int d = e / 4;
+  int rank = e % 4;
+  for (int c = 0; c < 8; ++c)
+    if (!corner_bit(c, d) && rank-- == 0) return c;
+  return -1;
+}
+
+// The six faces as corner cycles, counter-clockwise seen from outside.
+struct FaceCycles {
+  int c[6][4];
+  FaceCycles() {
+    int f = 0;
+    for (int a = 0; a < 3; ++a)
+      for (int s = 0; s < 2; ++s, ++f) {
+        const int u = (a + 1) % 3, v = (a + 2) % 3;
+        const int uv[4][2] = {{0, 0}, {1, 0}, {1, 1}, {0, 1}};
+        int cyc[4];
+        for (int k = 0; k < 4; ++k) cyc[k] = (s << a) | (uv[k][0] << u) | (uv[k][1] << v);
+        // (p1 - p0) x (p2 - p1) is +e_a for this u, v order; outward is (2s - 1) e_a
+        const bool ccw = s == 1;
+        for (int k = 0; k < 4; ++k) c[f][k] = ccw ? cyc[k] : cyc[3 - k];
+      }
+  }
+};
+const FaceCycles kFaces;
+
+// Polygons of one cell (lists of local edges) for the corners' inside flags:
+// on every face each run of inside corners gives a segment from the edge
+// where the cycle enters the run to the edge where it leaves it (so a face
+// with two diagonal inside corners keeps them apart), and the segments chain
+// into closed loops through the edges they share.
+std::vector<std::vector<int>> cell_polygons(const bool inside[8]) {
+  int next[12];
+  bool has[12] = {false};
+  for (int f = 0; f < 6; ++f) {
+    int cross[4], type[4], nc = 0;  // type 1 entering, 0 leaving
+    for (int k = 0; k < 4; ++k) {
+      const int a = kFaces.c[f][k], b = kFaces.c[f][(k + 1) % 4];
+      if (inside[a] != inside[b]) {
+        cross[nc] = edge_of(a, b);
+        type[nc] = inside[b] ? 1 : 0;
+        ++nc;
+      }
+    }
+    for (int k = 0; k < nc; ++k)
+      if (type[k] == 1) {
+        const int x = cross[(k + 1) % nc];
+        next[cross[k]] = x;
+        has[cross[k]] = true;
+      }
+  }
+  std::vector<std::vector<int>> loops;
+  bool used[12] = {false};
+  for (int e = 0; e < 12; ++e) {
+    if (!has[e] || used[e]) continue;
+    std::vector<int> loop;
+    int cur = e;
+    while (!used[cur]) {
+      used[cur] = true;
+      loop.push_back(cur);
+      cur = next[cur];
+    }
+    loops.push_back(loop);
+  }
+  return loops;
+}
+
+}  // namespace
+
+SurfaceGrid surface_grid(const std::vector<V3>& positions, double h, double cube) {
+  SurfaceGrid g;
+  g.cube = cube;
+  V3 lo{std::numeric_limits<double>::infinity(), std::numeric_limits<double>::infinity(),
+        std::numeric_limits<double>::infinity()};
+  V3 hi{-lo.x, -lo.y, -lo.z};
+  for (const V3& p : positions) {
+    lo = V3{std::min(lo.x, p.x), std::min(lo.y, p.y), std::min(lo.z, p.z)};
+    hi = V3{std::max(hi.x, p.x), std::max(hi.y, p.y), std::max(hi.z, p.z)};
+  }
+  const double l[3] = {lo.x, lo.y, lo.z}, u[3] = {hi.x, hi.y, hi.z};
+  for (int d = 0; d < 3; ++d) {
+    const int64_t a = (int64_t)std::floor((l[d] - h) / cube) - 1;
+    const int64_t b = (int64_t)std::floor((u[d] + h) / cube) + 1;
+    g.k0[d] = a;
+    g.n[d] = b - a + 1;
+  }
+  return g;
+}
+
+std::vector<SurfaceMesh> reconstruct_surfaces(const Fluid& fluid, double spacing, double rest_volume, double h) {
+  std::vector<SurfaceMesh> out;
+  // groups by fluid id in ascending order, each with its first particle's mass
+  std::vector<uint32_t> ids;
+  for (size_t i = 0; i < fluid.len(); ++i) ids.push_back(fluid.fluid_id[i]);
+  std::sort(ids.begin(), ids.end());
+  ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+  const double r = 0.5 * spacing, cube = 0.75 * r;
+  for (uint32_t id : ids) {
+    std::vector<V3> pos;
+    double mass0 = 0.0;
+    for (size_t i = 0; i < fluid.len(); ++i)
+      if (fluid.fluid_id[i] == id) {
+        if (pos.empty()) mass0 = fluid.mass[i];
+        pos.push_back(fluid.position[i]);
+      }
+    const double rest_density = mass0 / rest_volume;
+    const double m = rest_density * (4.0 / 3.0 * PI * (r * r * r));
+    // particle densities
+    SpatialHashing ns(h);
+    NeighborList nl;
+    ns.find_samples(h, pos, pos, nl);
+    std::vector<double> vol(pos.size());
+    for (size_t i = 0; i < pos.size(); ++i) {
+      double rho = 0.0;
+      for (const size_t* it = nl.begin(i); it != nl.end(i); ++it) rho += m * kernel_function(pos[i] - pos[*it], h);
+      vol[i] = m / rho;
+    }
+    // level set on the grid points
+    const SurfaceGrid g = surface_grid(pos, h, cube);
+    const int64_t nx = g.n[0], ny = g.n[1], nz = g.n[2];
+    std::vector<V3> pts((size_t)(nx * ny * nz));
+    for (int64_t k = 0; k < nz; ++k)
+      for (int64_t j = 0; j < ny; ++j)
+        for (int64_t i = 0; i < nx; ++i)
+          pts[(size_t)(i + nx * (j + ny * k))] = V3{g.coord(0, i), g.coord(1, j), g.coord(2, k)};
+    NeighborList gl;
+    SpatialHashing gs(h);
+    gs.find_samples(h, pts, pos, gl);
+    std::vector<double> phi(pts.size());
+    for (size_t q = 0; q < pts.size(); ++q) {
+      double s = 0.0;
+      for (const size_t* it = gl.begin(q); it != gl.end(q); ++it) s += vol[*it] * kernel_function(pts[q] - pos[*it], h);
+      phi[q] = s;
+    }
+    auto inside = [&](size_t q) { return phi[q] > kIsoSurfaceThreshold; };
+    // vertices: crossing lattice edges, in order of (point, direction)
+    SurfaceMesh mesh;
+    mesh.fluid_id = id;
+    std::unordered_map<uint64_t, uint32_t> vid;
+    const int64_t step[3] = {1, nx, nx * ny};
+    for (int64_t k = 0; k < nz; ++k)
+      for (int64_t j = 0; j < ny; ++j)
+        for (int64_t i = 0; i < nx; ++i) {
+          const int64_t q = i + nx * (j + ny * k);
+          const int64_t idx[3] = {i, j, k};
+          for (int d = 0; d < 3; ++d) {
+            if (idx[d] + 1 >= g.n[d]) continue;
+            const int64_t q2 = q + step[d];
+            if (inside((size_t)q) == inside((size_t)q2)) continue;
+            const double t = (kIsoSurfaceThreshold - phi[(size_t)q]) / (phi[(size_t)q2] - phi[(size_t)q]);
+            V3 a = pts[(size_t)q], b = pts[(size_t)q2];
+            vid[(uint64_t)q * 3 + (uint64_t)d] = (uint32_t)mesh.position.size();
+            mesh.position.push_back(a + t * (b - a));
+          }
+        }
+    // triangles: cells in order, each cell's polygons fanned from their first vertex
+    for (int64_t k = 0; k + 1 < nz; ++k)
+      for (int64_t j = 0; j + 1 < ny; ++j)
+        for (int64_t i = 0; i + 1 < nx; ++i) {
+          bool in[8];
+          int64_t corner_q[8];
+          int cnt = 0;
+          for (int c = 0; c < 8; ++c) {
+            corner_q[c] = (i + corner_bit(c, 0)) + nx * ((j + corner_bit(c, 1)) + ny * (k + corner_bit(c, 2)));
+            in[c] = inside((size_t)corner_q[c]);
+            cnt += in[c];
+          }
+          if (cnt == 0 || cnt == 8) continue;
+          for (const auto& loop : cell_polygons(in)) {
+            std::vector<uint32_t> v;
+            for (int e : loop) {
+              const int lo = edge_lower_corner(e);
+              v.push_back(vid.at((uint64_t)corner_q[lo] * 3 + (uint64_t)(e / 4)));
+            }
+            for (size_t t = 1; t + 1 < v.size(); ++t) {
+              mesh.indices.push_back(v[0]);
+              mesh.indices.push_back(v[t]);
+              mesh.indices.push_back(v[t + 1]);
+            }
+          }
+        }
+    if (mesh.indices.empty()) continue;
+    // fluid.rs:296-323: area-weighted vertex normals
+    mesh.normal.assign(mesh.position.size(), V3{0, 0, 0});
+    for (size_t t = 0; t < mesh.indices.size(); t += 3) {
+      const V3 v0 = mesh.position[mesh.indices[t]], v1 = mesh.position[mesh.indices[t + 1]],
+               v2 = mesh.position[mesh.indices[t + 2]];
+      const V3 fn = cross(v1 - v0, v2 - v0);
+      for (int c = 0; c < 3; ++c) mesh.normal[mesh.indices[t + c]] += fn;
+    }
+    for (V3& n : mesh.normal) {
+      const double len = std::sqrt(n.x * n.x + n.y * n.y + n.z * n.z);
+      if (len > 1e-10) n = V3{n.x / len, n.y / len, n.z / len};
+    }
+    out.push_back(std::move(mesh));
+  }
+  return out;
+}
+
 }  // namespace oracle

@@ -361,6 +361,31 @@ struct Measurement {  // SL/measurement.rs:59-78
   double relaxation_factor, time_step_wall_clock_time, predicted_density_error;
 };
 
+// ---------------------------------------------------------------------------
+// Fluid surface reconstruction for render frames (Fluid::reconstruct_surfaces,
+// SL/sph/fluid.rs:212-347), whose core is the third-party splashsurf_lib
+// 0.14.1 `reconstruct_surface` (absent from the reference tree). Restated
+// from its published method: particle densities with the cubic spline of the
+// compact support radius and particle mass rest_density * 4/3 pi r^3, the
+// level set phi(x) = sum_i (m / rho_i) W(x - x_i) on a grid of cube_size
+// aligned to multiples of the cube size, marching cubes at the iso value
+// (0.6) with vertices interpolated linearly on crossing edges, then the
+// area-weighted vertex normals of fluid.rs:296-323.
+// ---------------------------------------------------------------------------
+struct SurfaceMesh {
+  uint32_t fluid_id = 0;
+  std::vector<V3> position, normal;
+  std::vector<uint32_t> indices;
+};
+struct SurfaceGrid {  // the marching-cubes lattice of one group: point k at cube * (k0 + k)
+  int64_t k0[3] = {0, 0, 0};
+  double cube = 0;
+  int64_t n[3] = {0, 0, 0};  // points per axis
+  double coord(int d, int64_t k) const { return cube * (double)(k0[d] + k); }
+};
+SurfaceGrid surface_grid(const std::vector<V3>& positions, double h, double cube);
+std::vector<SurfaceMesh> reconstruct_surfaces(const Fluid& fluid, double spacing, double rest_volume, double h);
+
 struct System {
   SystemParameters params;
   SolverParams sp;
