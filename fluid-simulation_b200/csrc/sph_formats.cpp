@@ -626,6 +626,38 @@ std::vector<uint8_t> time_step_info_to_bincode(const sph_frame_view& f) {
   } else {
     throw Error(SPH_ERR_INVALID, "unknown fluid visualization");
   }
+  if (f.boundary_visualization == SPH_BOUNDARY_TRIANGLE_MESH) {
+    // TriangleMesh { meshes: Vec<(RenderMesh, RenderPose)>, coloring }
+    w.varint(0);
+    if (f.num_boundary_meshes && (!f.boundary_meshes || !f.boundary_poses))
+      throw Error(SPH_ERR_INVALID, "null boundary meshes or poses");
+    w.varint(f.num_boundary_meshes);
+    for (size_t k = 0; k < f.num_boundary_meshes; ++k) {
+      const sph_render_mesh& m = f.boundary_meshes[k];
+      if ((m.num_vertices && !m.vertices) || (m.num_indices && !m.indices))
+        throw Error(SPH_ERR_INVALID, "null render mesh arrays");
+      w.varint(m.num_vertices);
+      for (size_t i = 0; i < 6 * m.num_vertices; ++i) w.f64(m.vertices[i]);
+      w.vec_u32(m.indices, m.num_indices);
+      for (int c = 0; c < 7; ++c) w.f32(f.boundary_poses[7 * k + c]);  // RenderPose
+    }
+    switch (f.boundary_mesh_coloring) {  // BoundaryMeshColoring
+      case SPH_MESH_ORIGINAL: w.varint(0); break;
+      case SPH_MESH_UNIFORM: w.varint(1); break;
+      case SPH_MESH_BOUNDARY_ID: {
+        if (f.num_mesh_ids && !f.mesh_ids) throw Error(SPH_ERR_INVALID, "null mesh ids");
+        uint32_t mx = 0;
+        for (size_t i = 0; i < f.num_mesh_ids; ++i) mx = f.mesh_ids[i] > mx ? f.mesh_ids[i] : mx;
+        w.varint(2);
+        w.vec_u32(f.mesh_ids, f.num_mesh_ids);
+        w.varint(mx);
+        break;
+      }
+      default: throw Error(SPH_ERR_INVALID, "unknown boundary mesh coloring");
+    }
+    return std::move(w.b);
+  }
+  if (f.boundary_visualization != SPH_BOUNDARY_SAMPLES) throw Error(SPH_ERR_INVALID, "unknown boundary visualization");
   // BoundaryVisualization::Samples
   w.varint(1);
   if (f.num_boundary_samples && !f.boundary_positions) throw Error(SPH_ERR_INVALID, "null boundary positions");

@@ -2413,10 +2413,43 @@ int sph_encode_time_step_info(sph_system_t* h, const sph_frame_selector* sel, sp
       f.num_planes = planes.size();
       f.planes = planes.data();
     }
-    std::vector<float> bpos;
+    std::vector<float> bpos, poses;
     std::vector<uint32_t> bids;
     f.boundary_coloring = SPH_COLORING_UNIFORM;
-    if (h->cfg.boundary_handling == SPH_STATIC_SAMPLE_BOUNDARY) {
+    f.boundary_visualization = sel->boundary_visualization;
+    if (sel->boundary_visualization == SPH_BOUNDARY_TRIANGLE_MESH) {
+      // get_visualization (static_sample_boundary.rs:194-219, volume_map_boundary.rs:1459-1483):
+      // each boundary's render mesh with its pose; BoundaryId lists the mesh id per sample for
+      // sample boundaries and per boundary for volume maps
+      const size_t nb = h->order.size();
+      if (nb && !sel->render_meshes) throw Error(SPH_ERR_INVALID, "render meshes are needed for TriangleMesh");
+      f.boundary_mesh_coloring = sel->boundary_mesh_coloring;
+      f.num_boundary_meshes = nb;
+      f.boundary_meshes = sel->render_meshes;
+      poses.assign(7 * nb, 0.0f);
+      size_t si = 0, vi = 0;
+      for (size_t b = 0; b < nb; ++b) {
+        const bool is_sample = h->order[b] == 0;
+        const bool dyn = is_sample ? h->samples[si].dyn : h->vms[vi].dyn;
+        const uint32_t id = sel->render_mesh_ids ? sel->render_mesh_ids[b] : (uint32_t)b;
+        if (is_sample)
+          bids.insert(bids.end(), h->samples[si].x.size() / 3, id);
+        else
+          bids.push_back(id);
+        is_sample ? ++si : ++vi;
+        float* P = &poses[7 * b];
+        P[6] = 1.0f;  // RenderPose::IDENTITY
+        if (dyn) {    // RenderPose::from(pose): translation, rotation (i, j, k, w)
+          double st[19];
+          s->rigid_state((int)b, st);
+          P[0] = (float)st[0]; P[1] = (float)st[1]; P[2] = (float)st[2];
+          P[3] = (float)st[4]; P[4] = (float)st[5]; P[5] = (float)st[6]; P[6] = (float)st[3];
+        }
+      }
+      f.boundary_poses = poses.data();
+      f.num_mesh_ids = bids.size();
+      f.mesh_ids = bids.data();
+    } else if (h->cfg.boundary_handling == SPH_STATIC_SAMPLE_BOUNDARY) {
       f.boundary_coloring = sel->boundary_coloring;
       size_t si = 0;
       for (size_t b = 0; b < h->order.size(); ++b) {

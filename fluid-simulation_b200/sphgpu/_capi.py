@@ -142,6 +142,15 @@ class SphCheckpointView(C.Structure):
     ]
 
 
+BOUNDARY_SAMPLES, BOUNDARY_TRIANGLE_MESH = 0, 1
+MESH_ORIGINAL, MESH_UNIFORM, MESH_BOUNDARY_ID = 0, 1, 2
+
+
+class SphRenderMesh(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("num_vertices", C.c_size_t), ("indices", C.c_void_p),
+                ("num_indices", C.c_size_t)]
+
+
 class SphSensorPlane(C.Structure):
     _fields_ = [("positions", C.c_void_p), ("data", C.c_void_p), ("rows", C.c_size_t), ("cols", C.c_size_t)]
 
@@ -151,6 +160,8 @@ class SphFrameSelector(C.Structure):
         ("fluid", C.c_int), ("fluid_coloring", C.c_int), ("quantity", C.c_int),
         ("num_planes", C.c_size_t), ("planes", C.POINTER(SphSensorPlane)),
         ("boundary_coloring", C.c_int), ("render_mesh_ids", C.c_void_p),
+        ("boundary_visualization", C.c_int), ("boundary_mesh_coloring", C.c_int),
+        ("render_meshes", C.POINTER(SphRenderMesh)),
     ]
 
 
@@ -163,6 +174,9 @@ class SphFrameView(C.Structure):
         ("boundary_coloring", C.c_int), ("num_boundary_samples", C.c_size_t),
         ("boundary_positions", C.c_void_p), ("boundary_ids", C.c_void_p),
         ("meshes", C.c_void_p), ("max_fluid_id", C.c_uint32),
+        ("boundary_visualization", C.c_int), ("boundary_mesh_coloring", C.c_int),
+        ("num_boundary_meshes", C.c_size_t), ("boundary_meshes", C.POINTER(SphRenderMesh)),
+        ("boundary_poses", C.c_void_p), ("num_mesh_ids", C.c_size_t), ("mesh_ids", C.c_void_p),
     ]
 
 

@@ -164,12 +164,30 @@ def _measurement(m) -> A.SphMeasurement:
     return out
 
 
+def render_meshes(meshes, keep):
+    """ctypes array of sph_render_mesh for [(vertices (n, 6), indices)]; the
+    arrays are appended to `keep`."""
+    arr = (A.SphRenderMesh * max(1, len(meshes)))()
+    for k, (v, idx) in enumerate(meshes):
+        v = np.ascontiguousarray(np.asarray(v, np.float64).reshape(-1, 6))
+        idx = np.ascontiguousarray(idx, np.uint32).reshape(-1)
+        keep += [v, idx]
+        arr[k].vertices = v.ctypes.data if v.size else None
+        arr[k].num_vertices = v.shape[0]
+        arr[k].indices = idx.ctypes.data if idx.size else None
+        arr[k].num_indices = idx.shape[0]
+    keep.append(arr)
+    return arr
+
+
 def encode_frame(time_step_number: int, measurement, fluid: dict, boundary: dict) -> bytes:
     """TimeStepInfo from host arrays. `fluid` is {"kind": "samples",
     "positions", "coloring": "uniform" | ("id", ids) | ("quantity", q, data)}
     or {"kind": "sensor_plane", "quantity", "planes": [(positions, data,
     rows, cols)]}; `boundary` is {"positions", "coloring": "uniform" |
-    ("id", ids)}."""
+    ("id", ids)} or {"kind": "triangle_mesh", "meshes": [(vertices (n, 6),
+    indices)], "poses": [translation + rotation (i, j, k, w)], "coloring":
+    "original" | "uniform" | ("id", ids)}."""
     L = A.load()
     keep = []
 
@@ -207,15 +225,33 @@ def encode_frame(time_step_number: int, measurement, fluid: dict, boundary: dict
         keep.append(planes)
         f.num_planes = len(fluid["planes"])
         f.planes = planes
-    bpos = np.asarray(boundary.get("positions", np.zeros((0, 3))), np.float32).reshape(-1, 3)
-    f.num_boundary_samples = bpos.shape[0]
-    f.boundary_positions = ptr(bpos, np.float32)
-    col = boundary.get("coloring", "uniform")
-    if col == "uniform":
-        f.boundary_coloring = A.COLORING_UNIFORM
+    if boundary.get("kind", "samples") == "triangle_mesh":
+        f.boundary_visualization = A.BOUNDARY_TRIANGLE_MESH
+        meshes = boundary["meshes"]
+        arr = render_meshes(meshes, keep)
+        f.num_boundary_meshes = len(meshes)
+        f.boundary_meshes = arr
+        f.boundary_poses = ptr(np.asarray(boundary["poses"], np.float32).reshape(-1, 7), np.float32)
+        col = boundary.get("coloring", "original")
+        if col == "original":
+            f.boundary_mesh_coloring = A.MESH_ORIGINAL
+        elif col == "uniform":
+            f.boundary_mesh_coloring = A.MESH_UNIFORM
+        else:
+            f.boundary_mesh_coloring = A.MESH_BOUNDARY_ID
+            ids = np.asarray(col[1], np.uint32)
+            f.num_mesh_ids = ids.shape[0]
+            f.mesh_ids = ptr(ids, np.uint32)
     else:
-        f.boundary_coloring = A.COLORING_ID
-        f.boundary_ids = ptr(col[1], np.uint32)
+        bpos = np.asarray(boundary.get("positions", np.zeros((0, 3))), np.float32).reshape(-1, 3)
+        f.num_boundary_samples = bpos.shape[0]
+        f.boundary_positions = ptr(bpos, np.float32)
+        col = boundary.get("coloring", "uniform")
+        if col == "uniform":
+            f.boundary_coloring = A.COLORING_UNIFORM
+        else:
+            f.boundary_coloring = A.COLORING_ID
+            f.boundary_ids = ptr(col[1], np.uint32)
     out = C.c_void_p()
     A.check(L.sph_frame_encode(C.byref(f), C.byref(out)))
     return _bytes(out)

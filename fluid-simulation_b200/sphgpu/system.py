@@ -377,11 +377,14 @@ class GpuSystem:
             self._L.sph_checkpoint_free(h)
 
     def encode_time_step_info(self, fluid="samples", fluid_coloring="uniform", quantity=A.Q_SPEED,
-                              planes=(), boundary_coloring="uniform", render_mesh_ids=None) -> bytes:
+                              planes=(), boundary_coloring="uniform", render_mesh_ids=None,
+                              boundary="samples", render_meshes=None) -> bytes:
         """TimeStepInfo::from_system (render_info.rs:83-92) as bincode bytes.
         fluid: "samples", "sensor_plane" or "triangle_mesh"; fluid_coloring:
         "uniform", "id" or "quantity" (samples); planes: [(positions, rows,
-        cols)]; boundary_coloring: "uniform" or "id"."""
+        cols)]; boundary: "samples" (boundary_coloring "uniform" or "id") or
+        "triangle_mesh" with render_meshes [(vertices (n, 6), indices)] per
+        boundary (boundary_coloring "original", "uniform" or "id")."""
         from .formats import _bytes
         keep = []
         sel = A.SphFrameSelector()
@@ -398,7 +401,14 @@ class GpuSystem:
             arr[k].rows, arr[k].cols = int(rows), int(cols)
         sel.num_planes = len(planes)
         sel.planes = arr
-        sel.boundary_coloring = A.COLORING_ID if boundary_coloring == "id" else A.COLORING_UNIFORM
+        if boundary == "triangle_mesh":
+            from .formats import render_meshes as _rm
+            sel.boundary_visualization = A.BOUNDARY_TRIANGLE_MESH
+            sel.boundary_mesh_coloring = {"original": A.MESH_ORIGINAL, "uniform": A.MESH_UNIFORM,
+                                          "id": A.MESH_BOUNDARY_ID}[boundary_coloring]
+            sel.render_meshes = _rm(render_meshes or [], keep)
+        else:
+            sel.boundary_coloring = A.COLORING_ID if boundary_coloring == "id" else A.COLORING_UNIFORM
         if render_mesh_ids is not None:
             ids = np.ascontiguousarray(render_mesh_ids, np.uint32)
             keep.append(ids)

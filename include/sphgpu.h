@@ -507,7 +507,8 @@ int sph_restore_checkpoint(sph_system_t* h, const sph_checkpoint_t* c);
 
 /* Recording frames: TimeStepInfo with FluidVisualization::TriangleMesh
  * (reconstructed surfaces), ::Samples or ::SensorPlane, and
- * BoundaryVisualization::Samples (render_info.rs:110-245). */
+ * BoundaryVisualization::Samples or ::TriangleMesh (the caller's render
+ * meshes with the boundaries' current poses) (render_info.rs:110-245). */
 enum sph_fluid_visualization {
   SPH_FLUID_TRIANGLE_MESH = 0, SPH_FLUID_SAMPLES = 1, SPH_FLUID_SENSOR_PLANE = 2
 };
@@ -526,6 +527,22 @@ int sph_meshes_get(const sph_meshes_t* m, size_t k, uint32_t* fluid_id, size_t* 
 void sph_meshes_free(sph_meshes_t* m);
 enum sph_sample_coloring { SPH_COLORING_UNIFORM = 0, SPH_COLORING_ID = 1, SPH_COLORING_QUANTITY = 2 };
 
+/* BoundaryVisualization variants as this API selects them (the wire format
+ * keeps the reference's variant order, TriangleMesh first). */
+enum sph_boundary_visualization { SPH_BOUNDARY_SAMPLES = 0, SPH_BOUNDARY_TRIANGLE_MESH = 1 };
+/* BoundaryMeshColoring (render_info.rs:259-264). */
+enum sph_boundary_mesh_coloring {
+  SPH_MESH_ORIGINAL = 0, SPH_MESH_UNIFORM = 1, SPH_MESH_BOUNDARY_ID = 2
+};
+/* RenderMesh (utilities/triangle_mesh.rs:61-64) of a boundary in its body
+ * frame (world frame for a static boundary). */
+typedef struct sph_render_mesh {
+  const double* vertices;          /* 6 per vertex: position, normal */
+  size_t num_vertices;
+  const uint32_t* indices;
+  size_t num_indices;
+} sph_render_mesh;
+
 typedef struct sph_sensor_plane {  /* SensorPlaneData (render_info.rs:196-202) */
   const float* positions;          /* 3 * rows * cols */
   const float* data;               /* rows * cols (frame views only) */
@@ -542,6 +559,9 @@ typedef struct sph_frame_selector {
   const sph_sensor_plane* planes;  /* positions, rows, cols (data unused) */
   int boundary_coloring;           /* UNIFORM or ID (render mesh id) */
   const uint32_t* render_mesh_ids; /* per boundary; NULL = the boundary index */
+  int boundary_visualization;      /* sph_boundary_visualization */
+  int boundary_mesh_coloring;      /* TriangleMesh: sph_boundary_mesh_coloring */
+  const sph_render_mesh* render_meshes; /* TriangleMesh: one per boundary */
 } sph_frame_selector;
 
 /* A frame's contents (TimeStepInfo itself). */
@@ -561,6 +581,13 @@ typedef struct sph_frame_view {
   const uint32_t* boundary_ids;    /* per sample, ID coloring */
   const sph_meshes_t* meshes;      /* TriangleMesh */
   uint32_t max_fluid_id;           /* TriangleMesh: the largest fluid id */
+  int boundary_visualization;      /* sph_boundary_visualization */
+  int boundary_mesh_coloring;      /* sph_boundary_mesh_coloring */
+  size_t num_boundary_meshes;
+  const sph_render_mesh* boundary_meshes;
+  const float* boundary_poses;     /* 7 per mesh: translation, rotation (i, j, k, w) */
+  size_t num_mesh_ids;             /* BOUNDARY_ID coloring: the ids and their count */
+  const uint32_t* mesh_ids;
 } sph_frame_view;
 
 /* TimeStepInfo -> bincode bytes (render_info.rs:101-106). */

@@ -381,3 +381,49 @@ def test_save_state_refuses_an_existing_file(tmp_path):
     _same(F.load_state(path), _reference_test_checkpoint())
     with pytest.raises(FileExistsError):
         F.save_state(_reference_test_checkpoint(), path)
+
+
+def _decode_boundary_meshes(b, r):
+    """BoundaryVisualization at reader position: ("triangle_mesh", meshes,
+    poses, coloring) or ("samples", ...) is not expected here."""
+    assert r.varint() == 0
+    meshes, poses = [], []
+    for _ in range(r.varint()):
+        nv = r.varint()
+        v = np.frombuffer(b[r.i:r.i + 48 * nv], "<f8").reshape(nv, 6)
+        r.i += 48 * nv
+        idx = r.vec(r.varint)
+        pose = np.frombuffer(b[r.i:r.i + 28], "<f4")
+        r.i += 28
+        meshes.append((v, idx))
+        poses.append(pose)
+    c = r.varint()
+    col = ["original", "uniform", None][c] if c < 2 else ("id", r.vec(r.varint), r.varint())
+    assert r.i == len(b)
+    return meshes, poses, col
+
+
+@pytest.mark.parametrize("coloring", ["original", "uniform", "id"])
+def test_boundary_mesh_frames_decode_to_their_inputs(coloring):
+    rng = np.random.default_rng(8)
+    meshes = [(rng.normal(size=(5, 6)), rng.integers(0, 5, 9).astype(np.uint32)),
+              (rng.normal(size=(0, 6)), np.zeros(0, np.uint32))]
+    poses = np.array([[0, 0, 0, 0, 0, 0, 1], [1.5, -2, 0.25, 0.1, 0.2, 0.3, 0.9]], np.float32)
+    ids = np.array([4, 4, 4, 9], np.uint32)
+    col = {"original": "original", "uniform": "uniform", "id": ("id", ids)}[coloring]
+    b = F.encode_frame(3, _measurement(3), {"kind": "samples", "positions": np.zeros((0, 3))},
+                       {"kind": "triangle_mesh", "meshes": meshes, "poses": poses, "coloring": col})
+    r = _Reader(b)
+    r.varint()
+    r.i += 12 * 8  # the measurement: 12 f64, a u32 varint, 3 f64
+    r.varint()
+    r.i += 3 * 8
+    assert r.varint() == 1 and r.varint() == 0 and r.varint() == 0  # fluid Samples, empty, Uniform
+    got, gp, gc = _decode_boundary_meshes(b, r)
+    for (v, idx), (gv, gi) in zip(meshes, got):
+        assert np.array_equal(gv, v) and np.array_equal(gi, idx)
+    assert np.array_equal(np.array(gp), poses)
+    if coloring == "id":
+        assert gc[0] == "id" and np.array_equal(gc[1], ids) and gc[2] == 9
+    else:
+        assert gc == coloring

@@ -140,3 +140,38 @@ def test_sensor_plane_frames_equal_the_encoded_readbacks(A):
         # a volume-map system has no boundary samples: an empty, uniform set
         assert got == _frame_from_readbacks(g, {"kind": "sensor_plane", "quantity": q, "planes": want_planes})
     g.close()
+
+
+def test_boundary_mesh_frame_carries_the_device_poses(A):
+    """BoundaryVisualization::TriangleMesh (static_sample_boundary.rs:194-219):
+    the caller's render meshes, identity for the static container and the
+    rigid state's pose (f32 translation, rotation as i, j, k, w) for the
+    body; BoundaryId coloring lists each boundary's id once per sample."""
+    from sphgpu import scenes
+    from test_formats import _Reader, _decode_boundary_meshes
+    sc = scenes.floating_cube_scene()
+    g = scenes.build_system(sc)
+    g.step_forward_in_time(7)
+    rng = np.random.default_rng(2)
+    meshes = [(rng.normal(size=(8, 6)), rng.integers(0, 8, 12).astype(np.uint32)) for _ in range(2)]
+    frame = g.encode_time_step_info("samples", boundary="triangle_mesh", render_meshes=meshes,
+                                    boundary_coloring="id", render_mesh_ids=[5, 11])
+    r = _Reader(frame)
+    r.varint()
+    r.i += 12 * 8
+    r.varint()
+    r.i += 3 * 8
+    assert r.varint() == 1  # fluid Samples
+    n = r.varint()
+    r.i += 12 * n
+    assert r.varint() == 0  # uniform coloring
+    got, poses, col = _decode_boundary_meshes(frame, r)
+    for (v, idx), (gv, gi) in zip(meshes, got):
+        assert np.array_equal(gv, v) and np.array_equal(gi, idx)
+    assert np.array_equal(poses[0], np.array([0, 0, 0, 0, 0, 0, 1], np.float32))
+    st = g.rigid_state(1)
+    want = np.array([st[0], st[1], st[2], st[4], st[5], st[6], st[3]]).astype(np.float32)
+    assert np.array_equal(poses[1], want)
+    counts = [nb for _, nb in g._boundaries]
+    assert col[0] == "id" and np.array_equal(col[1], np.repeat([5, 11], counts)) and col[2] == 11
+    g.close()
