@@ -4,7 +4,8 @@ The reference (Rust) cannot be built here, so the oracle's fidelity rests on
 the formula-level assertions of the reference's test suite, restated below
 against the oracle (sim_lib = simulation_lib):
   kernel      tests/sph/kernel/cubic_spline.rs:17-232
-  hashing     src/neighbor_search/spatial_hashing.rs:173-390
+  hashing     src/neighbor_search/spatial_hashing.rs:173-390,
+              tests/neighbor_search/spatial_hashing.rs:19-330
   volume      src/sph/quantities.rs:437-633
   quantities  src/sph/quantities.rs:437-800 through sph/mod.rs:241-341
   IISPH       tests/sph/pressure_solver/iisph.rs:429-490
@@ -441,3 +442,51 @@ def test_quantity_density_error_takes_masses_in_the_volume_slot(oracle):
     # water-like masses (rest density 1000) are never below the rest volume: zero everywhere
     s2 = _isolated_system(oracle, pos, h=h, spacing=dx)
     assert np.all(s2.quantity_at_positions(Q_DENSITY_ERROR, pos) == 0.0)
+
+
+# ---- SpatialHashing::find_samples (tests/neighbor_search/spatial_hashing.rs:19-330) --------
+def _nb(oracle, rng_, pos, samples=None, cell=1.0):
+    off, idx, _ = oracle.find_samples(rng_, pos, pos if samples is None else samples, cell_size=cell)
+    return [sorted(_row(off, idx, i)) for i in range(len(pos))]
+
+
+def test_hashing_empty_and_self(oracle):
+    assert _nb(oracle, 2.0, np.zeros((0, 3))) == []
+    assert _nb(oracle, 2.0, [[0, 0, 0]]) == [[0]]
+    assert _nb(oracle, 2.0, [[0, 0, 0]], samples=np.zeros((0, 3))) == [[]]
+
+
+def test_hashing_close_far_and_boundary_samples(oracle):
+    assert _nb(oracle, 2.0, [[0, 0, 0], [0.5, 0, 0]]) == [[0, 1], [0, 1]]
+    assert _nb(oracle, 2.0, [[0, 0, 0], [100, 0, 0]]) == [[0], [1]]
+    assert _nb(oracle, 2.0, [[0, 0, 0]], samples=[[0.5, 0, 0], [100, 0, 0]]) == [[0]]
+
+
+def test_hashing_is_symmetric_and_finds_clusters(oracle):
+    nb = _nb(oracle, 1.5, [[0, 0, 0], [1, 0, 0], [0, 1, 0]])
+    assert all(i in nb[j] for i in range(3) for j in nb[i])
+    assert _nb(oracle, 1.0, [[0, 0, 0], [0.3, 0, 0], [0, 0.3, 0], [0, 0, 0.3]]) == [[0, 1, 2, 3]] * 4
+    nb = _nb(oracle, 2.0, [[0, 0, 0], [0.5, 0, 0], [50, 50, 50], [50.5, 50, 50]])
+    assert nb == [[0, 1], [0, 1], [2, 3], [2, 3]]
+
+
+def test_hashing_range_diagonal_duplicates_and_cell_boundaries(oracle):
+    assert 1 not in _nb(oracle, 1.0, [[0, 0, 0], [1.5, 0, 0]])[0]
+    assert 1 in _nb(oracle, 2.0, [[0, 0, 0], [1.5, 0, 0]])[0]
+    assert _nb(oracle, 1.0, [[0, 0, 0], [0.5, 0.5, 0.5]]) == [[0, 1], [0, 1]]
+    assert _nb(oracle, 0.5, [[1, 1, 1], [1, 1, 1]]) == [[0, 1], [0, 1]]
+    assert _nb(oracle, 1.0, [[0.9, 0, 0], [1.1, 0, 0]]) == [[0, 1], [0, 1]]
+
+
+def test_hashing_repeated_calls_grow_and_shrink(oracle):
+    assert 1 not in _nb(oracle, 2.0, [[0, 0, 0], [100, 0, 0]])[0]
+    nb = _nb(oracle, 1.0, [[0, 0, 0], [0.5, 0, 0], [0.3, 0, 0], [100, 0, 0]])
+    assert 2 in nb[0] and nb[3] == [3]
+    assert _nb(oracle, 1.0, [[0, 0, 0], [0.5, 0, 0]]) == [[0, 1], [0, 1]]
+
+
+def test_hashing_cell_size_is_only_a_performance_parameter(oracle):
+    assert 1 not in _nb(oracle, 2.0, [[0, 0, 0], [5, 0, 0]], cell=10.0)[0]
+    assert 1 in _nb(oracle, 6.0, [[0, 0, 0], [5, 0, 0]], cell=10.0)[0]
+    # a cell size far below the range searches ceil(range / cell) cells each way
+    assert _nb(oracle, 1.0, [[0, 0, 0], [0.5, 0, 0]], cell=0.1) == [[0, 1], [0, 1]]
