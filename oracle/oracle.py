@@ -103,6 +103,7 @@ def lib():
         "oracle_boundary_volumes": (i, [vp, sz, dp]),
         "oracle_vm_samples": (i, [vp, sz, u8p, dp, dp, dp]),
         "oracle_rigid_state": (i, [vp, sz, dp]),
+        "oracle_rigid_probe": (i, [dp, vp, i, dp, dp, i, d, i, i, dp, dp]),
         "oracle_kernel_w": (d, [d]),
         "oracle_kernel_dqw": (d, [d]),
         "oracle_kernel_function": (d, [dp, d]),
@@ -402,6 +403,29 @@ def iisph_initialize_probe(s_f, a_ff, omega, eps, clamp):
     p = np.zeros(s_f.shape[0])
     lib().oracle_iisph_initialize_probe(s_f.shape[0], s_f, a_ff, float(omega), float(eps), 1 if clamp else 0, p)
     return p
+
+
+def rigid_probe(init32, op, point=(0.0, 0.0, 0.0), restore=None, forces=(), locations=(),
+                reset=False, dt=0.0, n_steps=0):
+    """A RigidBodyMotion built from `init32`, optionally restored from a
+    19-value checkpoint (com, orientation w,i,j,k, linear velocity, angular
+    momentum, force, torque), given forces at locations, reset, and stepped.
+    op "velocity_at_point", "world_to_local", "local_to_world" or
+    "local_to_world_vector" of `point`, or "state": the checkpoint's 19
+    values and the angular velocity (22)."""
+    code = {"velocity_at_point": 0, "world_to_local": 1, "local_to_world": 2, "local_to_world_vector": 3,
+            "state": 4}[op]
+    fr = _f64(np.reshape(forces, (-1, 3)))
+    lc = _f64(np.reshape(locations, (-1, 3)))
+    assert fr.shape == lc.shape
+    keep = None if restore is None else _f64(restore)
+    assert keep is None or keep.size == 19
+    out = np.zeros(22)
+    rc = lib().oracle_rigid_probe(_f64(init32), None if keep is None else keep.ctypes.data, fr.shape[0],
+                                  fr.ravel(), lc.ravel(), int(bool(reset)), float(dt), int(n_steps), code,
+                                  _f64(point), out)
+    assert rc == 0
+    return out if code == 4 else out[:3]
 
 
 def set_num_threads(n):

@@ -395,6 +395,51 @@ void oracle_surface_grid(size_t n, const double* pos, double h, double cube, lon
   }
 }
 
+// RigidBodyMotion (rigid_body_motion.rs:38-222) driven the way its unit
+// tests drive it: built from the 32-double init (see read_rigid), then
+// restore_from_checkpoint when `restore` is given (19 doubles: center of
+// mass, orientation w,i,j,k, linear velocity, angular momentum, force,
+// torque), add_force for each (force, location), reset_forces when `reset`,
+// `n_steps` steps of `dt`. Then op 0 velocity_at_point(in), 1
+// world_to_local(in), 2 local_to_world(in), 3 local_to_world_vector(in)
+// (3 values), or 4 the checkpoint's 19 values followed by the angular
+// velocity (22 values).
+int oracle_rigid_probe(const double* init32, const double* restore, int n_forces,
+                       const double* force, const double* location, int reset, double dt,
+                       int n_steps, int op, const double* in, double* out) {
+  RigidBodyMotion m;
+  read_rigid(init32, m);
+  auto v3 = [](const double* p) { return V3{p[0], p[1], p[2]}; };
+  if (restore)
+    m.restore_from_checkpoint(v3(restore), Quat{restore[3], restore[4], restore[5], restore[6]},
+                              v3(restore + 7), v3(restore + 10), v3(restore + 13),
+                              v3(restore + 16));
+  for (int k = 0; k < n_forces; ++k) m.add_force(v3(force + 3 * k), v3(location + 3 * k));
+  if (reset) m.reset_forces();
+  for (int s = 0; s < n_steps; ++s) m.step_forward_in_time(dt);
+  const V3 p = v3(in);
+  V3 r;
+  switch (op) {
+    case 0: r = m.velocity_at_point(p); break;
+    case 1: r = m.world_to_local(p); break;
+    case 2: r = m.local_to_world(p); break;
+    case 3: r = m.local_to_world_vector(p); break;
+    case 4: {
+      const double v[22] = {m.center_of_mass.x, m.center_of_mass.y, m.center_of_mass.z,
+                            m.orientation.w, m.orientation.x, m.orientation.y, m.orientation.z,
+                            m.linear_velocity.x, m.linear_velocity.y, m.linear_velocity.z,
+                            m.angular_momentum.x, m.angular_momentum.y, m.angular_momentum.z,
+                            m.force.x, m.force.y, m.force.z, m.torque.x, m.torque.y, m.torque.z,
+                            m.angular_velocity.x, m.angular_velocity.y, m.angular_velocity.z};
+      std::memcpy(out, v, sizeof v);
+      return 0;
+    }
+    default: return 1;
+  }
+  out[0] = r.x; out[1] = r.y; out[2] = r.z;
+  return 0;
+}
+
 int oracle_initialize(void* hh) {
   auto* h = (OracleHandle*)hh;
   try {

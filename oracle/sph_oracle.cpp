@@ -259,6 +259,20 @@ void RigidBodyMotion::add_force(V3 f, V3 location) {  // :147-150
   force += f;
   torque += cross(location - center_of_mass, f);
 }
+void RigidBodyMotion::reset_forces() {  // :141-144
+  force = {0, 0, 0};
+  torque = {0, 0, 0};
+}
+void RigidBodyMotion::restore_from_checkpoint(V3 com, Quat q, V3 lv, V3 am, V3 f,
+                                              V3 t) {  // :214-222
+  center_of_mass = com;
+  orientation = q;
+  linear_velocity = lv;
+  angular_momentum = am;
+  force = f;
+  torque = t;
+  update_derived_variables();
+}
 void RigidBodyMotion::step_forward_in_time(double dt) {  // :183-201
   V3 lin_acc = force / mass;
   linear_velocity += lin_acc * dt;
@@ -266,8 +280,7 @@ void RigidBodyMotion::step_forward_in_time(double dt) {  // :183-201
   angular_momentum += torque * dt;
   angular_velocity = mul(inertia_tensor_inv_world, angular_momentum);
   orientation = qmul(qfrom_scaled_axis(angular_velocity * dt), orientation);
-  force = {0, 0, 0};
-  torque = {0, 0, 0};
+  reset_forces();
   update_derived_variables();
 }
 

@@ -178,7 +178,9 @@ struct RigidBodyMotion {
   V3 local_to_world_vector(V3 v) const;
   V3 velocity_at_point(V3 p) const;
   void add_force(V3 f, V3 location);
+  void reset_forces();
   void step_forward_in_time(double dt);
+  void restore_from_checkpoint(V3 com, Quat q, V3 lin_vel, V3 ang_momentum, V3 f, V3 t);
 };
 
 // ---------------------------------------------------------------------------
