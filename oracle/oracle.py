@@ -103,6 +103,7 @@ def lib():
         "oracle_boundary_volumes": (i, [vp, sz, dp]),
         "oracle_vm_samples": (i, [vp, sz, u8p, dp, dp, dp]),
         "oracle_rigid_state": (i, [vp, sz, dp]),
+        "oracle_integrate_probe": (i, [i, sz, dp, dp, dp, vp, vp, d]),
         "oracle_rigid_probe": (i, [dp, vp, i, dp, dp, i, d, i, i, dp, dp]),
         "oracle_kernel_w": (d, [d]),
         "oracle_kernel_dqw": (d, [d]),
@@ -403,6 +404,22 @@ def iisph_initialize_probe(s_f, a_ff, omega, eps, clamp):
     p = np.zeros(s_f.shape[0])
     lib().oracle_iisph_initialize_probe(s_f.shape[0], s_f, a_ff, float(omega), float(eps), 1 if clamp else 0, p)
     return p
+
+
+def integrate_probe(scheme, position, velocity, acceleration, dt, slot_position=None, slot_velocity=None):
+    """IntegrationScheme::integrate ("EulerCromer" or "TakePredicted") on the
+    given (n, 3) arrays; returns position, velocity, acceleration and, for
+    TakePredicted, the two integrator slots afterwards."""
+    code = {"EulerCromer": 0, "TakePredicted": 1}[scheme]
+    arrs = [np.array(a, np.float64, order="C").reshape(-1, 3) for a in (position, velocity, acceleration)]
+    slots = [None if a is None else np.array(a, np.float64, order="C").reshape(-1, 3)
+             for a in (slot_position, slot_velocity)]
+    n = arrs[0].shape[0]
+    assert all(a.shape[0] == n for a in arrs + [s for s in slots if s is not None])
+    rc = lib().oracle_integrate_probe(code, n, *arrs, *[None if s is None else s.ctypes.data for s in slots],
+                                      float(dt))
+    assert rc == 0, rc
+    return tuple(arrs) + ((tuple(slots),) if code == 1 else ())
 
 
 def rigid_probe(init32, op, point=(0.0, 0.0, 0.0), restore=None, forces=(), locations=(),

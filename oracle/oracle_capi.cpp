@@ -395,6 +395,41 @@ void oracle_surface_grid(size_t n, const double* pos, double h, double cube, lon
   }
 }
 
+// IntegrationScheme::integrate on given particle arrays, in place (3n
+// doubles each): scheme 0 EulerCromer (slot pointers unused, may be null),
+// 1 TakePredicted (one position and one velocity slot).
+int oracle_integrate_probe(int scheme, size_t n, double* pos, double* vel, double* acc,
+                           double* slot_pos, double* slot_vel, double dt) {
+  if (scheme != 0 && scheme != 1) return 1;
+  if (scheme == 1 && (!slot_pos || !slot_vel)) return 2;
+  Fluid f;
+  auto load = [n](const double* a) {
+    std::vector<V3> v(n);
+    for (size_t i = 0; i < n; ++i) v[i] = {a[3 * i], a[3 * i + 1], a[3 * i + 2]};
+    return v;
+  };
+  auto store = [n](const std::vector<V3>& v, double* a) {
+    for (size_t i = 0; i < n; ++i) { a[3 * i] = v[i].x; a[3 * i + 1] = v[i].y; a[3 * i + 2] = v[i].z; }
+  };
+  f.position = load(pos);
+  f.velocity = load(vel);
+  f.acceleration = load(acc);
+  if (scheme == 1) {
+    f.integrator_position_slots.push_back(load(slot_pos));
+    f.integrator_velocity_slots.push_back(load(slot_vel));
+  }
+  f.num_active = n;
+  integrate((Integrator)scheme, f, n, dt);
+  store(f.position, pos);
+  store(f.velocity, vel);
+  store(f.acceleration, acc);
+  if (scheme == 1) {
+    store(f.integrator_position_slots[0], slot_pos);
+    store(f.integrator_velocity_slots[0], slot_vel);
+  }
+  return 0;
+}
+
 // RigidBodyMotion (rigid_body_motion.rs:38-222) driven the way its unit
 // tests drive it: built from the 32-double init (see read_rigid), then
 // restore_from_checkpoint when `restore` is given (19 doubles: center of

@@ -1188,22 +1188,26 @@ void System::new_boxed() {  // :389-421
   update();
 }
 
+void integrate(Integrator scheme, Fluid& fluid, size_t n, double dt) {
+  if (scheme == Integrator::EulerCromer) {  // euler_cromer.rs:12-25
+    parallel_for(n, [&](size_t b, size_t e) {
+      for (size_t i = b; i < e; ++i) {
+        V3 v = fluid.velocity[i] + fluid.acceleration[i] * dt;
+        fluid.velocity[i] = v;
+        fluid.position[i] = fluid.position[i] + v * dt;
+      }
+    });
+  } else {  // take_predicted.rs:14-27: dt unused
+    std::swap(fluid.position, fluid.integrator_position_slots[0]);
+    std::swap(fluid.velocity, fluid.integrator_velocity_slots[0]);
+  }
+}
+
 void System::step_forward_in_time() {  // :125-144
   auto t0 = std::chrono::steady_clock::now();
   double dt = params.time_increment;
   const size_t n = fluid.len();
-  if (integrator == Integrator::EulerCromer) {  // euler_cromer.rs:12-25
-parallel_for((size_t)(n), [&](size_t b__, size_t e__) {
-    for (long long i = (long long)b__; i < (long long)e__; ++i) {
-      V3 v = fluid.velocity[i] + fluid.acceleration[i] * dt;
-      fluid.velocity[i] = v;
-      fluid.position[i] = fluid.position[i] + v * dt;
-    }
-  });
-  } else {  // take_predicted.rs:14-27
-    std::swap(fluid.position, fluid.integrator_position_slots[0]);
-    std::swap(fluid.velocity, fluid.integrator_velocity_slots[0]);
-  }
+  integrate(integrator, fluid, n, dt);
   boundary->step_forward_in_time(dt);
   time_steps_propagated += 1;
   if (params.cfl) params.current_time += params.time_increment;

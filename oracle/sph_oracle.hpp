@@ -339,6 +339,9 @@ double volume_at(const Serendipity& sdf, V3 p, double r, int degree, bool& ok);
 // ---------------------------------------------------------------------------
 enum class Solver { SESPH = 0, SESPHwSplitting = 1, IISPH = 2, IISPHwOST = 3 };
 enum class Integrator { EulerCromer = 0, TakePredicted = 1 };
+// IntegrationScheme::integrate of the first n particles (euler_cromer.rs:12-25,
+// take_predicted.rs:14-27); TakePredicted swaps whole slot 0 with the state.
+void integrate(Integrator scheme, Fluid& fluid, size_t n, double dt);
 
 struct SolverParams {
   double stiffness = 1000;
