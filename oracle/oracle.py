@@ -103,6 +103,17 @@ def lib():
         "oracle_boundary_volumes": (i, [vp, sz, dp]),
         "oracle_vm_samples": (i, [vp, sz, u8p, dp, dp, dp]),
         "oracle_rigid_state": (i, [vp, sz, dp]),
+        "oracle_ssb_create": (vp, []),
+        "oracle_ssb_free": (None, [vp]),
+        "oracle_ssb_count": (sz, [vp]),
+        "oracle_ssb_len": (sz, [vp, sz]),
+        "oracle_ssb_add": (i, [vp, sz, dp, vp]),
+        "oracle_ssb_initialize": (None, [vp, d, d]),
+        "oracle_ssb_find": (None, [vp, d, sz, dp, d]),
+        "oracle_ssb_neighbor_count": (sz, [vp, sz, sz]),
+        "oracle_ssb_add_force": (None, [vp, sz, dp, dp]),
+        "oracle_ssb_step": (None, [vp, d]),
+        "oracle_ssb_samples": (i, [vp, sz, dp, dp, dp, dp]),
         "oracle_integrate_probe": (i, [i, sz, dp, dp, dp, vp, vp, d]),
         "oracle_rigid_probe": (i, [dp, vp, i, dp, dp, i, d, i, i, dp, dp]),
         "oracle_kernel_w": (d, [d]),
@@ -404,6 +415,52 @@ def iisph_initialize_probe(s_f, a_ff, omega, eps, clamp):
     p = np.zeros(s_f.shape[0])
     lib().oracle_iisph_initialize_probe(s_f.shape[0], s_f, a_ff, float(omega), float(eps), 1 if clamp else 0, p)
     return p
+
+
+class SampleBoundaries:
+    """The oracle's StaticSampleBoundary on its own (no fluid, no system):
+    add static boundaries (world-frame samples) and dynamic ones (body-frame
+    samples and a 32-value rigid init), then initialize, find, add_force and
+    step as the reference's boundary API does."""
+
+    def __init__(self):
+        self._h = lib().oracle_ssb_create()
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().oracle_ssb_free(self._h)
+            self._h = None
+
+    def __len__(self):
+        return lib().oracle_ssb_count(self._h)
+
+    def add(self, samples, rigid=None):
+        x = _f64(np.reshape(samples, (-1, 3)))
+        keep = None if rigid is None else _f64(rigid)
+        assert lib().oracle_ssb_add(self._h, x.shape[0], x.ravel(), None if keep is None else keep.ctypes.data) == 0
+
+    def initialize(self, h, rest_volume_weighting=1.0):
+        lib().oracle_ssb_initialize(self._h, float(h), float(rest_volume_weighting))
+
+    def find_boundary_samples(self, search_range, positions, spacing):
+        x = _f64(np.reshape(positions, (-1, 3)))
+        lib().oracle_ssb_find(self._h, float(search_range), x.shape[0], x.ravel(), float(spacing))
+
+    def neighbor_count(self, bi, particle):
+        return lib().oracle_ssb_neighbor_count(self._h, bi, particle)
+
+    def add_force(self, bid, force, location):
+        lib().oracle_ssb_add_force(self._h, bid, _f64(force), _f64(location))
+
+    def step(self, dt):
+        lib().oracle_ssb_step(self._h, float(dt))
+
+    def samples(self, bi):
+        """(positions, velocities, volumes, center of mass or None)."""
+        n = lib().oracle_ssb_len(self._h, bi)
+        pos, vel, vol, com = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n), np.zeros(3)
+        dyn = lib().oracle_ssb_samples(self._h, bi, pos.reshape(-1), vel.reshape(-1), vol, com)
+        return pos, vel, vol, (com if dyn else None)
 
 
 def integrate_probe(scheme, position, velocity, acceleration, dt, slot_position=None, slot_velocity=None):

@@ -395,6 +395,65 @@ void oracle_surface_grid(size_t n, const double* pos, double h, double cube, lon
   }
 }
 
+// A StaticSampleBoundary driven on its own, the way the reference's unit
+// tests drive it (static_sample_boundary.rs:142-168, 354-412, 544-552):
+// boundaries of given samples (body frame for a dynamic one, world frame for
+// a static one), initialize, find_boundary_samples, add_force_onto_boundary
+// and step_forward_in_time, with the samples, volumes, neighbors and rigid
+// state read back.
+void* oracle_ssb_create() { return new StaticSampleBoundary(); }
+void oracle_ssb_free(void* b) { delete (StaticSampleBoundary*)b; }
+size_t oracle_ssb_count(void* b) { return ((StaticSampleBoundary*)b)->count(); }
+size_t oracle_ssb_len(void* b, size_t bi) { return ((StaticSampleBoundary*)b)->boundaries[bi].xb.size(); }
+int oracle_ssb_add(void* b, size_t nb, const double* pos, const double* rigid) {
+  auto* sb = (StaticSampleBoundary*)b;
+  SampleBoundary sbb;
+  sbb.dynamic = rigid != nullptr;
+  std::vector<V3> p(nb);
+  for (size_t i = 0; i < nb; ++i) p[i] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  if (sbb.dynamic) {
+    sbb.xb_body = p;
+    sbb.xb.assign(nb, V3{});
+    read_rigid(rigid, sbb.state);
+  } else {
+    sbb.xb = p;
+  }
+  sbb.vb.assign(nb, V3{});
+  sbb.vol.assign(nb, 0.);
+  sb->boundaries.push_back(std::move(sbb));
+  return 0;
+}
+void oracle_ssb_initialize(void* b, double h, double gamma) {
+  ((StaticSampleBoundary*)b)->initialize(h, gamma);
+}
+void oracle_ssb_find(void* b, double range, size_t n, const double* pos, double spacing) {
+  std::vector<V3> p(n);
+  for (size_t i = 0; i < n; ++i) p[i] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  ((StaticSampleBoundary*)b)->find_boundary_samples(range, p, spacing);
+}
+size_t oracle_ssb_neighbor_count(void* b, size_t bi, size_t id) {
+  return ((StaticSampleBoundary*)b)->boundaries[bi].nl.count(id);
+}
+void oracle_ssb_add_force(void* b, size_t id, const double* f, const double* loc) {
+  ((StaticSampleBoundary*)b)->add_force_onto_boundary(id, {f[0], f[1], f[2]},
+                                                      {loc[0], loc[1], loc[2]});
+}
+void oracle_ssb_step(void* b, double dt) { ((StaticSampleBoundary*)b)->step_forward_in_time(dt); }
+// positions, velocities (3 per sample) and volumes of boundary bi; returns
+// whether it is dynamic and, if so, writes its center of mass.
+int oracle_ssb_samples(void* b, size_t bi, double* pos, double* vel, double* vol, double* com) {
+  const SampleBoundary& s = ((StaticSampleBoundary*)b)->boundaries[bi];
+  for (size_t i = 0; i < s.xb.size(); ++i) {
+    pos[3 * i] = s.xb[i].x; pos[3 * i + 1] = s.xb[i].y; pos[3 * i + 2] = s.xb[i].z;
+    vel[3 * i] = s.vb[i].x; vel[3 * i + 1] = s.vb[i].y; vel[3 * i + 2] = s.vb[i].z;
+    vol[i] = s.vol[i];
+  }
+  if (!s.dynamic) return 0;
+  com[0] = s.state.center_of_mass.x; com[1] = s.state.center_of_mass.y;
+  com[2] = s.state.center_of_mass.z;
+  return 1;
+}
+
 // IntegrationScheme::integrate on given particle arrays, in place (3n
 // doubles each): scheme 0 EulerCromer (slot pointers unused, may be null),
 // 1 TakePredicted (one position and one velocity slot).

@@ -490,3 +490,23 @@ def test_hashing_cell_size_is_only_a_performance_parameter(oracle):
     assert 1 in _nb(oracle, 6.0, [[0, 0, 0], [5, 0, 0]], cell=10.0)[0]
     # a cell size far below the range searches ceil(range / cell) cells each way
     assert _nb(oracle, 1.0, [[0, 0, 0], [0.5, 0, 0]], cell=0.1) == [[0, 1], [0, 1]]
+
+
+def test_tiny_cube_volume_map_fields_give_usable_boundary_samples(oracle):
+    """volume_map_boundary.rs:169-222 (ignored upstream for its runtime): a
+    cube of half-size 0.1 with h = 0.045 and dx = 4 * 0.0225 builds fields
+    in which a fluid particle on the cube's surface finds a boundary sample
+    of positive, finite volume."""
+    from sphgpu import scenes
+    h, spacing = 0.045, 0.0225
+    verts = scenes.CUBE_VERTICES * 0.1
+    sdf, vm = oracle.build_fields(verts, scenes.CUBE_FACES_OUTWARD, 4 * spacing, h)
+    sc = scenes.Scene(
+        procedures={"integration_scheme": "EulerCromer", "pressure_solver": "SESPH",
+                    "boundary_handling": "VolumeMapBoundary"},
+        parameters={"rest_density_grid_spacing": spacing, "kernel_support_radius": h,
+                    "disable_particles_below": -50.0, "time_increment": 1e-3},
+        cfl_time_step=False, position=np.array([[0.1, 0.0, 0.0]]), mass=np.array([1000.0 * spacing ** 3]))
+    s = build_oracle(sc, fields=(sdf, vm))
+    has, xb, _, vol = s.vm_samples(0)
+    assert has[0] and vol[0] > 0 and np.isfinite(vol[0])
