@@ -1,7 +1,7 @@
 """Seeded synthetic scenes for the SPH engine.
 
 Fluid blocks are cubic lattices with uniform jitter, stored as f32-representable
-values so that an f64 checker sees exactly the positions the f32 engine holds
+values so that an f64 restatement sees exactly the positions the f32 engine holds
 (the reference injects such a state through its `--state` checkpoint path,
 sim_lib sph/setup/mod.rs:142-153). Containers are the reference's cube mesh
 (cube_face_normals_inwards.obj: 8 vertices, 12 inward-facing triangles) under

@@ -1,8 +1,8 @@
 // SPH oracle — TEST INFRASTRUCTURE ONLY.
 //
 // A CPU, f64 restatement of the reference's SPH time-step path
-// (SammyMcFly/fluid-simulation, crate `simulation_lib`). It is the checker the
-// GPU engine is compared against: only `tests/`, `__graft_entry__.smoke()` and
+// (SammyMcFly/fluid-simulation, crate `simulation_lib`). The GPU engine is
+// compared against it: only `tests/`, `__graft_entry__.smoke()` and
 // the `cpu_baseline` / `--impl reference` legs of `bench.py` load it. Nothing in
 // the product (`fluid-simulation_b200/`, `include/`) links or calls it.
 //
