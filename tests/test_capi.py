@@ -47,6 +47,34 @@ def test_config_defaults_follow_reference_parameters():
         make_config(parameters={"no_such_key": 1})
 
 
+def test_procedures_accept_every_documented_variant_name():
+    """Procedures deserialization (ST/sph/setup/input.rs:390-470,
+    ST/sph/pressure_solver/mod.rs:50-72, ST/sph/boundary_handling/mod.rs:49-63):
+    every combination of the path's variant names builds a config, the
+    doc-comment spelling "CubicBSpline" and unknown names are rejected.
+    ExplicitEuler and Verlet are reference variants outside this engine and
+    are rejected by name rather than run as something else."""
+    import itertools
+
+    from sphgpu import make_config
+    from sphgpu.system import PROCEDURES
+    names = {"kernel_function": ["CubicBSpline3D"], "integration_scheme": ["EulerCromer", "TakePredicted"],
+             "pressure_solver": ["SESPH", "SESPHwSplitting", "IISPH", "IISPHwOST"],
+             "neighbor_search": ["SpatialHashing"],
+             "boundary_handling": ["StaticSampleBoundary", "VolumeMapBoundary"]}
+    assert {k: sorted(v) for k, v in names.items()} == {k: sorted(v) for k, v in PROCEDURES.items()}
+    seen = set()
+    for combo in itertools.product(*names.values()):
+        c = make_config(dict(zip(names, combo)))
+        seen.add((c.kernel_fn, c.integration_scheme, c.pressure_solver, c.neighbor_search, c.boundary_handling))
+    assert len(seen) == 16  # every combination maps to its own config
+    for key, bad in (("kernel_function", "CubicBSpline"), ("kernel_function", "NotARealKernel"),
+                     ("pressure_solver", "NotARealSolver"), ("boundary_handling", "NotARealBoundaryHandling"),
+                     ("integration_scheme", "ExplicitEuler"), ("integration_scheme", "Verlet")):
+        with pytest.raises(ValueError, match=bad):
+            make_config({key: bad})
+
+
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
 def test_no_device_is_an_error_status_not_a_fallback():
     from sphgpu import GpuSystem, SPHError, make_config
