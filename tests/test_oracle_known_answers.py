@@ -53,6 +53,24 @@ def test_kernel_gradient_zero_at_origin_and_antisymmetric(oracle):
     assert np.dot(g1, r) < 0
 
 
+def test_kernel_trait_default_methods(oracle):
+    """KernelFn's default q / kernel_function / kernel_gradient
+    (ST/sph/kernel/mod.rs:42-166, there on a dummy kernel, here on the cubic
+    spline): W = alpha/h^3 w(|r|/h), grad W = alpha/h^4 r/|r| w'(q), radial
+    symmetry, h^-3 and h^-4 scaling, a gradient parallel to r."""
+    r, h = np.array([0.3, 0.4, 0.0]), 1.25  # |r| = 0.5, q = 0.4
+    q = 0.5 / h
+    assert abs(oracle.kernel_function(r, h) - ALPHA / h ** 3 * oracle.kernel_w(q)) < 1e-12
+    g = oracle.kernel_gradient(r, h)
+    assert np.linalg.norm(g - ALPHA / h ** 4 * r / 0.5 * oracle.kernel_dqw(q)) < 1e-12
+    assert abs(oracle.kernel_function([0.5, 0, 0], h) - oracle.kernel_function([0, 0, -0.5], h)) < 1e-12
+    a = np.array([0.2, -0.1, 0.3])
+    for k in (2.0, 3.0):
+        assert abs(oracle.kernel_function(k * a, k * h) - oracle.kernel_function(a, h) / k ** 3) < 1e-9
+        assert np.linalg.norm(oracle.kernel_gradient(k * a, k * h) - oracle.kernel_gradient(a, h) / k ** 4) < 1e-9
+    assert np.linalg.norm(np.cross(oracle.kernel_gradient(a, 1.0), a)) < 1e-12
+
+
 def test_kernel_integrates_to_one(oracle):
     # radial Gauss-Legendre quadrature of 4 pi r^2 W(r) on the two polynomial
     # pieces [0, h/2] and [h/2, h] (exact for these degrees)
