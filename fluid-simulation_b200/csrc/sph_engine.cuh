@@ -28,6 +28,11 @@
 namespace sph {
 
 constexpr int kBlock = 256;
+// List batches the Jacobi sweep passes keep in flight ahead of the one they consume.
+#ifndef SPH_SWEEP_PREFETCH
+#define SPH_SWEEP_PREFETCH 2
+#endif
+constexpr int kSweepPrefetch = SPH_SWEEP_PREFETCH;
 constexpr int kMaxBodies = 32;
 
 // Per-scene scalars that stay on the device so that a step needs no host

@@ -1214,48 +1214,56 @@ __device__ __forceinline__ void body_accum_flush(double* sh, int nbodies, double
 // records are loaded, then consumed, so NB loads are in flight per thread.
 // Slots past the count read position 0, which every non-empty halo has.
 // ---------------------------------------------------------------------------
-// The first batch of a particle's list, requested ahead of use (a kernel can
-// issue it before it waits for its halo staging).
-template <int NB>
+// The first D batches of a particle's list, requested ahead of use (a kernel
+// can issue them before it waits for its halo staging).
+template <int NB, int D = 1>
 struct ListHead {
-  uint2 g[NB / 4];
+  uint2 g[D][NB / 4];
 };
-template <int NB>
-__device__ __forceinline__ ListHead<NB> list_head(const uint16_t* __restrict__ nbr, int K, int i, int cnt) {
-  ListHead<NB> h;
+template <int NB, int D = 1>
+__device__ __forceinline__ ListHead<NB, D> list_head(const uint16_t* __restrict__ nbr, int K, int i, int cnt) {
+  ListHead<NB, D> h;
   const uint2* base = reinterpret_cast<const uint2*>(nbr) + nbr_slot(i, 0, K) / 4;
   const int ngroups = (cnt + 3) >> 2;
 #pragma unroll
-  for (int g = 0; g < NB / 4; ++g) h.g[g] = g < ngroups ? __ldcs(base + (size_t)g * 32) : make_uint2(0u, 0u);
+  for (int d = 0; d < D; ++d)
+#pragma unroll
+    for (int g = 0; g < NB / 4; ++g) {
+      const int gi = d * (NB / 4) + g;
+      h.g[d][g] = gi < ngroups ? __ldcs(base + (size_t)gi * 32) : make_uint2(0u, 0u);
+    }
   return h;
 }
 
-template <int NB, class Load, class Use>
+// Visits the neighbors of particle i in batches of NB: while a batch is
+// consumed, the list words of the batch D ahead are in flight.
+template <int NB, int D, class Load, class Use>
 __device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ nbr, int K, int i, int cnt,
-                                                  const ListHead<NB>& head, Load&& load, Use&& use) {
+                                                  const ListHead<NB, D>& head, Load&& load, Use&& use) {
   static_assert(NB % 4 == 0, "neighbors are read in groups of four");
-  // group g of this lane sits 32 uint2 after group g-1; the next batch's
-  // groups are requested before the current batch is consumed
+  // group g of this lane sits 32 uint2 after group g-1
   const uint2* base = reinterpret_cast<const uint2*>(nbr) + nbr_slot(i, 0, K) / 4;
   const int ngroups = (cnt + 3) >> 2;
-  uint2 cur[NB / 4];
+  uint2 q[D][NB / 4];
 #pragma unroll
-  for (int g = 0; g < NB / 4; ++g) cur[g] = head.g[g];
+  for (int d = 0; d < D; ++d)
+#pragma unroll
+    for (int g = 0; g < NB / 4; ++g) q[d][g] = head.g[d][g];
   for (int k0 = 0; k0 < cnt; k0 += NB) {
     uint2 nxt[NB / 4];
 #pragma unroll
     for (int g = 0; g < NB / 4; ++g) {
-      const int gi = (k0 + NB) / 4 + g;
+      const int gi = (k0 + D * NB) / 4 + g;
       nxt[g] = gi < ngroups ? __ldcs(base + (size_t)gi * 32) : make_uint2(0u, 0u);
     }
     uint32_t l[NB];
 #pragma unroll
     for (int g = 0; g < NB / 4; ++g) {
-      const uint2 q = cur[g];
-      l[4 * g + 0] = k0 + 4 * g + 0 < cnt ? (q.x & 0xffffu) : 0u;
-      l[4 * g + 1] = k0 + 4 * g + 1 < cnt ? (q.x >> 16) : 0u;
-      l[4 * g + 2] = k0 + 4 * g + 2 < cnt ? (q.y & 0xffffu) : 0u;
-      l[4 * g + 3] = k0 + 4 * g + 3 < cnt ? (q.y >> 16) : 0u;
+      const uint2 w = q[0][g];
+      l[4 * g + 0] = k0 + 4 * g + 0 < cnt ? (w.x & 0xffffu) : 0u;
+      l[4 * g + 1] = k0 + 4 * g + 1 < cnt ? (w.x >> 16) : 0u;
+      l[4 * g + 2] = k0 + 4 * g + 2 < cnt ? (w.y & 0xffffu) : 0u;
+      l[4 * g + 3] = k0 + 4 * g + 3 < cnt ? (w.y >> 16) : 0u;
     }
     decltype(load(0u)) d[NB];
 #pragma unroll
@@ -1264,13 +1272,17 @@ __device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ n
     for (int u = 0; u < NB; ++u)
       if (k0 + u < cnt) use(d[u]);
 #pragma unroll
-    for (int g = 0; g < NB / 4; ++g) cur[g] = nxt[g];
+    for (int e = 0; e + 1 < D; ++e)
+#pragma unroll
+      for (int g = 0; g < NB / 4; ++g) q[e][g] = q[e + 1][g];
+#pragma unroll
+    for (int g = 0; g < NB / 4; ++g) q[D - 1][g] = nxt[g];
   }
 }
 template <int NB, class Load, class Use>
 __device__ __forceinline__ void for_each_neighbor(const uint16_t* __restrict__ nbr, int K, int i, int cnt,
                                                   Load&& load, Use&& use) {
-  for_each_neighbor<NB>(nbr, K, i, cnt, list_head<NB>(nbr, K, i, cnt), load, use);
+  for_each_neighbor<NB, 1>(nbr, K, i, cnt, list_head<NB, 1>(nbr, K, i, cnt), load, use);
 }
 
 // Shared-memory layout of staged halo records: arrays of R4 then arrays of R,
@@ -1431,12 +1443,12 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = i < sc->n_active;
   int cnt = 0;
-  ListHead<NB> head{};
+  ListHead<NB, kSweepPrefetch> head{};
   R4<R> xi{};
   R mi = 1, pi = 0;
   if (act) {
     cnt = min((int)N.ncnt[i], N.K);
-    head = list_head<NB>(N.nbr, N.K, i, cnt);
+    head = list_head<NB, kSweepPrefetch>(N.nbr, N.K, i, cnt);
     xi = xv[i];
     mi = vel[i].w;
     pi = press[i];
@@ -1582,12 +1594,12 @@ __global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
   const int n = sc->n_active;
   const bool act = i < n;
   int cnt = 0;
-  ListHead<NB> head{};
+  ListHead<NB, kSweepPrefetch> head{};
   R4<R> xi{}, ai{}, bg{};
   R aii = 0, s = 0, p0 = 0;
   if (act) {
     cnt = min((int)N.ncnt[i], N.K);
-    head = list_head<NB>(N.nbr, N.K, i, cnt);
+    head = list_head<NB, kSweepPrefetch>(N.nbr, N.K, i, cnt);
     xi = xv[i];
     ai = accp[i];
     aii = aii_in[i];
