@@ -103,6 +103,8 @@ def lib():
         "oracle_boundary_volumes": (i, [vp, sz, dp]),
         "oracle_vm_samples": (i, [vp, sz, u8p, dp, dp, dp]),
         "oracle_rigid_state": (i, [vp, sz, dp]),
+        "oracle_fluid_probe": (i, [sz, dp, dp, u32p, vp, sz, vp, i, dp, dp, u32p,
+                                   np.ctypeslib.ndpointer(np.uintp, flags="C")]),
         "oracle_ssb_create": (vp, []),
         "oracle_ssb_free": (None, [vp]),
         "oracle_ssb_count": (sz, [vp]),
@@ -415,6 +417,30 @@ def iisph_initialize_probe(s_f, a_ff, omega, eps, clamp):
     p = np.zeros(s_f.shape[0])
     lib().oracle_iisph_initialize_probe(s_f.shape[0], s_f, a_ff, float(omega), float(eps), 1 if clamp else 0, p)
     return p
+
+
+def fluid_probe(positions, masses, fluid_ids=None, disable=(), drop=False, slots=None):
+    """The oracle's Fluid built from positions, masses and ids, then
+    resize_slots(*slots), disable(id) for each id in turn and drop_inactive.
+    Returns positions, masses and ids (total length), the active and total
+    lengths, the four slot-pool counts and the slot length. A disable that
+    fails the reference's `id < num_active` assertion raises IndexError."""
+    x = _f64(np.reshape(positions, (-1, 3)))
+    n = x.shape[0]
+    m = _f64(np.broadcast_to(masses, (n,)))
+    fid = np.ascontiguousarray(np.zeros(n) if fluid_ids is None else fluid_ids, np.uint32)
+    sl = None if slots is None else np.ascontiguousarray(slots, np.int64)
+    ids = np.ascontiguousarray(disable, np.int64)
+    op, om, of = np.zeros(3 * n), np.zeros(n), np.zeros(n, np.uint32)
+    lens = np.zeros(7, np.uintp)
+    rc = lib().oracle_fluid_probe(n, x.ravel(), m, fid, None if sl is None else sl.ctypes.data, ids.size,
+                                  ids.ctypes.data if ids.size else None, int(bool(drop)), op, om, of, lens)
+    if rc == 1:
+        raise IndexError("Fluid::disable: id >= num_active")
+    total = int(lens[1])
+    return {"position": op.reshape(n, 3)[:total], "mass": om[:total], "fluid_id": of[:total],
+            "len": int(lens[0]), "total_len": total, "slot_counts": [int(v) for v in lens[2:6]],
+            "slot_len": int(lens[6])}
 
 
 class SampleBoundaries:

@@ -395,6 +395,59 @@ void oracle_surface_grid(size_t n, const double* pos, double h, double cube, lon
   }
 }
 
+// Fluid bookkeeping (fluid.rs:113-128, 159-204) driven the way its unit
+// tests drive it: n particles (positions, masses, fluid ids; the rest zero),
+// resize_slots(slots[0..4]) when `slots` is given, disable(id) for each of
+// `ids` in order, drop_inactive when `drop`. Writes the first total_len
+// positions, masses and ids, the active and total lengths, and the four slot
+// pool counts and their length. Returns 1 where the reference's
+// `id < num_active` assertion fails (at the failing disable).
+int oracle_fluid_probe(size_t n, const double* pos, const double* mass, const uint32_t* fid,
+                       const long long* slots, size_t nd, const long long* ids, int drop,
+                       double* out_pos, double* out_mass, uint32_t* out_fid, size_t* out_len) {
+  Fluid f;
+  f.position.resize(n);
+  for (size_t i = 0; i < n; ++i) f.position[i] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  f.velocity.assign(n, V3{});
+  f.acceleration.assign(n, V3{});
+  f.mass.assign(mass, mass + n);
+  f.volume.assign(n, 0.0);
+  f.pressure.assign(n, 0.0);
+  f.fluid_id.assign(fid, fid + n);
+  f.origin.resize(n);
+  for (size_t i = 0; i < n; ++i) f.origin[i] = (uint32_t)i;
+  f.num_active = n;
+  if (slots) f.resize_slots((size_t)slots[0], (size_t)slots[1], (size_t)slots[2], (size_t)slots[3]);
+  for (size_t k = 0; k < nd; ++k) {
+    if (ids[k] < 0) return 1;
+    try {
+      f.disable((size_t)ids[k]);
+    } catch (const std::out_of_range&) {
+      return 1;
+    }
+  }
+  if (drop) f.drop_inactive();
+  const size_t total = f.position.size();
+  for (size_t i = 0; i < total; ++i) {
+    out_pos[3 * i] = f.position[i].x; out_pos[3 * i + 1] = f.position[i].y;
+    out_pos[3 * i + 2] = f.position[i].z;
+    out_mass[i] = f.mass[i];
+    out_fid[i] = f.fluid_id[i];
+  }
+  out_len[0] = f.len();
+  out_len[1] = total;
+  out_len[2] = f.integrator_position_slots.size();
+  out_len[3] = f.integrator_velocity_slots.size();
+  out_len[4] = f.solver_position_slots.size();
+  out_len[5] = f.solver_velocity_slots.size();
+  size_t slot_len = 0;
+  for (auto* pool : {&f.integrator_position_slots, &f.integrator_velocity_slots,
+                     &f.solver_position_slots, &f.solver_velocity_slots})
+    for (auto& sl : *pool) slot_len = std::max(slot_len, sl.size());
+  out_len[6] = slot_len;
+  return 0;
+}
+
 // A StaticSampleBoundary driven on its own, the way the reference's unit
 // tests drive it (static_sample_boundary.rs:142-168, 354-412, 544-552):
 // boundaries of given samples (body frame for a dynamic one, world frame for

@@ -216,7 +216,8 @@ void Fluid::swap(size_t a, size_t b) {
                      &solver_position_slots, &solver_velocity_slots})
     for (auto& s : *pool) std::swap(s[a], s[b]);
 }
-void Fluid::disable(size_t id) {
+void Fluid::disable(size_t id) {  // fluid.rs:159-163
+  if (id >= num_active) throw std::out_of_range("Fluid::disable: id >= num_active");
   num_active -= 1;
   swap(id, num_active);
 }
