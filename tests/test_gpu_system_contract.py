@@ -1,7 +1,9 @@
 """The SPHSystem contract of the reference's system-level tests
-(simulation_lib/tests/sph/mod.rs:149-530), restated on the engine through the
-C ABI: a fluid-only scene (no boundary geometry) built the way the
-reference's minimal scene is, stepped, measured, read back and cloned.
+(simulation_lib/tests/sph/mod.rs:149-530) and of its system constructor's
+(tests/sph/setup/mod.rs:286-465), restated on the engine through the C ABI:
+a fluid-only scene (no boundary geometry) built the way the reference's
+minimal scene is, stepped, measured, read back and cloned, for every solver
+with its integration scheme, and the pairings the constructor refuses.
 """
 import numpy as np
 import pytest
@@ -150,3 +152,37 @@ def test_clones_evolve_independently(A):
     assert g.time_steps_propagated() == 1 and c.time_steps_propagated() == 0
     g.close()
     c.close()
+
+
+def test_every_pressure_solver_builds_and_steps_with_its_integrator(A):
+    # setup/mod.rs:382-431: each solver with the scheme it pairs with, on
+    # volume-map handling without geometry; a sweep cap bounds IISPH here
+    from sphgpu import scenes
+    for solver, scheme in (("SESPH", "EulerCromer"), ("SESPHwSplitting", "EulerCromer"), ("IISPH", "EulerCromer"),
+                           ("IISPHwOST", "TakePredicted")):
+        sc = _scene()
+        sc.procedures = dict(sc.procedures, pressure_solver=solver, integration_scheme=scheme,
+                             boundary_handling="VolumeMapBoundary")
+        g = scenes.build_system(sc, extra_parameters={"max_solver_iterations": 100})
+        t0 = g.time()
+        g.step_forward_in_time()
+        assert g.time() >= t0 and g.time_steps_propagated() == 1, solver
+        assert np.all(np.isfinite(g.download(A.FIELD_POSITION))), solver
+        g.close()
+
+
+def test_pairing_checks_of_the_system_constructor(A):
+    # setup/mod.rs:286-336 and the pairing rules of setup/mod.rs:229-244:
+    # IISPHwOST only with TakePredicted and never with a dynamic boundary
+    from sphgpu import scenes
+    for solver, scheme in (("SESPH", "TakePredicted"), ("IISPHwOST", "EulerCromer")):
+        sc = _scene()
+        sc.procedures = dict(sc.procedures, pressure_solver=solver, integration_scheme=scheme)
+        with pytest.raises(A.SPHError) as e:
+            scenes.build_system(sc)
+        assert e.value.code == A.SPH_ERR_INVALID
+    sc = scenes.floating_cube_scene()
+    sc.procedures = dict(sc.procedures, pressure_solver="IISPHwOST", integration_scheme="TakePredicted")
+    with pytest.raises(A.SPHError) as e:
+        scenes.build_system(sc)
+    assert e.value.code == A.SPH_ERR_INVALID and "dynamic" in str(e.value)
