@@ -325,6 +325,31 @@ def test_serendipity_reproduces_constant_and_linear_fields(oracle):
     assert F.function([2.0, 0.1, 0.1]) is None   # out of bounds
 
 
+def test_serendipity_bounds_clamping_and_pruning(oracle):
+    """ST/utilities/discretization.rs:116-190: out of bounds below and above
+    the domain, the upper corner valid through clamping to the last cell, an
+    entirely pruned domain (absent nodes) and a never-pruned one."""
+    F = _field(oracle, lambda p: 0.0, n=(1, 1, 1), dx=1.0)
+    assert F.function([-0.01, 0.5, 0.5]) is None and F.function([1.01, 0.5, 0.5]) is None
+    C = _field(oracle, lambda p: 4.2, n=(1, 1, 1), dx=1.0)
+    assert abs(C.function([1.0, 1.0, 1.0]) - 4.2) < 1e-9
+    P = _field(oracle, lambda p: 0.0, n=(1, 1, 1), dx=1.0)
+    P.nodes[:] = np.nan
+    assert P.function([0.5, 0.5, 0.5]) is None
+    N = _field(oracle, lambda p: -1000.0, n=(1, 1, 1), dx=1.0)
+    assert abs(N.function([0.5, 0.5, 0.5]) + 1000.0) < 1e-6
+
+
+def test_serendipity_gradient_interior_and_near_the_boundary(oracle):
+    """ST/utilities/discretization.rs:192-230: central differences with
+    h = dx/6 recover a linear field's gradient inside, and a stencil point
+    beyond the domain is an error, not a one-sided fallback."""
+    L = _field(oracle, lambda p: 2 * p[0] - p[1] + 0.5 * p[2], n=(2, 2, 2), dx=1.0, x_min=(-1, -1, -1))
+    assert np.linalg.norm(L.gradient([0.0, 0.0, 0.0]) - [2, -1, 0.5]) < 1e-2
+    one = _field(oracle, lambda p: 0.0, n=(1, 1, 1), dx=2.0, x_min=(-1, -1, -1))
+    assert one.gradient([0.9, 0.0, 0.0]) is None
+
+
 def test_gauss_legendre_ball_volume(oracle):
     # SDF uniformly far inside the boundary -> integrand 1 -> ball volume, and
     # the band case integrates the cubic extension function
