@@ -142,6 +142,7 @@ def lib():
         "oracle_volume_at": (i, [dp, i64p, dp, dp, d, i, dp]),
         "oracle_rigid_body_step": (i, [dp, dp, dp, i, d, i, dp]),
         "oracle_iisph_probe": (i, [dp, dp, d, d, d, d, d, d, d, d, vp, d, i, dp]),
+        "oracle_iisph_solve_probe": (i, [dp, dp, d, d, dp, d, d, d, d, d, d, d, vp, d, vp, dp]),
         "oracle_num_threads": (i, []),
         "oracle_set_num_threads": (None, [i]),
     }
@@ -283,6 +284,21 @@ def rigid_body_step(init32, forces, locations, dt, n_steps=1):
     lib().oracle_rigid_body_step(_f64(init32), fr.ravel(), lc.ravel(), fr.shape[0], float(dt),
                                  int(n_steps), out)
     return out
+
+
+def iisph_solve_probe(pos, vel, mass, volume, acc0, dt, h, spacing, gamma_p, omega, eps, tde, bpos=None,
+                      bvol=0.0, com=None):
+    """IISPH::solve_and_add_acceleration for one particle and at most one
+    boundary sample (dynamic when `com` is given). Returns pressure,
+    acceleration, sweeps, predicted density error, body force, body torque."""
+    out = np.zeros(12)
+    keep = [None if v is None else _f64(v) for v in (bpos, com)]
+    rc = lib().oracle_iisph_solve_probe(_f64(pos), _f64(vel), float(mass), float(volume), _f64(acc0), float(dt),
+                                        float(h), float(spacing), float(gamma_p), float(omega), float(eps),
+                                        float(tde), None if keep[0] is None else keep[0].ctypes.data, float(bvol),
+                                        None if keep[1] is None else keep[1].ctypes.data, out)
+    assert rc == 0
+    return out[0], out[1:4], int(out[4]), out[5], out[6:9], out[9:12]
 
 
 def iisph_probe(pos, vel, mass, volume, dt, h, spacing, gamma_p, omega, eps, bpos, bvol, after):

@@ -877,6 +877,71 @@ void oracle_set_num_threads(int n) { set_num_threads(n); }
 }  // extern "C"
 
 extern "C" {
+// IISPH::solve_and_add_acceleration (iisph.rs:55-96) for one fluid particle
+// with a pre-existing acceleration and at most one boundary sample that is its
+// Normal neighbor; `com` non-null makes that boundary a dynamic body with the
+// given center of mass (the reference's MockBoundary tests,
+// simulation_lib/tests/sph/pressure_solver/iisph.rs:495-592). out: pressure,
+// acceleration (3), sweeps, predicted density error, the force and torque the
+// body received (6).
+int oracle_iisph_solve_probe(const double* pos, const double* vel, double mass, double volume,
+                             const double* acc0, double dt, double h, double spacing,
+                             double gamma_p, double omega, double eps, double tde,
+                             const double* bpos, double bvol, const double* com, double* out) {
+  System s;
+  s.params.time_increment = dt;
+  s.params.kernel_support_radius = h;
+  s.params.rest_density_grid_spacing = spacing;
+  s.params.rest_volume = spacing * spacing * spacing;
+  s.params.boundary_pressure_acceleration_weighting = gamma_p;
+  s.sp.relaxation_factor = omega;
+  s.sp.min_diagonal_element = eps;
+  s.sp.target_density_error = tde;
+  auto sb = std::make_unique<StaticSampleBoundary>();
+  if (bpos) {
+    SampleBoundary b;
+    b.xb = {V3{bpos[0], bpos[1], bpos[2]}};
+    b.vb = {V3{}};
+    b.vol = {bvol};
+    b.nl.indices = {0};
+    b.nl.offsets = {0, 1};
+    if (com) {
+      b.dynamic = true;
+      b.xb_body = b.xb;
+      b.state.center_of_mass = V3{com[0], com[1], com[2]};
+    }
+    sb->boundaries.push_back(std::move(b));
+  }
+  s.boundary = std::move(sb);
+  Fluid& f = s.fluid;
+  f.num_active = 1;
+  f.position = {V3{pos[0], pos[1], pos[2]}};
+  f.velocity = {V3{vel[0], vel[1], vel[2]}};
+  f.acceleration = {V3{acc0[0], acc0[1], acc0[2]}};
+  f.mass = {mass};
+  f.volume = {volume};
+  f.pressure = {0.0};
+  f.fluid_id = {0};
+  f.origin = {0};
+  f.resize_slots(0, 0, 1, 1);
+  s.fluid_nl.indices.clear();
+  s.fluid_nl.offsets = {0, 0};
+  s.iisph_solve();
+  out[0] = f.pressure[0];
+  out[1] = f.acceleration[0].x; out[2] = f.acceleration[0].y; out[3] = f.acceleration[0].z;
+  out[4] = s.iisph.last_solver_iterations;
+  out[5] = s.iisph.predicted_density_error;
+  V3 F{}, T{};
+  if (bpos && com) {
+    RigidBodyMotion* m = s.boundary->at(0).motion();
+    F = m->force;
+    T = m->torque;
+  }
+  out[6] = F.x; out[7] = F.y; out[8] = F.z;
+  out[9] = T.x; out[10] = T.y; out[11] = T.z;
+  return 0;
+}
+
 // Single fluid particle with one static boundary sample of given volume
 // (the reference's IISPH MockBoundary tests, simulation_lib/tests/sph/
 // pressure_solver/iisph.rs:158-490): runs set_pred_vel, the volume-preserving

@@ -263,6 +263,31 @@ def test_iisph_expansion_never_gives_negative_pressure(oracle):
     assert sf > 0 and p == 0.0
 
 
+def test_iisph_isolated_particle_at_rest_volume_is_a_noop(oracle):
+    """ST/sph/pressure_solver/iisph.rs:495-535: no neighbors -> zero diagonal,
+    zero pressure, the pre-existing acceleration untouched. The test there
+    expects 2 sweeps; the code's TargetDensityError stop (`iter > 2 && err <
+    tde`, iisph.rs:378-393) gives 3, and the oracle follows the code."""
+    acc0 = np.array([0.0, 0.0, -9.81])
+    v0 = 0.3 * 0.3 * 0.3  # powi(3) multiplies, as the oracle's rest volume does
+    p, acc, sweeps, err, _, _ = oracle.iisph_solve_probe(
+        [0, 0, 0], [0, 0, 0], 0.5, v0, acc0, 0.05, 1.0, 0.3, 0.0, 0.5, 1e-9, 0.01)
+    assert p == 0.0 and np.array_equal(acc, acc0)
+    assert sweeps == 3 and err == 0.0
+
+
+def test_iisph_registers_the_reaction_on_a_dynamic_body_once(oracle):
+    """ST/sph/pressure_solver/iisph.rs:538-592: only the final pressure
+    acceleration registers a reaction force, equal and opposite to the
+    particle's pressure force, however many sweeps ran."""
+    p, acc, sweeps, _, F, T = oracle.iisph_solve_probe(
+        [0, 0, 0], [0, 0, 0], 0.5, 0.3 * 0.3 * 0.3 * 0.5, [0, 0, 0], 0.05, 1.0, 0.3, 1.0, 0.5, 1e-9, 0.01,
+        bpos=[0.2, 0, 0], bvol=0.01, com=[5.0, 0, 0])
+    assert p > 0 and sweeps >= 3 and np.linalg.norm(F) > 0
+    assert np.linalg.norm(F - (-0.5 * acc)) < 1e-9
+    assert np.linalg.norm(T - np.cross(np.array([0.2, 0, 0]) - [5.0, 0, 0], F)) < 1e-9
+
+
 # ---- rigid body -----------------------------------------------------------------------------
 def _rigid_init(mass=2.0, I=(1.0, 2.0, 3.0), com=(0, 0, 0), q=(1, 0, 0, 0), v=(0, 0, 0), w=(0, 0, 0)):
     Ib = np.diag(I)
