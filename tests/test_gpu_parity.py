@@ -6,7 +6,7 @@ every kernel exists for the precision study):
     per-particle sort) on identical input states, both precisions;
   * per-particle fields from the same input state: f64 engine within 1e-9
     relative of the oracle; f32 engine within the tolerances stated per test
-    (volume/density 1e-5 relative, the north-star bar being 1e-4);
+    (volume/density 1e-5 relative, inside the 1e-4 density bar of the design);
   * IISPH sweep counts: equal for f64, within +-1 for f32.
 """
 import numpy as np
@@ -141,9 +141,9 @@ def test_sesph_multistep_tracks_oracle(A, oracle, sesph_scene):
 # ---------------------------------------------------------------------------------------
 # IISPH with a VolumeMapBoundary box (small, fields built by the oracle)
 # ---------------------------------------------------------------------------------------
-# Both the engine and the oracle cap the solve (the north-star configuration
-# caps at 100); with the fluid 1.5 spacings from the walls it converges in a
-# few sweeps, so the cap only bounds the test's run time.
+# Both the engine and the oracle cap the solve (the 1M benchmark caps at 100
+# sweeps); with the fluid 1.5 spacings from the walls it converges in a few
+# sweeps, so the cap only bounds the test's run time.
 VM_CAP = 40
 
 
