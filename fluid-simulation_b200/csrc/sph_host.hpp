@@ -95,6 +95,9 @@ class SystemBase {
   virtual bool chunk_ready() = 0;
   virtual ChunkOutcome chunk_finish() = 0;
   virtual uint64_t graph_replays() const = 0;
+  // Result-invariant launch parameters of the neighbor passes (sph_tuning).
+  virtual void get_tuning(sph_tuning* out) const = 0;
+  virtual void set_tuning(const sph_tuning& t) = 0;
   int device = 0;
 };
 

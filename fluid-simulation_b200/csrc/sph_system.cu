@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -74,6 +75,10 @@ static void allow_smem(const void* fn, size_t bytes) {
   have = bytes;
 }
 
+// Shared memory one block may use (sm_100: 227 KB with the opt-in) and what
+// the staging passes keep aside for their static arrays.
+constexpr size_t kMaxSmemPerBlock = 232448;
+constexpr size_t kStaticSmemReserve = 4096;
 static int blocks_for(long long n) { return (int)std::max(1LL, (n + kBlock - 1) / kBlock); }
 static size_t round_up(size_t n, size_t m) { return (n + m - 1) / m * m; }
 
@@ -1522,6 +1527,23 @@ class System : public SystemBase {
   uint32_t step_graph_chunk() const override { return graph_chunk_; }
   uint64_t graph_replays() const override { return graph_replays_; }
 
+  void get_tuning(sph_tuning* out) const override {
+    out->gather_batch = (uint32_t)nb_;
+    out->halo_stage = (uint32_t)hs_;
+  }
+  void set_tuning(const sph_tuning& t) override {
+    if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
+    if (t.gather_batch != 4 && t.gather_batch != 8) throw Error(SPH_ERR_INVALID, "gather batch must be 4 or 8");
+    // the widest staged record is {x, v, m} of the source/diagonal pass
+    const size_t record = 2 * sizeof(R4<R>) + sizeof(R);
+    if (t.halo_stage > 65535u || (size_t)t.halo_stage * record + kStaticSmemReserve > kMaxSmemPerBlock)
+      throw Error(SPH_ERR_INVALID, "halo stage exceeds a block's shared memory");
+    if ((int)t.gather_batch == nb_ && (int)t.halo_stage == hs_) return;
+    nb_ = (int)t.gather_batch;
+    hs_ = (int)t.halo_stage;
+    destroy_graphs();  // the captured launches carry the old parameters
+  }
+
   void chunk_begin(uint32_t c) override {
     if (!initialized_) throw Error(SPH_ERR_STATE, "initialize before stepping");
     if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
@@ -2557,6 +2579,9 @@ int sph_clone(const sph_system_t* src, sph_system_t** out) {
     }
     h->impl->restore(s->steps(), s->time(), n, x.data(), v.data(), m.data(), fid.data(),
                      xi.empty() ? nullptr : xi.data(), vvi.empty() ? nullptr : vvi.data());
+    sph_tuning t;
+    s->get_tuning(&t);
+    h->impl->set_tuning(t);
     h->impl->set_step_graphs(s->step_graph_chunk());
     *out = guard.release();
   });
@@ -2566,6 +2591,67 @@ int sph_launch_count(const sph_system_t* h, uint64_t* out) {
   return guarded([&] {
     if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
     *out = h->impl->launches();
+  });
+}
+int sph_get_tuning(const sph_system_t* h, sph_tuning* out) {
+  return guarded([&] {
+    if (!h || !out) throw Error(SPH_ERR_INVALID, "null argument");
+    h->impl->get_tuning(out);
+  });
+}
+int sph_set_tuning(sph_system_t* h, const sph_tuning* tuning) {
+  return guarded([&] {
+    if (!h || !tuning) throw Error(SPH_ERR_INVALID, "null argument");
+    set_device(h);
+    h->impl->set_tuning(*tuning);
+  });
+}
+int sph_autotune(sph_system_t* h, uint32_t steps, sph_tuning* best, double* best_ms_per_step) {
+  return guarded([&] {
+    if (!h || !best) throw Error(SPH_ERR_INVALID, "null argument");
+    if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize before tuning");
+    if (steps == 0) throw Error(SPH_ERR_INVALID, "tuning needs at least one timed step");
+    set_device(h);
+    const bool f32 = h->cfg.precision == SPH_F32;
+    std::vector<sph_tuning> cand;
+    for (uint32_t nb : {4u, 8u})
+      for (uint32_t hs : f32 ? std::vector<uint32_t>{1024, 1536, 2048} : std::vector<uint32_t>{512, 1024, 1536})
+        cand.push_back(sph_tuning{nb, hs});
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    sph::cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+    std::unique_ptr<CUevent_st, cudaError_t (*)(cudaEvent_t)> g0(e0, cudaEventDestroy);
+    sph::cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+    std::unique_ptr<CUevent_st, cudaError_t (*)(cudaEvent_t)> g1(e1, cudaEventDestroy);
+    auto advance = [](sph_system_t* k, uint32_t n) {
+      const int rc = sph_step(k, n);
+      if (rc != SPH_OK && rc != SPH_NOT_CONVERGED) throw Error(rc, sph_last_error());
+    };
+    double best_t = std::numeric_limits<double>::infinity();
+    sph_tuning pick{};
+    h->impl->get_tuning(&pick);
+    for (const sph_tuning& c : cand) {
+      sph_system_t* k = nullptr;
+      int rc = sph_clone(h, &k);
+      if (rc) throw Error(rc, sph_last_error());
+      std::unique_ptr<sph_system_t, void (*)(sph_system_t*)> guard(k, sph_destroy);
+      k->impl->set_tuning(c);
+      advance(k, 1);  // warm-up: graph capture and list capacity
+      cudaStream_t st = (cudaStream_t)k->impl->stream();
+      sph::cuda_check(cudaEventRecord(e0, st), "cudaEventRecord");
+      advance(k, steps);
+      sph::cuda_check(cudaEventRecord(e1, st), "cudaEventRecord");
+      sph::cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+      float ms = 0.f;
+      sph::cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+      const double per = (double)ms / (double)steps;
+      if (per < best_t) {
+        best_t = per;
+        pick = c;
+      }
+    }
+    h->impl->set_tuning(pick);
+    *best = pick;
+    if (best_ms_per_step) *best_ms_per_step = best_t;
   });
 }
 int sph_set_step_graphs(sph_system_t* h, uint32_t chunk_steps) {

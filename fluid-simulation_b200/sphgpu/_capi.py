@@ -120,6 +120,10 @@ class SphSceneResult(C.Structure):
                 ("graph_replays", C.c_uint64), ("kernel_launches", C.c_uint64)]
 
 
+class SphTuning(C.Structure):
+    _fields_ = [("gather_batch", C.c_uint32), ("halo_stage", C.c_uint32)]
+
+
 class SphServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in (
         "submitted", "completed", "queued", "active", "peak_active", "budget_bytes", "reserved_bytes",
@@ -245,6 +249,9 @@ SIGNATURES = {
     "sph_device_bytes": (C.c_int, [_vp, C.POINTER(_sz)]),
     "sph_set_step_graphs": (C.c_int, [_vp, C.c_uint32]),
     "sph_graph_replays": (C.c_int, [_vp, C.POINTER(C.c_uint64)]),
+    "sph_get_tuning": (C.c_int, [_vp, C.POINTER(SphTuning)]),
+    "sph_set_tuning": (C.c_int, [_vp, C.POINTER(SphTuning)]),
+    "sph_autotune": (C.c_int, [_vp, C.c_uint32, C.POINTER(SphTuning), C.POINTER(C.c_double)]),
     "sph_server_create": (C.c_int, [C.POINTER(SphServerConfig), C.POINTER(_vp)]),
     "sph_server_submit": (C.c_int, [_vp, C.POINTER(SphSceneRequest), C.POINTER(C.c_uint64)]),
     "sph_server_poll": (C.c_int, [_vp, C.c_uint64, C.POINTER(SphSceneResult)]),

@@ -467,6 +467,23 @@ class GpuSystem:
         A.check(self._L.sph_graph_replays(self._h, C.byref(out)))
         return out.value
 
+    def tuning(self) -> dict:
+        """Result-invariant launch parameters of the neighbor passes."""
+        t = A.SphTuning()
+        A.check(self._L.sph_get_tuning(self._h, C.byref(t)))
+        return {"gather_batch": t.gather_batch, "halo_stage": t.halo_stage}
+
+    def set_tuning(self, gather_batch: int, halo_stage: int):
+        t = A.SphTuning(int(gather_batch), int(halo_stage))
+        A.check(self._L.sph_set_tuning(self._h, C.byref(t)))
+
+    def autotune(self, steps: int = 5) -> dict:
+        """Times each candidate tuning on a clone, applies the fastest and
+        returns it with its milliseconds per step; this system does not step."""
+        t, ms = A.SphTuning(), C.c_double()
+        A.check(self._L.sph_autotune(self._h, int(steps), C.byref(t), C.byref(ms)))
+        return {"gather_batch": t.gather_batch, "halo_stage": t.halo_stage, "ms_per_step": ms.value}
+
 
 # ---- per-trait shims ------------------------------------------------------------------
 def find_samples(search_range, positions, samples, device=0):

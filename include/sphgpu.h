@@ -342,6 +342,28 @@ int sph_set_step_graphs(sph_system_t* h, uint32_t chunk_steps);
 /* Chunks replayed on the per-step path since creation. */
 int sph_graph_replays(const sph_system_t* h, uint64_t* out);
 
+/* ---- launch tuning -------------------------------------------------------- */
+/* Launch parameters of the neighbor passes that leave every result bit for bit
+ * unchanged (the reference has no counterpart; its passes run on the CPU):
+ * the number of neighbors a thread gathers per batch (4 or 8) and the halo
+ * records a block copies to shared memory before its neighbor loop (blocks
+ * with larger halos, and every block at 0, gather from global memory). The
+ * records must fit one block's shared memory. Setting them re-captures the
+ * step graphs; clones inherit them. */
+typedef struct sph_tuning {
+  uint32_t gather_batch;
+  uint32_t halo_stage;
+} sph_tuning;
+int sph_get_tuning(const sph_system_t* h, sph_tuning* out);
+int sph_set_tuning(sph_system_t* h, const sph_tuning* tuning);
+/* Autotuner: for each candidate tuning (gather batch 4 and 8 times three
+ * staging capacities per precision) it clones the system, runs one warm-up
+ * step and times `steps` steps on the clone's stream with CUDA events, then
+ * applies the fastest to `h` and returns it with its time per step in
+ * milliseconds (best_ms_per_step may be NULL). The system's own state does
+ * not advance. */
+int sph_autotune(sph_system_t* h, uint32_t steps, sph_tuning* best, double* best_ms_per_step);
+
 /* ---- diagnostics -------------------------------------------------------- */
 /* Scalars of the last completed update, read from the host copy the step
  * already made (no device work). */

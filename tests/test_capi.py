@@ -92,6 +92,9 @@ def test_null_arguments_are_rejected():
     assert lib.sph_create(None, None) == _capi.SPH_ERR_INVALID
     assert lib.sph_step(None, 1) == _capi.SPH_ERR_INVALID
     assert lib.sph_last_error() == b"null argument"
+    assert lib.sph_get_tuning(None, None) == _capi.SPH_ERR_INVALID
+    assert lib.sph_set_tuning(None, None) == _capi.SPH_ERR_INVALID
+    assert lib.sph_autotune(None, 1, None, None) == _capi.SPH_ERR_INVALID
 
 
 def test_scene_builders_follow_reference_sampling():
