@@ -118,3 +118,18 @@ def test_scene_builders_follow_reference_sampling():
 
 def test_oracle_library_builds_and_loads(oracle):
     assert oracle.num_threads() >= 1
+
+
+def test_volume_map_grids_match_the_oracle(oracle):
+    """sph_volume_map_grids (host only) gives the lattices of
+    DiscretizedBoundaryFields::new (volume_map_boundary.rs:1554-1636: the mesh
+    box padded by 3.1 r for the signed distance and by 2 r + dx/6 for the
+    volume map, discretization.rs:108-112 cell counts) exactly as the oracle
+    builds them."""
+    from sphgpu import fields, scenes
+    verts = scenes.CUBE_VERTICES * 0.1
+    sg, vg = fields.grids(verts, 0.09, 0.045)
+    sdf, vm = oracle.build_fields(verts, scenes.CUBE_FACES_OUTWARD, 0.09, 0.045)
+    for g, f in ((sg, sdf), (vg, vm)):
+        assert list(g.x_min) == list(f.x_min) and list(g.x_max) == list(f.x_max)
+        assert g.dx == f.dx and list(g.n) == list(f.n)
