@@ -14,13 +14,18 @@ Arms:
   default          the CUDA engine through the C ABI; `value` is device time
                    (CUDA events on the engine's stream), `e2e` runs the same
                    steps through sph_step_host with host buffers in and out.
-                   The line's `serving` object is the scene sweep (256
-                   Poisson-arrival dam breaks of 5k-500k particles, 500
-                   steps each) served batched by the scene server and, for
-                   its first 64 requests, one at a time on the plain path.
-  --impl reference the reference's CPU algorithm (the f64 C++ restatement in
-                   oracle/, all host threads) on a bounded sample of the same
-                   configuration (a 50^3 block), same metric.
+                   `cpu_baseline` is the reference's CPU algorithm (the f64
+                   C++ restatement in oracle/, all host threads) on the same
+                   1M scene from the same seeded state and warm-up, timed on
+                   its first steps after the warm-up (about 10-30 s of CPU
+                   work). The line's `serving` object is the scene sweep
+                   (Poisson-arrival dam breaks of 5k-500k particles, 500 steps
+                   each) served batched by the scene server and one at a time
+                   on the plain path, the same requests in both arms.
+  --impl reference the reference's CPU algorithm (the oracle restatement, all
+                   host threads) on the same 1M scene: same seeded state, same
+                   warm-up steps, then the timed steps (all of --steps unless
+                   --ref-seconds runs out first; the line says how many).
 Multi-GPU: scenes are independent, so N GPUs run N replicas (weak scaling,
 no collective on the data path); rank 0 prints the JSON line.
 """
@@ -70,15 +75,18 @@ def parse():
     p.add_argument("--impl", default="engine", choices=["engine", "reference"])
     p.add_argument("--n-side", type=int, default=100)
     p.add_argument("--max-iters", type=int, default=100)
-    p.add_argument("--cpu-sample-side", type=int, default=50)
-    p.add_argument("--cpu-steps", type=int, default=3)
-    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    p.add_argument("--cpu-steps", type=int, default=2,
+                   help="timed CPU-baseline steps at least (more while under --cpu-seconds)")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--ref-seconds", type=float, default=150.0,
+                   help="reference arm: stop timing after this much CPU time (at least one step)")
+    p.add_argument("--no-f64", action="store_true", help="skip the f64-twin engine timing")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--serving-requests", type=int, default=256,
                    help="scene-sweep requests served batched and one at a time (0: skip)")
-    p.add_argument("--serving-plain-requests", type=int, default=64,
-                   help="requests of the one-at-a-time arm, the first ones of the sweep (-1: all)")
+    p.add_argument("--serving-plain-requests", type=int, default=-1,
+                   help="requests of both serving arms, the first ones of the sweep (-1: all)")
     p.add_argument("--serving-steps", type=int, default=500)
     return p.parse_args()
 
@@ -88,12 +96,6 @@ def scene(n_side, max_iters, box=(2.0, 1.0, 1.0)):
     sc = scenes.dam_break_iisph_box(n_side=n_side, box=box)
     sc.parameters = dict(sc.parameters, max_solver_iterations=max_iters)
     return sc
-
-
-def workload_box(args):
-    """Container of the benchmark scene (widened for the wall gap); the CPU
-    samples run in the same container with the same fields."""
-    return scene(args.n_side, args.max_iters).container
 
 
 class ClockSampler:
@@ -165,31 +167,17 @@ def peaks():
     return 6650.0, "fallback"
 
 
-# ncu summaries of the dominant kernels (committed under profiles/): DRAM
-# read + write bytes of one launch of the bench workload.
-TRAFFIC_PROFILES = {"iisph_jacobi": "profiles/iisph_jacobi_1M_volume_map.md",
-                    "neighbors_density": "profiles/neighbors_density_1M_volume_map.md"}
-
-
-def profiled_traffic(kernel):
-    path = os.path.join(ROOT, TRAFFIC_PROFILES.get(kernel, ""))
-    if not os.path.isfile(path):
-        return None
-    for line in open(path):
-        if line.startswith("traffic_bytes_per_launch:"):
-            return int(line.split(":")[1])
-    return None
-
-
-def run_cpu(n_side, steps, warmup, max_iters, fields, min_seconds=0.0, box=(2.0, 1.0, 1.0)):
-    """The reference's CPU algorithm (oracle restatement, all host threads) on
-    a bounded n_side^3 sample of the workload: `steps` timed steps, more while
-    less than `min_seconds` of CPU work has been timed (at most 4x `steps`).
-    Returns (updates/s, seconds, cores, particles, steps, mean sweeps)."""
+def run_cpu(args, fields, steps, min_seconds, max_seconds):
+    """The reference's CPU algorithm (oracle restatement, f64, all host
+    threads) on the benchmark scene: the same seeded state and fields, the
+    same `args.warmup` untimed steps, then at least `steps` timed steps, more
+    while less than `min_seconds` of CPU time has been timed, stopping at
+    `args.steps` steps or once `max_seconds` have been timed. Returns
+    (updates/s, seconds, cores, particles, steps timed, sweeps per timed step)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from sphgpu.system import PROCEDURES
-    sc = scene(n_side, max_iters, box)
+    sc = scene(args.n_side, args.max_iters)
     cfg = dict(sc.parameters)
     cfg.update(integration_scheme=PROCEDURES["integration_scheme"][sc.procedures["integration_scheme"]],
                pressure_solver=PROCEDURES["pressure_solver"][sc.procedures["pressure_solver"]],
@@ -202,17 +190,20 @@ def run_cpu(n_side, steps, warmup, max_iters, fields, min_seconds=0.0, box=(2.0,
                               O.Field(fields[1].x_min, fields[1].x_max, fields[1].dx, fields[1].n,
                                       fields[1].nodes))
     s.initialize()
-    if warmup:
-        s.step(warmup)
+    if args.warmup:
+        s.step(args.warmup)
     t0 = time.perf_counter()
     updates, done, sweeps = 0, 0, []
-    while done < steps or (time.perf_counter() - t0 < min_seconds and done < 4 * steps):
+    while done < args.steps:
+        el = time.perf_counter() - t0
+        if done >= steps and (el >= min_seconds or el >= max_seconds):
+            break
         s.step(1)
         updates += s.n
         done += 1
-        sweeps.append(s.measurement()["solver_iterations"])
+        sweeps.append(int(s.measurement()["solver_iterations"]))
     dt = time.perf_counter() - t0
-    return updates / dt, dt, O.num_threads(), sc.position.shape[0], done, statistics.mean(sweeps)
+    return updates / dt, dt, O.num_threads(), sc.position.shape[0], done, sweeps
 
 
 def _pct(values, q):
@@ -221,16 +212,18 @@ def _pct(values, q):
 
 def serving_sweep(args, device, rank, ws):
     """The scene sweep (Poisson arrivals at 20/s, 5k-500k particles, SESPH or
-    IISPH, 500 steps each) served two ways on this GPU: batched by the scene
-    server (continuous admission, concurrent graph-captured scenes) and one
-    scene at a time through the plain single-scene C ABI path, in arrival
-    order. Scenes/s = completed scenes / (last completion - first arrival);
+    IISPH, 500 steps each) served two ways on this GPU, the same requests in
+    both: batched by the scene server (continuous admission, concurrent
+    graph-captured scenes) and one scene at a time through the plain
+    single-scene C ABI path, in arrival order. Scenes/s = completed scenes / (last completion - first arrival);
     latency = completion - arrival. The first requests of both arms keep their
     final state, which must agree bit for bit."""
     from sphgpu import scenes
     from sphgpu.replicas import aggregate, share
     from sphgpu.server import SceneServer
     reqs = share(scenes.scene_sweep(count=args.serving_requests, steps=args.serving_steps), rank, ws)
+    if args.serving_plain_requests >= 0:
+        reqs = reqs[:args.serving_plain_requests]
     built = [r.scene() for r in reqs]
     n_check = min(4, len(reqs))
 
@@ -256,7 +249,7 @@ def serving_sweep(args, device, rank, ws):
                "graph_replays": st["graph_replays"], "kernel_launches": st["kernel_launches"],
                "statuses": sorted({x["status"] for x in res})}
 
-    m = len(reqs) if args.serving_plain_requests < 0 else min(len(reqs), args.serving_plain_requests)
+    m = len(reqs)
     from sphgpu import capi
     t0 = time.perf_counter()
     lat, same = [], 0
@@ -285,6 +278,44 @@ def serving_sweep(args, device, rank, ws):
             "identical_final_state": f"{same}/{n_check if m >= n_check else min(m, n_check)}"}
 
 
+WORKLOAD = ("IISPH dam break, {n}^3 particles at 0.01 m in a 2 x 1.02 x 1.02 m VolumeMapBoundary box "
+            "(1.5-spacing wall gap), CFL dt <= 2e-3, omega 0.5, 0.1 % target density error")
+
+
+def workload_config(args):
+    return {"workload": WORKLOAD.format(n=args.n_side), "particles_per_gpu": args.n_side ** 3,
+            "solver": "IISPH", "omega": 0.5, "target_density_error_pct": 0.1,
+            "max_solver_iterations": args.max_iters, "cfl": 0.4, "max_dt": 2e-3,
+            "initial_state": "seeded lattice + 1 % jitter (seed 0), then the warm-up steps"}
+
+
+def gpu_fields(sc, device):
+    from sphgpu.fields import build_volume_map_fields
+    verts, faces = sc.mesh
+    sp = sc.parameters["rest_density_grid_spacing"]
+    return build_volume_map_fields(verts, faces, 4 * sp, sc.parameters["kernel_support_radius"], 30,
+                                   device=device)
+
+
+def time_steps(torch, sysm, steps, stream, clocks=None):
+    """CUDA-event time of `steps` per-step calls on the engine's stream.
+    Returns (ms, particle updates, sweeps per step)."""
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    updates, iters = 0, []
+    for _ in range(steps):
+        sysm.step_forward_in_time(1)
+        st = sysm.step_stats()
+        updates += st["particles"]
+        iters.append(st["solver_iterations"])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1), updates, iters
+
+
 def main():
     args = parse()
     ws, rank, local = dist_env()
@@ -297,44 +328,33 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
     torch.cuda.set_device(local)
     from sphgpu import capi, scenes
-    from sphgpu.fields import build_volume_map_fields
 
     sc = scene(args.n_side, args.max_iters)
-    verts, faces = sc.mesh
-    sp = sc.parameters["rest_density_grid_spacing"]
-    fields = build_volume_map_fields(verts, faces, 4 * sp, sc.parameters["kernel_support_radius"],
-                                     30, device=local)
+    fields = gpu_fields(sc, local)
     sysm = scenes.build_system(sc, precision="f32", device=local, fields=fields)
     stream = torch.cuda.ExternalStream(sysm.stream(), device=local)
     for _ in range(args.warmup):
         sysm.step_forward_in_time(1)
-    # Copies of the warmed-up state: the kernel shares and the end-to-end
+    # Copies of the warmed-up state: the kernel times and the end-to-end
     # number run exactly the steps the device-timed region runs.
     sys_prof = sysm.clone()
     sys_e2e = None if args.no_e2e else sysm.clone()
     launches0 = sysm.launch_count()
-    torch.cuda.synchronize()
     if ws > 1:
+        torch.cuda.synchronize()
         dist.barrier()
     clocks = ClockSampler(local)
-    clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    updates, iters = 0, []
-    for _ in range(args.steps):
-        sysm.step_forward_in_time(1)
-        st = sysm.step_stats()
-        updates += st["particles"]
-        iters.append(st["solver_iterations"])
-    ev1.record(stream)
-    torch.cuda.synchronize()
+    ms, updates, iters = time_steps(torch, sysm, args.steps, stream, clocks)
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
     launches = sysm.launch_count() - launches0
-    # per-kernel CUDA-event times of the same steps on the first copy
+    # Per-kernel CUDA-event times of the same steps on the first copy. Timed
+    # solves run one sweep per host check, so every timed sweep launch is a
+    # sweep the solve needed (no launch that finds the loop converged).
     sys_prof.set_profiling(True)
+    prof_iters = []
     for _ in range(args.steps):
         sys_prof.step_forward_in_time(1)
+        prof_iters.append(sys_prof.step_stats()["solver_iterations"])
     kernel_times = {}
     for name in BYTES_PER_PARTICLE:
         kt = sys_prof.kernel_time(name)
@@ -376,50 +396,77 @@ def main():
         e2e = {"value": e_updates / (ems / 1000.0), "unit": UNIT,
                "h2d_bytes_per_step": 2 * 3 * 8 * n, "d2h_bytes_per_step": 2 * 3 * 8 * n}
 
+    # the f64 twin of every kernel on the same scene and steps (the reference's
+    # own precision), device time
+    f64 = None
+    if not args.no_f64:
+        s64 = scenes.build_system(sc, precision="f64", device=local, fields=fields)
+        for _ in range(args.warmup):
+            s64.step_forward_in_time(1)
+        st64 = torch.cuda.ExternalStream(s64.stream(), device=local)
+        ms64, upd64, it64 = time_steps(torch, s64, args.steps, st64)
+        s64.close()
+        ms64, upd64 = aggregate(ms64, upd64, device="cuda")
+        f64 = {"value": upd64 / (ms64 / 1000.0), "unit": UNIT, "ms_per_step": ms64 / args.steps,
+               "mean_solver_iterations": statistics.mean(it64) if it64 else None}
+
     peak, peak_kind = peaks()
     roofline = None
     if kernel_times:
+        n_particles = updates / max(args.steps, 1)
+        shares = {k: round(v[0] / sum(x[0] for x in kernel_times.values()), 4)
+                  for k, v in sorted(kernel_times.items(), key=lambda kv: -kv[1][0])}
         dom = max(kernel_times, key=lambda k: kernel_times[k][0])
         tot_ms, cnt = kernel_times[dom]
         avg_s = tot_ms / cnt / 1000.0
-        n_particles = updates / max(args.steps, 1)
         bytes_per_launch = BYTES_PER_PARTICLE[dom] * n_particles
         achieved = bytes_per_launch / avg_s / 1e9
-        traffic = profiled_traffic(dom)
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak,
                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                    "traffic": traffic, "bytes_per_launch": bytes_per_launch,
-                    "avg_launch_us": round(avg_s * 1e6, 2), "launches": cnt,
-                    "kernel_share": {k: round(v[0] / sum(x[0] for x in kernel_times.values()), 4)
-                                     for k, v in sorted(kernel_times.items(), key=lambda kv: -kv[1][0])}}
+                    "traffic": None,
+                    "traffic_note": "DRAM bytes per launch come from ncu captures (profiles/), not from this run",
+                    "bytes_per_launch": bytes_per_launch, "avg_launch_us": round(avg_s * 1e6, 2),
+                    "launches": cnt, "kernel_share": shares}
+        if "iisph_jacobi" in kernel_times and "iisph_pressure_accel" in kernel_times:
+            # one Jacobi sweep = pass A (pressure accelerations) + pass B
+            # (pressure update and residual): 52 + 60 B per particle
+            ta, ca = kernel_times["iisph_pressure_accel"]
+            tb, cb = kernel_times["iisph_jacobi"]
+            sweeps = sum(prof_iters)
+            pair_s = (ta / ca + tb / cb) / 1000.0
+            pair_bytes = (BYTES_PER_PARTICLE["iisph_pressure_accel"] + BYTES_PER_PARTICLE["iisph_jacobi"]) * n_particles
+            roofline["sweep"] = {"sweeps_run": sweeps, "pass_a_launches": ca, "pass_b_launches": cb,
+                                 "pass_a_us": round(ta / ca * 1000.0, 2), "pass_b_us": round(tb / cb * 1000.0, 2),
+                                 "bytes_per_sweep": pair_bytes,
+                                 "achieved": round(pair_bytes / pair_s / 1e9, 1),
+                                 "frac": round(pair_bytes / pair_s / 1e9 / peak, 4)}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        v, secs, cores, n_cpu, done, sweeps = run_cpu(args.cpu_sample_side, args.cpu_steps, 1, args.max_iters,
-                                                      fields, args.cpu_seconds, box=sc.container)
+        v, secs, cores, n_cpu, done, sweeps = run_cpu(args, fields, args.cpu_steps, args.cpu_seconds,
+                                                      args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{done} steps (after 1 warm-up step) of a {n_cpu}-particle ({args.cpu_sample_side}^3) "
-                         f"block of the same configuration, {sweeps:.0f} IISPH sweeps per step, f64 C++ "
-                         f"restatement of the reference CPU path on all host threads, {secs:.1f} s"}
+               "sample": f"steps {args.warmup + 1}-{args.warmup + done} of the same {n_cpu}-particle scene "
+                         f"(same seeded state and fields, {args.warmup} untimed warm-up steps), "
+                         f"{statistics.mean(sweeps):.1f} IISPH sweeps per step {sweeps}, f64 C++ restatement "
+                         f"of the reference CPU path on all host threads, {secs:.1f} s"}
 
     sysm.close()
     serving = serving_sweep(args, local, rank, ws) if args.serving_requests > 0 else None
     if ws > 1:
         dist.barrier()
     if rank == 0:
+        cfg = workload_config(args)
+        cfg.update({"precision": "f32 state, f64 reductions", "parallelism": f"replicas x{ws}",
+                    "l2": "no flush: a step touches about 260 MB of distinct data (> 126 MB L2)",
+                    "mean_solver_iterations": statistics.mean(iters) if iters else None,
+                    "solver_iterations": iters})
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded lattice + jitter)",
-            "config": {"workload": f"IISPH dam break, {args.n_side}^3 particles, 2 x 1.02 x 1.02 m VolumeMapBoundary box (1.5-spacing wall gap)",
-                       "particles_per_gpu": args.n_side ** 3, "solver": "IISPH", "omega": 0.5,
-                       "target_density_error_pct": 0.1, "max_solver_iterations": args.max_iters,
-                       "cfl": 0.4, "max_dt": 2e-3, "precision": "f32 state, f64 reductions",
-                       "parallelism": f"replicas x{ws}",
-                       "l2": "working set > L2 (neighbor lists alone exceed 126 MB); no flush needed",
-                       "mean_solver_iterations": statistics.mean(iters) if iters else None},
-            "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "serving": serving,
+            "config": cfg, "gpu_launches": launches, "clocks": clk, "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": e2e, "f64_engine": f64, "serving": serving,
         }
         print(json.dumps(line))
     if ws > 1:
@@ -427,32 +474,36 @@ def main():
 
 
 def reference_arm(args, ws, rank):
+    """The reference's CPU algorithm on the benchmark scene itself (f64 C++
+    restatement; the Rust reference cannot be built here). Fields are built
+    by the oracle's CPU restatement of the reference's field construction."""
     if rank != 0:
         return
-    # the CPU arm needs the same boundary fields; build them with the oracle's
-    # CPU restatement of the reference's field construction when no GPU build
-    # is available (bounded: coarse box fields, once)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    box = workload_box(args)
-    sc = scene(args.cpu_sample_side, args.max_iters, box)
+    sc = scene(args.n_side, args.max_iters)
     verts, faces = sc.mesh
     sp = sc.parameters["rest_density_grid_spacing"]
-    sdf, vm = O.build_fields(verts, faces, 4 * sp, sc.parameters["kernel_support_radius"], 30)
-    v, secs, cores, n_cpu, done, sweeps = run_cpu(args.cpu_sample_side, args.steps, args.warmup, args.max_iters,
-                                                  (sdf, vm), box=box)
+    t0 = time.perf_counter()
+    fields = O.build_fields(verts, faces, 4 * sp, sc.parameters["kernel_support_radius"], 30)
+    t_fields = time.perf_counter() - t0
+    v, secs, cores, n_cpu, done, sweeps = run_cpu(args, fields, 1, 0.0, args.ref_seconds)
+    cfg = workload_config(args)
+    cfg.update({"precision": "f64", "steps_timed": done,
+                "mean_solver_iterations": statistics.mean(sweeps) if sweeps else None,
+                "solver_iterations": sweeps})
     line = {
         "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": secs * 1000.0 / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": secs * 1000.0 / max(done, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded lattice + jitter)",
-        "impl": "reference",
-        "config": {"workload": f"IISPH dam break, {args.n_side}^3 particles, 2 x 1.02 x 1.02 m VolumeMapBoundary box (1.5-spacing wall gap)",
-                   "sample_particles": n_cpu, "max_solver_iterations": args.max_iters},
+        "impl": "reference", "config": cfg,
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{done} timed steps of a {n_cpu}-particle ({args.cpu_sample_side}^3) block of "
-                                   f"the same configuration, {sweeps:.0f} IISPH sweeps per step (f64 C++ "
-                                   f"restatement of the reference CPU path; the Rust reference cannot be built "
-                                   f"here)"},
+                         "sample": f"steps {args.warmup + 1}-{args.warmup + done} of the {n_cpu}-particle scene "
+                                   f"after {args.warmup} untimed warm-up steps"
+                                   f"{'' if done == args.steps else f' (the first {done} of the {args.steps} steps: --ref-seconds ran out)'}, "
+                                   f"{statistics.mean(sweeps):.1f} IISPH sweeps per step; f64 C++ restatement of "
+                                   f"the reference CPU path (the Rust reference cannot be built here); fields built "
+                                   f"on the CPU in {t_fields:.0f} s, untimed"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

@@ -242,28 +242,39 @@ constexpr size_t kStaticMaxSamples = size_t(1) << 20;    // sample positions
 constexpr size_t kStaticMaxPositions = size_t(1) << 20;  // query positions
 constexpr int kStaticBits = 6;                           // 2^(3*6) buckets
 constexpr size_t kStaticBuckets = size_t(1) << (3 * kStaticBits);
-// keys, slots and sorted indices of the samples, then bucket counts and starts
-constexpr size_t kStaticScratchBytes =
-    3 * kStaticMaxSamples * sizeof(uint32_t) + 2 * (kStaticBuckets + 2) * sizeof(uint32_t);
+// The bucket order comes from a stable LSD radix sort of the 18-bit keys:
+// three passes of 6-bit digits over tiles of 256 samples in index order.
+constexpr int kRadixBits = 6;
+constexpr int kRadixDigits = 1 << kRadixBits;
+constexpr int kRadixPasses = 3 * kStaticBits / kRadixBits;
+constexpr int kRadixTile = 256;
+constexpr size_t kStaticMaxTiles = kStaticMaxSamples / kRadixTile;
+// keys, two order buffers (radix ping-pong), bucket counts and starts, and the
+// per-(digit, tile) offsets of one radix pass
+constexpr size_t kStaticScratchBytes = 3 * kStaticMaxSamples * sizeof(uint32_t) +
+                                       2 * (kStaticBuckets + 2) * sizeof(uint32_t) +
+                                       kRadixDigits * kStaticMaxTiles * sizeof(uint32_t);
 
 static __device__ __align__(256) unsigned char g_find_scratch[kStaticScratchBytes];
 
 struct StaticScratch {
   uint32_t* key;
-  uint32_t* slot;
-  uint32_t* order;
+  uint32_t* order;   // sorted sample indices (radix output of the last pass)
+  uint32_t* order2;  // ping-pong buffer of the radix passes
   uint32_t* count;
   uint32_t* start;
+  uint32_t* digit;   // [kRadixDigits][tiles] digit counts, then their offsets
 };
 
 StaticScratch carve(void* base) {
   unsigned char* p = (unsigned char*)base;
   StaticScratch s;
   s.key = (uint32_t*)p;
-  s.slot = s.key + kStaticMaxSamples;
-  s.order = s.slot + kStaticMaxSamples;
-  s.count = s.order + kStaticMaxSamples;
+  s.order = s.key + kStaticMaxSamples;
+  s.order2 = s.order + kStaticMaxSamples;
+  s.count = s.order2 + kStaticMaxSamples;
   s.start = s.count + (kStaticBuckets + 2);
+  s.digit = s.start + (kStaticBuckets + 2);
   return s;
 }
 
@@ -287,15 +298,16 @@ __global__ void k_static_zero(uint32_t* __restrict__ a, size_t n) {
     a[i] = 0u;
 }
 
+// Bucket key of every sample and the bucket sizes (the counts do not depend
+// on the order of the atomic additions).
 __global__ void k_static_keys(int ns, const double* __restrict__ samp, double cell, uint32_t mask,
-                              uint32_t* __restrict__ key, uint32_t* __restrict__ slot,
-                              uint32_t* __restrict__ count) {
+                              uint32_t* __restrict__ key, uint32_t* __restrict__ count) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   const uint32_t k = sph::morton_key(sph::cell_coord(samp[3 * s], cell), sph::cell_coord(samp[3 * s + 1], cell),
                                      sph::cell_coord(samp[3 * s + 2], cell), mask);
   key[s] = k;
-  slot[s] = atomicAdd(&count[k], 1u);
+  atomicAdd(&count[k], 1u);
 }
 
 // Scan by one block (exclusive, or inclusive when INCL): each thread scans a
@@ -332,34 +344,57 @@ __global__ void __launch_bounds__(1024) k_static_scan(const T* in, T* out, size_
   }
 }
 
-__global__ void k_static_scatter(int ns, const uint32_t* __restrict__ key, const uint32_t* __restrict__ slot,
-                                 const uint32_t* __restrict__ start, uint32_t* __restrict__ order) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
-  order[start[key[s]] + slot[s]] = (uint32_t)s;
+// Radix pass `shift`, step 1: per tile of 256 entries of `in` (sample indices
+// in the current order; the identity when `in` is null), the count of each
+// digit, stored digit-major so that one exclusive scan gives every (digit,
+// tile) its first output slot.
+__global__ void __launch_bounds__(kRadixTile) k_radix_hist(int ns, const uint32_t* __restrict__ in,
+                                                           const uint32_t* __restrict__ key, int shift,
+                                                           uint32_t* __restrict__ digit, int tiles) {
+  __shared__ uint32_t h[kRadixDigits];
+  if (threadIdx.x < kRadixDigits) h[threadIdx.x] = 0u;
+  __syncthreads();
+  const int e = blockIdx.x * kRadixTile + threadIdx.x;
+  if (e < ns) {
+    const uint32_t s = in ? in[e] : (uint32_t)e;
+    atomicAdd(&h[(key[s] >> shift) & (kRadixDigits - 1)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < kRadixDigits) digit[(size_t)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// Ascending sample index inside each bucket, as SpatialHashing::populate
-// pushes them (spatial_hashing.rs:27-37).
-__global__ void k_static_bucket_sort(int ns, const uint32_t* __restrict__ key, const uint32_t* __restrict__ start,
-                                     uint32_t* __restrict__ order) {
-  const int d = blockIdx.x * blockDim.x + threadIdx.x;
-  if (d >= ns) return;
-  const uint32_t k = key[order[d]];
-  const uint32_t b = start[k];
-  if ((uint32_t)d != b) return;
-  const uint32_t e = start[k + 1];
-  for (uint32_t a = b + 1; a < e; ++a) {
-    const uint32_t v = order[a];
-    uint32_t c = a;
-    while (c > b && order[c - 1] > v) {
-      order[c] = order[c - 1];
-      --c;
-    }
-    order[c] = v;
+// Radix pass step 2: stable scatter. An entry's slot is its (digit, tile)
+// offset plus the number of entries of the tile before it with the same
+// digit: lanes of equal digit within the warp (match), then the counts of
+// the warps before it.
+__global__ void __launch_bounds__(kRadixTile) k_radix_scatter(int ns, const uint32_t* __restrict__ in,
+                                                              const uint32_t* __restrict__ key, int shift,
+                                                              const uint32_t* __restrict__ digit, int tiles,
+                                                              uint32_t* __restrict__ out) {
+  constexpr int kWarps = kRadixTile / 32;
+  __shared__ uint32_t wc[kWarps][kRadixDigits];
+  for (int t = threadIdx.x; t < kWarps * kRadixDigits; t += kRadixTile) (&wc[0][0])[t] = 0u;
+  __syncthreads();
+  const int e = blockIdx.x * kRadixTile + threadIdx.x;
+  const bool valid = e < ns;
+  const unsigned act = __ballot_sync(0xffffffffu, valid);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t s = 0, d = 0, rank = 0;
+  if (valid) {
+    s = in ? in[e] : (uint32_t)e;
+    d = (key[s] >> shift) & (kRadixDigits - 1);
+    const unsigned peers = __match_any_sync(act, d);
+    rank = __popc(peers & ((1u << lane) - 1u));
+    if (lane == __ffs(peers) - 1) wc[w][d] = __popc(peers);
+  }
+  __syncthreads();
+  if (valid) {
+    for (int v = 0; v < w; ++v) rank += wc[v][d];
+    out[digit[(size_t)d * tiles + blockIdx.x] + rank] = s;
   }
 }
 
+// Per-position neighbor counts into offsets[i + 1] (offsets[0] = 0).
 // Per-position neighbor counts into offsets[i + 1] (offsets[0] = 0).
 __global__ void k_static_count(int n, const double* __restrict__ pos, const double* __restrict__ samp,
                                const uint32_t* __restrict__ order, const uint32_t* __restrict__ start,
@@ -402,13 +437,22 @@ extern "C" int sph_spatial_hashing_find_samples_noalloc(double search_range, siz
     const uint32_t T = (uint32_t)kStaticBuckets;
     // the array keeps the previous call's contents: clear the bucket counts
     k_static_zero<<<256, 256>>>(S.count, (size_t)T + 2);
-    if (ns)
-      k_static_keys<<<(unsigned)((ns + 255) / 256), 256>>>((int)ns, d_samples, search_range, mask, S.key, S.slot,
-                                                           S.count);
+    const unsigned sb = (unsigned)((ns + 255) / 256);
+    if (ns) k_static_keys<<<sb, 256>>>((int)ns, d_samples, search_range, mask, S.key, S.count);
     k_static_scan<uint32_t, false><<<1, 1024>>>(S.count, S.start, (size_t)T + 2);
     if (ns) {
-      k_static_scatter<<<(unsigned)((ns + 255) / 256), 256>>>((int)ns, S.key, S.slot, S.start, S.order);
-      k_static_bucket_sort<<<(unsigned)((ns + 255) / 256), 256>>>((int)ns, S.key, S.start, S.order);
+      // bucket order with ascending sample index inside each bucket, as
+      // SpatialHashing::populate pushes them (spatial_hashing.rs:27-37)
+      const int tiles = (int)((ns + kRadixTile - 1) / kRadixTile);
+      const uint32_t* in = nullptr;
+      uint32_t* bufs[2] = {(kRadixPasses & 1) ? S.order : S.order2, (kRadixPasses & 1) ? S.order2 : S.order};
+      for (int pass = 0; pass < kRadixPasses; ++pass) {
+        uint32_t* out = bufs[pass & 1];
+        k_radix_hist<<<tiles, kRadixTile>>>((int)ns, in, S.key, pass * kRadixBits, S.digit, tiles);
+        k_static_scan<uint32_t, false><<<1, 1024>>>(S.digit, S.digit, (size_t)kRadixDigits * tiles);
+        k_radix_scatter<<<tiles, kRadixTile>>>((int)ns, in, S.key, pass * kRadixBits, S.digit, tiles, out);
+        in = out;
+      }
     }
     const unsigned nb = (unsigned)std::max<size_t>(1, (n + 255) / 256);
     k_static_count<<<nb, 256>>>((int)n, d_positions, d_samples, S.order, S.start, mask, search_range, d_offsets);

@@ -159,7 +159,13 @@ class System : public SystemBase {
   explicit System(const sph_config& c) : cfg_(c) {
     device = c.device;
     if (const char* e = std::getenv("SPHGPU_SORTED_LISTS")) sorted_lists_ = std::atoi(e) != 0;
-    if (const char* e = std::getenv("SPHGPU_HALO_STAGE")) hs_ = std::max(0, std::min(std::atoi(e), 4096));
+    if (const char* e = std::getenv("SPHGPU_HALO_STAGE")) {
+      // the same bound as set_tuning: the widest staged record ({x, v, m})
+      // times the capacity must fit one block's shared memory
+      const size_t record = 2 * sizeof(R4<R>) + sizeof(R);
+      const int fit = (int)((kMaxSmemPerBlock - kStaticSmemReserve) / record);
+      hs_ = std::max(0, std::min(std::atoi(e), std::min(fit, 4096)));
+    }
     if (const char* e = std::getenv("SPHGPU_HALO_CAPACITY")) hcap_ = std::max(64, std::min(std::atoi(e), 65535));
     if (const char* e = std::getenv("SPHGPU_GATHER_BATCH")) {
       const int v = std::atoi(e);
@@ -1307,6 +1313,10 @@ class System : public SystemBase {
     }
     int batch = after >= 0 ? after + 1 : std::max(3, last_iters_);
     if (after < 0 && cfg_.max_solver_iterations) batch = std::min(batch, (int)cfg_.max_solver_iterations);
+    // Timed (profiling) solves run one sweep per host check, so that every
+    // timed sweep launch does a sweep's work (no launch that finds the loop
+    // converged and returns); the results are the same either way.
+    if (profiling_ && after < 0) batch = 1;
     for (int k = 0; k < batch; ++k) iisph_iteration(after);
     if (after >= 0) return;
     int launched = batch;
@@ -1314,7 +1324,7 @@ class System : public SystemBase {
       cuda_check(cudaMemcpyAsync(&h_sc_->converged, &d_sc_.p->converged, sizeof(int), cudaMemcpyDeviceToHost, stream_), "memcpy");
       sync();
       if (h_sc_->converged) break;
-      const int more = launched < 16 ? 2 : 4;
+      const int more = profiling_ ? 1 : launched < 16 ? 2 : 4;
       for (int k = 0; k < more; ++k) iisph_iteration(after);
       launched += more;
     }

@@ -292,13 +292,16 @@ int sph_spatial_hashing_find_samples(double search_range, size_t n, const double
  * that forbids allocation). Inputs and outputs are DEVICE pointers owned by
  * the caller (positions 3n doubles, samples 3ns doubles, offsets n+1, indices
  * `capacity`); `total` is a host pointer. Every temporary lives in one static
- * device array of about 14 MB that each GPU loading the library holds until
+ * device array of about 15 MB that each GPU loading the library holds until
  * the process exits; at most 1,048,576 samples and 1,048,576 positions
  * (larger inputs return SPH_ERR_INVALID). The first call on a device resolves
- * that array's address and should come before any stream capture. All calls
- * share the array, so calls that overlap on the GPU race; the call
- * synchronizes the device before it returns. Results equal those of
- * sph_spatial_hashing_find_samples. */
+ * that array's address and should come before any stream capture. The work
+ * runs on the legacy default stream of `device`: a caller that writes the
+ * inputs on a non-blocking stream must finish that work (synchronize the
+ * stream or the device) before the call. All calls share the array, so calls
+ * that overlap on the GPU race; the call synchronizes the device before it
+ * returns. Results equal those of sph_spatial_hashing_find_samples, rows in
+ * the same order. */
 int sph_spatial_hashing_find_samples_noalloc(double search_range, size_t n, const double* d_positions,
                                              size_t ns, const double* d_samples, uint64_t* d_offsets,
                                              uint32_t* d_indices, size_t capacity, size_t* total,

@@ -76,3 +76,19 @@ def rel_err(a, b, floor):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return np.max(np.abs(a - b) / np.maximum(np.abs(b), floor)) if a.size else 0.0
+
+
+def csr_multisets_equal(off_a, idx_a, off_b, idx_b):
+    """True when two CSR neighbor tables hold the same multiset in every row
+    (rows compared after a per-row sort), vectorized for millions of rows."""
+    off_a = np.asarray(off_a, np.int64)
+    off_b = np.asarray(off_b, np.int64)
+    if off_a.shape != off_b.shape or not np.array_equal(off_a, off_b):
+        return False
+    n = off_a.size - 1
+    row = np.repeat(np.arange(n, dtype=np.int64), np.diff(off_a))
+    ka = (row << 32) | np.asarray(idx_a, np.int64)
+    kb = (row << 32) | np.asarray(idx_b, np.int64)
+    ka.sort()
+    kb.sort()
+    return np.array_equal(ka, kb)

@@ -31,12 +31,6 @@ def test_library_exports_every_declared_symbol():
     assert set(names) <= set(_capi.SIGNATURES)
 
 
-def test_integration_notes_bind_every_declared_symbol():
-    # every entry point of the header has a binding a maintainer can copy
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    assert [s for s in declared_symbols() if s not in text] == []
-
-
 def test_config_defaults_follow_reference_parameters():
     from sphgpu import make_config
     c = make_config()

@@ -184,10 +184,14 @@ def test_iisph_volume_map_first_update_matches_oracle(A, oracle, vm_case, precis
         assert abs(mg["solver_iterations"] - mo["solver_iterations"]) <= 1
     p_g, p_o = g.download(A.FIELD_PRESSURE), o.download(oracle.F_PRESSURE)
     pscale = np.abs(p_o).max()
-    assert np.max(np.abs(p_g - p_o)) <= (1e-7 if precision == "f64" else 5e-2) * pscale
     acc_g, acc_o = g.download(A.FIELD_ACCELERATION), o.download(oracle.F_ACCELERATION)
     ascale = np.abs(acc_o).max()
-    assert np.max(np.abs(acc_g - acc_o)) <= (1e-7 if precision == "f64" else 5e-2) * ascale
+    e_p = np.max(np.abs(p_g - p_o)) / pscale
+    e_a = np.max(np.abs(acc_g - acc_o)) / ascale
+    print(f"[IISPH 16^3 {precision}] sweeps {mg['solver_iterations']} vs {mo['solver_iterations']}, "
+          f"s err {np.max(np.abs(s_g - s_o)):.2e}, pressure err/max {e_p:.2e}, acceleration err/max {e_a:.2e}")
+    assert e_p <= (1e-7 if precision == "f64" else 5e-2)
+    assert e_a <= (1e-7 if precision == "f64" else 5e-2)
 
 
 @pytest.mark.parametrize("precision", ["f64", "f32"])
