@@ -88,6 +88,12 @@ def parse():
     p.add_argument("--serving-plain-requests", type=int, default=-1,
                    help="requests of both serving arms, the first ones of the sweep (-1: all)")
     p.add_argument("--serving-steps", type=int, default=500)
+    p.add_argument("--study", choices=["sesph8k", "ball", "tank"],
+                   help="run one configuration study instead of the benchmark: 'sesph8k' (8k SESPH "
+                        "dam break, 1,000 steps against the oracle, and the CPU path timed), 'ball' "
+                        "(4M IISPHwOST two-fluid ball, f32 against the f64 engine, per-field errors), "
+                        "'tank' (2M IISPH tank with 8 coupled bodies, 1,500 CFL steps, f32 against f64)")
+    p.add_argument("--study-steps", type=int, default=0, help="steps of the study (0: its configuration's)")
     return p.parse_args()
 
 
@@ -167,13 +173,13 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def run_cpu(args, fields, steps, min_seconds, max_seconds):
+def run_cpu(args, fields, min_steps, stop_seconds):
     """The reference's CPU algorithm (oracle restatement, f64, all host
     threads) on the benchmark scene: the same seeded state and fields, the
-    same `args.warmup` untimed steps, then at least `steps` timed steps, more
-    while less than `min_seconds` of CPU time has been timed, stopping at
-    `args.steps` steps or once `max_seconds` have been timed. Returns
-    (updates/s, seconds, cores, particles, steps timed, sweeps per timed step)."""
+    same `args.warmup` untimed steps, then the timed steps: `args.steps` of
+    them, or fewer once at least `min_steps` have run and `stop_seconds` of
+    CPU time have been timed. Returns (updates/s, seconds, cores, particles,
+    steps timed, sweeps per timed step)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     from sphgpu.system import PROCEDURES
@@ -195,8 +201,7 @@ def run_cpu(args, fields, steps, min_seconds, max_seconds):
     t0 = time.perf_counter()
     updates, done, sweeps = 0, 0, []
     while done < args.steps:
-        el = time.perf_counter() - t0
-        if done >= steps and (el >= min_seconds or el >= max_seconds):
+        if done >= min_steps and time.perf_counter() - t0 >= stop_seconds:
             break
         s.step(1)
         updates += s.n
@@ -319,6 +324,8 @@ def time_steps(torch, sysm, steps, stream, clocks=None):
 def main():
     args = parse()
     ws, rank, local = dist_env()
+    if args.study:
+        return STUDIES[args.study](args, local)
     if args.impl == "reference":
         return reference_arm(args, ws, rank)
     import torch
@@ -443,8 +450,7 @@ def main():
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
-        v, secs, cores, n_cpu, done, sweeps = run_cpu(args, fields, args.cpu_steps, args.cpu_seconds,
-                                                      args.cpu_seconds)
+        v, secs, cores, n_cpu, done, sweeps = run_cpu(args, fields, args.cpu_steps, args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"steps {args.warmup + 1}-{args.warmup + done} of the same {n_cpu}-particle scene "
                          f"(same seeded state and fields, {args.warmup} untimed warm-up steps), "
@@ -487,7 +493,7 @@ def reference_arm(args, ws, rank):
     t0 = time.perf_counter()
     fields = O.build_fields(verts, faces, 4 * sp, sc.parameters["kernel_support_radius"], 30)
     t_fields = time.perf_counter() - t0
-    v, secs, cores, n_cpu, done, sweeps = run_cpu(args, fields, 1, 0.0, args.ref_seconds)
+    v, secs, cores, n_cpu, done, sweeps = run_cpu(args, fields, 1, args.ref_seconds)
     cfg = workload_config(args)
     cfg.update({"precision": "f64", "steps_timed": done,
                 "mean_solver_iterations": statistics.mean(sweeps) if sweeps else None,
@@ -507,6 +513,148 @@ def reference_arm(args, ws, rank):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# Configuration studies (one JSON line each)
+# ---------------------------------------------------------------------------
+def _field_errors(A, got, ref, spacing):
+    """Per-field errors of a run (`got`) against a reference run (`ref`)."""
+    def mx(a):
+        return float(np.abs(a).max()) if a.size else 0.0
+    out = {}
+    out["position_max_over_spacing"] = mx(got[A.FIELD_POSITION] - ref[A.FIELD_POSITION]) / spacing
+    out["position_rms_over_spacing"] = float(np.sqrt(np.mean(np.sum(
+        (got[A.FIELD_POSITION] - ref[A.FIELD_POSITION]) ** 2, axis=1)))) / spacing
+    out["velocity_max_rel_to_max"] = mx(got[A.FIELD_VELOCITY] - ref[A.FIELD_VELOCITY]) / max(mx(ref[A.FIELD_VELOCITY]), 1e-30)
+    if A.FIELD_VOLUME in ref:
+        out["volume_max_rel"] = float(np.max(np.abs(got[A.FIELD_VOLUME] - ref[A.FIELD_VOLUME]) /
+                                             np.abs(ref[A.FIELD_VOLUME])))
+    if A.FIELD_PRESSURE in ref:
+        out["pressure_max"] = mx(ref[A.FIELD_PRESSURE])
+        out["pressure_max_rel_to_max"] = mx(got[A.FIELD_PRESSURE] - ref[A.FIELD_PRESSURE]) / max(mx(ref[A.FIELD_PRESSURE]), 1e-30)
+        out["pressure_rms_rel_to_max"] = float(np.sqrt(np.mean((got[A.FIELD_PRESSURE] - ref[A.FIELD_PRESSURE]) ** 2))) / max(mx(ref[A.FIELD_PRESSURE]), 1e-30)
+    if A.FIELD_ACCELERATION in ref:
+        out["acceleration_max_rel_to_max"] = mx(got[A.FIELD_ACCELERATION] - ref[A.FIELD_ACCELERATION]) / max(mx(ref[A.FIELD_ACCELERATION]), 1e-30)
+    return {k: float(f"{v:.3e}") for k, v in out.items()}
+
+
+def _grab(sysm, A, fields):
+    return {f: sysm.download(f) for f in fields}
+
+
+def study_sesph8k(args, device):
+    """Configuration 1: the 8,000-particle SESPH dam break (sample-boundary
+    container, fixed dt 1e-3) for 1,000 steps on the f32 engine and on the
+    oracle (the reference's CPU path, timed: the CPU-1 baseline), with the
+    drift between them every 100 steps."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle as O
+    from conftest import build_oracle
+    from sphgpu import _capi as A, scenes
+    steps = args.study_steps or 1000
+    sc = scenes.dam_break_sesph_8k()
+    g = scenes.build_system(sc, precision="f32", device=device)
+    o = build_oracle(sc)
+    h = sc.parameters["rest_density_grid_spacing"]
+    stream = torch.cuda.ExternalStream(g.stream(), device=device)
+    rows, gpu_ms, cpu_s = [], 0.0, 0.0
+    for k in range(0, steps, 100):
+        n = min(100, steps - k)
+        ms, _, _ = time_steps(torch, g, n, stream)
+        gpu_ms += ms
+        t0 = time.perf_counter()
+        o.step(n)
+        cpu_s += time.perf_counter() - t0
+        mg, mo = g.take_measurement(), o.measurement()
+        got = _grab(g, A, (A.FIELD_POSITION, A.FIELD_VELOCITY, A.FIELD_VOLUME))
+        ref = {A.FIELD_POSITION: o.download(O.F_POSITION), A.FIELD_VELOCITY: o.download(O.F_VELOCITY),
+               A.FIELD_VOLUME: o.download(O.F_VOLUME)}
+        row = {"step": k + n, **_field_errors(A, got, ref, h),
+               "density_rel": float(f"{abs(mg['density'] - mo['density']) / mo['density']:.3e}"),
+               "kinetic_energy_rel": float(f"{abs(mg['kinetic_energy'] - mo['kinetic_energy']) / max(mo['kinetic_energy'], 1e-30):.3e}")}
+        rows.append(row)
+    n = g.n
+    print(json.dumps({"study": "sesph8k", "particles": n, "steps": steps,
+                      "engine_f32_updates_per_s": n * steps / (gpu_ms / 1000.0),
+                      "cpu_updates_per_s": n * steps / cpu_s, "cpu_cores": O.num_threads(),
+                      "cpu_kind": "f64 C++ restatement of the reference CPU path (CPU-1)",
+                      "drift": rows}))
+
+
+def study_ball(args, device):
+    """Configuration 3: the IISPHwOST two-fluid ball, 4M particles in the
+    lower half of a radius-1 m sphere (inward icosphere of 5,120 triangles,
+    fields at dx 0.032), rest densities 1000 / 500 split by a seeded plane,
+    TakePredicted at dt 5e-4 for 500 steps. The f32 engine runs against its
+    f64 twin from the same state; per-field errors every 100 steps."""
+    from sphgpu import _capi as A, scenes
+    steps = args.study_steps or 500
+    sc = scenes.two_fluid_ball(radius=1.0, spacing=0.008, seed=0, subdivisions=4)
+    sc.parameters = dict(sc.parameters, max_solver_iterations=args.max_iters)
+    t0 = time.perf_counter()
+    fields = gpu_fields(sc, device)
+    t_fields = time.perf_counter() - t0
+    g32 = scenes.build_system(sc, precision="f32", device=device, fields=fields)
+    g64 = scenes.build_system(sc, precision="f64", device=device, fields=fields)
+    keep = (A.FIELD_POSITION, A.FIELD_VELOCITY, A.FIELD_VOLUME, A.FIELD_PRESSURE, A.FIELD_ACCELERATION)
+    rows = []
+    t32 = t64 = 0.0
+    for k in range(0, steps, 100):
+        n = min(100, steps - k)
+        t0 = time.perf_counter(); g32.step_forward_in_time(n); t32 += time.perf_counter() - t0
+        t0 = time.perf_counter(); g64.step_forward_in_time(n); t64 += time.perf_counter() - t0
+        m32, m64 = g32.take_measurement(), g64.take_measurement()
+        rows.append({"step": k + n, **_field_errors(A, _grab(g32, A, keep), _grab(g64, A, keep),
+                                                    sc.parameters["rest_density_grid_spacing"]),
+                     "sweeps_f32": m32["solver_iterations"], "sweeps_f64": m64["solver_iterations"],
+                     "density_error_f32": m32["density_error"], "density_error_f64": m64["density_error"]})
+        print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    print(json.dumps({"study": "ball", "particles": g32.n, "steps": steps, "fields_s": round(t_fields, 1),
+                      "f32_ms_per_step": 1000.0 * t32 / steps, "f64_ms_per_step": 1000.0 * t64 / steps,
+                      "errors_f32_vs_f64": rows}))
+
+
+def study_tank(args, device):
+    """Configuration 4: IISPH tank with eight two-way coupled bodies (4 cubes
+    of side 0.15 m, 4 spheres of radius 0.08 m, densities U[300, 1500]), all
+    StaticSampleBoundary, 2M fluid particles at 0.01 m (a 2 x 1 x 1.5 m tank
+    filled to 1.03 m, the bodies above the surface), CFL steps; f32 engine
+    against its f64 twin, body states and fluid fields every 100 steps."""
+    from sphgpu import _capi as A, scenes
+    steps = args.study_steps or 1500
+    sc = scenes.rigid_body_tank(spacing=0.01, tank=(2.0, 1.0, 1.5), fill=1.03, seed=0)
+    sc.parameters = dict(sc.parameters, max_solver_iterations=args.max_iters)
+    g32 = scenes.build_system(sc, precision="f32", device=device)
+    g64 = scenes.build_system(sc, precision="f64", device=device)
+    keep = (A.FIELD_POSITION, A.FIELD_VELOCITY, A.FIELD_VOLUME, A.FIELD_PRESSURE)
+    nb = len(sc.sample_boundaries)
+    rows = []
+    t32 = t64 = 0.0
+    for k in range(0, steps, 100):
+        n = min(100, steps - k)
+        t0 = time.perf_counter(); g32.step_forward_in_time(n); t32 += time.perf_counter() - t0
+        t0 = time.perf_counter(); g64.step_forward_in_time(n); t64 += time.perf_counter() - t0
+        b32 = np.stack([g32.rigid_state(b) for b in range(1, nb)])
+        b64 = np.stack([g64.rigid_state(b) for b in range(1, nb)])
+        rows.append({"step": k + n, "time_f32": g32.time(), "time_f64": g64.time(),
+                     "body_com_max_abs_m": float(f"{np.abs(b32[:, 0:3] - b64[:, 0:3]).max():.3e}"),
+                     "body_q_max_abs": float(f"{np.abs(b32[:, 3:7] - b64[:, 3:7]).max():.3e}"),
+                     "body_v_max_abs": float(f"{np.abs(b32[:, 7:10] - b64[:, 7:10]).max():.3e}"),
+                     "body_com_travel_m": float(f"{np.abs(b64[:, 0:3] - np.array([r.center_of_mass for _, r in sc.sample_boundaries[1:]])).max():.3e}"),
+                     **_field_errors(A, _grab(g32, A, keep), _grab(g64, A, keep),
+                                     sc.parameters["rest_density_grid_spacing"]),
+                     "sweeps_f32": g32.take_measurement()["solver_iterations"],
+                     "sweeps_f64": g64.take_measurement()["solver_iterations"]})
+        print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    print(json.dumps({"study": "tank", "particles": g32.n, "bodies": nb - 1, "steps": steps,
+                      "f32_ms_per_step": 1000.0 * t32 / steps, "f64_ms_per_step": 1000.0 * t64 / steps,
+                      "f32_vs_f64": rows}))
+
+
+STUDIES = {"sesph8k": study_sesph8k, "ball": study_ball, "tank": study_tank}
 
 
 if __name__ == "__main__":

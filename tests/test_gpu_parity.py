@@ -190,8 +190,9 @@ def test_iisph_volume_map_first_update_matches_oracle(A, oracle, vm_case, precis
     e_a = np.max(np.abs(acc_g - acc_o)) / ascale
     print(f"[IISPH 16^3 {precision}] sweeps {mg['solver_iterations']} vs {mo['solver_iterations']}, "
           f"s err {np.max(np.abs(s_g - s_o)):.2e}, pressure err/max {e_p:.2e}, acceleration err/max {e_a:.2e}")
-    assert e_p <= (1e-7 if precision == "f64" else 5e-2)
-    assert e_a <= (1e-7 if precision == "f64" else 5e-2)
+    # measured on B200: f32 pressure 4.1e-6, acceleration 7.4e-7 of the maxima
+    assert e_p <= (1e-7 if precision == "f64" else 5e-5)
+    assert e_a <= (1e-7 if precision == "f64" else 1e-5)
 
 
 @pytest.mark.parametrize("precision", ["f64", "f32"])

@@ -26,12 +26,14 @@ pytestmark = pytest.mark.gpu
 
 N_SIDE = 100
 CAP = 100
-# f32 engine vs f64 oracle on the same input state
+# f32 engine vs f64 oracle on the same input state. Measured on B200: V
+# 2.8e-7, s 3.0e-7, a_ii 2.0e-7, pressure 4.8e-6, acceleration 1.0e-6; the
+# bounds leave a factor of about 20.
 V_RTOL = 1e-5          # volume (density) relative error
-S_ATOL = 2e-5          # source term (dimensionless density deviation)
-AII_RTOL = 1e-4        # diagonal, relative to its largest magnitude
-P_FRAC = 1e-2          # pressure, fraction of the largest pressure
-ACC_FRAC = 1e-2        # total acceleration, fraction of the largest magnitude
+S_ATOL = 5e-6          # source term (dimensionless density deviation)
+AII_RTOL = 5e-6        # diagonal, relative to its largest magnitude
+P_FRAC = 1e-4          # pressure, fraction of the largest pressure
+ACC_FRAC = 5e-5        # total acceleration, fraction of the largest magnitude
 STEPS = 5
 
 
@@ -93,7 +95,7 @@ def test_first_update_matches_oracle(case, oracle):
     assert e_acc < ACC_FRAC
     e_rho = abs(mg["density"] - mo["density"]) / mo["density"]
     _report("average density rel err", e_rho)
-    assert e_rho < 1e-6
+    assert e_rho < 1e-7
 
 
 def test_cfl_steps_track_oracle(case, oracle):
@@ -109,8 +111,8 @@ def test_cfl_steps_track_oracle(case, oracle):
         print(f"[1M parity] step {k + 1}: dt rel err {e_dt:.2e}, density rel err {e_rho:.2e}, "
               f"predicted density error {mg['predicted_density_error']:.4f} vs {mo['predicted_density_error']:.4f} %, "
               f"sweeps {mg['solver_iterations']} vs {mo['solver_iterations']}")
-        assert e_dt < 1e-4
-        assert e_rho < 1e-5
+        assert e_dt < 1e-6
+        assert e_rho < 1e-6
         assert abs(mg["solver_iterations"] - mo["solver_iterations"]) <= 1
         # both solves stop below the 0.1 % target; when the sweep counts agree
         # the errors agree closely
@@ -120,7 +122,11 @@ def test_cfl_steps_track_oracle(case, oracle):
     x_g, x_o = g.download(A.FIELD_POSITION), o.download(oracle.F_POSITION)
     e_x = float(np.max(np.abs(x_g - x_o)))
     _report(f"positions after {STEPS} steps, max abs err (m)", e_x)
-    assert e_x < 1e-5
+    assert e_x < 2e-6
+    # The f32 and f64 trajectories now differ by rounding, which moves pairs
+    # at the range across it; the neighbor sets are compared on the engine's
+    # own state: the reference's search over the engine's positions.
     off_g, idx_g = g.fluid_neighbors()
-    off_o, idx_o = o.fluid_neighbors()
+    off_o, idx_o, dups = oracle.find_samples(g.take_measurement()["kernel_support_radius"], x_g, x_g)
+    assert dups == 0
     assert csr_multisets_equal(off_g, idx_g, off_o, idx_o)
