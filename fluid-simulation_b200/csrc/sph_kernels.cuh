@@ -734,6 +734,10 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
         }
       }
     }
+    // The unused slots of the last group of four hold the particle's own halo
+    // position: a sweep pass reads whole groups, and the self pair adds zero.
+    for (int k = min(cnt, P.K); k < ((min(cnt, P.K) + 3) & ~3); ++k)
+      list[(k >> 2) * 128 + (k & 3)] = (uint16_t)(own_local < usable ? own_local : 0u);
     R denom = P.V0 * sum;
     if (has_boundary) denom += bW[i];
     const R V = P.V0 / denom;
@@ -1425,15 +1429,14 @@ __global__ void __launch_bounds__(kBlock) k_accel(
 // ---------------------------------------------------------------------------
 // 7. pressure acceleration from stored pressures (pressure_solver/mod.rs:121-195)
 // ---------------------------------------------------------------------------
-// MODE: 0 -> accp = accel (Jacobi probe, overwrite, no reaction forces)
-//       1 -> acc += accel (reaction forces if mirror)
+// MODE: 1 -> acc += accel (reaction forces if mirror)
 //       2 -> acc  = accel (reaction forces if mirror)
+// (the Jacobi sweep's own pressure accelerations are k_sweep_accel)
 template <class R, int MODE, int NB>
 __global__ void __launch_bounds__(kBlock) k_pressure_accel(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     const R* __restrict__ press, NbrArgs N, BoundaryArgs<R> B, R4<R>* __restrict__ out, int mirror,
-    int skip_if_converged, StepParams<R> P) {
-  if (skip_if_converged && sc->converged) return;
+    StepParams<R> P) {
   __shared__ double sh_body[kMaxBodies * 6];
   extern __shared__ __align__(32) unsigned char dsm[];
   const bool bodies = mirror && B.any_dynamic != 0;
@@ -1516,7 +1519,8 @@ template <class R, int VP, int NB>
 __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     const R4<R>* __restrict__ vstar, NbrArgs N, BoundaryArgs<R> B, R* __restrict__ s_out,
-    R* __restrict__ aii_out, R* __restrict__ press, StepParams<R> P) {
+    R* __restrict__ aii_out, R* __restrict__ press, R4<R>* __restrict__ S_out, R4<R>* __restrict__ xq_out,
+    StepParams<R> P) {
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
@@ -1575,65 +1579,184 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
   R p0 = 0;
   if (aii > P.min_diag || aii < -P.min_diag) p0 = fmax(P.omega * s / aii, R(0));
   press[i] = p0;
+  // the Jacobi sweeps' inputs: S_i = sum_j V_j gradW_ij and the record {x, V p}
+  S_out[i] = R4<R>{sfx, sfy, sfz, R(0)};
+  xq_out[i] = R4<R>{xi.x, xi.y, xi.z, Vi * p0};
 }
 
-// Jacobi sweep: A_i = dt^2 [sum V_j (a_i - a_j) . gradW + a_i . bG];
-// p_i <- max(p_i + omega (s_i - A_i) / a_ii, 0); residual in f64.
+// ---------------------------------------------------------------------------
+// Jacobi sweep (iisph.rs:401-560): pass A, the pressure accelerations of the
+// current pressures (pressure_solver/mod.rs:121-195, overwrite, no reaction
+// forces), then pass B, A_i, the relaxed pressure update and the residual.
+// Positions and volumes are fixed during a solve, so the pair sums split:
+//   sum_j V_j (p_i + p_j) gradW_ij    = p_i S_i + sum_j (V_j p_j) gradW_ij
+//   sum_j V_j (a_i - a_j) . gradW_ij  = a_i . S_i - sum_j (V_j a_j) . gradW_ij
+// with S_i = sum_j V_j gradW_ij from the source pass. Each pass then gathers
+// one record per neighbor from the block's halo in shared memory:
+//   pass A: xq = {x, y, z, V p}            (written by pass B and the source pass)
+//   pass B: xu = {x, y, z, V a_x}, uu = {V a_y, V a_z}   (written by pass A)
+// A neighbor group of four always holds four valid halo positions (unused
+// slots repeat the particle's own, whose pair adds zero), so the loops carry
+// no per-neighbor test. The kernel constant cg multiplies each pair sum once.
+// ---------------------------------------------------------------------------
+template <class R>
+struct SweepList {
+  const uint2* p;  // this particle's first group of four; group g sits 32 uint2 further
+  int ng;          // groups
+  uint2 w0, w1;    // the next two groups, in flight
+  __device__ __forceinline__ void begin(const NbrArgs& N, int i, int cnt) {
+    p = reinterpret_cast<const uint2*>(N.nbr) + nbr_slot(i, 0, N.K) / 4;
+    ng = (cnt + 3) >> 2;
+    w0 = ng > 0 ? __ldcs(p) : make_uint2(0u, 0u);
+    w1 = ng > 1 ? __ldcs(p + 32) : make_uint2(0u, 0u);
+  }
+  // the group to use now; requests the one two groups ahead
+  __device__ __forceinline__ uint2 next(int g) {
+    const uint2 w = w0;
+    w0 = w1;
+    w1 = g + 2 < ng ? __ldcs(p + (size_t)(g + 2) * 32) : make_uint2(0u, 0u);
+    return w;
+  }
+};
+
+// pass A: a_i = -(V_i/m_i) [p_i S_i + sum_j (V_j p_j) gradW_ij + 2 gamma_p p_i bG_i],
+// stored as the records of pass B (V_i a_i).
+template <class R>
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_accel(
+    const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
+    const R* __restrict__ press, const R4<R>* __restrict__ Sv, const R4<R>* __restrict__ xq, NbrArgs N,
+    const R4<R>* __restrict__ bG, int has_b, R4<R>* __restrict__ xu, R2<R>* __restrict__ uu, StepParams<R> P) {
+  if (sc->converged) return;
+  extern __shared__ __align__(32) unsigned char dsm[];
+  const HaloView H = halo_view(N);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < sc->n_active;
+  // the list head and this particle's data travel while the halo stages
+  SweepList<R> L;
+  L.begin(N, act ? i : 0, act ? min((int)N.ncnt[i], N.K) : 0);
+  R4<R> xi{}, Si{}, bg{};
+  R mi = 1, pi = 0;
+  if (act) {
+    xi = xv[i];
+    mi = vel[i].w;
+    pi = press[i];
+    Si = Sv[i];
+    if (has_b) bg = bG[i];
+  }
+  R4<R>* s_r = reinterpret_cast<R4<R>*>(dsm);
+  if (H.staged) stage_halo(H, [&](int l, uint32_t g) { async_copy(&s_r[l], &xq[g]); });
+  stage_done();
+  if (!act) return;
+  const R ih = P.k.inv_h;
+  R px = 0, py = 0, pz = 0;
+  auto pair = [&](const R4<R>& r) {
+    const R rx = xi.x - r.x, ry = xi.y - r.y, rz = xi.z - r.z;
+    const R t = r.w * grad_core(rx * rx + ry * ry + rz * rz, ih);
+    px += t * rx; py += t * ry; pz += t * rz;
+  };
+  if (H.staged) {
+    for (int g = 0; g < L.ng; ++g) {
+      const uint2 w = L.next(g);
+      const R4<R> r0 = s_r[w.x & 0xffffu], r1 = s_r[w.x >> 16], r2 = s_r[w.y & 0xffffu], r3 = s_r[w.y >> 16];
+      pair(r0); pair(r1); pair(r2); pair(r3);
+    }
+  } else {
+    for (int g = 0; g < L.ng; ++g) {
+      const uint2 w = L.next(g);
+      const R4<R> r0 = xq[H.idx[w.x & 0xffffu]], r1 = xq[H.idx[w.x >> 16]], r2 = xq[H.idx[w.y & 0xffffu]],
+                  r3 = xq[H.idx[w.y >> 16]];
+      pair(r0); pair(r1); pair(r2); pair(r3);
+    }
+  }
+  const R cg = P.k.cg;
+  R fx = pi * Si.x + cg * px, fy = pi * Si.y + cg * py, fz = pi * Si.z + cg * pz;
+  if (has_b) {
+    const R c = R(2) * P.gamma_p * pi;
+    fx += c * bg.x; fy += c * bg.y; fz += c * bg.z;
+  }
+  const R Vi = xi.w;
+  const R c = -(Vi / mi) * Vi;  // V_i a_i = -(V_i^2 / m_i) F
+  xu[i] = R4<R>{xi.x, xi.y, xi.z, c * fx};
+  uu[i] = R2<R>{c * fy, c * fz};
+}
+
+// pass B: A_i = dt^2 [a_i . (S_i + bG_i) - sum_j (V_j a_j) . gradW_ij];
+// p_i <- max(p_i + omega (s_i - A_i) / a_ii, 0) where a_ii < -eps; the
+// residual e_i = |A_i - s_i| where s_i < 0, summed in f64 over all N (last
+// block: error, sweep count and the stop test of iisph.rs:378-393).
 // AFTER >= 0: stop after AFTER+1 sweeps; AFTER < 0: target density error.
-template <class R, int NB>
-__global__ void __launch_bounds__(kBlock) k_iisph_jacobi(
-    Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ accp,
-    NbrArgs N, BoundaryArgs<R> B, const R* __restrict__ s_in, const R* __restrict__ aii_in,
-    R* __restrict__ press, double* __restrict__ partials, int after, StepParams<R> P) {
+template <class R>
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_jacobi(
+    Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ Sv,
+    const R4<R>* __restrict__ xu, const R2<R>* __restrict__ uu, NbrArgs N, const R4<R>* __restrict__ bG,
+    int has_b, const R* __restrict__ s_in, const R* __restrict__ aii_in, R* __restrict__ press,
+    R4<R>* __restrict__ xq, double* __restrict__ partials, int after, StepParams<R> P) {
   if (sc->converged) return;
   __shared__ double sh[32];
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
-  // this particle's own data and first list batch travel while the halo stages
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = sc->n_active;
   const bool act = i < n;
-  int cnt = 0;
-  ListHead<NB, kSweepPrefetch> head{};
-  R4<R> xi{}, ai{}, bg{};
+  SweepList<R> L;
+  L.begin(N, act ? i : 0, act ? min((int)N.ncnt[i], N.K) : 0);
+  R4<R> xi{}, Si{}, bg{}, u4{};
+  R2<R> u2{};
   R aii = 0, s = 0, p0 = 0;
   if (act) {
-    cnt = min((int)N.ncnt[i], N.K);
-    head = list_head<NB, kSweepPrefetch>(N.nbr, N.K, i, cnt);
     xi = xv[i];
-    ai = accp[i];
+    Si = Sv[i];
+    u4 = xu[i];
+    u2 = uu[i];
     aii = aii_in[i];
     s = s_in[i];
     p0 = press[i];
-    if (B.kind != 0) bg = B.bG[i];
+    if (has_b) bg = bG[i];
   }
-  R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
-  R4<R>* s_a = staged_vec<R>(dsm, N.hs, 1);
+  R4<R>* s_a = reinterpret_cast<R4<R>*>(dsm);
+  R2<R>* s_b = reinterpret_cast<R2<R>*>(s_a + N.hs);
   if (H.staged)
     stage_halo(H, [&](int l, uint32_t g) {
-      async_copy(&s_x[l], &xv[g]);
-      async_copy(&s_a[l], &accp[g]);
+      async_copy(&s_a[l], &xu[g]);
+      async_copy(&s_b[l], &uu[g]);
     });
   stage_done();
   double e = 0.0;
   if (act) {
-    const R dt = (R)sc->dt;
+    const R ih = P.k.inv_h;
     R sum = 0;
-    for_each_neighbor<NB>(
-        N.nbr, N.K, i, cnt, head,
-        [&](uint32_t l) {
-          if (H.staged) return XV<R>{s_x[l], s_a[l]};
-          const uint32_t g = H.idx[l];
-          return XV<R>{xv[g], accp[g]};
-        },
-        [&](const XV<R>& d) {
-          const R rx = xi.x - d.x.x, ry = xi.y - d.x.y, rz = xi.z - d.x.z;
-          const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
-          sum += d.x.w * f * ((ai.x - d.v.x) * rx + (ai.y - d.v.y) * ry + (ai.z - d.v.z) * rz);
-        });
-    if (B.kind != 0) sum += ai.x * bg.x + ai.y * bg.y + ai.z * bg.z;
-    const R A = dt * dt * sum;
-    if (aii < -P.min_diag) press[i] = fmax(p0 + P.omega * (s - A) / aii, R(0));
+    auto pair = [&](const R4<R>& a, const R2<R>& b) {
+      const R rx = xi.x - a.x, ry = xi.y - a.y, rz = xi.z - a.z;
+      sum += grad_core(rx * rx + ry * ry + rz * rz, ih) * (a.w * rx + b.x * ry + b.y * rz);
+    };
+    if (H.staged) {
+      for (int g = 0; g < L.ng; ++g) {
+        const uint2 w = L.next(g);
+        const uint32_t l0 = w.x & 0xffffu, l1 = w.x >> 16, l2 = w.y & 0xffffu, l3 = w.y >> 16;
+        const R4<R> a0 = s_a[l0], a1 = s_a[l1], a2 = s_a[l2], a3 = s_a[l3];
+        const R2<R> b0 = s_b[l0], b1 = s_b[l1], b2 = s_b[l2], b3 = s_b[l3];
+        pair(a0, b0); pair(a1, b1); pair(a2, b2); pair(a3, b3);
+      }
+    } else {
+      for (int g = 0; g < L.ng; ++g) {
+        const uint2 w = L.next(g);
+        const uint32_t g0 = H.idx[w.x & 0xffffu], g1 = H.idx[w.x >> 16], g2 = H.idx[w.y & 0xffffu],
+                       g3 = H.idx[w.y >> 16];
+        const R4<R> a0 = xu[g0], a1 = xu[g1], a2 = xu[g2], a3 = xu[g3];
+        const R2<R> b0 = uu[g0], b1 = uu[g1], b2 = uu[g2], b3 = uu[g3];
+        pair(a0, b0); pair(a1, b1); pair(a2, b2); pair(a3, b3);
+      }
+    }
+    const R dt = (R)sc->dt;
+    const R iV = R(1) / xi.w;
+    const R ax = u4.w * iV, ay = u2.x * iV, az = u2.y * iV;
+    R tot = ax * Si.x + ay * Si.y + az * Si.z - P.k.cg * sum;
+    if (has_b) tot += ax * bg.x + ay * bg.y + az * bg.z;
+    const R A = dt * dt * tot;
+    R pn = p0;
+    if (aii < -P.min_diag) pn = fmax(p0 + P.omega * (s - A) / aii, R(0));
+    press[i] = pn;
+    xq[i] = R4<R>{xi.x, xi.y, xi.z, xi.w * pn};
     if (s < R(0)) e = fabs((double)A - (double)s);
   }
   const double bs = block_sum(e, sh);

@@ -17,6 +17,12 @@ struct alignas(4 * sizeof(R)) R4 {
   R x, y, z, w;
 };
 
+// 2-wide packed pair (the second record of a sweep gather).
+template <class R>
+struct alignas(2 * sizeof(R)) R2 {
+  R x, y;
+};
+
 template <class R>
 struct V3 {
   R x, y, z;
@@ -97,6 +103,30 @@ __device__ __forceinline__ float kernel_grad_factor<float>(float r2, const Kerne
   const float a = q < 1.f ? 1.f - q : 0.f;
   const float b = q < 0.5f ? 0.5f - q : 0.f;
   return k.cg * (-3.f * (a * a) + 12.f * (b * b)) * inv;
+}
+
+// The gradient factor without its constant: gradW(r) = cg * grad_core(r2) * r,
+// grad_core = w'(q) / |r| with w'(q) = 12 (1/2-q)_+^2 - 3 (1-q)_+^2 (zero at
+// r = 0 and outside the support). Sums of grad_core terms are scaled by cg
+// once, after the loop.
+template <class R>
+__device__ __forceinline__ R grad_core(R r2, R inv_h) {
+  const R rn = sqrt(r2);
+  const R q = rn * inv_h;
+  const R a = q < R(1) ? R(1) - q : R(0);
+  const R b = q < R(0.5) ? R(0.5) - q : R(0);
+  return r2 > R(0) ? (R(12) * (b * b) - R(3) * (a * a)) / rn : R(0);
+}
+// f32: one approximate reciprocal square root (relative error ~2^-23, far
+// inside the f32 state's tolerance) and no branch.
+template <>
+__device__ __forceinline__ float grad_core<float>(float r2, float inv_h) {
+  float inv;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(r2));
+  inv = r2 > 0.f ? inv : 0.f;
+  const float q = r2 * inv * inv_h;
+  const float a = fmaxf(1.f - q, 0.f), b = fmaxf(0.5f - q, 0.f);
+  return fmaf(12.f * b, b, -3.f * a * a) * inv;
 }
 
 // Both W and the gradient factor from one square root.
