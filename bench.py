@@ -173,6 +173,37 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def oracle_module():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle
+
+
+def oracle_system(sc, fields=None):
+    """The oracle (f64 restatement of the reference CPU path) set up with
+    `sc`'s fluid, sample boundaries and, when given, the (sdf, vm) fields of
+    its container, initialized (first update done)."""
+    O = oracle_module()
+    from sphgpu.system import PROCEDURES
+    cfg = dict(sc.parameters)
+    cfg.pop("device", None)
+    cfg.pop("neighbor_capacity", None)
+    cfg.setdefault("max_solver_iterations", 0)
+    cfg.setdefault("time_increment", 0.0)
+    cfg.update(integration_scheme=PROCEDURES["integration_scheme"][sc.procedures["integration_scheme"]],
+               pressure_solver=PROCEDURES["pressure_solver"][sc.procedures["pressure_solver"]],
+               boundary_handling=PROCEDURES["boundary_handling"][sc.procedures["boundary_handling"]],
+               cfl_time_step=1 if sc.cfl_time_step else 0)
+    s = O.OracleSystem(cfg)
+    s.upload_fluid(sc.position, sc.velocity, sc.mass, sc.fluid_id)
+    for pts, rigid in sc.sample_boundaries:
+        s.add_sample_boundary(pts, None if rigid is None else rigid.to_array32())
+    if fields is not None:
+        s.add_volume_map_boundary(*(O.Field(f.x_min, f.x_max, f.dx, f.n, f.nodes) for f in fields))
+    s.initialize()
+    return s
+
+
 def run_cpu(args, fields, min_steps, stop_seconds):
     """The reference's CPU algorithm (oracle restatement, f64, all host
     threads) on the benchmark scene: the same seeded state and fields, the
@@ -180,22 +211,9 @@ def run_cpu(args, fields, min_steps, stop_seconds):
     them, or fewer once at least `min_steps` have run and `stop_seconds` of
     CPU time have been timed. Returns (updates/s, seconds, cores, particles,
     steps timed, sweeps per timed step)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    from sphgpu.system import PROCEDURES
+    O = oracle_module()
     sc = scene(args.n_side, args.max_iters)
-    cfg = dict(sc.parameters)
-    cfg.update(integration_scheme=PROCEDURES["integration_scheme"][sc.procedures["integration_scheme"]],
-               pressure_solver=PROCEDURES["pressure_solver"][sc.procedures["pressure_solver"]],
-               boundary_handling=1, cfl_time_step=1, time_increment=0.0)
-    cfg.pop("device", None)
-    s = O.OracleSystem(cfg)
-    s.upload_fluid(sc.position, None, sc.mass)
-    s.add_volume_map_boundary(O.Field(fields[0].x_min, fields[0].x_max, fields[0].dx, fields[0].n,
-                                      fields[0].nodes),
-                              O.Field(fields[1].x_min, fields[1].x_max, fields[1].dx, fields[1].n,
-                                      fields[1].nodes))
-    s.initialize()
+    s = oracle_system(sc, fields)
     if args.warmup:
         s.step(args.warmup)
     t0 = time.perf_counter()
@@ -485,8 +503,7 @@ def reference_arm(args, ws, rank):
     by the oracle's CPU restatement of the reference's field construction."""
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    O = oracle_module()
     sc = scene(args.n_side, args.max_iters)
     verts, faces = sc.mesh
     sp = sc.parameters["rest_density_grid_spacing"]
@@ -549,15 +566,12 @@ def study_sesph8k(args, device):
     oracle (the reference's CPU path, timed: the CPU-1 baseline), with the
     drift between them every 100 steps."""
     import torch
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle as O
-    from conftest import build_oracle
+    O = oracle_module()
     from sphgpu import _capi as A, scenes
     steps = args.study_steps or 1000
     sc = scenes.dam_break_sesph_8k()
     g = scenes.build_system(sc, precision="f32", device=device)
-    o = build_oracle(sc)
+    o = oracle_system(sc)
     h = sc.parameters["rest_density_grid_spacing"]
     stream = torch.cuda.ExternalStream(g.stream(), device=device)
     rows, gpu_ms, cpu_s = [], 0.0, 0.0

@@ -1519,8 +1519,8 @@ template <class R, int VP, int NB>
 __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     const R4<R>* __restrict__ vstar, NbrArgs N, BoundaryArgs<R> B, R* __restrict__ s_out,
-    R* __restrict__ aii_out, R* __restrict__ press, R4<R>* __restrict__ S_out, R4<R>* __restrict__ xq_out,
-    StepParams<R> P) {
+    R* __restrict__ aii_out, R* __restrict__ press, R4<R>* __restrict__ TA, R4<R>* __restrict__ TB,
+    R2<R>* __restrict__ SA, R4<R>* __restrict__ xq_out, StepParams<R> P) {
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
@@ -1579,8 +1579,12 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
   R p0 = 0;
   if (aii > P.min_diag || aii < -P.min_diag) p0 = fmax(P.omega * s / aii, R(0));
   press[i] = p0;
-  // the Jacobi sweeps' inputs: S_i = sum_j V_j gradW_ij and the record {x, V p}
-  S_out[i] = R4<R>{sfx, sfy, sfz, R(0)};
+  // the Jacobi sweeps' per-solve constants (S_i = sum_j V_j gradW_ij with the
+  // boundary terms folded in) and the first pass A record {x, V p}
+  const R g2 = R(2) * P.gamma_p;
+  TA[i] = R4<R>{sfx + g2 * bx, sfy + g2 * by, sfz + g2 * bz, -(Vi / mi) * Vi};
+  TB[i] = R4<R>{sfx + bx, sfy + by, sfz + bz, Vi};
+  SA[i] = R2<R>{s, aii};
   xq_out[i] = R4<R>{xi.x, xi.y, xi.z, Vi * p0};
 }
 
@@ -1591,7 +1595,9 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
 // Positions and volumes are fixed during a solve, so the pair sums split:
 //   sum_j V_j (p_i + p_j) gradW_ij    = p_i S_i + sum_j (V_j p_j) gradW_ij
 //   sum_j V_j (a_i - a_j) . gradW_ij  = a_i . S_i - sum_j (V_j a_j) . gradW_ij
-// with S_i = sum_j V_j gradW_ij from the source pass. Each pass then gathers
+// with S_i = sum_j V_j gradW_ij from the source pass (stored with the boundary
+// terms and the particle's own constants: TA = {S_i + 2 gamma_p bG_i, -V_i^2/m_i},
+// TB = {S_i + bG_i, V_i}, SA = {s_i, a_ii}). Each pass then gathers
 // one record per neighbor from the block's halo in shared memory:
 //   pass A: xq = {x, y, z, V p}            (written by pass B and the source pass)
 //   pass B: xu = {x, y, z, V a_x}, uu = {V a_y, V a_z}   (written by pass A)
@@ -1619,13 +1625,12 @@ struct SweepList {
   }
 };
 
-// pass A: a_i = -(V_i/m_i) [p_i S_i + sum_j (V_j p_j) gradW_ij + 2 gamma_p p_i bG_i],
+// pass A: a_i = -(V_i/m_i) [p_i (S_i + 2 gamma_p bG_i) + sum_j (V_j p_j) gradW_ij],
 // stored as the records of pass B (V_i a_i).
 template <class R>
 __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_accel(
-    const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
-    const R* __restrict__ press, const R4<R>* __restrict__ Sv, const R4<R>* __restrict__ xq, NbrArgs N,
-    const R4<R>* __restrict__ bG, int has_b, R4<R>* __restrict__ xu, R2<R>* __restrict__ uu, StepParams<R> P) {
+    const Scalars* __restrict__ sc, const R* __restrict__ press, const R4<R>* __restrict__ TA,
+    const R4<R>* __restrict__ xq, NbrArgs N, R4<R>* __restrict__ xu, R2<R>* __restrict__ uu, StepParams<R> P) {
   if (sc->converged) return;
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
@@ -1634,14 +1639,12 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_accel(
   // the list head and this particle's data travel while the halo stages
   SweepList<R> L;
   L.begin(N, act ? i : 0, act ? min((int)N.ncnt[i], N.K) : 0);
-  R4<R> xi{}, Si{}, bg{};
-  R mi = 1, pi = 0;
+  R4<R> xi{}, Ti{};
+  R pi = 0;
   if (act) {
-    xi = xv[i];
-    mi = vel[i].w;
+    xi = xq[i];
+    Ti = TA[i];
     pi = press[i];
-    Si = Sv[i];
-    if (has_b) bg = bG[i];
   }
   R4<R>* s_r = reinterpret_cast<R4<R>*>(dsm);
   if (H.staged) stage_halo(H, [&](int l, uint32_t g) { async_copy(&s_r[l], &xq[g]); });
@@ -1669,13 +1672,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_accel(
     }
   }
   const R cg = P.k.cg;
-  R fx = pi * Si.x + cg * px, fy = pi * Si.y + cg * py, fz = pi * Si.z + cg * pz;
-  if (has_b) {
-    const R c = R(2) * P.gamma_p * pi;
-    fx += c * bg.x; fy += c * bg.y; fz += c * bg.z;
-  }
-  const R Vi = xi.w;
-  const R c = -(Vi / mi) * Vi;  // V_i a_i = -(V_i^2 / m_i) F
+  const R fx = pi * Ti.x + cg * px, fy = pi * Ti.y + cg * py, fz = pi * Ti.z + cg * pz;
+  const R c = Ti.w;  // V_i a_i = -(V_i^2 / m_i) F
   xu[i] = R4<R>{xi.x, xi.y, xi.z, c * fx};
   uu[i] = R2<R>{c * fy, c * fz};
 }
@@ -1687,9 +1685,8 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_accel(
 // AFTER >= 0: stop after AFTER+1 sweeps; AFTER < 0: target density error.
 template <class R>
 __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_jacobi(
-    Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ Sv,
-    const R4<R>* __restrict__ xu, const R2<R>* __restrict__ uu, NbrArgs N, const R4<R>* __restrict__ bG,
-    int has_b, const R* __restrict__ s_in, const R* __restrict__ aii_in, R* __restrict__ press,
+    Scalars* __restrict__ sc, const R4<R>* __restrict__ TB, const R2<R>* __restrict__ SA,
+    const R4<R>* __restrict__ xu, const R2<R>* __restrict__ uu, NbrArgs N, R* __restrict__ press,
     R4<R>* __restrict__ xq, double* __restrict__ partials, int after, StepParams<R> P) {
   if (sc->converged) return;
   __shared__ double sh[32];
@@ -1700,19 +1697,17 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_jacobi
   const bool act = i < n;
   SweepList<R> L;
   L.begin(N, act ? i : 0, act ? min((int)N.ncnt[i], N.K) : 0);
-  R4<R> xi{}, Si{}, bg{}, u4{};
-  R2<R> u2{};
-  R aii = 0, s = 0, p0 = 0;
+  R4<R> Ti{}, u4{};
+  R2<R> u2{}, sa{};
+  R p0 = 0;
   if (act) {
-    xi = xv[i];
-    Si = Sv[i];
     u4 = xu[i];
     u2 = uu[i];
-    aii = aii_in[i];
-    s = s_in[i];
+    Ti = TB[i];
+    sa = SA[i];
     p0 = press[i];
-    if (has_b) bg = bG[i];
   }
+  const R4<R> xi{u4.x, u4.y, u4.z, Ti.w};
   R4<R>* s_a = reinterpret_cast<R4<R>*>(dsm);
   R2<R>* s_b = reinterpret_cast<R2<R>*>(s_a + N.hs);
   if (H.staged)
@@ -1750,9 +1745,9 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_jacobi
     const R dt = (R)sc->dt;
     const R iV = R(1) / xi.w;
     const R ax = u4.w * iV, ay = u2.x * iV, az = u2.y * iV;
-    R tot = ax * Si.x + ay * Si.y + az * Si.z - P.k.cg * sum;
-    if (has_b) tot += ax * bg.x + ay * bg.y + az * bg.z;
+    const R tot = ax * Ti.x + ay * Ti.y + az * Ti.z - P.k.cg * sum;
     const R A = dt * dt * tot;
+    const R s = sa.x, aii = sa.y;
     R pn = p0;
     if (aii < -P.min_diag) pn = fmax(p0 + P.omega * (s - A) / aii, R(0));
     press[i] = pn;

@@ -80,7 +80,7 @@ static uint64_t estimate_bytes(const SceneJob& j) {
   const double K = std::max<double>(j.cfg.neighbor_capacity ? j.cfg.neighbor_capacity : 128, 128) * 1.5;
   double per = 4 * w * 8 + 4 * 8 + w * 2 + 2 * K + 4 * 8192.0 / 256;  // state, sort, p/bW, lists, halo table
   if (ps != SPH_SESPH) per += 4 * w;                    // predicted velocity
-  if (ps == SPH_IISPH || ps == SPH_IISPH_W_OST) per += 2 * w + 14 * w;  // s, a_ii; sweep records xq, xu, uu, S
+  if (ps == SPH_IISPH || ps == SPH_IISPH_W_OST) per += 2 * w + 18 * w;  // s, a_ii; sweep records xq, xu, uu, TA, TB, SA
   if (ps == SPH_SESPH_W_SPLITTING) per += w;
   if (j.cfg.integration_scheme == SPH_TAKE_PREDICTED) per += 2 * 4 * w * 2;
   per += 3 * 4 * w + 8;                                 // snapshot

@@ -724,12 +724,12 @@ class System : public SystemBase {
   }
   size_t device_bytes() const override {
     size_t b = d_sc_.bytes() + d_meas_.bytes();
-    for (const auto* d : {&pos_, &pos2_, &vel_, &vel2_, &xv_, &acc_, &vstar_, &xq_, &xu_, &S_, &xint_, &vint_, &bG_, &bGu_,
+    for (const auto* d : {&pos_, &pos2_, &vel_, &vel2_, &xv_, &acc_, &vstar_, &xq_, &xu_, &TA_, &TB_, &xint_, &vint_, &bG_, &bGu_,
                           &xb_, &xb2_, &vb_, &vb2_, &xbody_, &vmx_, &vmv_, &snap_pos_, &snap_vel_, &snap_acc_,
                           &snap_xint_, &snap_vint_})
       b += d->bytes();
     for (const auto* d : {&press_, &s_, &aii_, &bW_, &rho_pred_}) b += d->bytes();
-    b += uu_.bytes();
+    b += uu_.bytes() + SA_.bytes();
     b += nbr_.bytes();
     for (const auto* d : {&ref_, &ref2_, &fid_, &fid2_, &key_, &slot_, &perm_, &halo_idx_, &halo_n_, &vm_near_, &ncnt_,
                           &count_, &start_,
@@ -791,8 +791,9 @@ class System : public SystemBase {
 
   // particle state
   DBuf<R4<R>> pos_, pos2_, vel_, vel2_, xv_, acc_, vstar_, xint_, vint_, bG_, bGu_;
-  DBuf<R4<R>> xq_, xu_, S_;  // IISPH sweep records {x, V p}, {x, V a_x} and sum_j V_j gradW_ij
-  DBuf<R2<R>> uu_;           // IISPH sweep records {V a_y, V a_z}
+  DBuf<R4<R>> xq_, xu_;      // IISPH sweep records {x, V p}, {x, V a_x}
+  DBuf<R4<R>> TA_, TB_;      // IISPH per-solve constants of the two sweep passes
+  DBuf<R2<R>> uu_, SA_;      // IISPH sweep records {V a_y, V a_z}; {s, a_ii}
   DBuf<R> press_, s_, aii_, bW_, rho_pred_;
   DBuf<uint32_t> ref_, ref2_, fid_, fid2_, key_, slot_, perm_, ncnt_, halo_idx_, halo_n_;
   DBuf<uint16_t> nbr_;
@@ -933,7 +934,7 @@ class System : public SystemBase {
     const bool needs_vstar = cfg_.pressure_solver != SPH_SESPH;
     if (needs_vstar) vstar_.alloc(c);
     if (cfg_.pressure_solver == SPH_IISPH || cfg_.pressure_solver == SPH_IISPH_W_OST) {
-      s_.alloc(c); aii_.alloc(c); xq_.alloc(c); xu_.alloc(c); uu_.alloc(c); S_.alloc(c);
+      s_.alloc(c); aii_.alloc(c); xq_.alloc(c); xu_.alloc(c); uu_.alloc(c); TA_.alloc(c); TB_.alloc(c); SA_.alloc(c);
     }
     if (cfg_.pressure_solver == SPH_SESPH_W_SPLITTING) rho_pred_.alloc(c);
     if (cfg_.integration_scheme == SPH_TAKE_PREDICTED) { xint_.alloc(c); vint_.alloc(c); }
@@ -1295,14 +1296,12 @@ class System : public SystemBase {
   // the pressure update with the residual reduction.
   void iisph_iteration(int after) {
     const int nb = blocks_for((long long)n_);
-    const int hb = boundary_kind_ != 0 ? 1 : 0;
     launch_s("iisph_pressure_accel", k_sweep_accel<R>, dim3(nb), dim3(kBlock), (size_t)hs_ * sizeof(R4<R>),
-             (const Scalars*)d_sc_.p, (const R4<R>*)xv_.p, (const R4<R>*)vel_.p, (const R*)press_.p,
-             (const R4<R>*)S_.p, (const R4<R>*)xq_.p, nargs(), (const R4<R>*)bG_.p, hb, xu_.p, uu_.p, P_);
+             (const Scalars*)d_sc_.p, (const R*)press_.p, (const R4<R>*)TA_.p, (const R4<R>*)xq_.p, nargs(),
+             xu_.p, uu_.p, P_);
     launch_s("iisph_jacobi", k_sweep_jacobi<R>, dim3(nb), dim3(kBlock),
-             (size_t)hs_ * (sizeof(R4<R>) + sizeof(R2<R>)), d_sc_.p, (const R4<R>*)xv_.p, (const R4<R>*)S_.p,
-             (const R4<R>*)xu_.p, (const R2<R>*)uu_.p, nargs(), (const R4<R>*)bG_.p, hb, (const R*)s_.p,
-             (const R*)aii_.p, press_.p, xq_.p, partials_.p, after, P_);
+             (size_t)hs_ * (sizeof(R4<R>) + sizeof(R2<R>)), d_sc_.p, (const R4<R>*)TB_.p, (const R2<R>*)SA_.p,
+             (const R4<R>*)xu_.p, (const R2<R>*)uu_.p, nargs(), press_.p, xq_.p, partials_.p, after, P_);
   }
 
   // resolve_pressure_globally's loop (iisph.rs:419-550). Sweeps run on the
@@ -1365,7 +1364,7 @@ class System : public SystemBase {
                acc_.p, vstar_.p, press_.p, 1, P_);
         body_reduce(nb);
         launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
-               (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, S_.p, xq_.p, P_);
+               (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, TA_.p, TB_.p, SA_.p, xq_.p, P_);
         solve_loop(-1);
         launch_s("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
                (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
@@ -1375,13 +1374,13 @@ class System : public SystemBase {
         launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
         launch_s("iisph_source_diag", k_iisph_source_diag<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
-               (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, S_.p, xq_.p, P_);
+               (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, TA_.p, TB_.p, SA_.p, xq_.p, P_);
         solve_loop(3);
         launch_s("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
                (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
         launch("ost_predict", k_ost_predict<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)acc_.p, vstar_.p);
         launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
-               (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, S_.p, xq_.p, P_);
+               (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, TA_.p, TB_.p, SA_.p, xq_.p, P_);
         solve_loop(-1);
         launch_s("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
                (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
