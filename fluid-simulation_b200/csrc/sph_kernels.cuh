@@ -476,6 +476,25 @@ constexpr int kHashSlots = 4096;   // halo bucket set of a block (hash path)
 constexpr int kHashElems = 3072;   // stencil keys the hash path takes (27 per cell)
 __device__ __forceinline__ uint32_t hash_slot(uint32_t k) { return (k * 0x9E3779B1u) >> 20; }  // 12 bits
 
+// Writes a neighbor list in whole groups of four 16-bit halo positions (one
+// 8-byte store per group instead of one 2-byte store per neighbor); the last
+// group is completed with the particle's own position.
+struct ListWriter {
+  uint2* groups;  // this particle's group 0; group g sits 32 uint2 further
+  int cap;        // list capacity (a multiple of four)
+  uint32_t g0 = 0, g1 = 0;
+  __device__ __forceinline__ void add(int cnt, uint32_t l) {
+    const int q = cnt & 3;
+    if (q < 2) g0 = q == 0 ? l : (g0 | (l << 16));
+    else g1 = q == 2 ? l : (g1 | (l << 16));
+    if (q == 3 && cnt < cap) groups[(size_t)(cnt >> 2) * 32] = make_uint2(g0, g1);
+  }
+  __device__ __forceinline__ void finish(int cnt, uint32_t self) {
+    if (cnt >= cap || (cnt & 3) == 0) return;
+    for (int k = cnt; (k & 3) != 0; ++k) add(k, self);
+  }
+};
+
 template <class R>
 __global__ void __launch_bounds__(kBlock) k_neighbors_density(
     Scalars* __restrict__ sc, const R4<R>* __restrict__ pos, const uint32_t* __restrict__ start,
@@ -675,7 +694,9 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
     const int hr = head ? (int)rank : (int)rank - 1;  // this cell's row of the span table
     const uint32_t* row = hashed ? span_tab + 27 * hr : nullptr;
     const uint32_t own_local = (uint32_t)((hashed ? s_own[hr] : s_own[tid]) + i);
-    uint16_t* list = nbr + nbr_slot(i, 0, P.K);
+    ListWriter lw;
+    lw.groups = reinterpret_cast<uint2*>(nbr + nbr_slot(i, 0, P.K));
+    lw.cap = P.K;
     R sum = P.k.cw * R(0.5);  // self: W(0) = alpha/h^3 * 1/2
     R comp = 0;
     if (staged) {
@@ -703,17 +724,24 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
           const uint32_t local = off + r;
           const R4<R> xj = s_x[local];
           if (local != own_local && in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) {
-            if (cnt < P.K) list[(cnt >> 2) * 128 + (cnt & 3)] = (uint16_t)local;
+            lw.add(cnt, local);
             ++cnt;
           }
         }
       }
+      lw.finish(cnt, own_local);
       // pass 2: the kernel sum over the neighbors, in list order
       const int stored = min(cnt, P.K);
-      for (int k = 0; k < stored; ++k) {
-        const R4<R> xj = s_x[list[(k >> 2) * 128 + (k & 3)]];
-        const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-        kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
+      for (int k0 = 0; k0 < stored; k0 += 4) {
+        const uint2 w = lw.groups[(size_t)(k0 >> 2) * 32];
+        const uint32_t l[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (k0 + u >= stored) break;
+          const R4<R> xj = s_x[l[u]];
+          const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+          kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
+        }
       }
     } else {
 #pragma unroll 1
@@ -727,7 +755,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
           const R4<R> xj = pos[j];
           if (!in_range(xi, xj, P.range, P.range2_lo, P.range2_hi)) continue;
           const uint32_t local = off + r;
-          if (cnt < P.K) list[(cnt >> 2) * 128 + (cnt & 3)] = (uint16_t)(local < usable ? local : 0u);
+          lw.add(cnt, local < usable ? local : 0u);
           ++cnt;
           const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
           kahan_add(sum, comp, kernel_w_r2(rx * rx + ry * ry + rz * rz, P.k));
@@ -736,8 +764,7 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
     }
     // The unused slots of the last group of four hold the particle's own halo
     // position: a sweep pass reads whole groups, and the self pair adds zero.
-    for (int k = min(cnt, P.K); k < ((min(cnt, P.K) + 3) & ~3); ++k)
-      list[(k >> 2) * 128 + (k & 3)] = (uint16_t)(own_local < usable ? own_local : 0u);
+    if (!staged) lw.finish(cnt, own_local < usable ? own_local : 0u);
     R denom = P.V0 * sum;
     if (has_boundary) denom += bW[i];
     const R V = P.V0 / denom;

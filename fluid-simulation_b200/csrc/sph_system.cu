@@ -185,6 +185,11 @@ class System : public SystemBase {
     destroy_graphs();
     if (chunk_event_) cudaEventDestroy(chunk_event_);
     if (body_stream_) cudaStreamDestroy(body_stream_);
+    if (io_stream_) {
+      cudaStreamSynchronize(io_stream_);
+      cudaStreamDestroy(io_stream_);
+    }
+    if (io_ready_) cudaEventDestroy(io_ready_);
     if (h_chunk_sc_) cudaFreeHost(h_chunk_sc_);
     for (auto& kv : prof_) {
       for (auto& e : kv.second.pool) {
@@ -686,7 +691,39 @@ class System : public SystemBase {
       // the positions the step integrates from live in xv too
       if (xi) cuda_check(cudaMemcpyAsync(xv_.p, pos_.p, n_ * sizeof(R4<R>), cudaMemcpyDeviceToDevice, stream_), "D2D");
     }
-    const int st = step(nsteps);
+    // The state a step returns is final once its update has sorted the
+    // integrated particles, so the last step's readback is issued right
+    // there on a copy stream and overlaps the rest of that update (neighbor
+    // search, solve). Graph-captured stepping, and an update that disabled
+    // particles (which renumbers them afterwards), read back at the end.
+    int st = SPH_OK;
+    early_done_ = false;
+    if ((xo || vo) && nsteps > 0) {
+      if (nsteps > 1) st = step(nsteps - 1);
+      stage_x_.alloc(std::max<size_t>(n3, 3));
+      stage_v_.alloc(std::max<size_t>(n3, 3));
+      if (!io_stream_) {
+        cuda_check(cudaStreamCreateWithFlags(&io_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreateWithFlags(&io_ready_, cudaEventDisableTiming), "cudaEventCreate");
+      }
+      early_xo_ = xo;
+      early_vo_ = vo;
+      const size_t n_before = n_;
+      int st1;
+      try {
+        st1 = step(1);
+      } catch (...) {
+        early_xo_ = early_vo_ = nullptr;
+        if (early_done_) cudaStreamSynchronize(io_stream_);
+        throw;
+      }
+      early_xo_ = early_vo_ = nullptr;
+      if (st == SPH_OK) st = st1;
+      if (early_done_) cuda_check(cudaStreamSynchronize(io_stream_), "readback");
+      if (early_done_ && n_ == n_before) return st;
+    } else {
+      st = step(nsteps);
+    }
     if (xo || vo) {
       stage_x_.alloc(std::max<size_t>(n3, 3));
       stage_v_.alloc(std::max<size_t>(n3, 3));
@@ -716,6 +753,15 @@ class System : public SystemBase {
   void set_profiling(bool on) override { profiling_ = on; }
   bool kernel_time(const std::string& name, double* ms, uint64_t* count) override {
     collect_profile();
+    if (name == "*") {  // every timed launch of the handle
+      *ms = 0.0;
+      *count = 0;
+      for (const auto& kv : prof_) {
+        *ms += kv.second.ms;
+        *count += kv.second.count;
+      }
+      return !prof_.empty();
+    }
     auto it = prof_.find(name);
     if (it == prof_.end()) return false;
     *ms = it->second.ms;
@@ -764,6 +810,12 @@ class System : public SystemBase {
 
   sph_config cfg_;
   cudaStream_t stream_ = nullptr;
+  // sph_step_host's overlapped readback of the last step
+  cudaStream_t io_stream_ = nullptr;
+  cudaEvent_t io_ready_ = nullptr;
+  double* early_xo_ = nullptr;
+  double* early_vo_ = nullptr;
+  bool early_done_ = false;
   Scalars* h_sc_ = nullptr;
   double* h_meas_ = nullptr;
   DBuf<Scalars> d_sc_;
@@ -1425,6 +1477,7 @@ class System : public SystemBase {
     launch("prologue", k_prologue<R>, dim3(1), dim3(1), d_sc_.p, P_,
            (capturing_ && cfg_.cfl_time_step) ? 1 : 0);
     sort_particles();
+    if ((early_xo_ || early_vo_) && !capturing_ && !early_done_) issue_early_readback();
     if (sample_dyn) {
       const int sb = blocks_for((long long)ns_);
       launch("body_samples", k_body_samples<R>, dim3(sb), dim3(kBlock), (const int*)ns_d_.p,
@@ -1449,6 +1502,23 @@ class System : public SystemBase {
     calc_acceleration();
     launch("avg_density", k_avg_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
            (const R4<R>*)vel_.p, partials_.p, P_);
+  }
+
+  // sph_step_host's readback of the sorted, integrated state in reference
+  // order: scatter on the engine's stream, copy on the copy stream.
+  void issue_early_readback() {
+    launch("state_io", k_state_out<R>, dim3(blocks_for((long long)n_)), dim3(kBlock), (int)n_,
+           (const uint32_t*)ref_.p, (const R4<R>*)pos_.p, (const R4<R>*)vel_.p, early_xo_ ? stage_x_.p : nullptr,
+           early_vo_ ? stage_v_.p : nullptr);
+    cuda_check(cudaEventRecord(io_ready_, stream_), "event");
+    cuda_check(cudaStreamWaitEvent(io_stream_, io_ready_, 0), "event");
+    if (early_xo_)
+      cuda_check(cudaMemcpyAsync(early_xo_, stage_x_.p, 3 * n_ * sizeof(double), cudaMemcpyDeviceToHost, io_stream_),
+                 "D2H");
+    if (early_vo_)
+      cuda_check(cudaMemcpyAsync(early_vo_, stage_v_.p, 3 * n_ * sizeof(double), cudaMemcpyDeviceToHost, io_stream_),
+                 "D2H");
+    early_done_ = true;
   }
 
   // Grows the neighbor-list and halo capacities past the counts a step

@@ -387,8 +387,11 @@ const char* sph_last_error(void);
 /* Kernel launches issued by this handle since creation (all of its CUDA
  * kernels, every step). */
 int sph_launch_count(const sph_system_t* h, uint64_t* out);
-/* Event-timed duration (ms) of the named kernel class over the last
- * sph_step call when profiling is enabled with sph_set_profiling. */
+/* Event-timed duration (ms) and launch count of the named kernel class,
+ * summed over every launch timed while profiling was enabled with
+ * sph_set_profiling ("*": all classes). With profiling on, an IISPH solve
+ * runs one sweep per host check, so every timed sweep launch does a sweep's
+ * work; the results are the same as without profiling. */
 int sph_set_profiling(sph_system_t* h, int enabled);
 int sph_kernel_time(sph_system_t* h, const char* kernel, double* ms, uint64_t* launches);
 /* Device-resident bytes held by the handle. */

@@ -168,6 +168,38 @@ def test_host_buffer_step_equals_device_step(A):
     assert np.array_equal(a.download(A.FIELD_VELOCITY), vout)
 
 
+def test_host_buffer_step_readback_cases(A):
+    """sph_step_host reads the last step's state back while that step's
+    update still runs: several steps in one call, an IISPH scene, and a step
+    that disables particles (renumbered afterwards, read back at the end)
+    all return what the device path downloads."""
+    from sphgpu import scenes
+    for sc, steps in ((scenes.dam_break_sesph_8k(n_side=12), 3),
+                      (scenes.serving_dam_break(2000, solver="IISPH"), 2)):
+        a = scenes.build_system(sc, precision="f32")
+        b = scenes.build_system(sc, precision="f32")
+        n = b.n
+        xin, vin = b.download(A.FIELD_POSITION), b.download(A.FIELD_VELOCITY)
+        xout, vout = np.zeros((n, 3)), np.zeros((n, 3))
+        a.step_forward_in_time(steps)
+        b.step_host(steps, xin, vin, xout, vout)
+        assert np.array_equal(a.download(A.FIELD_POSITION), xout)
+        assert np.array_equal(a.download(A.FIELD_VELOCITY), vout)
+    sc = scenes.dam_break_sesph_8k(n_side=12)
+    sc.parameters = dict(sc.parameters, disable_particles_below=-0.29)
+    a = scenes.build_system(sc, precision="f32")
+    b = scenes.build_system(sc, precision="f32")
+    n = b.n
+    xin, vin = b.download(A.FIELD_POSITION), b.download(A.FIELD_VELOCITY)
+    xin[::50, 2] = -0.295  # below the threshold: disabled by the step's update
+    a.step_host(1, xin, vin, None, None)
+    xout, vout = np.zeros((n, 3)), np.zeros((n, 3))
+    b.step_host(1, xin, vin, xout, vout)
+    assert a.n == b.n < n
+    assert np.array_equal(a.download(A.FIELD_POSITION), xout[:b.n])
+    assert np.array_equal(a.download(A.FIELD_VELOCITY), vout[:b.n])
+
+
 @pytest.mark.parametrize("mesh", ["box", "sphere"])
 def test_gpu_volume_map_field_builder_matches_oracle(oracle, mesh):
     from sphgpu import scenes
