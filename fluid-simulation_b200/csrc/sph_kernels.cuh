@@ -1654,8 +1654,10 @@ struct SweepList {
 
 // pass A: a_i = -(V_i/m_i) [p_i (S_i + 2 gamma_p bG_i) + sum_j (V_j p_j) gradW_ij],
 // stored as the records of pass B (V_i a_i).
+// (f32: at most 48 registers, so five blocks share an SM; the records are
+// gathered two at a time to fit)
 template <class R>
-__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_accel(
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
     const Scalars* __restrict__ sc, const R* __restrict__ press, const R4<R>* __restrict__ TA,
     const R4<R>* __restrict__ xq, NbrArgs N, R4<R>* __restrict__ xu, R2<R>* __restrict__ uu, StepParams<R> P) {
   if (sc->converged) return;
@@ -1687,8 +1689,14 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_accel(
   if (H.staged) {
     for (int g = 0; g < L.ng; ++g) {
       const uint2 w = L.next(g);
-      const R4<R> r0 = s_r[w.x & 0xffffu], r1 = s_r[w.x >> 16], r2 = s_r[w.y & 0xffffu], r3 = s_r[w.y >> 16];
-      pair(r0); pair(r1); pair(r2); pair(r3);
+      {
+        const R4<R> r0 = s_r[w.x & 0xffffu], r1 = s_r[w.x >> 16];
+        pair(r0); pair(r1);
+      }
+      {
+        const R4<R> r2 = s_r[w.y & 0xffffu], r3 = s_r[w.y >> 16];
+        pair(r2); pair(r3);
+      }
     }
   } else {
     for (int g = 0; g < L.ng; ++g) {

@@ -681,11 +681,21 @@ class System : public SystemBase {
     if (!initialized_) throw Error(SPH_ERR_STATE, "initialize before stepping");
     const size_t n3 = 3 * n_;
     const int nb = blocks_for((long long)n_);
+    if (!io_stream_) {
+      cuda_check(cudaStreamCreateWithFlags(&io_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+      cuda_check(cudaEventCreateWithFlags(&io_ready_, cudaEventDisableTiming), "cudaEventCreate");
+    }
     if (xi || vi) {
       stage_x_.alloc(std::max<size_t>(n3, 3));
       stage_v_.alloc(std::max<size_t>(n3, 3));
+      // positions and velocities travel on two streams, so two copy engines
+      // can carry them at once
       if (xi) cuda_check(cudaMemcpyAsync(stage_x_.p, xi, n3 * sizeof(double), cudaMemcpyHostToDevice, stream_), "H2D");
-      if (vi) cuda_check(cudaMemcpyAsync(stage_v_.p, vi, n3 * sizeof(double), cudaMemcpyHostToDevice, stream_), "H2D");
+      if (vi) {
+        cuda_check(cudaMemcpyAsync(stage_v_.p, vi, n3 * sizeof(double), cudaMemcpyHostToDevice, io_stream_), "H2D");
+        cuda_check(cudaEventRecord(io_ready_, io_stream_), "event");
+        cuda_check(cudaStreamWaitEvent(stream_, io_ready_, 0), "event");
+      }
       launch("state_io", k_state_in<R>, dim3(nb), dim3(kBlock), (int)n_, (const uint32_t*)ref_.p,
              (const double*)(xi ? stage_x_.p : nullptr), (const double*)(vi ? stage_v_.p : nullptr), pos_.p, vel_.p);
       // the positions the step integrates from live in xv too
@@ -702,10 +712,6 @@ class System : public SystemBase {
       if (nsteps > 1) st = step(nsteps - 1);
       stage_x_.alloc(std::max<size_t>(n3, 3));
       stage_v_.alloc(std::max<size_t>(n3, 3));
-      if (!io_stream_) {
-        cuda_check(cudaStreamCreateWithFlags(&io_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-        cuda_check(cudaEventCreateWithFlags(&io_ready_, cudaEventDisableTiming), "cudaEventCreate");
-      }
       early_xo_ = xo;
       early_vo_ = vo;
       const size_t n_before = n_;
