@@ -2458,7 +2458,8 @@ __device__ __forceinline__ double block_sum_all(double v, double* sh, double* ou
 constexpr int kContactSolveThreads = 1024;
 __global__ void __launch_bounds__(kContactSolveThreads) k_contact_solve(
     Body* __restrict__ bodies, int nb, const ContactCell* __restrict__ cells, ContactScalars* __restrict__ cs,
-    int* __restrict__ cell_idx, ContactState* __restrict__ st, const Scalars* __restrict__ sc, int sweep_cap) {
+    int* __restrict__ cell_idx, ContactState* __restrict__ st, const Scalars* __restrict__ sc, int sweep_cap,
+    int fixed_sweeps) {
   constexpr double kMu = 0.5, kOmega = 0.5, kMinDiag = 1e-35, kTolP = 1e-6, kTolF = 1e-3;
   __shared__ double sh[32];
   __shared__ double bc;
@@ -2657,8 +2658,9 @@ __global__ void __launch_bounds__(kContactSolveThreads) k_contact_solve(
   accumulate();
   predict();
   int it = 0;
-  bool done = converged();
-  while (!done && it < sweep_cap) {
+  // fixed_sweeps > 0: exactly that many sweeps, no merit test
+  bool done = fixed_sweeps > 0 ? false : converged();
+  while (fixed_sweeps > 0 ? it < fixed_sweeps : (!done && it < sweep_cap)) {
     jacobi();
     double g2 = 0.0;
     for (int c = tid; c < n; c += nthreads) {
@@ -2709,7 +2711,7 @@ __global__ void __launch_bounds__(kContactSolveThreads) k_contact_solve(
     prev = gsum;
     accumulate();
     predict();
-    done = converged();
+    if (fixed_sweeps == 0) done = converged();
     ++it;
   }
   accumulate();
@@ -2722,7 +2724,7 @@ __global__ void __launch_bounds__(kContactSolveThreads) k_contact_solve(
   if (tid == 0) {
     cs->ncells = n;
     cs->iterations = it;
-    cs->capped = done ? 0 : 1;
+    cs->capped = (fixed_sweeps > 0 || done) ? 0 : 1;
   }
 }
 

@@ -816,6 +816,7 @@ class System : public SystemBase {
 
   sph_config cfg_;
   cudaStream_t stream_ = nullptr;
+  uint32_t contact_fixed_sweeps_ = 0;  // 0: the reference's merit test
   // sph_step_host's overlapped readback of the last step
   cudaStream_t io_stream_ = nullptr;
   cudaEvent_t io_ready_ = nullptr;
@@ -1282,9 +1283,16 @@ class System : public SystemBase {
            (const ContactScalars*)contact_scalars_.p, contact_cells_.p, contact_gl_, h, (const Scalars*)d_sc_.p);
     launch("contact_solve", k_contact_solve, dim3(1), dim3(kContactSolveThreads), bodies_d_.p, nbodies_,
            (const ContactCell*)contact_cells_.p, contact_scalars_.p, contact_idx_.p, contact_state_.p,
-           (const Scalars*)d_sc_.p, kContactSweepCap);
+           (const Scalars*)d_sc_.p, kContactSweepCap, (int)contact_fixed_sweeps_);
   }
 
+  void set_contact_sweeps(uint32_t fixed) override {
+    if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
+    if (fixed > (uint32_t)kContactSweepCap) throw Error(SPH_ERR_INVALID, "more contact sweeps than the cap");
+    if (fixed == contact_fixed_sweeps_) return;
+    contact_fixed_sweeps_ = fixed;
+    destroy_graphs();  // the captured contact solve carries the old count
+  }
   void contact_stats(uint32_t* out) override {
     ContactScalars c{};
     if (contact_) c = fetch(contact_scalars_.p, 1)[0];
@@ -2209,6 +2217,14 @@ int sph_get_contact_stats(sph_system_t* h, uint32_t* out4) {
     if (!h->initialized) throw Error(SPH_ERR_STATE, "initialize first");
     set_device(h);
     h->impl->contact_stats(out4);
+  });
+}
+
+int sph_set_contact_sweeps(sph_system_t* h, uint32_t fixed_sweeps) {
+  return guarded([&] {
+    if (!h) throw Error(SPH_ERR_INVALID, "null argument");
+    set_device(h);
+    h->impl->set_contact_sweeps(fixed_sweeps);
   });
 }
 

@@ -269,6 +269,7 @@ SIGNATURES = {
                                  C.POINTER(C.POINTER(C.c_uint32))]),
     "sph_meshes_free": (None, [_vp]),
     "sph_get_contact_stats": (C.c_int, [_vp, _u32p]),
+    "sph_set_contact_sweeps": (C.c_int, [_vp, C.c_uint32]),
     "sph_bytes_get": (C.c_int, [_vp, C.POINTER(C.POINTER(C.c_uint8)), C.POINTER(_sz)]),
     "sph_bytes_free": (None, [_vp]),
     "sph_checkpoint_from_view": (C.c_int, [C.POINTER(SphCheckpointView), C.POINTER(_vp)]),

@@ -179,6 +179,11 @@ class GpuSystem:
             A.check(self._L.sph_set_volume_map_aabb(self._h, bi.value, c, h))
         return bi.value
 
+    def set_contact_sweeps(self, fixed_sweeps: int):
+        """0: the reference's merit test ends each contact solve; n > 0:
+        exactly n sweeps after the first (sph_set_contact_sweeps)."""
+        A.check(self._L.sph_set_contact_sweeps(self._h, int(fixed_sweeps)))
+
     def contact_stats(self) -> dict:
         """Rigid-rigid contact of the last step: cells, solver sweeps, whether
         sub-cells were dropped for capacity, whether the sweep cap stopped it."""

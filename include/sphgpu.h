@@ -201,6 +201,13 @@ int sph_set_volume_map_aabb(sph_system_t* h, int bi, const double* center, const
 /* Contact cells, solver sweeps, whether sub-cells were dropped for capacity,
  * and whether the sweep cap (10000) stopped the solve, for the last step. */
 int sph_get_contact_stats(sph_system_t* h, uint32_t* out4);
+/* Contact solve stopping rule. 0 (default): the reference's test, stop once
+ * the mean Fischer-Burmeister merits of pressure and friction pass their
+ * tolerances (volume_map_boundary.rs:163-176). n > 0: exactly n sweeps after
+ * the first, like IISPH's AfterIteration, so that two solvers summing in
+ * different orders can be compared on the same iterate. Re-captures the step
+ * graphs. */
+int sph_set_contact_sweeps(sph_system_t* h, uint32_t fixed_sweeps);
 
 /* BoundaryHandling::initialize (boundary_handling/mod.rs:62-67) followed by
  * the first update() of System::new_boxed (sph/mod.rs:418-419). */

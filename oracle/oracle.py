@@ -43,7 +43,7 @@ class OracleConfig(C.Structure):
         ("min_diagonal_element", C.c_double), ("time_increment", C.c_double),
         ("max_time_increment", C.c_double), ("cfl_number", C.c_double),
         ("gravity_mode", C.c_int), ("gravity_center", C.c_double * 3),
-        ("max_solver_iterations", C.c_uint),
+        ("max_solver_iterations", C.c_uint), ("contact_fixed_sweeps", C.c_uint),
     ]
 
 

@@ -25,6 +25,7 @@ typedef struct oracle_config {
   int gravity_mode;
   double gravity_center[3];
   unsigned max_solver_iterations;  // 0 = unbounded (reference semantics)
+  unsigned contact_fixed_sweeps;   // 0 = the reference's merit test
 } oracle_config;
 
 struct OracleHandle {
@@ -48,8 +49,13 @@ void* oracle_system_create(const oracle_config* c) {
   System& s = h->sys;
   s.integrator = (Integrator)c->integration_scheme;
   s.solver = (Solver)c->pressure_solver;
-  if (c->boundary_handling == 0) s.boundary = std::make_unique<StaticSampleBoundary>();
-  else s.boundary = std::make_unique<VolumeMapBoundary>();
+  if (c->boundary_handling == 0) {
+    s.boundary = std::make_unique<StaticSampleBoundary>();
+  } else {
+    auto vmb = std::make_unique<VolumeMapBoundary>();
+    vmb->contact_fixed_sweeps = c->contact_fixed_sweeps;
+    s.boundary = std::move(vmb);
+  }
   SystemParameters& p = s.params;
   p.cfl = c->cfl_time_step != 0;
   p.time_increment = p.cfl ? 0.0 : c->time_increment;

@@ -850,9 +850,13 @@ ContactResult VolumeMapBoundary::solve_contacts(double dt, bool commit) {
   predict();
   merits();
   uint32_t it = 0;
-  while (!(mean_fischer_burmeister(pp, v_err) < kFbTolPressure &&
-           mean_fischer_burmeister(vtn, dev) < kFbTolFriction) &&
-         it < contact_iteration_cap) {
+  auto more = [&]() {
+    if (contact_fixed_sweeps) return it < contact_fixed_sweeps;
+    return !(mean_fischer_burmeister(pp, v_err) < kFbTolPressure &&
+             mean_fischer_burmeister(vtn, dev) < kFbTolFriction) &&
+           it < contact_iteration_cap;
+  };
+  while (more()) {
     jacobi(pj, lj);
     double gpn = 0, gln = 0;
     for (size_t c = 0; c < n; ++c) {

@@ -303,6 +303,9 @@ struct VolumeMapBoundary : BoundaryHandling {
   double kernel_support_radius = 0;
   // Sweep cap of the contact solve; the reference loops until converged.
   uint32_t contact_iteration_cap = 100000;
+  // > 0: exactly this many sweeps after the first (no merit test), so that
+  // solvers that sum in other orders can be compared on the same iterate.
+  uint32_t contact_fixed_sweeps = 0;
   void initialize(double ksr, double) override { kernel_support_radius = ksr; }
   // Contact cells, NNCG-accelerated projected Jacobi for the contact
   // pressures and frictions, and the resulting forces and torques; with

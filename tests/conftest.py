@@ -45,9 +45,14 @@ def oracle_config(scene):
     return cfg
 
 
-def build_oracle(scene, fields=None):
+def build_oracle(scene, fields=None, extra=None):
+    """The oracle set up like `scene` (plus optional volume-map `fields`);
+    `extra` adds oracle-only config fields (e.g. contact_fixed_sweeps)."""
     import oracle as O
-    s = O.OracleSystem(oracle_config(scene))
+    cfg = oracle_config(scene)
+    if extra:
+        cfg.update(extra)
+    s = O.OracleSystem(cfg)
     s.upload_fluid(scene.position, scene.velocity, scene.mass, scene.fluid_id)
     boxes = []
     for pts, rigid in scene.sample_boundaries:

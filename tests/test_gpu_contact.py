@@ -108,6 +108,37 @@ def test_bodies_follow_the_oracle(A, oracle, fields, boxes):
     g.close()
 
 
+FIXED_SWEEPS = 40
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_fixed_sweep_contact_matches_oracle_tightly(A, oracle, fields, precision):
+    """Both solvers run exactly FIXED_SWEEPS contact sweeps per solve (no
+    merit test), so they stop on the same iterate and only summation order
+    separates them; the bodies then agree far more tightly than under the
+    merit test. The fluid is away from the balls, so the f32 engine's bodies
+    (f64 state, f64 contact solve) follow the same bounds."""
+    from sphgpu import scenes
+    sc = _scene(fields, True)
+    g = scenes.build_system(sc, precision=precision)
+    g.set_contact_sweeps(FIXED_SWEEPS)
+    o = build_oracle(sc, extra={"contact_fixed_sweeps": FIXED_SWEEPS})
+    worst = np.zeros(4)
+    for step in range(6):
+        g.step_forward_in_time(1)
+        o.step(1)
+        st = g.contact_stats()
+        assert st["cells"] > 0 and st["sweeps"] == FIXED_SWEEPS and st["capped"] == 0, st
+        bg, bo = _bodies(g), _bodies(o)
+        for k, (sl, scale) in enumerate(((slice(0, 3), 0.3), (slice(3, 7), 1.0), (slice(7, 10), 0.5),
+                                         (slice(10, 13), 1e-4))):
+            worst[k] = max(worst[k], np.abs(bg[:, sl] - bo[:, sl]).max() / (scale + np.abs(bo[:, sl]).max()))
+    print(f"[contact {precision}] fixed {FIXED_SWEEPS} sweeps, relative errors com {worst[0]:.2e} "
+          f"q {worst[1]:.2e} v {worst[2]:.2e} L {worst[3]:.2e}")
+    assert worst[0] < 1e-9 and worst[1] < 1e-8 and worst[2] < 1e-7 and worst[3] < 1e-6
+    g.close()
+
+
 def test_contact_pushes_bodies_apart(A, fields):
     from sphgpu import scenes
     with_c = scenes.build_system(_scene(fields, True), precision="f64")
