@@ -71,6 +71,7 @@ class SystemBase {
   virtual void set_volume_map_aabb(int bi, const double* center, const double* half_extents) = 0;
   virtual void contact_stats(uint32_t* out4) = 0;  // cells, sweeps, overflow, capped of the last step
   virtual void set_contact_sweeps(uint32_t fixed) = 0;  // 0: merit test; n: exactly n sweeps
+  virtual uint32_t contact_sweeps() const = 0;
   virtual void rigid_state(int bi, double* out) = 0;
   virtual void set_rigid_state(int bi, const double* in) = 0;
   virtual uint64_t hash_collisions() = 0;

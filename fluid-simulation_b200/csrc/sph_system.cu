@@ -858,6 +858,7 @@ class System : public SystemBase {
   DBuf<uint16_t> nbr_;
   int hcap_ = 8192;   // halo table capacity per block (grows on overflow, at most 65535)
   int hs_ = sizeof(R) == 4 ? 1536 : 1024;  // halo records staged in shared memory per block
+  int sweep_hs_ = sizeof(R) == 4 ? 2048 : 1024;  // the same for the IISPH sweep passes
   DBuf<uint32_t> count_, start_, tile_sums_;
   DBuf<double> partials_, body_partials_, stage_x_, stage_v_;
   // boundaries
@@ -1293,6 +1294,7 @@ class System : public SystemBase {
     contact_fixed_sweeps_ = fixed;
     destroy_graphs();  // the captured contact solve carries the old count
   }
+  uint32_t contact_sweeps() const override { return contact_fixed_sweeps_; }
   void contact_stats(uint32_t* out) override {
     ContactScalars c{};
     if (contact_) c = fetch(contact_scalars_.p, 1)[0];
@@ -1362,12 +1364,15 @@ class System : public SystemBase {
   // the pressure update with the residual reduction.
   void iisph_iteration(int after) {
     const int nb = blocks_for((long long)n_);
-    launch_s("iisph_pressure_accel", k_sweep_accel<R>, dim3(nb), dim3(kBlock), (size_t)hs_ * sizeof(R4<R>),
-             (const Scalars*)d_sc_.p, (const R*)press_.p, (const R4<R>*)TA_.p, (const R4<R>*)xq_.p, nargs(),
+    NbrArgs N = nargs();
+    N.hs = sweep_hs_;
+    launch_s("iisph_pressure_accel", k_sweep_accel<R>, dim3(nb), dim3(kBlock), (size_t)sweep_hs_ * sizeof(R4<R>),
+             (const Scalars*)d_sc_.p, (const R*)press_.p, (const R4<R>*)TA_.p, (const R4<R>*)xq_.p, N,
              xu_.p, uu_.p, P_);
     launch_s("iisph_jacobi", k_sweep_jacobi<R>, dim3(nb), dim3(kBlock),
-             (size_t)hs_ * (sizeof(R4<R>) + sizeof(R2<R>)), d_sc_.p, (const R4<R>*)TB_.p, (const R2<R>*)SA_.p,
-             (const R4<R>*)xu_.p, (const R2<R>*)uu_.p, nargs(), press_.p, xq_.p, partials_.p, after, P_);
+             (size_t)sweep_hs_ * (sizeof(R4<R>) + sizeof(R2<R>)), d_sc_.p, (const R4<R>*)TB_.p,
+             (const R2<R>*)SA_.p, (const R4<R>*)xu_.p, (const R2<R>*)uu_.p, N, press_.p, xq_.p, partials_.p,
+             after, P_);
   }
 
   // resolve_pressure_globally's loop (iisph.rs:419-550). Sweeps run on the
@@ -1625,6 +1630,7 @@ class System : public SystemBase {
   void get_tuning(sph_tuning* out) const override {
     out->gather_batch = (uint32_t)nb_;
     out->halo_stage = (uint32_t)hs_;
+    out->sweep_stage = (uint32_t)sweep_hs_;
   }
   void set_tuning(const sph_tuning& t) override {
     if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
@@ -1633,9 +1639,14 @@ class System : public SystemBase {
     const size_t record = 2 * sizeof(R4<R>) + sizeof(R);
     if (t.halo_stage > 65535u || (size_t)t.halo_stage * record + kStaticSmemReserve > kMaxSmemPerBlock)
       throw Error(SPH_ERR_INVALID, "halo stage exceeds a block's shared memory");
-    if ((int)t.gather_batch == nb_ && (int)t.halo_stage == hs_) return;
+    // the sweep's widest staging is pass B's {x, V a_x} and {V a_y, V a_z}
+    const size_t sweep_record = sizeof(R4<R>) + sizeof(R2<R>);
+    if (t.sweep_stage > 65535u || (size_t)t.sweep_stage * sweep_record + kStaticSmemReserve > kMaxSmemPerBlock)
+      throw Error(SPH_ERR_INVALID, "sweep stage exceeds a block's shared memory");
+    if ((int)t.gather_batch == nb_ && (int)t.halo_stage == hs_ && (int)t.sweep_stage == sweep_hs_) return;
     nb_ = (int)t.gather_batch;
     hs_ = (int)t.halo_stage;
+    sweep_hs_ = (int)t.sweep_stage;
     destroy_graphs();  // the captured launches carry the old parameters
   }
 
@@ -2685,6 +2696,7 @@ int sph_clone(const sph_system_t* src, sph_system_t** out) {
     sph_tuning t;
     s->get_tuning(&t);
     h->impl->set_tuning(t);
+    h->impl->set_contact_sweeps(s->contact_sweeps());
     h->impl->set_step_graphs(s->step_graph_chunk());
     *out = guard.release();
   });
@@ -2716,10 +2728,12 @@ int sph_autotune(sph_system_t* h, uint32_t steps, sph_tuning* best, double* best
     if (steps == 0) throw Error(SPH_ERR_INVALID, "tuning needs at least one timed step");
     set_device(h);
     const bool f32 = h->cfg.precision == SPH_F32;
+    sph_tuning cur{};
+    h->impl->get_tuning(&cur);
     std::vector<sph_tuning> cand;
     for (uint32_t nb : {4u, 8u})
       for (uint32_t hs : f32 ? std::vector<uint32_t>{1024, 1536, 2048} : std::vector<uint32_t>{512, 1024, 1536})
-        cand.push_back(sph_tuning{nb, hs});
+        cand.push_back(sph_tuning{nb, hs, cur.sweep_stage});
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     sph::cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
     std::unique_ptr<CUevent_st, cudaError_t (*)(cudaEvent_t)> g0(e0, cudaEventDestroy);
@@ -2730,9 +2744,8 @@ int sph_autotune(sph_system_t* h, uint32_t steps, sph_tuning* best, double* best
       if (rc != SPH_OK && rc != SPH_NOT_CONVERGED) throw Error(rc, sph_last_error());
     };
     double best_t = std::numeric_limits<double>::infinity();
-    sph_tuning pick{};
-    h->impl->get_tuning(&pick);
-    for (const sph_tuning& c : cand) {
+    sph_tuning pick = cur;
+    auto time_candidate = [&](const sph_tuning& c) {
       sph_system_t* k = nullptr;
       int rc = sph_clone(h, &k);
       if (rc) throw Error(rc, sph_last_error());
@@ -2751,7 +2764,12 @@ int sph_autotune(sph_system_t* h, uint32_t steps, sph_tuning* best, double* best
         best_t = per;
         pick = c;
       }
-    }
+    };
+    for (const sph_tuning& c : cand) time_candidate(c);
+    // then the sweep passes' staging capacity, with the best of the above
+    const sph_tuning base = pick;
+    for (uint32_t ss : f32 ? std::vector<uint32_t>{1536, 2048, 3072} : std::vector<uint32_t>{1024, 1536})
+      if (ss != base.sweep_stage) time_candidate(sph_tuning{base.gather_batch, base.halo_stage, ss});
     h->impl->set_tuning(pick);
     *best = pick;
     if (best_ms_per_step) *best_ms_per_step = best_t;

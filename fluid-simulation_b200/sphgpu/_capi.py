@@ -121,7 +121,7 @@ class SphSceneResult(C.Structure):
 
 
 class SphTuning(C.Structure):
-    _fields_ = [("gather_batch", C.c_uint32), ("halo_stage", C.c_uint32)]
+    _fields_ = [("gather_batch", C.c_uint32), ("halo_stage", C.c_uint32), ("sweep_stage", C.c_uint32)]
 
 
 class SphServerStats(C.Structure):

@@ -476,10 +476,13 @@ class GpuSystem:
         """Result-invariant launch parameters of the neighbor passes."""
         t = A.SphTuning()
         A.check(self._L.sph_get_tuning(self._h, C.byref(t)))
-        return {"gather_batch": t.gather_batch, "halo_stage": t.halo_stage}
+        return {"gather_batch": t.gather_batch, "halo_stage": t.halo_stage, "sweep_stage": t.sweep_stage}
 
-    def set_tuning(self, gather_batch: int, halo_stage: int):
-        t = A.SphTuning(int(gather_batch), int(halo_stage))
+    def set_tuning(self, gather_batch: int, halo_stage: int, sweep_stage: int | None = None):
+        """sweep_stage None keeps the current staging capacity of the IISPH sweep passes."""
+        if sweep_stage is None:
+            sweep_stage = self.tuning()["sweep_stage"]
+        t = A.SphTuning(int(gather_batch), int(halo_stage), int(sweep_stage))
         A.check(self._L.sph_set_tuning(self._h, C.byref(t)))
 
     def autotune(self, steps: int = 5) -> dict:
@@ -487,7 +490,8 @@ class GpuSystem:
         returns it with its milliseconds per step; this system does not step."""
         t, ms = A.SphTuning(), C.c_double()
         A.check(self._L.sph_autotune(self._h, int(steps), C.byref(t), C.byref(ms)))
-        return {"gather_batch": t.gather_batch, "halo_stage": t.halo_stage, "ms_per_step": ms.value}
+        return {"gather_batch": t.gather_batch, "halo_stage": t.halo_stage, "sweep_stage": t.sweep_stage,
+                "ms_per_step": ms.value}
 
 
 # ---- per-trait shims ------------------------------------------------------------------

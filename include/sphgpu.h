@@ -363,15 +363,17 @@ int sph_graph_replays(const sph_system_t* h, uint64_t* out);
 typedef struct sph_tuning {
   uint32_t gather_batch;
   uint32_t halo_stage;
+  uint32_t sweep_stage;  /* halo records the IISPH sweep passes stage (their
+                          * records are 16 and 24 bytes in f32, 32 and 48 in f64) */
 } sph_tuning;
 int sph_get_tuning(const sph_system_t* h, sph_tuning* out);
 int sph_set_tuning(sph_system_t* h, const sph_tuning* tuning);
-/* Autotuner: for each candidate tuning (gather batch 4 and 8 times three
- * staging capacities per precision) it clones the system, runs one warm-up
- * step and times `steps` steps on the clone's stream with CUDA events, then
- * applies the fastest to `h` and returns it with its time per step in
- * milliseconds (best_ms_per_step may be NULL). The system's own state does
- * not advance. */
+/* Autotuner: it times candidate tunings on clones of the system (one warm-up
+ * step, then `steps` steps on the clone's stream with CUDA events): first the
+ * gather batch (4, 8) times three staging capacities per precision, then,
+ * with the best of those, three sweep staging capacities. It applies the
+ * fastest to `h` and returns it with its time per step in milliseconds
+ * (best_ms_per_step may be NULL). The system's own state does not advance. */
 int sph_autotune(sph_system_t* h, uint32_t steps, sph_tuning* best, double* best_ms_per_step);
 
 /* ---- diagnostics -------------------------------------------------------- */

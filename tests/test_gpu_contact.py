@@ -108,7 +108,13 @@ def test_bodies_follow_the_oracle(A, oracle, fields, boxes):
     g.close()
 
 
-FIXED_SWEEPS = 40
+# With a fixed count both solvers run the same projected-Jacobi iterates. Up
+# to about ten sweeps these agree with the oracle to the last bits (measured
+# on B200: body velocities within 4e-16 after 1, 3, 5 and 10 sweeps); at 40
+# sweeps a restart or projection decision of the NNCG iteration flips on a
+# rounding difference and the impulses differ at 1e-2, which is the looseness
+# the merit-stopped comparison above allows for.
+FIXED_SWEEPS = 10
 
 
 @pytest.mark.parametrize("precision", ["f64", "f32"])
@@ -135,7 +141,7 @@ def test_fixed_sweep_contact_matches_oracle_tightly(A, oracle, fields, precision
             worst[k] = max(worst[k], np.abs(bg[:, sl] - bo[:, sl]).max() / (scale + np.abs(bo[:, sl]).max()))
     print(f"[contact {precision}] fixed {FIXED_SWEEPS} sweeps, relative errors com {worst[0]:.2e} "
           f"q {worst[1]:.2e} v {worst[2]:.2e} L {worst[3]:.2e}")
-    assert worst[0] < 1e-9 and worst[1] < 1e-8 and worst[2] < 1e-7 and worst[3] < 1e-6
+    assert worst[0] < 1e-12 and worst[1] < 1e-12 and worst[2] < 1e-11 and worst[3] < 1e-10
     g.close()
 
 

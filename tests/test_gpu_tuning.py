@@ -40,14 +40,14 @@ def test_every_tuning_gives_identical_results(A, case, graphs):
     ref.step_forward_in_time(10)
     want = _fields(A, ref)
     ref.close()
-    for gb, hs in ((8, 1536), (4, 0), (8, 1024), (4, 2048)):
+    for gb, hs, ss in ((8, 1536, 1536), (4, 0, 0), (8, 1024, 3072), (4, 2048, 256)):
         g = scenes.build_system(sc, fields=fields)
-        g.set_tuning(gb, hs)
+        g.set_tuning(gb, hs, ss)
         g.set_step_graphs(graphs)
-        assert g.tuning() == {"gather_batch": gb, "halo_stage": hs}
+        assert g.tuning() == {"gather_batch": gb, "halo_stage": hs, "sweep_stage": ss}
         g.step_forward_in_time(10)
         for got, w in zip(_fields(A, g), want):
-            assert np.array_equal(got, w), (gb, hs)
+            assert np.array_equal(got, w), (gb, hs, ss)
         g.close()
 
 
@@ -59,7 +59,8 @@ def test_autotune_applies_its_pick_without_stepping(A, case):
     before = _fields(A, g)
     t = g.autotune(steps=3)
     assert t["gather_batch"] in (4, 8) and t["halo_stage"] in (1024, 1536, 2048) and t["ms_per_step"] > 0
-    assert g.tuning() == {"gather_batch": t["gather_batch"], "halo_stage": t["halo_stage"]}
+    assert t["sweep_stage"] in (1536, 2048, 3072)
+    assert g.tuning() == {k: t[k] for k in ("gather_batch", "halo_stage", "sweep_stage")}
     assert g.time_steps_propagated() == 2
     for got, w in zip(_fields(A, g), before):
         assert np.array_equal(got, w)
@@ -80,9 +81,9 @@ def test_tunings_that_do_not_fit_are_refused(A):
     from sphgpu import scenes
     g = scenes.build_system(scenes.dam_break_sesph_8k(n_side=8))
     before = g.tuning()
-    for gb, hs in ((5, 1024), (4, 100000), (8, 7000)):
+    for gb, hs, ss in ((5, 1024, 1536), (4, 100000, 1536), (8, 7000, 1536), (4, 1024, 10000)):
         with pytest.raises(A.SPHError) as e:
-            g.set_tuning(gb, hs)
+            g.set_tuning(gb, hs, ss)
         assert e.value.code == A.SPH_ERR_INVALID
     assert g.tuning() == before
     g.close()
