@@ -64,6 +64,7 @@ BYTES_PER_PARTICLE = {
     "boundary_samples": 28,      # R x                                     W samples
     "integrate_key": 60,         # R x,v,a                                 W x,v
     "sort": 84,                  # R x,key,idx; permute x,v,ids
+    "order_lists": 128,          # R lists (about 64 B) W lists
 }
 
 

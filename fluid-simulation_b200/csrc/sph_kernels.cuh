@@ -547,12 +547,17 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
       for (int q = 0; q < 27; ++q) span_tab[27 * rank + q] = keys[q];
     }
     __syncthreads();
+    // Ordered linear probing: a slot keeps the smaller of its key and the
+    // one being inserted, and the larger moves on. The table (and so the
+    // halo layout) then does not depend on the order the threads insert in
+    // (kNoKey, the empty mark, is the largest key).
     for (int e = tid; e < nk; e += kBlock) {
-      const uint32_t k = span_tab[e];
+      uint32_t k = span_tab[e];
       uint32_t h = hash_slot(k);
       for (int probe = 0; probe < kHashSlots; ++probe, h = (h + 1) & (kHashSlots - 1)) {
-        const uint32_t old = atomicCAS(&hkey[h], kNoKey, k);
+        const uint32_t old = atomicMin(&hkey[h], k);
         if (old == kNoKey || old == k) break;
+        if (old > k) k = old;
       }
     }
     __syncthreads();
@@ -774,6 +779,81 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
   // block max of the neighbor count
   for (int o = 16; o > 0; o >>= 1) cnt = max(cnt, __shfl_down_sync(0xffffffffu, cnt, o));
   if ((threadIdx.x & 31) == 0 && cnt > 0) atomicMax(&sc->max_nbrs, cnt);
+}
+
+// Reorders each particle's neighbor list so that, at one list slot, the lanes
+// of a warp tend to read different shared-memory banks in the neighbor
+// passes: lane j's slot k takes an entry whose halo position is j + k modulo
+// 8 when it has one left, else the next residue it has (cyclically). A 16-byte
+// staged record at halo position l sits in bank group l mod 8, so the eight
+// lanes of one 16-byte load phase then mostly hit eight different groups.
+// The list stays the same multiset; its padding slots keep the particle's own
+// position. Lists longer than KMAX keep their order.
+template <int KMAX>
+__global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restrict__ sc, uint16_t* __restrict__ nbr,
+                                                       const uint32_t* __restrict__ ncnt, int K) {
+  static_assert(KMAX <= 255, "slot positions are 8-bit fields");
+  __shared__ uint16_t ent[KMAX * kBlock];  // entry e of thread t at ent[e * kBlock + t]
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = threadIdx.x;
+  if (i >= sc->n_active) return;
+  const int cnt = min((int)ncnt[i], K);
+  if (cnt < 2 || cnt > KMAX) return;
+  uint2* groups = reinterpret_cast<uint2*>(nbr + nbr_slot(i, 0, K));
+  const int ng = (cnt + 3) >> 2;
+  // residue counts in eight 8-bit fields
+  unsigned long long c = 0;
+  for (int g = 0; g < ng; ++g) {
+    const uint2 w = groups[(size_t)g * 32];
+    const uint32_t e[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (4 * g + u < cnt) c += 1ull << (8 * (e[u] & 7u));
+  }
+  const unsigned long long incl = c * 0x0101010101010101ull;  // byte r: entries of residues <= r
+  unsigned long long fill = incl - c;                          // byte r: first slot of residue r
+  // the entries grouped by residue, list order inside a residue
+  uint2 last = make_uint2(0u, 0u);
+  for (int g = 0; g < ng; ++g) {
+    const uint2 w = groups[(size_t)g * 32];
+    last = w;
+    const uint32_t e[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (4 * g + u < cnt) {
+        const uint32_t sh = 8 * (e[u] & 7u);
+        const uint32_t pos = (uint32_t)(fill >> sh) & 0xffu;
+        ent[pos * kBlock + t] = (uint16_t)e[u];
+        fill += 1ull << sh;
+      }
+  }
+  fill = incl - c;
+  uint32_t avail = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r)
+    if ((c >> (8 * r)) & 0xffull) avail |= 1u << r;
+  const uint32_t lane = (uint32_t)(i & 31);
+  const uint32_t pad[4] = {last.x & 0xffffu, last.x >> 16, last.y & 0xffffu, last.y >> 16};
+  for (int g = 0; g < ng; ++g) {
+    uint32_t v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = 4 * g + u;
+      if (k >= cnt) {
+        v[u] = pad[u];
+        continue;
+      }
+      const uint32_t target = (lane + (uint32_t)k) & 7u;
+      const uint32_t rot = ((avail >> target) | (avail << (8u - target))) & 0xffu;
+      const uint32_t r = (target + (uint32_t)(__ffs(rot) - 1)) & 7u;
+      const uint32_t sh = 8 * r;
+      const uint32_t pos = (uint32_t)(fill >> sh) & 0xffu;
+      v[u] = ent[pos * kBlock + t];
+      fill += 1ull << sh;
+      if (pos + 1 == ((uint32_t)(incl >> sh) & 0xffu)) avail &= ~(1u << r);
+    }
+    groups[(size_t)g * 32] = make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -1518,6 +1518,11 @@ class System : public SystemBase {
     launch_s("neighbors_density", k_neighbors_density<R>, dim3(nb), dim3(kBlock), kSearchSmem, d_sc_.p,
              (const R4<R>*)pos_.p, (const uint32_t*)start_.p, xv_.p, nbr_.p, ncnt_.p, halo_idx_.p, halo_n_.p,
              (const R*)bW_.p, boundary_kind_ ? 1 : 0, hcap_, P_);
+    // IISPH in f32 re-reads the lists in every sweep pass: order them for
+    // shared-memory banks once per update
+    if (sizeof(R) == 4 && (cfg_.pressure_solver == SPH_IISPH || cfg_.pressure_solver == SPH_IISPH_W_OST))
+      launch("order_lists", k_order_lists<64>, dim3(nb), dim3(kBlock), (const Scalars*)d_sc_.p, nbr_.p,
+             (const uint32_t*)ncnt_.p, K_);
     calc_acceleration();
     launch("avg_density", k_avg_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
            (const R4<R>*)vel_.p, partials_.p, P_);
