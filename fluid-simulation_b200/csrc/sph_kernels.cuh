@@ -1418,11 +1418,41 @@ struct XV {  // position+volume and one vector
   R4<R> v;
 };
 template <class R>
-struct XVM {  // position+volume, one vector and one scalar
-  R4<R> x;
-  R4<R> v;
-  R m;
+struct SweepList {
+  const uint2* p;  // this particle's first group of four; group g sits 32 uint2 further
+  int ng;          // groups
+  uint2 w0, w1;    // the next two groups, in flight
+  __device__ __forceinline__ void begin(const NbrArgs& N, int i, int cnt) {
+    p = reinterpret_cast<const uint2*>(N.nbr) + nbr_slot(i, 0, N.K) / 4;
+    ng = (cnt + 3) >> 2;
+    w0 = ng > 0 ? __ldcs(p) : make_uint2(0u, 0u);
+    w1 = ng > 1 ? __ldcs(p + 32) : make_uint2(0u, 0u);
+  }
+  // the group to use now; requests the one two groups ahead
+  __device__ __forceinline__ uint2 next(int g) {
+    const uint2 w = w0;
+    w0 = w1;
+    w1 = g + 2 < ng ? __ldcs(p + (size_t)(g + 2) * 32) : make_uint2(0u, 0u);
+    return w;
+  }
 };
+
+// Visits every slot of a particle's neighbor list in whole groups of four,
+// padding included: the unused slots of the last group repeat the particle's
+// own halo position, so a pass whose pair term is zero at r = 0 needs no
+// per-neighbor count test. The four records of a group are gathered before
+// they are used.
+template <class R, class Load, class Use>
+__device__ __forceinline__ void sweep_groups(SweepList<R>& L, Load&& load, Use&& use) {
+  for (int g = 0; g < L.ng; ++g) {
+    const uint2 w = L.next(g);
+    const auto d0 = load(w.x & 0xffffu);
+    const auto d1 = load(w.x >> 16);
+    const auto d2 = load(w.y & 0xffffu);
+    const auto d3 = load(w.y >> 16);
+    use(d0); use(d1); use(d2); use(d3);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // 6. accelerations: gravity + viscosity (+ SESPH pressure) (+ v* = v + dt a)
@@ -1438,6 +1468,10 @@ __global__ void __launch_bounds__(kBlock) k_accel(
   const bool bodies = B.any_dynamic != 0;
   if (bodies) body_accum_init(sh_body, B.nbodies);
   const HaloView H = halo_view(N);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < sc->n_active;
+  SweepList<R> L;  // the list head travels while the halo stages
+  L.begin(N, act ? i : 0, act ? min((int)N.ncnt[i], N.K) : 0);
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
   R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
   if (H.staged)
@@ -1446,8 +1480,7 @@ __global__ void __launch_bounds__(kBlock) k_accel(
       async_copy(&s_v[l], &vel[g]);
     });
   stage_done();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < sc->n_active) {
+  if (act) {
     const R4<R> xi = xv[i];
     const R4<R> vi = vel[i];
     const R mi = vi.w, Vi = xi.w;
@@ -1463,15 +1496,8 @@ __global__ void __launch_bounds__(kBlock) k_accel(
     if (PRESS == 1) pi = P.stiffness * fmax(P.V0 / Vi - R(1), R(0));
     R sx = 0, sy = 0, sz = 0;   // viscosity
     R px = 0, py = 0, pz = 0;   // pressure
-    const int cnt = min((int)N.ncnt[i], N.K);
-    for_each_neighbor<NB>(
-        N.nbr, N.K, i, cnt,
-        [&](uint32_t l) {
-          if (H.staged) return XV<R>{s_x[l], s_v[l]};
-          const uint32_t g = H.idx[l];
-          return XV<R>{xv[g], vel[g]};
-        },
-        [&](const XV<R>& d) {
+    // pair terms are zero at r = 0 (self padding adds nothing)
+    auto pair = [&](const XV<R>& d) {
           const R4<R>& xj = d.x;
           const R4<R>& vj = d.v;
           const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
@@ -1485,7 +1511,11 @@ __global__ void __launch_bounds__(kBlock) k_accel(
             const R t = xj.w * (pi + pj) * f;
             px += t * rx; py += t * ry; pz += t * rz;
           }
-        });
+        };
+    if (H.staged)
+      sweep_groups(L, [&](uint32_t l) { return XV<R>{s_x[l], s_v[l]}; }, pair);
+    else
+      sweep_groups(L, [&](uint32_t l) { const uint32_t g = H.idx[l]; return XV<R>{xv[g], vel[g]}; }, pair);
     if (B.kind != 0) {
       BodyAccum acc_b{sh_body};
       for_each_visc_sample<R>(B, xi, i, P, [&](V3<R> xb, V3<R> vb, R Vb, int body) {
@@ -1526,7 +1556,7 @@ __global__ void __launch_bounds__(kBlock) k_accel(
     acc[i] = R4<R>{ax, ay, az, R(0)};
     if (write_vstar) {
       const R dt = (R)sc->dt;
-      vstar[i] = R4<R>{vi.x + dt * ax, vi.y + dt * ay, vi.z + dt * az, R(0)};
+      vstar[i] = R4<R>{vi.x + dt * ax, vi.y + dt * ay, vi.z + dt * az, mi};  // the mass rides along
     }
     if (PRESS == 1) press[i] = pi;
   }
@@ -1552,13 +1582,11 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
   // this particle's own data and first list batch travel while the halo stages
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = i < sc->n_active;
-  int cnt = 0;
-  ListHead<NB, kSweepPrefetch> head{};
+  SweepList<R> L;
+  L.begin(N, act ? i : 0, act ? min((int)N.ncnt[i], N.K) : 0);
   R4<R> xi{};
   R mi = 1, pi = 0;
   if (act) {
-    cnt = min((int)N.ncnt[i], N.K);
-    head = list_head<NB, kSweepPrefetch>(N.nbr, N.K, i, cnt);
     xi = xv[i];
     mi = vel[i].w;
     pi = press[i];
@@ -1574,19 +1602,16 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
   if (act) {
     const R Vi = xi.w;
     R px = 0, py = 0, pz = 0;
-    for_each_neighbor<NB>(
-        N.nbr, N.K, i, cnt, head,
-        [&](uint32_t l) {
-          if (H.staged) return XP<R>{s_x[l], s_p[l]};
-          const uint32_t g = H.idx[l];
-          return XP<R>{xv[g], press[g]};
-        },
-        [&](const XP<R>& d) {
-          const R rx = xi.x - d.x.x, ry = xi.y - d.x.y, rz = xi.z - d.x.z;
-          const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
-          const R t = d.x.w * (pi + d.s) * f;
-          px += t * rx; py += t * ry; pz += t * rz;
-        });
+    auto pair = [&](const XP<R>& d) {  // zero at r = 0 (self padding)
+      const R rx = xi.x - d.x.x, ry = xi.y - d.x.y, rz = xi.z - d.x.z;
+      const R f = kernel_grad_factor(rx * rx + ry * ry + rz * rz, P.k);
+      const R t = d.x.w * (pi + d.s) * f;
+      px += t * rx; py += t * ry; pz += t * rz;
+    };
+    if (H.staged)
+      sweep_groups(L, [&](uint32_t l) { return XP<R>{s_x[l], s_p[l]}; }, pair);
+    else
+      sweep_groups(L, [&](uint32_t l) { const uint32_t g = H.idx[l]; return XP<R>{xv[g], press[g]}; }, pair);
     if (B.kind != 0) {
       const R4<R> g = B.bG[i];
       const R c = R(2) * P.gamma_p * pi;
@@ -1630,44 +1655,42 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
     R2<R>* __restrict__ SA, R4<R>* __restrict__ xq_out, StepParams<R> P) {
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < sc->n_active;
+  SweepList<R> L;  // the list head travels while the halo stages
+  L.begin(N, act ? i : 0, act ? min((int)N.ncnt[i], N.K) : 0);
+  // records {x, V} and {v*, m} (the acceleration pass stores m in v*.w)
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
   R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
-  R* s_m = staged_scalar<R>(dsm, N.hs, 2, 0);
   if (H.staged)
     stage_halo(H, [&](int l, uint32_t g) {
       async_copy(&s_x[l], &xv[g]);
       async_copy(&s_v[l], &vstar[g]);
-      async_copy(&s_m[l], &vel[g].w);
     });
   stage_done();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= sc->n_active) return;
+  if (!act) return;
   const R dt = (R)sc->dt;
   const R4<R> xi = xv[i];
   const R4<R> vsi = vstar[i];
-  const R Vi = xi.w, mi = vel[i].w;
+  const R Vi = xi.w, mi = vsi.w;
   R div = 0;                       // sum V_j (v*_i - v*_j) . gradW
   R sfx = 0, sfy = 0, sfz = 0;     // S_f = sum V_j gradW
   R s2 = 0;                        // sum V_j^2 / m_j |gradW|^2
-  const int cnt = min((int)N.ncnt[i], N.K);
-  for_each_neighbor<NB>(
-      N.nbr, N.K, i, cnt,
-      [&](uint32_t l) {
-        if (H.staged) return XVM<R>{s_x[l], s_v[l], s_m[l]};
-        const uint32_t g = H.idx[l];
-        return XVM<R>{xv[g], vstar[g], vel[g].w};
-      },
-      [&](const XVM<R>& d) {
-        const R4<R>& xj = d.x;
-        const R4<R>& vsj = d.v;
-        const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
-        const R r2 = rx * rx + ry * ry + rz * rz;
-        const R f = kernel_grad_factor(r2, P.k);
-        const R Vf = xj.w * f;
-        div += Vf * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
-        sfx += Vf * rx; sfy += Vf * ry; sfz += Vf * rz;
-        s2 += xj.w * xj.w / d.m * (f * f * r2);
-      });
+  auto pair = [&](const XV<R>& d) {  // zero at r = 0 (self padding)
+    const R4<R>& xj = d.x;
+    const R4<R>& vsj = d.v;
+    const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
+    const R r2 = rx * rx + ry * ry + rz * rz;
+    const R f = kernel_grad_factor(r2, P.k);
+    const R Vf = xj.w * f;
+    div += Vf * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
+    sfx += Vf * rx; sfy += Vf * ry; sfz += Vf * rz;
+    s2 += xj.w * xj.w / vsj.w * (f * f * r2);
+  };
+  if (H.staged)
+    sweep_groups(L, [&](uint32_t l) { return XV<R>{s_x[l], s_v[l]}; }, pair);
+  else
+    sweep_groups(L, [&](uint32_t l) { const uint32_t g = H.idx[l]; return XV<R>{xv[g], vstar[g]}; }, pair);
   R bx = 0, by = 0, bz = 0, bdiv = 0;
   if (B.kind != 0) {
     const R4<R> g = B.bG[i];
@@ -1712,35 +1735,20 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
 // slots repeat the particle's own, whose pair adds zero), so the loops carry
 // no per-neighbor test. The kernel constant cg multiplies each pair sum once.
 // ---------------------------------------------------------------------------
-template <class R>
-struct SweepList {
-  const uint2* p;  // this particle's first group of four; group g sits 32 uint2 further
-  int ng;          // groups
-  uint2 w0, w1;    // the next two groups, in flight
-  __device__ __forceinline__ void begin(const NbrArgs& N, int i, int cnt) {
-    p = reinterpret_cast<const uint2*>(N.nbr) + nbr_slot(i, 0, N.K) / 4;
-    ng = (cnt + 3) >> 2;
-    w0 = ng > 0 ? __ldcs(p) : make_uint2(0u, 0u);
-    w1 = ng > 1 ? __ldcs(p + 32) : make_uint2(0u, 0u);
-  }
-  // the group to use now; requests the one two groups ahead
-  __device__ __forceinline__ uint2 next(int g) {
-    const uint2 w = w0;
-    w0 = w1;
-    w1 = g + 2 < ng ? __ldcs(p + (size_t)(g + 2) * 32) : make_uint2(0u, 0u);
-    return w;
-  }
-};
 
 // pass A: a_i = -(V_i/m_i) [p_i (S_i + 2 gamma_p bG_i) + sum_j (V_j p_j) gradW_ij],
 // stored as the records of pass B (V_i a_i).
 // (f32: at most 48 registers, so five blocks share an SM; the records are
 // gathered two at a time to fit)
-template <class R>
+// OUT 0: the records of pass B; OUT 1: acc += a_i, OUT 2: acc = a_i (the
+// final pressure acceleration of a solve, pressure_solver/mod.rs:121-195,
+// when no boundary takes reaction forces).
+template <class R, int OUT = 0>
 __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
     const Scalars* __restrict__ sc, const R* __restrict__ press, const R4<R>* __restrict__ TA,
-    const R4<R>* __restrict__ xq, NbrArgs N, R4<R>* __restrict__ xu, R2<R>* __restrict__ uu, StepParams<R> P) {
-  if (sc->converged) return;
+    const R4<R>* __restrict__ xq, NbrArgs N, R4<R>* __restrict__ xu, R2<R>* __restrict__ uu, StepParams<R> P,
+    R4<R>* __restrict__ acc, const R4<R>* __restrict__ TB) {
+  if (OUT == 0 && sc->converged) return;
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1789,8 +1797,15 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
   const R cg = P.k.cg;
   const R fx = pi * Ti.x + cg * px, fy = pi * Ti.y + cg * py, fz = pi * Ti.z + cg * pz;
   const R c = Ti.w;  // V_i a_i = -(V_i^2 / m_i) F
-  xu[i] = R4<R>{xi.x, xi.y, xi.z, c * fx};
-  uu[i] = R2<R>{c * fy, c * fz};
+  if (OUT == 0) {
+    xu[i] = R4<R>{xi.x, xi.y, xi.z, c * fx};
+    uu[i] = R2<R>{c * fy, c * fz};
+  } else {
+    const R m = c / TB[i].w;  // a_i = -(V_i / m_i) F, TB.w = V_i
+    R4<R> o = OUT == 1 ? acc[i] : R4<R>{R(0), R(0), R(0), R(0)};
+    o.x += m * fx; o.y += m * fy; o.z += m * fz;
+    acc[i] = o;
+  }
 }
 
 // pass B: A_i = dt^2 [a_i . (S_i + bG_i) - sum_j (V_j a_j) . gradW_ij];
@@ -1940,14 +1955,13 @@ __global__ void __launch_bounds__(kBlock) k_split_density(
     R* __restrict__ rho_pred, StepParams<R> P) {
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
+  // records {x, V} and {v*, m} (the acceleration pass stores m in v*.w)
   R4<R>* s_x = staged_vec<R>(dsm, N.hs, 0);
   R4<R>* s_v = staged_vec<R>(dsm, N.hs, 1);
-  R* s_m = staged_scalar<R>(dsm, N.hs, 2, 0);
   if (H.staged)
     stage_halo(H, [&](int l, uint32_t g) {
       async_copy(&s_x[l], &xv[g]);
       async_copy(&s_v[l], &vstar[g]);
-      async_copy(&s_m[l], &vel[g].w);
     });
   stage_done();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1955,23 +1969,23 @@ __global__ void __launch_bounds__(kBlock) k_split_density(
   const R dt = (R)sc->dt;
   const R4<R> xi = xv[i];
   const R4<R> vsi = vstar[i];
-  const R mi = vel[i].w;
+  const R mi = vsi.w;
   R rho = mi * P.k.cw * R(0.5), comp = 0;  // self term m_i W(0)
   const int cnt = min((int)N.ncnt[i], N.K);
   for_each_neighbor<NB>(
       N.nbr, N.K, i, cnt,
       [&](uint32_t l) {
-        if (H.staged) return XVM<R>{s_x[l], s_v[l], s_m[l]};
+        if (H.staged) return XV<R>{s_x[l], s_v[l]};
         const uint32_t g = H.idx[l];
-        return XVM<R>{xv[g], vstar[g], vel[g].w};
+        return XV<R>{xv[g], vstar[g]};
       },
-      [&](const XVM<R>& d) {
+      [&](const XV<R>& d) {
         const R4<R>& xj = d.x;
         const R4<R>& vsj = d.v;
         const R rx = xi.x - xj.x, ry = xi.y - xj.y, rz = xi.z - xj.z;
         R w, f;
         kernel_w_and_grad(rx * rx + ry * ry + rz * rz, P.k, w, f);
-        const R t = d.m * w + dt * f * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
+        const R t = vsj.w * w + dt * f * ((vsi.x - vsj.x) * rx + (vsi.y - vsj.y) * ry + (vsi.z - vsj.z) * rz);
         kahan_add(rho, comp, t);
       });
   if (B.kind != 0) {

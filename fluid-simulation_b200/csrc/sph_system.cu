@@ -1368,11 +1368,25 @@ class System : public SystemBase {
     N.hs = sweep_hs_;
     launch_s("iisph_pressure_accel", k_sweep_accel<R>, dim3(nb), dim3(kBlock), (size_t)sweep_hs_ * sizeof(R4<R>),
              (const Scalars*)d_sc_.p, (const R*)press_.p, (const R4<R>*)TA_.p, (const R4<R>*)xq_.p, N,
-             xu_.p, uu_.p, P_);
+             xu_.p, uu_.p, P_, (R4<R>*)nullptr, (const R4<R>*)nullptr);
     launch_s("iisph_jacobi", k_sweep_jacobi<R>, dim3(nb), dim3(kBlock),
              (size_t)sweep_hs_ * (sizeof(R4<R>) + sizeof(R2<R>)), d_sc_.p, (const R4<R>*)TB_.p,
              (const R2<R>*)SA_.p, (const R4<R>*)xu_.p, (const R2<R>*)uu_.p, N, press_.p, xq_.p, partials_.p,
              after, P_);
+  }
+
+  // The pressure acceleration after a solve (a13 with the solved pressures;
+  // OUT 1: +=, OUT 2: overwrite) as one more sweep pass A: the per-solve
+  // constants and the {x, V p} records of the last sweep are still current.
+  // Only without reaction forces onto dynamic bodies.
+  template <int OUT>
+  void final_pressure_accel() {
+    const int nb = blocks_for((long long)n_);
+    NbrArgs N = nargs();
+    N.hs = sweep_hs_;
+    launch_s("pressure_accel", k_sweep_accel<R, OUT>, dim3(nb), dim3(kBlock), (size_t)sweep_hs_ * sizeof(R4<R>),
+             (const Scalars*)d_sc_.p, (const R*)press_.p, (const R4<R>*)TA_.p, (const R4<R>*)xq_.p, N,
+             (R4<R>*)nullptr, (R2<R>*)nullptr, P_, acc_.p, (const R4<R>*)TB_.p);
   }
 
   // resolve_pressure_globally's loop (iisph.rs:419-550). Sweeps run on the
@@ -1411,7 +1425,7 @@ class System : public SystemBase {
     const auto xv = (const R4<R>*)xv_.p;
     const auto vel = (const R4<R>*)vel_.p;
     const NbrArgs nbr = nargs();
-    const size_t sm_xv = smem_of(2, 0), sm_xp = smem_of(1, 1), sm_xvm = smem_of(2, 1);
+    const size_t sm_xv = smem_of(2, 0), sm_xp = smem_of(1, 1);
     with_nb([&](auto NBc) {
     constexpr int NB = decltype(NBc)::value;
     switch (cfg_.pressure_solver) {
@@ -1424,7 +1438,7 @@ class System : public SystemBase {
         launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
         body_reduce(nb);
-        launch_s("split_density", k_split_density<R, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
+        launch_s("split_density", k_split_density<R, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, bargs(), press_.p, rho_pred_.p, P_);
         launch_s("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
                (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
@@ -1434,27 +1448,29 @@ class System : public SystemBase {
         launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
         body_reduce(nb);
-        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
+        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, TA_.p, TB_.p, SA_.p, xq_.p, P_);
         solve_loop(-1);
-        launch_s("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
-               (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
-        body_reduce(nb);
+        if (any_dynamic_) {
+          launch_s("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
+                 (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
+          body_reduce(nb);
+        } else {
+          final_pressure_accel<1>();
+        }
         break;
       case SPH_IISPH_W_OST:
         launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
-        launch_s("iisph_source_diag", k_iisph_source_diag<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
+        launch_s("iisph_source_diag", k_iisph_source_diag<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, TA_.p, TB_.p, SA_.p, xq_.p, P_);
         solve_loop(3);
-        launch_s("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
-               (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
+        final_pressure_accel<2>();  // IISPHwOST takes no dynamic boundaries
         launch("ost_predict", k_ost_predict<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)acc_.p, vstar_.p);
-        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xvm, csc, xv, vel,
+        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, TA_.p, TB_.p, SA_.p, xq_.p, P_);
         solve_loop(-1);
-        launch_s("pressure_accel", k_pressure_accel<R, 2, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
-               (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
+        final_pressure_accel<2>();
         launch("ost_commit", k_ost_commit<R>, dim3(nb), dim3(kBlock), csc, xv, vel, (const R4<R>*)vstar_.p,
                (const R4<R>*)acc_.p, xint_.p, vint_.p);
         break;
