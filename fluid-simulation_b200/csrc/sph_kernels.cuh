@@ -388,7 +388,31 @@ struct NbrArgs {
   int K;                 // list capacity per particle
   int hcap;              // halo table capacity per block
   int hs;                // halo records a launch stages in shared memory
+  int ahead = 0;         // sweep passes: blocks resident at once (L2 prefetch distance), 0 = none
 };
+
+// L2 prefetch for the block one wave ahead (block b + ahead runs on the slot
+// this block frees, about one block lifetime later): its particles' records,
+// the first list groups of its warps and its halo indices, so that its start
+// reads from L2 instead of DRAM.
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+__device__ __forceinline__ void prefetch_lines(const void* p, size_t bytes) {
+  const char* c = static_cast<const char*>(p);
+  for (size_t o = (size_t)threadIdx.x * 128; o < bytes; o += (size_t)kBlock * 128) prefetch_l2(c + o);
+}
+constexpr int kPrefetchGroups = 10;     // list groups per warp (about 36 neighbors)
+constexpr int kPrefetchHalo = 1408;     // halo indices (the typical halo of a block)
+// (m: the block's particles; its warps beyond them hold no lists)
+__device__ __forceinline__ void prefetch_block_lists(const NbrArgs& N, int b, int m) {
+  const int G = min(N.K >> 2, kPrefetchGroups);
+  const char* base = reinterpret_cast<const char*>(N.nbr + nbr_slot(b * kBlock, 0, N.K));
+  const size_t warp_bytes = (size_t)(N.K >> 2) * 256;
+  for (int q = threadIdx.x; q < ((m + 31) >> 5) * G * 2; q += kBlock)
+    prefetch_l2(base + (size_t)(q / (2 * G)) * warp_bytes + (size_t)(q % (2 * G)) * 128);
+  prefetch_lines(N.hidx + (size_t)b * N.hcap, (size_t)min(N.hcap, kPrefetchHalo) * sizeof(uint32_t));
+}
 
 // The block's halo: its particle indices, its size and whether the launch
 // copies its records to shared memory.
@@ -426,12 +450,58 @@ __device__ __forceinline__ void stage_done() {
   __syncthreads();
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while the kernel before it finishes its last wave.
+// grid_dep_wait() returns once that kernel has completed and its writes are
+// visible; everything before it may read only data the earlier kernel does
+// not write. grid_dep_release() lets the next kernel start launching (once
+// every block of this grid has started). Both are no-ops in a plain launch.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_release() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
 // Copies the block's halo records to shared memory: copy(l, g) moves the
 // record of particle g to position l. Four halo indices per thread are read
 // at a time, then their records are requested.
 template <class F>
 __device__ __forceinline__ void stage_halo(const HaloView& H, F&& copy) {
   for (int l0 = threadIdx.x; l0 < H.size; l0 += 4 * kBlock) {
+    uint32_t g[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int l = l0 + u * kBlock;
+      g[u] = l < H.size ? __ldg(H.idx + l) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int l = l0 + u * kBlock;
+      if (l < H.size) copy(l, g[u]);
+    }
+  }
+}
+// stage_halo in two steps for the sweep passes: halo_first() reads the
+// first batch of halo indices (fixed during a solve, so before the grid
+// dependency wait), stage_halo_from() requests the records and the rest.
+struct HaloFirst {
+  uint32_t g[4];
+};
+__device__ __forceinline__ HaloFirst halo_first(const HaloView& H) {
+  HaloFirst f;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int l = threadIdx.x + u * kBlock;
+    f.g[u] = H.staged && l < H.size ? __ldg(H.idx + l) : 0u;
+  }
+  return f;
+}
+template <class F>
+__device__ __forceinline__ void stage_halo_from(const HaloView& H, const HaloFirst& f, F&& copy) {
+  if (!H.staged) return;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int l = threadIdx.x + u * kBlock;
+    if (l < H.size) copy(l, f.g[u]);
+  }
+  for (int l0 = threadIdx.x + 4 * kBlock; l0 < H.size; l0 += 4 * kBlock) {
     uint32_t g[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -794,6 +864,8 @@ __global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restric
                                                        const uint32_t* __restrict__ ncnt, int K) {
   static_assert(KMAX <= 255, "slot positions are 8-bit fields");
   __shared__ uint16_t ent[KMAX * kBlock];  // entry e of thread t at ent[e * kBlock + t]
+  __shared__ uint32_t s_cur[8 * kBlock];   // per residue r of thread t, at [r * kBlock + t]:
+  __shared__ uint32_t s_end[8 * kBlock];   //   the next slot to read and the end of its entries
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = threadIdx.x;
   if (i >= sc->n_active) return;
@@ -801,18 +873,9 @@ __global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restric
   if (cnt < 2 || cnt > KMAX) return;
   uint2* groups = reinterpret_cast<uint2*>(nbr + nbr_slot(i, 0, K));
   const int ng = (cnt + 3) >> 2;
-  // residue counts in eight 8-bit fields
-  unsigned long long c = 0;
-  for (int g = 0; g < ng; ++g) {
-    const uint2 w = groups[(size_t)g * 32];
-    const uint32_t e[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
-      if (4 * g + u < cnt) c += 1ull << (8 * (e[u] & 7u));
-  }
-  const unsigned long long incl = c * 0x0101010101010101ull;  // byte r: entries of residues <= r
-  unsigned long long fill = incl - c;                          // byte r: first slot of residue r
-  // the entries grouped by residue, list order inside a residue
+  for (int r = 0; r < 8; ++r) s_end[r * kBlock + t] = 0;
+  // entries per residue
   uint2 last = make_uint2(0u, 0u);
   for (int g = 0; g < ng; ++g) {
     const uint2 w = groups[(size_t)g * 32];
@@ -820,20 +883,33 @@ __global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restric
     const uint32_t e[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
 #pragma unroll
     for (int u = 0; u < 4; ++u)
+      if (4 * g + u < cnt) ++s_end[(e[u] & 7u) * kBlock + t];
+  }
+  // the entries grouped by residue (list order inside a residue); s_end
+  // advances from each residue's first slot to its end
+  uint32_t avail = 0, run = 0;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    const uint32_t c = s_end[r * kBlock + t];
+    s_cur[r * kBlock + t] = run;
+    s_end[r * kBlock + t] = run;
+    if (c) avail |= 0x101u << r;  // both bytes: a rotation is one shift
+    run += c;
+  }
+  for (int g = 0; g < ng; ++g) {
+    const uint2 w = groups[(size_t)g * 32];
+    const uint32_t e[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
       if (4 * g + u < cnt) {
-        const uint32_t sh = 8 * (e[u] & 7u);
-        const uint32_t pos = (uint32_t)(fill >> sh) & 0xffu;
+        uint32_t& f = s_end[(e[u] & 7u) * kBlock + t];
+        const uint32_t pos = f;
         ent[pos * kBlock + t] = (uint16_t)e[u];
-        fill += 1ull << sh;
+        f = pos + 1;
       }
   }
-  fill = incl - c;
-  uint32_t avail = 0;
-#pragma unroll
-  for (int r = 0; r < 8; ++r)
-    if ((c >> (8 * r)) & 0xffull) avail |= 1u << r;
-  const uint32_t lane = (uint32_t)(i & 31);
   const uint32_t pad[4] = {last.x & 0xffffu, last.x >> 16, last.y & 0xffffu, last.y >> 16};
+  uint32_t target = (uint32_t)i & 7u;  // lane j's slot k wants residue j + k (mod 8)
   for (int g = 0; g < ng; ++g) {
     uint32_t v[4];
 #pragma unroll
@@ -843,14 +919,14 @@ __global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restric
         v[u] = pad[u];
         continue;
       }
-      const uint32_t target = (lane + (uint32_t)k) & 7u;
-      const uint32_t rot = ((avail >> target) | (avail << (8u - target))) & 0xffu;
-      const uint32_t r = (target + (uint32_t)(__ffs(rot) - 1)) & 7u;
-      const uint32_t sh = 8 * r;
-      const uint32_t pos = (uint32_t)(fill >> sh) & 0xffu;
+      // the first residue at or after the target (cyclically) with entries left
+      const uint32_t r = (target + (uint32_t)(__ffs(avail >> target) - 1)) & 7u;
+      uint32_t& c = s_cur[r * kBlock + t];
+      const uint32_t pos = c;
       v[u] = ent[pos * kBlock + t];
-      fill += 1ull << sh;
-      if (pos + 1 == ((uint32_t)(incl >> sh) & 0xffu)) avail &= ~(1u << r);
+      c = pos + 1;
+      if (pos + 1 == (uint32_t)s_end[r * kBlock + t]) avail &= ~(0x101u << r);
+      target = (target + 1) & 7u;
     }
     groups[(size_t)g * 32] = make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
   }
@@ -1748,23 +1824,39 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
     const Scalars* __restrict__ sc, const R* __restrict__ press, const R4<R>* __restrict__ TA,
     const R4<R>* __restrict__ xq, NbrArgs N, R4<R>* __restrict__ xu, R2<R>* __restrict__ uu, StepParams<R> P,
     R4<R>* __restrict__ acc, const R4<R>* __restrict__ TB) {
-  if (OUT == 0 && sc->converged) return;
+  grid_dep_release();
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool act = i < sc->n_active;
-  // the list head and this particle's data travel while the halo stages
+  // what is fixed during a solve (list head, constants, halo indices) is read
+  // before the wait on the previous pass; p and the records after it
   SweepList<R> L;
   L.begin(N, act ? i : 0, act ? min((int)N.ncnt[i], N.K) : 0);
   R4<R> xi{}, Ti{};
   R pi = 0;
+  if (act) Ti = TA[i];
+  const HaloFirst hf = halo_first(H);
+  grid_dep_wait();
+  if (OUT == 0 && sc->converged) return;
   if (act) {
     xi = xq[i];
-    Ti = TA[i];
     pi = press[i];
   }
   R4<R>* s_r = reinterpret_cast<R4<R>*>(dsm);
-  if (H.staged) stage_halo(H, [&](int l, uint32_t g) { async_copy(&s_r[l], &xq[g]); });
+  stage_halo_from(H, hf, [&](int l, uint32_t g) { async_copy(&s_r[l], &xq[g]); });
+  if (N.ahead > 0) {
+    const int b = blockIdx.x + N.ahead;
+    const int n = sc->n_active;
+    if (b * kBlock < n) {
+      const int i0 = b * kBlock, m = min(kBlock, n - i0);
+      prefetch_lines(xq + i0, (size_t)m * sizeof(R4<R>));
+      prefetch_lines(TA + i0, (size_t)m * sizeof(R4<R>));
+      prefetch_lines(press + i0, (size_t)m * sizeof(R));
+      prefetch_lines(N.ncnt + i0, (size_t)m * sizeof(uint32_t));
+      prefetch_block_lists(N, b, m);
+    }
+  }
   stage_done();
   if (!act) return;
   const R ih = P.k.inv_h;
@@ -1818,33 +1910,51 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_jacobi
     Scalars* __restrict__ sc, const R4<R>* __restrict__ TB, const R2<R>* __restrict__ SA,
     const R4<R>* __restrict__ xu, const R2<R>* __restrict__ uu, NbrArgs N, R* __restrict__ press,
     R4<R>* __restrict__ xq, double* __restrict__ partials, int after, StepParams<R> P) {
-  if (sc->converged) return;
+  grid_dep_release();
   __shared__ double sh[32];
   extern __shared__ __align__(32) unsigned char dsm[];
   const HaloView H = halo_view(N);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = sc->n_active;
   const bool act = i < n;
+  // fixed during a solve: read before the wait on pass A
   SweepList<R> L;
   L.begin(N, act ? i : 0, act ? min((int)N.ncnt[i], N.K) : 0);
   R4<R> Ti{}, u4{};
   R2<R> u2{}, sa{};
   R p0 = 0;
   if (act) {
-    u4 = xu[i];
-    u2 = uu[i];
     Ti = TB[i];
     sa = SA[i];
+  }
+  const HaloFirst hf = halo_first(H);
+  grid_dep_wait();
+  if (sc->converged) return;
+  if (act) {
+    u4 = xu[i];
+    u2 = uu[i];
     p0 = press[i];
   }
   const R4<R> xi{u4.x, u4.y, u4.z, Ti.w};
   R4<R>* s_a = reinterpret_cast<R4<R>*>(dsm);
   R2<R>* s_b = reinterpret_cast<R2<R>*>(s_a + N.hs);
-  if (H.staged)
-    stage_halo(H, [&](int l, uint32_t g) {
-      async_copy(&s_a[l], &xu[g]);
-      async_copy(&s_b[l], &uu[g]);
-    });
+  stage_halo_from(H, hf, [&](int l, uint32_t g) {
+    async_copy(&s_a[l], &xu[g]);
+    async_copy(&s_b[l], &uu[g]);
+  });
+  if (N.ahead > 0) {
+    const int b = blockIdx.x + N.ahead;
+    if (b * kBlock < n) {
+      const int i0 = b * kBlock, m = min(kBlock, n - i0);
+      prefetch_lines(xu + i0, (size_t)m * sizeof(R4<R>));
+      prefetch_lines(uu + i0, (size_t)m * sizeof(R2<R>));
+      prefetch_lines(TB + i0, (size_t)m * sizeof(R4<R>));
+      prefetch_lines(SA + i0, (size_t)m * sizeof(R2<R>));
+      prefetch_lines(press + i0, (size_t)m * sizeof(R));
+      prefetch_lines(N.ncnt + i0, (size_t)m * sizeof(uint32_t));
+      prefetch_block_lists(N, b, m);
+    }
+  }
   stage_done();
   double e = 0.0;
   if (act) {
@@ -2235,6 +2345,7 @@ __global__ void k_chunk_begin(Scalars* sc, double time) {
 // body execution either finds `converged` set or adds one to `iterations`,
 // so the loop ends after at most `limit` bodies.
 __global__ void k_loop_cond(cudaGraphConditionalHandle h, const Scalars* __restrict__ sc, int limit) {
+  grid_dep_wait();
   const unsigned int more = (!sc->converged && sc->iterations < limit) ? 1u : 0u;
   cudaGraphSetConditional(h, more);
 }

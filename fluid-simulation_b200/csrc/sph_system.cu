@@ -159,6 +159,8 @@ class System : public SystemBase {
   explicit System(const sph_config& c) : cfg_(c) {
     device = c.device;
     if (const char* e = std::getenv("SPHGPU_SORTED_LISTS")) sorted_lists_ = std::atoi(e) != 0;
+    if (const char* e = std::getenv("SPHGPU_DEPENDENT_LAUNCH")) pdl_ = std::atoi(e) != 0;
+    if (const char* e = std::getenv("SPHGPU_SWEEP_PREFETCH")) prefetch_ = std::atoi(e) != 0;
     if (const char* e = std::getenv("SPHGPU_HALO_STAGE")) {
       // the same bound as set_tuning: the widest staged record ({x, v, m})
       // times the capacity must fit one block's shared memory
@@ -842,6 +844,9 @@ class System : public SystemBase {
   // order no longer matters for memory locality, and stencil order lets the
   // search skip buckets whose cell lies beyond the support radius).
   bool sorted_lists_ = false;
+  bool pdl_ = true;       // programmatic dependent launch between the sweep passes
+  bool prefetch_ = true;  // sweep passes prefetch the next wave's streams into L2
+  std::map<std::pair<const void*, size_t>, int> resident_;
   uint64_t launches_ = 0;
   bool profiling_ = false;
   std::map<std::string, ProfEntry> prof_;
@@ -1087,6 +1092,18 @@ class System : public SystemBase {
   }
   template <class Kern, class... Args>
   void launch_s(const char* name, Kern kernel, dim3 g, dim3 b, size_t smem, Args... args) {
+    launch_impl(false, name, kernel, g, b, smem, args...);
+  }
+  // A launch that may overlap the end of the kernel before it (programmatic
+  // dependent launch): only for kernels that call grid_dep_wait() before
+  // reading what that kernel writes. Timed (profiling) runs launch plainly so
+  // that the events around each kernel bracket it alone.
+  template <class Kern, class... Args>
+  void launch_dep(const char* name, Kern kernel, dim3 g, dim3 b, size_t smem, Args... args) {
+    launch_impl(pdl_ && !profiling_, name, kernel, g, b, smem, args...);
+  }
+  template <class Kern, class... Args>
+  void launch_impl(bool dep, const char* name, Kern kernel, dim3 g, dim3 b, size_t smem, Args... args) {
     if (smem) allow_smem((const void*)kernel, smem);
     cudaEvent_t e1 = nullptr;
     if (profiling_ && !capturing_) {
@@ -1103,7 +1120,21 @@ class System : public SystemBase {
       cuda_check(cudaEventRecord(pr.first, stream_), "event");
       e1 = pr.second;
     }
-    kernel<<<g, b, smem, stream_>>>(args...);
+    if (dep) {
+      cudaLaunchConfig_t lc{};
+      lc.gridDim = g;
+      lc.blockDim = b;
+      lc.dynamicSmemBytes = smem;
+      lc.stream = stream_;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      lc.attrs = at;
+      lc.numAttrs = 1;
+      cuda_check(cudaLaunchKernelEx(&lc, kernel, args...), name);
+    } else {
+      kernel<<<g, b, smem, stream_>>>(args...);
+    }
     cuda_check(cudaGetLastError(), name);
     if (!capturing_) ++launches_;
     else if (!in_loop_body_) ++capture_kernels_;
@@ -1362,17 +1393,36 @@ class System : public SystemBase {
 
   // One Jacobi iteration: pressure accelerations of the current pressures, then
   // the pressure update with the residual reduction.
-  void iisph_iteration(int after) {
+  // first: the solve's first sweep, whose pass A follows the source pass
+  // (which writes TA) and so must not overlap it.
+  void iisph_iteration(int after, bool first) {
     const int nb = blocks_for((long long)n_);
     NbrArgs N = nargs();
     N.hs = sweep_hs_;
-    launch_s("iisph_pressure_accel", k_sweep_accel<R>, dim3(nb), dim3(kBlock), (size_t)sweep_hs_ * sizeof(R4<R>),
-             (const Scalars*)d_sc_.p, (const R*)press_.p, (const R4<R>*)TA_.p, (const R4<R>*)xq_.p, N,
+    const size_t sm_a = (size_t)sweep_hs_ * sizeof(R4<R>);
+    const size_t sm_b = (size_t)sweep_hs_ * (sizeof(R4<R>) + sizeof(R2<R>));
+    N.ahead = resident_blocks((const void*)k_sweep_accel<R>, sm_a);
+    launch_impl(!first && pdl_ && !profiling_, "iisph_pressure_accel", k_sweep_accel<R>, dim3(nb), dim3(kBlock),
+             sm_a, (const Scalars*)d_sc_.p, (const R*)press_.p, (const R4<R>*)TA_.p, (const R4<R>*)xq_.p, N,
              xu_.p, uu_.p, P_, (R4<R>*)nullptr, (const R4<R>*)nullptr);
-    launch_s("iisph_jacobi", k_sweep_jacobi<R>, dim3(nb), dim3(kBlock),
-             (size_t)sweep_hs_ * (sizeof(R4<R>) + sizeof(R2<R>)), d_sc_.p, (const R4<R>*)TB_.p,
+    N.ahead = resident_blocks((const void*)k_sweep_jacobi<R>, sm_b);
+    launch_dep("iisph_jacobi", k_sweep_jacobi<R>, dim3(nb), dim3(kBlock), sm_b, d_sc_.p, (const R4<R>*)TB_.p,
              (const R2<R>*)SA_.p, (const R4<R>*)xu_.p, (const R2<R>*)uu_.p, N, press_.p, xq_.p, partials_.p,
              after, P_);
+  }
+  // Blocks of a sweep pass resident on the whole GPU at once: the distance,
+  // in blocks, of the L2 prefetch for the next wave (0 when it is off).
+  int resident_blocks(const void* fn, size_t smem) {
+    if (!prefetch_) return 0;
+    auto it = resident_.find({fn, smem});
+    if (it != resident_.end()) return it->second;
+    allow_smem(fn, smem);
+    int per_sm = 0, sms = 0;
+    cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kBlock, smem), "occupancy");
+    cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "attribute");
+    const int r = std::max(0, per_sm * sms);
+    resident_[{fn, smem}] = r;
+    return r;
   }
 
   // The pressure acceleration after a solve (a13 with the solved pressures;
@@ -1403,7 +1453,7 @@ class System : public SystemBase {
     // timed sweep launch does a sweep's work (no launch that finds the loop
     // converged and returns); the results are the same either way.
     if (profiling_ && after < 0) batch = 1;
-    for (int k = 0; k < batch; ++k) iisph_iteration(after);
+    for (int k = 0; k < batch; ++k) iisph_iteration(after, k == 0);
     if (after >= 0) return;
     int launched = batch;
     for (;;) {
@@ -1411,7 +1461,7 @@ class System : public SystemBase {
       sync();
       if (h_sc_->converged) break;
       const int more = profiling_ ? 1 : launched < 16 ? 2 : 4;
-      for (int k = 0; k < more; ++k) iisph_iteration(after);
+      for (int k = 0; k < more; ++k) iisph_iteration(after, false);
       launched += more;
     }
   }
@@ -1832,8 +1882,8 @@ class System : public SystemBase {
     std::swap(stream_, body_stream_);
     in_loop_body_ = true;
     try {
-      iisph_iteration(-1);
-      launch("solve_loop", k_loop_cond, dim3(1), dim3(1), handle, (const Scalars*)d_sc_.p, limit);
+      iisph_iteration(-1, true);
+      launch_dep("solve_loop", k_loop_cond, dim3(1), dim3(1), 0, handle, (const Scalars*)d_sc_.p, limit);
     } catch (...) {
       in_loop_body_ = false;
       std::swap(stream_, body_stream_);
