@@ -859,13 +859,22 @@ __global__ void __launch_bounds__(kBlock) k_neighbors_density(
 // lanes of one 16-byte load phase then mostly hit eight different groups.
 // The list stays the same multiset; its padding slots keep the particle's own
 // position. Lists longer than KMAX keep their order.
-template <int KMAX>
+// RES residues (8: 16-byte records, eight lanes per shared-memory phase; 16:
+// also the 8-byte records of the second sweep pass, sixteen lanes per phase).
+// Dynamic shared memory: order_lists_smem(KMAX, RES) bytes.
+__host__ __device__ constexpr size_t order_lists_smem(int kmax, int res) {
+  return (size_t)kmax * kBlock * sizeof(uint16_t) + 2 * (size_t)res * kBlock * sizeof(uint32_t);
+}
+constexpr int kOrderResidues = 8;
+template <int KMAX, int RES>
 __global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restrict__ sc, uint16_t* __restrict__ nbr,
                                                        const uint32_t* __restrict__ ncnt, int K) {
-  static_assert(KMAX <= 255, "slot positions are 8-bit fields");
-  __shared__ uint16_t ent[KMAX * kBlock];  // entry e of thread t at ent[e * kBlock + t]
-  __shared__ uint32_t s_cur[8 * kBlock];   // per residue r of thread t, at [r * kBlock + t]:
-  __shared__ uint32_t s_end[8 * kBlock];   //   the next slot to read and the end of its entries
+  static_assert(RES == 8 || RES == 16, "8 or 16 residues");
+  extern __shared__ __align__(32) unsigned char dsm[];
+  uint32_t* s_cur = reinterpret_cast<uint32_t*>(dsm);  // per residue r of thread t, at [r * kBlock + t]:
+  uint32_t* s_end = s_cur + RES * kBlock;               //   the next slot to read and the end of its entries
+  uint16_t* ent = reinterpret_cast<uint16_t*>(s_end + RES * kBlock);  // entry e of thread t at [e * kBlock + t]
+  constexpr uint32_t M = RES - 1;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int t = threadIdx.x;
   if (i >= sc->n_active) return;
@@ -874,7 +883,7 @@ __global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restric
   uint2* groups = reinterpret_cast<uint2*>(nbr + nbr_slot(i, 0, K));
   const int ng = (cnt + 3) >> 2;
 #pragma unroll
-  for (int r = 0; r < 8; ++r) s_end[r * kBlock + t] = 0;
+  for (int r = 0; r < RES; ++r) s_end[r * kBlock + t] = 0;
   // entries per residue
   uint2 last = make_uint2(0u, 0u);
   for (int g = 0; g < ng; ++g) {
@@ -883,17 +892,17 @@ __global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restric
     const uint32_t e[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
 #pragma unroll
     for (int u = 0; u < 4; ++u)
-      if (4 * g + u < cnt) ++s_end[(e[u] & 7u) * kBlock + t];
+      if (4 * g + u < cnt) ++s_end[(e[u] & M) * kBlock + t];
   }
   // the entries grouped by residue (list order inside a residue); s_end
   // advances from each residue's first slot to its end
   uint32_t avail = 0, run = 0;
 #pragma unroll
-  for (int r = 0; r < 8; ++r) {
+  for (int r = 0; r < RES; ++r) {
     const uint32_t c = s_end[r * kBlock + t];
     s_cur[r * kBlock + t] = run;
     s_end[r * kBlock + t] = run;
-    if (c) avail |= 0x101u << r;  // both bytes: a rotation is one shift
+    if (c) avail |= ((1u << RES) + 1u) << r;  // the mask twice: a rotation is one shift
     run += c;
   }
   for (int g = 0; g < ng; ++g) {
@@ -902,14 +911,14 @@ __global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restric
 #pragma unroll
     for (int u = 0; u < 4; ++u)
       if (4 * g + u < cnt) {
-        uint32_t& f = s_end[(e[u] & 7u) * kBlock + t];
+        uint32_t& f = s_end[(e[u] & M) * kBlock + t];
         const uint32_t pos = f;
         ent[pos * kBlock + t] = (uint16_t)e[u];
         f = pos + 1;
       }
   }
   const uint32_t pad[4] = {last.x & 0xffffu, last.x >> 16, last.y & 0xffffu, last.y >> 16};
-  uint32_t target = (uint32_t)i & 7u;  // lane j's slot k wants residue j + k (mod 8)
+  uint32_t target = (uint32_t)i & M;  // lane j's slot k wants residue j + k (mod RES)
   for (int g = 0; g < ng; ++g) {
     uint32_t v[4];
 #pragma unroll
@@ -920,13 +929,13 @@ __global__ void __launch_bounds__(kBlock) k_order_lists(const Scalars* __restric
         continue;
       }
       // the first residue at or after the target (cyclically) with entries left
-      const uint32_t r = (target + (uint32_t)(__ffs(avail >> target) - 1)) & 7u;
+      const uint32_t r = (target + (uint32_t)(__ffs(avail >> target) - 1)) & M;
       uint32_t& c = s_cur[r * kBlock + t];
       const uint32_t pos = c;
       v[u] = ent[pos * kBlock + t];
       c = pos + 1;
-      if (pos + 1 == (uint32_t)s_end[r * kBlock + t]) avail &= ~(0x101u << r);
-      target = (target + 1) & 7u;
+      if (pos + 1 == s_end[r * kBlock + t]) avail &= ~(((1u << RES) + 1u) << r);
+      target = (target + 1) & M;
     }
     groups[(size_t)g * 32] = make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
   }
@@ -1791,7 +1800,8 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
   TA[i] = R4<R>{sfx + g2 * bx, sfy + g2 * by, sfz + g2 * bz, -(Vi / mi) * Vi};
   TB[i] = R4<R>{sfx + bx, sfy + by, sfz + bz, Vi};
   SA[i] = R2<R>{s, aii};
-  xq_out[i] = R4<R>{xi.x, xi.y, xi.z, Vi * p0};
+  const R ih = P.k.inv_h;  // the sweep records hold positions in units of h
+  xq_out[i] = R4<R>{xi.x * ih, xi.y * ih, xi.z * ih, Vi * p0};
 }
 
 // ---------------------------------------------------------------------------
@@ -1807,9 +1817,11 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
 // one record per neighbor from the block's halo in shared memory:
 //   pass A: xq = {x, y, z, V p}            (written by pass B and the source pass)
 //   pass B: xu = {x, y, z, V a_x}, uu = {V a_y, V a_z}   (written by pass A)
-// A neighbor group of four always holds four valid halo positions (unused
-// slots repeat the particle's own, whose pair adds zero), so the loops carry
-// no per-neighbor test. The kernel constant cg multiplies each pair sum once.
+// with positions in units of the support radius h, so the gradient factor is
+// a function of q = |r|/h alone (grad_q). A neighbor group of four always
+// holds four valid halo positions (unused slots repeat the particle's own,
+// whose pair adds zero), so the loops carry no per-neighbor test. The kernel
+// constant (-3 cg, with grad_q's factor) multiplies each pair sum once.
 // ---------------------------------------------------------------------------
 
 // pass A: a_i = -(V_i/m_i) [p_i (S_i + 2 gamma_p bG_i) + sum_j (V_j p_j) gradW_ij],
@@ -1859,11 +1871,10 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
   }
   stage_done();
   if (!act) return;
-  const R ih = P.k.inv_h;
   R px = 0, py = 0, pz = 0;
-  auto pair = [&](const R4<R>& r) {
+  auto pair = [&](const R4<R>& r) {  // positions in units of h
     const R rx = xi.x - r.x, ry = xi.y - r.y, rz = xi.z - r.z;
-    const R t = r.w * grad_core(rx * rx + ry * ry + rz * rz, ih);
+    const R t = r.w * grad_q(rx * rx + ry * ry + rz * rz);
     px += t * rx; py += t * ry; pz += t * rz;
   };
   if (H.staged) {
@@ -1886,7 +1897,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
       pair(r0); pair(r1); pair(r2); pair(r3);
     }
   }
-  const R cg = P.k.cg;
+  const R cg = R(-3) * P.k.cg;  // grad_q is w'(q)/q divided by -3
   const R fx = pi * Ti.x + cg * px, fy = pi * Ti.y + cg * py, fz = pi * Ti.z + cg * pz;
   const R c = Ti.w;  // V_i a_i = -(V_i^2 / m_i) F
   if (OUT == 0) {
@@ -1958,11 +1969,10 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_jacobi
   stage_done();
   double e = 0.0;
   if (act) {
-    const R ih = P.k.inv_h;
     R sum = 0;
-    auto pair = [&](const R4<R>& a, const R2<R>& b) {
+    auto pair = [&](const R4<R>& a, const R2<R>& b) {  // positions in units of h
       const R rx = xi.x - a.x, ry = xi.y - a.y, rz = xi.z - a.z;
-      sum += grad_core(rx * rx + ry * ry + rz * rz, ih) * (a.w * rx + b.x * ry + b.y * rz);
+      sum += grad_q_full(rx * rx + ry * ry + rz * rz) * (a.w * rx + b.x * ry + b.y * rz);
     };
     if (H.staged) {
       for (int g = 0; g < L.ng; ++g) {

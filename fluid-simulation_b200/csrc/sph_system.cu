@@ -1587,8 +1587,8 @@ class System : public SystemBase {
     // IISPH in f32 re-reads the lists in every sweep pass: order them for
     // shared-memory banks once per update
     if (sizeof(R) == 4 && (cfg_.pressure_solver == SPH_IISPH || cfg_.pressure_solver == SPH_IISPH_W_OST))
-      launch("order_lists", k_order_lists<64>, dim3(nb), dim3(kBlock), (const Scalars*)d_sc_.p, nbr_.p,
-             (const uint32_t*)ncnt_.p, K_);
+      launch_s("order_lists", k_order_lists<64, kOrderResidues>, dim3(nb), dim3(kBlock),
+               order_lists_smem(64, kOrderResidues), (const Scalars*)d_sc_.p, nbr_.p, (const uint32_t*)ncnt_.p, K_);
     calc_acceleration();
     launch("avg_density", k_avg_density<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)xv_.p,
            (const R4<R>*)vel_.p, partials_.p, P_);
