@@ -1917,7 +1917,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
 // block: error, sweep count and the stop test of iisph.rs:378-393).
 // AFTER >= 0: stop after AFTER+1 sweeps; AFTER < 0: target density error.
 template <class R>
-__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 4 : 1) k_sweep_jacobi(
+__global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_jacobi(
     Scalars* __restrict__ sc, const R4<R>* __restrict__ TB, const R2<R>* __restrict__ SA,
     const R4<R>* __restrict__ xu, const R2<R>* __restrict__ uu, NbrArgs N, R* __restrict__ press,
     R4<R>* __restrict__ xq, double* __restrict__ partials, int after, StepParams<R> P) {

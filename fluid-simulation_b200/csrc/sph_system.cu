@@ -863,7 +863,9 @@ class System : public SystemBase {
   DBuf<uint16_t> nbr_;
   int hcap_ = 8192;   // halo table capacity per block (grows on overflow, at most 65535)
   int hs_ = sizeof(R) == 4 ? 1536 : 1024;  // halo records staged in shared memory per block
-  int sweep_hs_ = sizeof(R) == 4 ? 2048 : 1024;  // the same for the IISPH sweep passes
+  // the same for the IISPH sweep passes (f32: 1792 x 24 B lets five pass-B
+  // blocks share an SM's shared memory)
+  int sweep_hs_ = sizeof(R) == 4 ? 1792 : 1024;
   DBuf<uint32_t> count_, start_, tile_sums_;
   DBuf<double> partials_, body_partials_, stage_x_, stage_v_;
   // boundaries
@@ -2839,7 +2841,7 @@ int sph_autotune(sph_system_t* h, uint32_t steps, sph_tuning* best, double* best
     for (const sph_tuning& c : cand) time_candidate(c);
     // then the sweep passes' staging capacity, with the best of the above
     const sph_tuning base = pick;
-    for (uint32_t ss : f32 ? std::vector<uint32_t>{1536, 2048, 3072} : std::vector<uint32_t>{1024, 1536})
+    for (uint32_t ss : f32 ? std::vector<uint32_t>{1536, 1792, 2048} : std::vector<uint32_t>{1024, 1536})
       if (ss != base.sweep_stage) time_candidate(sph_tuning{base.gather_batch, base.halo_stage, ss});
     h->impl->set_tuning(pick);
     *best = pick;

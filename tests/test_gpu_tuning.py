@@ -59,7 +59,7 @@ def test_autotune_applies_its_pick_without_stepping(A, case):
     before = _fields(A, g)
     t = g.autotune(steps=3)
     assert t["gather_batch"] in (4, 8) and t["halo_stage"] in (1024, 1536, 2048) and t["ms_per_step"] > 0
-    assert t["sweep_stage"] in (1536, 2048, 3072)
+    assert t["sweep_stage"] in (1536, 1792, 2048)
     assert g.tuning() == {k: t[k] for k in ("gather_batch", "halo_stage", "sweep_stage")}
     assert g.time_steps_propagated() == 2
     for got, w in zip(_fields(A, g), before):
