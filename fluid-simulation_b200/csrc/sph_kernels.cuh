@@ -413,6 +413,18 @@ __device__ __forceinline__ void prefetch_block_lists(const NbrArgs& N, int b, in
     prefetch_l2(base + (size_t)(q / (2 * G)) * warp_bytes + (size_t)(q % (2 * G)) * 128);
   prefetch_lines(N.hidx + (size_t)b * N.hcap, (size_t)min(N.hcap, kPrefetchHalo) * sizeof(uint32_t));
 }
+// The prefetch of a neighbor pass: the per-particle streams it reads (and
+// the neighbor counts) for block blockIdx.x + N.ahead, its lists and halo.
+template <class... T>
+__device__ __forceinline__ void prefetch_ahead(const NbrArgs& N, int n, const T*... streams) {
+  if (N.ahead <= 0) return;
+  const int b = blockIdx.x + N.ahead;
+  if (b * kBlock >= n) return;
+  const int i0 = b * kBlock, m = min(kBlock, n - i0);
+  (prefetch_lines(streams + i0, (size_t)m * sizeof(T)), ...);
+  prefetch_lines(N.ncnt + i0, (size_t)m * sizeof(uint32_t));
+  prefetch_block_lists(N, b, m);
+}
 
 // The block's halo: its particle indices, its size and whether the launch
 // copies its records to shared memory.
@@ -1857,18 +1869,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
   }
   R4<R>* s_r = reinterpret_cast<R4<R>*>(dsm);
   stage_halo_from(H, hf, [&](int l, uint32_t g) { async_copy(&s_r[l], &xq[g]); });
-  if (N.ahead > 0) {
-    const int b = blockIdx.x + N.ahead;
-    const int n = sc->n_active;
-    if (b * kBlock < n) {
-      const int i0 = b * kBlock, m = min(kBlock, n - i0);
-      prefetch_lines(xq + i0, (size_t)m * sizeof(R4<R>));
-      prefetch_lines(TA + i0, (size_t)m * sizeof(R4<R>));
-      prefetch_lines(press + i0, (size_t)m * sizeof(R));
-      prefetch_lines(N.ncnt + i0, (size_t)m * sizeof(uint32_t));
-      prefetch_block_lists(N, b, m);
-    }
-  }
+  prefetch_ahead(N, sc->n_active, xq, TA, press);
   stage_done();
   if (!act) return;
   R px = 0, py = 0, pz = 0;
@@ -1953,19 +1954,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_jacobi
     async_copy(&s_a[l], &xu[g]);
     async_copy(&s_b[l], &uu[g]);
   });
-  if (N.ahead > 0) {
-    const int b = blockIdx.x + N.ahead;
-    if (b * kBlock < n) {
-      const int i0 = b * kBlock, m = min(kBlock, n - i0);
-      prefetch_lines(xu + i0, (size_t)m * sizeof(R4<R>));
-      prefetch_lines(uu + i0, (size_t)m * sizeof(R2<R>));
-      prefetch_lines(TB + i0, (size_t)m * sizeof(R4<R>));
-      prefetch_lines(SA + i0, (size_t)m * sizeof(R2<R>));
-      prefetch_lines(press + i0, (size_t)m * sizeof(R));
-      prefetch_lines(N.ncnt + i0, (size_t)m * sizeof(uint32_t));
-      prefetch_block_lists(N, b, m);
-    }
-  }
+  prefetch_ahead(N, n, xu, uu, TB, SA, (const R*)press);
   stage_done();
   double e = 0.0;
   if (act) {
