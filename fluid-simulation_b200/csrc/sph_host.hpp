@@ -71,6 +71,9 @@ class SystemBase {
   virtual void set_volume_map_aabb(int bi, const double* center, const double* half_extents) = 0;
   virtual void contact_stats(uint32_t* out4) = 0;  // cells, sweeps, overflow, capped of the last step
   virtual void set_contact_sweeps(uint32_t fixed) = 0;  // 0: merit test; n: exactly n sweeps
+  // programmatic dependent launch between the sweep passes (on by default;
+  // the scene server turns it off: its scenes share the SMs)
+  virtual void set_dependent_launch(bool on) = 0;
   virtual uint32_t contact_sweeps() const = 0;
   virtual void rigid_state(int bi, double* out) = 0;
   virtual void set_rigid_state(int bi, const double* in) = 0;

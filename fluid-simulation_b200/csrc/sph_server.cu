@@ -257,6 +257,9 @@ class Server {
     for (const auto& f : j.vmaps)
       s->add_volume_map(f.sd, f.sn.data(), f.vd, f.vn.data(), f.dyn ? &f.rigid : nullptr);
     s->initialize();
+    // concurrent scenes share the SMs: blocks of an early-launched dependent
+    // kernel would hold SM resources another scene's kernels could use
+    s->set_dependent_launch(false);
     s->set_step_graphs(cfg_.chunk_steps);
     j.sys = std::move(s);
     // the inputs are on the device now

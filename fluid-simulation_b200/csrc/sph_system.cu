@@ -1100,9 +1100,10 @@ class System : public SystemBase {
   // dependent launch): only for kernels that call grid_dep_wait() before
   // reading what that kernel writes. Timed (profiling) runs launch plainly so
   // that the events around each kernel bracket it alone.
+  bool dep_launch() const { return pdl_ && !profiling_; }
   template <class Kern, class... Args>
   void launch_dep(const char* name, Kern kernel, dim3 g, dim3 b, size_t smem, Args... args) {
-    launch_impl(pdl_ && !profiling_, name, kernel, g, b, smem, args...);
+    launch_impl(dep_launch(), name, kernel, g, b, smem, args...);
   }
   template <class Kern, class... Args>
   void launch_impl(bool dep, const char* name, Kern kernel, dim3 g, dim3 b, size_t smem, Args... args) {
@@ -1320,6 +1321,12 @@ class System : public SystemBase {
            (const Scalars*)d_sc_.p, kContactSweepCap, (int)contact_fixed_sweeps_);
   }
 
+  void set_dependent_launch(bool on) override {
+    if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
+    if (pdl_ == on) return;
+    pdl_ = on;
+    destroy_graphs();  // the captured launches carry the old setting
+  }
   void set_contact_sweeps(uint32_t fixed) override {
     if (chunk_steps_) throw Error(SPH_ERR_STATE, "a chunk of graph steps is in flight");
     if (fixed > (uint32_t)kContactSweepCap) throw Error(SPH_ERR_INVALID, "more contact sweeps than the cap");
@@ -1404,7 +1411,7 @@ class System : public SystemBase {
     const size_t sm_a = (size_t)sweep_hs_ * sizeof(R4<R>);
     const size_t sm_b = (size_t)sweep_hs_ * (sizeof(R4<R>) + sizeof(R2<R>));
     N.ahead = resident_blocks((const void*)k_sweep_accel<R>, sm_a);
-    launch_impl(!first && pdl_ && !profiling_, "iisph_pressure_accel", k_sweep_accel<R>, dim3(nb), dim3(kBlock),
+    launch_impl(!first && dep_launch(), "iisph_pressure_accel", k_sweep_accel<R>, dim3(nb), dim3(kBlock),
              sm_a, (const Scalars*)d_sc_.p, (const R*)press_.p, (const R4<R>*)TA_.p, (const R4<R>*)xq_.p, N,
              xu_.p, uu_.p, P_, (R4<R>*)nullptr, (const R4<R>*)nullptr);
     N.ahead = resident_blocks((const void*)k_sweep_jacobi<R>, sm_b);
