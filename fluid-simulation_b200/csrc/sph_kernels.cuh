@@ -214,13 +214,29 @@ __device__ __forceinline__ uint32_t block_excl_scan_u32(uint32_t v, uint32_t* sh
   return base + x - v;
 }
 
+// A thread's kScanItems consecutive counts: two 16-byte loads when they lie
+// inside [0, m) (the arrays are 16-byte aligned and base is a multiple of 8).
+static_assert(kScanItems == 8, "two uint4 per thread");
+__device__ __forceinline__ void scan_load8(const uint32_t* __restrict__ in, int base, int m, uint32_t v[8]) {
+  if (base + 8 <= m) {
+    const uint4 a = __ldcs(reinterpret_cast<const uint4*>(in + base));
+    const uint4 b = __ldcs(reinterpret_cast<const uint4*>(in + base) + 1);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = base + k < m ? in[base + k] : 0u;
+  }
+}
+
 __global__ void __launch_bounds__(kBlock) k_scan_tiles(const uint32_t* __restrict__ in, int m,
                                                       uint32_t* __restrict__ tile_sums) {
   __shared__ uint32_t sh[32];
   const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  scan_load8(in, base, m, v);
   uint32_t s = 0;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) s += base + k < m ? in[base + k] : 0u;
+  for (int k = 0; k < kScanItems; ++k) s += v[k];
   uint32_t total;
   block_excl_scan_u32(s, sh, &total);
   if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
@@ -248,20 +264,33 @@ __global__ void __launch_bounds__(kBlock) k_scan_apply(uint32_t* __restrict__ in
   __shared__ uint32_t sh[32];
   const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
   uint32_t v[kScanItems];
+  scan_load8(in, base, m, v);
   uint32_t s = 0;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    v[k] = base + k < m ? in[base + k] : 0u;
-    s += v[k];
-  }
+  for (int k = 0; k < kScanItems; ++k) s += v[k];
   uint32_t run = block_excl_scan_u32(s, sh, nullptr) + tile_sums[blockIdx.x];
+  if (base + 8 <= m) {
+    uint32_t o[8];
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k)
-    if (base + k < m) {
-      out[base + k] = run;
+    for (int k = 0; k < 8; ++k) {
+      o[k] = run;
       run += v[k];
-      in[base + k] = 0u;  // counts are rebuilt by the next histogram
     }
+    uint4* po = reinterpret_cast<uint4*>(out + base);
+    po[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    po[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    uint4* pz = reinterpret_cast<uint4*>(in + base);  // counts are rebuilt by the next histogram
+    pz[0] = make_uint4(0u, 0u, 0u, 0u);
+    pz[1] = make_uint4(0u, 0u, 0u, 0u);
+  } else {
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+      if (base + k < m) {
+        out[base + k] = run;
+        run += v[k];
+        in[base + k] = 0u;
+      }
+  }
 }
 
 // ---------------------------------------------------------------------------
