@@ -1841,8 +1841,7 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
   TA[i] = R4<R>{sfx + g2 * bx, sfy + g2 * by, sfz + g2 * bz, -(Vi / mi) * Vi};
   TB[i] = R4<R>{sfx + bx, sfy + by, sfz + bz, Vi};
   SA[i] = R2<R>{s, aii};
-  const R ih = P.k.inv_h;  // the sweep records hold positions in units of h
-  xq_out[i] = R4<R>{xi.x * ih, xi.y * ih, xi.z * ih, Vi * p0};
+  xq_out[i] = R4<R>{xi.x, xi.y, xi.z, Vi * p0};
 }
 
 // ---------------------------------------------------------------------------
@@ -1858,11 +1857,10 @@ __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
 // one record per neighbor from the block's halo in shared memory:
 //   pass A: xq = {x, y, z, V p}            (written by pass B and the source pass)
 //   pass B: xu = {x, y, z, V a_x}, uu = {V a_y, V a_z}   (written by pass A)
-// with positions in units of the support radius h, so the gradient factor is
-// a function of q = |r|/h alone (grad_q). A neighbor group of four always
-// holds four valid halo positions (unused slots repeat the particle's own,
-// whose pair adds zero), so the loops carry no per-neighbor test. The kernel
-// constant (-3 cg, with grad_q's factor) multiplies each pair sum once.
+// A neighbor group of four always holds four valid halo positions (unused
+// slots repeat the particle's own, whose pair adds zero), so the loops carry
+// no per-neighbor test. The kernel constant cg (-3 cg for pass A's piecewise
+// gradient factor) multiplies each pair sum once.
 // ---------------------------------------------------------------------------
 
 // pass A: a_i = -(V_i/m_i) [p_i (S_i + 2 gamma_p bG_i) + sum_j (V_j p_j) gradW_ij],
@@ -1901,10 +1899,11 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
   prefetch_ahead(N, sc->n_active, xq, TA, press);
   stage_done();
   if (!act) return;
+  const R ih = P.k.inv_h;
   R px = 0, py = 0, pz = 0;
-  auto pair = [&](const R4<R>& r) {  // positions in units of h
+  auto pair = [&](const R4<R>& r) {
     const R rx = xi.x - r.x, ry = xi.y - r.y, rz = xi.z - r.z;
-    const R t = r.w * grad_q(rx * rx + ry * ry + rz * rz);
+    const R t = r.w * grad_piecewise(rx * rx + ry * ry + rz * rz, ih);
     px += t * rx; py += t * ry; pz += t * rz;
   };
   if (H.staged) {
@@ -1927,7 +1926,7 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_accel(
       pair(r0); pair(r1); pair(r2); pair(r3);
     }
   }
-  const R cg = R(-3) * P.k.cg;  // grad_q is w'(q)/q divided by -3
+  const R cg = R(-3) * P.k.cg;  // grad_piecewise is grad_core divided by -3
   const R fx = pi * Ti.x + cg * px, fy = pi * Ti.y + cg * py, fz = pi * Ti.z + cg * pz;
   const R c = Ti.w;  // V_i a_i = -(V_i^2 / m_i) F
   if (OUT == 0) {
@@ -1987,10 +1986,11 @@ __global__ void __launch_bounds__(kBlock, sizeof(R) == 4 ? 5 : 1) k_sweep_jacobi
   stage_done();
   double e = 0.0;
   if (act) {
+    const R ih = P.k.inv_h;
     R sum = 0;
-    auto pair = [&](const R4<R>& a, const R2<R>& b) {  // positions in units of h
+    auto pair = [&](const R4<R>& a, const R2<R>& b) {
       const R rx = xi.x - a.x, ry = xi.y - a.y, rz = xi.z - a.z;
-      sum += grad_q_full(rx * rx + ry * ry + rz * rz) * (a.w * rx + b.x * ry + b.y * rz);
+      sum += grad_core(rx * rx + ry * ry + rz * rz, ih) * (a.w * rx + b.x * ry + b.y * rz);
     };
     if (H.staged) {
       for (int g = 0; g < L.ng; ++g) {

@@ -105,48 +105,53 @@ __device__ __forceinline__ float kernel_grad_factor<float>(float r2, const Kerne
   return k.cg * (-3.f * (a * a) + 12.f * (b * b)) * inv;
 }
 
-// The gradient factor for positions in units of the support radius h
-// (r' = r / h, q = |r'|): gradW(r) = cg * w'(q)/q * r', with
-// w'(q) = 12 (1/2-q)_+^2 - 3 (1-q)_+^2, so w'(q)/q = 9q - 6 for q < 1/2,
-// -3 (1-q)^2 / q for 1/2 <= q < 1 and 0 beyond. grad_q returns it divided by
-// -3 (2 - 3q, resp. (1-q)^2 / q); the caller scales its sums by -3 cg once.
-// Its product with r' is zero at r' = 0.
+// The gradient factor without its constant: gradW(r) = cg * grad_core(r2) * r,
+// grad_core = w'(q) / |r| with w'(q) = 12 (1/2-q)_+^2 - 3 (1-q)_+^2 (zero at
+// r = 0 and outside the support). Sums of grad_core terms are scaled by cg
+// once, after the loop.
 template <class R>
-__device__ __forceinline__ R grad_q(R r2) {
-  const R q = sqrt(r2);
-  if (q < R(0.5)) return R(2) - R(3) * q;
-  const R t = R(1) - q;
-  return q < R(1) ? t * t / q : R(0);
-}
-// w'(q)/q itself, in the product form (12 (1/2-q)_+^2 - 3 (1-q)_+^2) / q
-// (zero at r' = 0).
-template <class R>
-__device__ __forceinline__ R grad_q_full(R r2) {
-  const R q = sqrt(r2);
+__device__ __forceinline__ R grad_core(R r2, R inv_h) {
+  const R rn = sqrt(r2);
+  const R q = rn * inv_h;
   const R a = q < R(1) ? R(1) - q : R(0);
   const R b = q < R(0.5) ? R(0.5) - q : R(0);
-  return r2 > R(0) ? (R(12) * (b * b) - R(3) * (a * a)) / q : R(0);
+  return r2 > R(0) ? (R(12) * (b * b) - R(3) * (a * a)) / rn : R(0);
 }
+// f32: one approximate reciprocal square root (relative error ~2^-23, far
+// inside the f32 state's tolerance) and no branch.
 template <>
-__device__ __forceinline__ float grad_q_full<float>(float r2) {
+__device__ __forceinline__ float grad_core<float>(float r2, float inv_h) {
   float inv;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(r2));
   inv = r2 > 0.f ? inv : 0.f;
-  const float q = r2 * inv;
+  const float q = r2 * inv * inv_h;
   const float a = fmaxf(1.f - q, 0.f), b = fmaxf(0.5f - q, 0.f);
   return fmaf(12.f * b, b, -3.f * a * a) * inv;
 }
-// f32: one approximate reciprocal square root (relative error ~2^-23, far
-// inside the f32 state's tolerance) and no branch; r2 is clamped away from 0
-// so that the self pair (r' = 0) gives a finite factor.
+
+// The same factor in its piecewise form, divided by -3: with q = |r|/h,
+// w'(q) = 9q^2 - 6q for q < 1/2 and -3 (1-q)^2 for 1/2 <= q < 1, so
+// grad_core / -3 = (2 - 3q) / h, resp. (1-q)^2 / |r| (no division in f32;
+// the caller scales its sums by -3 cg once). Its product with r is zero at
+// r = 0.
+template <class R>
+__device__ __forceinline__ R grad_piecewise(R r2, R inv_h) {
+  const R rn = sqrt(r2);
+  const R q = rn * inv_h;
+  if (q < R(0.5)) return (R(2) - R(3) * q) * inv_h;
+  const R t = R(1) - q;
+  return q < R(1) ? t * t / rn : R(0);
+}
+// f32: r2 is clamped away from 0 so that the self pair (r = 0) gives a finite
+// factor; one approximate reciprocal square root.
 template <>
-__device__ __forceinline__ float grad_q<float>(float r2) {
+__device__ __forceinline__ float grad_piecewise<float>(float r2, float inv_h) {
   const float r2c = fmaxf(r2, 1e-30f);
   float inv;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(r2c));
-  const float q = r2c * inv;
+  const float q = r2c * inv * inv_h;
   const float t = fmaxf(1.f - q, 0.f);
-  return q < 0.5f ? fmaf(-3.f, q, 2.f) : t * t * inv;
+  return q < 0.5f ? fmaf(-3.f * inv_h, q, 2.f * inv_h) : t * t * inv;
 }
 
 // Both W and the gradient factor from one square root.
