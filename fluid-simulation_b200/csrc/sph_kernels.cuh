@@ -1584,7 +1584,7 @@ __device__ __forceinline__ void sweep_groups(SweepList<R>& L, Load&& load, Use&&
 // 6. accelerations: gravity + viscosity (+ SESPH pressure) (+ v* = v + dt a)
 // ---------------------------------------------------------------------------
 // PRESS: 0 none, 1 SESPH state equation from the volume on the fly
-template <class R, int PRESS, int NB>
+template <class R, int PRESS>
 __global__ void __launch_bounds__(kBlock) k_accel(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     NbrArgs N, BoundaryArgs<R> B, R4<R>* __restrict__ acc, R4<R>* __restrict__ vstar,
@@ -1695,7 +1695,7 @@ __global__ void __launch_bounds__(kBlock) k_accel(
 // MODE: 1 -> acc += accel (reaction forces if mirror)
 //       2 -> acc  = accel (reaction forces if mirror)
 // (the Jacobi sweep's own pressure accelerations are k_sweep_accel)
-template <class R, int MODE, int NB>
+template <class R, int MODE>
 __global__ void __launch_bounds__(kBlock) k_pressure_accel(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     const R* __restrict__ press, NbrArgs N, BoundaryArgs<R> B, R4<R>* __restrict__ out, int mirror,
@@ -1773,7 +1773,7 @@ __global__ void __launch_bounds__(kBlock) k_pressure_accel(
 // ---------------------------------------------------------------------------
 // VP = 1: volume-preserving source s = 1 - V0/V - dt sum ..., VP = 0: the
 // velocity-divergence source of IISPHwOST's first solve.
-template <class R, int VP, int NB>
+template <class R, int VP>
 __global__ void __launch_bounds__(kBlock) k_iisph_source_diag(
     const Scalars* __restrict__ sc, const R4<R>* __restrict__ xv, const R4<R>* __restrict__ vel,
     const R4<R>* __restrict__ vstar, NbrArgs N, BoundaryArgs<R> B, R* __restrict__ s_out,

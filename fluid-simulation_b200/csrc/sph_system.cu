@@ -1491,29 +1491,29 @@ class System : public SystemBase {
     constexpr int NB = decltype(NBc)::value;
     switch (cfg_.pressure_solver) {
       case SPH_SESPH:
-        launch_s("accel_sesph", k_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(), acc_.p,
+        launch_s("accel_sesph", k_accel<R, 1>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(), acc_.p,
                vstar_.p, press_.p, 0, P_);
         body_reduce(nb);
         break;
       case SPH_SESPH_W_SPLITTING:
-        launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
+        launch_s("accel_nonpressure", k_accel<R, 0>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
         body_reduce(nb);
         launch_s("split_density", k_split_density<R, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, bargs(), press_.p, rho_pred_.p, P_);
-        launch_s("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
+        launch_s("pressure_accel", k_pressure_accel<R, 1>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
                (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
         body_reduce(nb);
         break;
       case SPH_IISPH:
-        launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
+        launch_s("accel_nonpressure", k_accel<R, 0>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
         body_reduce(nb);
-        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
+        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, TA_.p, TB_.p, SA_.p, xq_.p, P_);
         solve_loop(-1);
         if (any_dynamic_) {
-          launch_s("pressure_accel", k_pressure_accel<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
+          launch_s("pressure_accel", k_pressure_accel<R, 1>, dim3(nb), dim3(kBlock), sm_xp, csc, xv, vel,
                  (const R*)press_.p, nbr, bargs(), acc_.p, 1, P_);
           body_reduce(nb);
         } else {
@@ -1521,14 +1521,14 @@ class System : public SystemBase {
         }
         break;
       case SPH_IISPH_W_OST:
-        launch_s("accel_nonpressure", k_accel<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
+        launch_s("accel_nonpressure", k_accel<R, 0>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel, nbr, bargs(),
                acc_.p, vstar_.p, press_.p, 1, P_);
-        launch_s("iisph_source_diag", k_iisph_source_diag<R, 0, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
+        launch_s("iisph_source_diag", k_iisph_source_diag<R, 0>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, TA_.p, TB_.p, SA_.p, xq_.p, P_);
         solve_loop(3);
         final_pressure_accel<2>();  // IISPHwOST takes no dynamic boundaries
         launch("ost_predict", k_ost_predict<R>, dim3(nb), dim3(kBlock), d_sc_.p, (const R4<R>*)acc_.p, vstar_.p);
-        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1, NB>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
+        launch_s("iisph_source_diag", k_iisph_source_diag<R, 1>, dim3(nb), dim3(kBlock), sm_xv, csc, xv, vel,
                (const R4<R>*)vstar_.p, nbr, bargs(), s_.p, aii_.p, press_.p, TA_.p, TB_.p, SA_.p, xq_.p, P_);
         solve_loop(-1);
         final_pressure_accel<2>();

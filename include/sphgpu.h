@@ -355,7 +355,9 @@ int sph_graph_replays(const sph_system_t* h, uint64_t* out);
 /* ---- launch tuning -------------------------------------------------------- */
 /* Launch parameters of the neighbor passes that leave every result bit for bit
  * unchanged (the reference has no counterpart; its passes run on the CPU):
- * the number of neighbors a thread gathers per batch (4 or 8) and the halo
+ * the number of neighbors a thread gathers per batch (4 or 8; it applies to
+ * the passes that test the neighbor count per slot, i.e. SESPHwSplitting's
+ * predicted density; the others walk whole groups of four) and the halo
  * records a block copies to shared memory before its neighbor loop (blocks
  * with larger halos, and every block at 0, gather from global memory). The
  * records must fit one block's shared memory. Setting them re-captures the
